@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 null-geodesic tracer on the headline workload.
+
+Workload: Kerr a=0.94 M, 2048x2048 pinhole camera at r=100 M, inclination
+17 deg, FOV 12 deg, thin disk [r_ISCO, 20 M], DP45 rtol=atol=1e-10, <= 20000
+attempts per ray (synthetic camera grid; no dataset).  A step = one trace of
+the whole image.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+  python bench.py --impl reference      # the reference's own CPU image path
+
+value: Mrays/s with outputs resident in HBM, tracer kernel timed with CUDA
+events on its stream, L2 flushed between steps (a 256 MiB write).
+e2e:   Mrays/s through rt_dispatch (the dispatch_and_readback-shaped C call)
+       with pinned host buffers, host<->device copies inside the timed region.
+N > 1: one independent image per GPU (replicas, no collective); value is the
+       total over ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "relativity-simulator_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Mrays/s on Kerr a=0.94 2048^2, mixed vs FP64 at stated error; p50/p99 latency"
+FLOP_PER_ATTEMPT = 1578.0  # Kerr-Schild RHS as written (206 ops) x 6 + DP45 stage/error ops
+SIDE = 2048
+RECORD_FIELDS = ["status", "r", "theta", "phi", "r_hit", "g"]
+
+
+def headline_camera(relsim, precision: int, side: int = SIDE):
+    return relsim.make_camera(spin=0.94, r_obs=100.0, incl_deg=17.0, fov_deg=12.0, width=side, height=side,
+                              precision=precision)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 10:
+                        rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+
+        def num(s):
+            try:
+                return float(s)
+            except ValueError:
+                return float("nan")
+
+        load = [r for r in rows if num(r[4]) > 50] or rows
+        sm = [num(r[1]) for r in load]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in load for i in range(4) if r[6 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": num(load[0][2]), "reasons": reasons,
+                "samples": len(load), "power_w_max": max(num(r[3]) for r in load)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_port_baseline(cam_dict: dict, seconds: float = 15.0) -> dict:
+    """The FP64 oracle (same DP45 algorithm) on a random sample of the workload's rays, all host cores."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(0)
+    n_pix = cam_dict["screen_width"] * cam_dict["screen_height"]
+    cores = os.cpu_count() or 1
+    probe = rng.choice(n_pix, 2000, replace=False).astype(np.uint64)
+    t0 = time.perf_counter()
+    O.trace(cam_dict, pixels=probe, threads=cores)
+    rate = probe.size / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(max(rate * seconds, 4000), n_pix))
+    sample = rng.choice(n_pix, n, replace=False).astype(np.uint64)
+    t0 = time.perf_counter()
+    O.trace(cam_dict, pixels=sample, threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "port",
+            "sample": f"{n} uniformly random rays of the 2048^2 image, FP64 DP45 oracle (oracle/ks_oracle.c), "
+                      f"{dt:.1f} s"}
+
+
+def reference_arm(args) -> None:
+    """The reference's own CPU image path (SoftwareComputeEngine::dispatch_fp64, heuristic-step RK4,
+    built from its headers into oracle/_ref) on row bands of the same camera."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    import relsim
+
+    cam = headline_camera(relsim, relsim.PRECISION_FP64)
+    d = relsim.camera_dict(cam)
+    W = H = SIDE
+    cores = os.cpu_count() or 1
+    if not O.ref_available():
+        try:
+            O.build(ref=True)
+        except Exception:
+            pass
+    if O.ref_available():
+        R = O.ref()
+        obs = np.ascontiguousarray(d["observer_position"], dtype=np.float64)
+        e1 = np.ascontiguousarray(d["tetrad_e1"], dtype=np.float64)
+        e2 = np.ascontiguousarray(d["tetrad_e2"], dtype=np.float64)
+        e3 = np.ascontiguousarray(d["tetrad_e3"], dtype=np.float64)
+
+        def band(row0, rows):
+            st = np.zeros(W * rows, np.uint32)
+            it = np.zeros(W * rows, np.uint32)
+            z = np.zeros(W * rows, np.float32)
+            return R.ref_dispatch_fp64(O._p(obs), O._p(e1), O._p(e2), O._p(e3), d["field_of_view_rad"], 1.0, 0.94,
+                                       1000.0, 20.0, W, H, 20000, row0, rows, O._p(st), O._p(it), O._p(z))
+        kind = "reference"
+        what = "SoftwareComputeEngine::dispatch_fp64 (reference image path, heuristic-step RK4), hardware_concurrency threads"
+        # calibrate a band of about 6 s around the image centre (the shadow and inner disk)
+        t = band(H // 2 - 8, 16)
+        rows = int(min(max(16 * 6.0 / max(t, 1e-3), 16), H))
+        rows -= rows % 2
+        times = []
+        for i in range(args.warmup + args.steps):
+            r0 = max(0, H // 2 - rows // 2)
+            dt = band(r0, rows)
+            if i >= args.warmup:
+                times.append(dt)
+        n = W * rows
+    else:
+        kind = "port"
+        what = "FP64 DP45 oracle (oracle/ks_oracle.c); the reference library was not built"
+        rng = np.random.default_rng(1)
+        n = 20000
+        times = []
+        for i in range(args.warmup + args.steps):
+            pix = rng.choice(W * H, n, replace=False).astype(np.uint64)
+            t0 = time.perf_counter()
+            O.trace(d, pixels=pix, threads=cores)
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t0)
+    value = n * len(times) / sum(times) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "Kerr a=0.94 2048^2 pinhole r=100 i=17 FOV 12 disk [r_isco,20]",
+                   "sample": f"{n} rays per step ({what})"},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": cores, "kind": kind,
+                         "sample": f"{n} rays per step, {what}"},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def ours(args) -> None:
+    import torch
+
+    import relsim
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    precision = relsim.PRECISION_MIXED if args.precision == "mixed" else relsim.PRECISION_FP64
+    cam = headline_camera(relsim, precision, args.side)
+    n = cam.screen_width * cam.screen_height
+    tr = relsim.Tracer(local)
+    fp64_peak, fp32_peak = tr.measure_fma_peak()
+    ro, tensors = relsim.device_ray_out(n, RECORD_FIELDS, device=f"cuda:{local}")
+    pix = torch.empty(n * 32, dtype=torch.uint8, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step():
+        tr.dispatch_device(cam, ro, pix.data_ptr(), n)
+        s = tr.stats()  # waits; kernel_ms from events on the tracer's stream
+        return s
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ms, attempts, rhs = [], 0, 0
+    with ClockSampler(local) as clk:
+        wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            s = step()
+            ms.append(s.kernel_ms)
+            attempts += s.attempts
+            rhs += s.rhs_evals
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+    clocks = clk.summary()
+    total_ms = float(sum(ms))
+    if ws > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ws * n * args.steps / (total_ms * 1e-3) / 1e6
+    mrays_per_gpu = n * args.steps / (float(sum(ms)) * 1e-3) / 1e6
+    achieved = attempts * FLOP_PER_ATTEMPT / (float(sum(ms)) * 1e-3) / 1e12
+    peak = fp64_peak if precision == relsim.PRECISION_FP64 else fp32_peak
+
+    # e2e through rt_dispatch with pinned host buffers
+    host = {f: torch.empty(n, dtype=(torch.int32 if f == "status" else torch.float64), pin_memory=True)
+            for f in RECORD_FIELDS}
+    hpix = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
+    hro = relsim.RayOut()
+    for f, t in host.items():
+        setattr(hro, f, t.data_ptr())
+    L = relsim.lib()
+    lat = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        st = L.rt_dispatch(tr.handle, ctypes.byref(cam), hpix.data_ptr(), ctypes.byref(hro), n, None)
+        dt = time.perf_counter() - t0
+        if st != 0:
+            raise RuntimeError(L.rt_last_error(tr.handle).decode())
+        if i >= args.warmup:
+            lat.append(dt)
+    e2e_wall = sum(lat)
+    if ws > 1:
+        t = torch.tensor([e2e_wall], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_wall = float(t.item())
+    e2e_value = ws * n * args.steps / e2e_wall / 1e6
+    d2h = n * (32 + 4 + 8 * (len(RECORD_FIELDS) - 1))
+
+    # error of this run against the FP64 oracle on a sample of rays (stated error)
+    err = None
+    if rank == 0 and args.check_rays > 0:
+        err = sample_error(relsim, cam, host, args.check_rays)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_port_baseline(relsim.camera_dict(cam), seconds=args.cpu_seconds)
+
+    traffic = committed_traffic(precision)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if precision == relsim.PRECISION_FP64 else "f32+f64",
+            "data": "synthetic camera grid",
+            "config": {"workload": f"Kerr a=0.94 {args.side}^2 pinhole r=100 M i=17 deg FOV 12 deg, "
+                                   "disk [r_isco, 20 M], DP45 rtol=atol=1e-10",
+                       "precision": args.precision, "parallelism": f"replicas x{ws}",
+                       "l2": "flushed between steps (256 MiB write)",
+                       "launch": vars_of(tr.launch_config())},
+            "msteps_per_s": attempts / (float(sum(ms)) * 1e-3) / 1e6,
+            "attempts_per_ray": attempts / (n * args.steps),
+            "roofline": {"bound": "fp64" if precision == relsim.PRECISION_FP64 else "fp32+fp64",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": "measured: register FMA-chain kernel (rt_measure_fma_peak)",
+                         "flop_per_attempt": FLOP_PER_ATTEMPT, "traffic": traffic},
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 448,
+                    "d2h_bytes_per_step": d2h,
+                    "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
+                    "latency_ms_p99": 1e3 * float(np.percentile(lat, 99))},
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+            "fma_peak_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
+            "wall_s_timed_region": wall,
+            "mrays_per_gpu": mrays_per_gpu,
+        }
+        if err is not None:
+            line["error_vs_fp64_oracle"] = err
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    tr.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def vars_of(c) -> dict:
+    return {f: getattr(c, f) for f, _ in c._fields_}
+
+
+def committed_traffic(precision: int):
+    """DRAM bytes per launch of the tracer kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("fp64" if precision == 0 else "mixed")
+    except (OSError, ValueError):
+        return None
+
+
+def sample_error(relsim, cam, host: dict, n: int) -> dict:
+    """Classes and disk radius of the last e2e image against the FP64 oracle on random rays."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(11)
+    N = cam.screen_width * cam.screen_height
+    pix = rng.choice(N, n, replace=False)
+    ref = O.trace(relsim.camera_dict(relsim.make_camera(spin=0.94, r_obs=100.0, incl_deg=17.0, fov_deg=12.0,
+                                                         width=cam.screen_width, height=cam.screen_height)),
+                  pixels=pix.astype(np.uint64))
+    st = host["status"].numpy()[pix].astype(np.uint32)
+    r_in = O.lib().orc_isco_radius(1.0, 0.94)
+    band = O.boundary_band(ref, r_in, 20.0, 1e-6)
+    mism = int(((st != ref["status"]) & ~band).sum())
+    both = (st == 3) & (ref["status"] == 3)
+    rh = host["r_hit"].numpy()[pix]
+    rel = np.abs(rh[both] - ref["r_hit"][both]) / ref["r_hit"][both]
+    g = host["g"].numpy()[pix]
+    relg = np.abs(g[both] - ref["g"][both]) / ref["g"][both]
+    return {"rays": int(n), "class_mismatch_outside_band": mism, "in_band": int(band.sum()),
+            "r_hit_rel_max": float(rel.max()) if rel.size else None,
+            "r_hit_rel_p99": float(np.percentile(rel, 99)) if rel.size else None,
+            "g_rel_max": float(relg.max()) if relg.size else None}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--side", type=int, default=SIDE)
+    ap.add_argument("--check-rays", type=int, default=2000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

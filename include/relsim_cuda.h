@@ -1,0 +1,222 @@
+/*
+ * relsim_cuda.h -- C ABI of the B200 (sm_100a) backward null-geodesic tracer.
+ *
+ * Drop-in compute backend for Wartets/Relativity-Simulator's image path.  Each
+ * entry point names the reference interface it replaces (paths relative to the
+ * reference source tree):
+ *
+ *   rt_create / rt_destroy     VulkanComputeExecutor::initialize / shutdown
+ *                              (include/relativistic/render/vulkan_compute_executor.hpp:983-987, 1272)
+ *   rt_is_ready                VulkanComputeExecutor::is_ready (:1257)
+ *   rt_is_platform_supported   VulkanComputeExecutor::is_platform_supported (:1634)
+ *   rt_dispatch                VulkanComputeExecutor::dispatch_and_readback (:1399-1464)
+ *   rt_dispatch_tile           VulkanComputeExecutor::dispatch_tile_and_readback (:1372-1391)
+ *   rt_camera                  hot-path subset of GpuCameraPushConstants
+ *                              (include/relativistic/render/gpu_types.hpp:966-1109)
+ *   rt_pixel_out               GpuPixelOutput, same 32-byte layout (gpu_types.hpp:1111-1121)
+ *   RT_PIXEL_*                 PixelFlags (gpu_types.hpp:1123-1130)
+ *
+ * Beyond the reference: a per-ray SoA record (class, final BL position, disk
+ * radius, redshift, invariant drift), device-resident dispatch, batched camera
+ * bundles in one persistent launch, and a continuous-batching request server.
+ *
+ * Conventions: every call returns rt_status, never throws; host buffers are
+ * caller-owned; device buffers are owned by the handle and grow on demand.  A
+ * handle is thread-compatible (one CUDA stream per handle): callers serialise
+ * calls on one handle, as the reference's pipeline does with gpu_mutex_.
+ * There is no CPU fallback inside this library; a missing or failed device
+ * is reported as RT_ERR_DEVICE / RT_ERR_NOT_READY.
+ */
+#ifndef RELSIM_CUDA_H
+#define RELSIM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RT_ABI_VERSION 1
+
+typedef enum rt_status {
+    RT_OK = 0,
+    RT_ERR_INVALID_ARG = 1,
+    RT_ERR_OOM = 2,
+    RT_ERR_TIMEOUT = 3,
+    RT_ERR_DEVICE = 4,
+    RT_ERR_CANCELLED = 5,
+    RT_ERR_NOT_READY = 6,
+    RT_ERR_BUDGET = 7,   /* request larger than the device-memory budget */
+    RT_ERR_AGAIN = 8     /* server queue full; retry after rt_server_poll */
+} rt_status;
+
+typedef enum rt_precision {
+    RT_PRECISION_FP64 = 0,  /* every stage in FP64 (the plain tracer) */
+    RT_PRECISION_MIXED = 1  /* FP32 far-field stages, FP64 state / near zone */
+} rt_precision;
+
+/* Ray classes written to rt_ray_out.status. */
+enum {
+    RT_RAY_UNFINISHED = 0,  /* step budget exhausted */
+    RT_RAY_CAPTURED = 1,    /* r_BL < capture_scale * r_+, or non-finite state */
+    RT_RAY_ESCAPED = 2,     /* r_BL > escape_radius */
+    RT_RAY_DISK = 3         /* first z = 0 crossing with r in [r_in, r_out] */
+};
+/* Ray flags written to rt_ray_out.flags. */
+enum {
+    RT_RAYFLAG_NONFINITE = 1u << 0,
+    RT_RAYFLAG_STEP_UNDERFLOW = 1u << 1,
+    RT_RAYFLAG_MAX_STEPS = 1u << 2,
+    RT_RAYFLAG_EARLY_CAPTURE = 1u << 3
+};
+/* PixelFlags (gpu_types.hpp:1123-1130). */
+#define RT_PIXEL_HORIZON_ABSORBED (1u << 0)
+#define RT_PIXEL_CELESTIAL_HIT (1u << 1)
+#define RT_PIXEL_ACCRETION_DISK_HIT (1u << 2)
+
+/* Camera and integration parameters of one image (one "bundle"). */
+typedef struct rt_camera {
+    double observer_position[4]; /* t, r, theta, phi (Boyer-Lindquist), as GpuCameraPushConstants */
+    double tetrad_e1[4];         /* forward; spatial part in [1..3] */
+    double tetrad_e2[4];         /* right */
+    double tetrad_e3[4];         /* up */
+    double field_of_view_rad;
+    double metric_mass;          /* clamped to >= 1e-4 */
+    double metric_spin;          /* clamped to |a| <= 0.999 M (software_compute_engine.hpp:3801) */
+    double escape_radius;
+    double capture_scale;        /* captured when r_BL < capture_scale * r_+ */
+    double disk_inner_radius;    /* <= 0: r_ISCO(a) */
+    double disk_outer_radius;    /* <= 0: no disk */
+    double rtol;                 /* DP45 relative tolerance */
+    double atol;                 /* DP45 absolute tolerance */
+    double step_cap_fraction;    /* |h| <= c * max(r_BL - r_+, 0.01 M) */
+    double initial_step_fraction;/* |h0| = f * r_obs */
+    double projection_tol;       /* project onto H = 0 when |H| >= tol */
+    double mixed_fp64_radius;    /* MIXED: FP64 stages inside this r_BL (<= 0: max(3 r_+, 5 M)) */
+    uint32_t screen_width;
+    uint32_t screen_height;
+    uint32_t max_integration_steps; /* step attempts per ray, accepted + rejected */
+    uint32_t early_capture;      /* 1: end a ray once capture is certain */
+    uint32_t precision_mode;     /* rt_precision */
+    uint32_t dispatch_row_offset;/* row window as GpuCameraPushConstants; count 0 = all rows */
+    uint32_t dispatch_row_count;
+    uint32_t tile_origin_x;      /* tile window for rt_dispatch_tile */
+    uint32_t tile_origin_y;
+    uint32_t tile_extent_x;
+    uint32_t tile_extent_y;
+    uint32_t reserved;
+} rt_camera;
+
+/* GpuPixelOutput (gpu_types.hpp:1111-1121): 32 bytes. */
+typedef struct rt_pixel_out {
+    float r, g, b, a;
+    float redshift;
+    float affine_parameter;
+    uint32_t status_flags;
+    uint32_t iterations_used;
+} rt_pixel_out;
+
+/* Per-ray record, structure of arrays.  Any pointer may be NULL (not written).
+ * Pointers are host pointers for rt_dispatch* and device pointers for the
+ * *_device entry points. */
+typedef struct rt_ray_out {
+    uint32_t* status;
+    uint32_t* flags;
+    uint32_t* steps_accepted;
+    uint32_t* steps_rejected;
+    double* r;       /* final BL radius */
+    double* theta;   /* final BL polar angle */
+    double* phi;     /* final azimuth, unwrapped along the ray */
+    double* r_hit;   /* disk-hit radius, NaN without a hit */
+    double* g;       /* disk redshift factor, 1 without a hit */
+    double* lambda;  /* affine parameter at termination (negative: traced backwards) */
+    double* dH;      /* max |H| before each projection */
+    double* dE;      /* -p_t recomputed from the null condition at the end, minus 1 */
+    double* dLz;     /* L_z(end) - L_z(start) */
+    double* dQ;      /* Carter Q(end) - Q(start) */
+} rt_ray_out;
+
+/* Launch shape of the persistent tracer (set by the autotuner). */
+typedef struct rt_launch_config {
+    uint32_t block_size;       /* threads per CTA: 64, 128, 256 */
+    uint32_t ctas_per_sm;      /* persistent CTAs per SM; 0 = occupancy maximum */
+    uint32_t refill_threshold; /* idle lanes of a warp before it refills from the queue */
+    uint32_t rays_per_claim;   /* rays a warp claims per lane and refill (1..4) */
+} rt_launch_config;
+
+/* Counters of the last dispatch (device-side totals). */
+typedef struct rt_stats {
+    uint64_t rays;
+    uint64_t attempts;       /* DP45 step attempts, accepted + rejected */
+    uint64_t accepted;
+    uint64_t rhs_evals;
+    uint64_t fp64_attempts;  /* attempts taken in FP64 (all of them in FP64 mode) */
+    double kernel_ms;        /* device time of the tracer kernel(s) */
+} rt_stats;
+
+typedef struct rt_handle rt_handle;
+
+/* Lifetime (VulkanComputeExecutor::initialize / shutdown). */
+rt_status rt_create(rt_handle** out, int device_ordinal);
+void rt_destroy(rt_handle* h);
+int rt_is_ready(const rt_handle* h);
+int rt_is_platform_supported(void);
+const char* rt_last_error(const rt_handle* h);
+int rt_abi_version(void);
+
+/* Defaults: r=100, i=17 deg, FOV 12 deg, a=0.94, 2048^2, disk [r_ISCO, 20],
+ * rtol=atol=1e-10, cap 0.1, h0 = 0.01 r_obs, 20000 attempts, FP64. */
+void rt_camera_defaults(rt_camera* cam);
+/* Fill observer_position and the forward/right/up tetrad of a static observer
+ * at (r, theta, phi) looking at the hole (forward = -e_r, right = e_phi, up = -e_theta). */
+void rt_camera_look_at_hole(rt_camera* cam, double r, double theta, double phi);
+
+/* Trace the row window of the image (VulkanComputeExecutor::dispatch_and_readback).
+ * Host buffers; pixels and/or rays may be NULL; capacity = elements available,
+ * which must be >= width * rows of the window.  cancel (optional) is polled
+ * between bands: a non-zero value returns RT_ERR_CANCELLED. */
+rt_status rt_dispatch(rt_handle* h, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
+                      size_t capacity, const volatile int* cancel);
+
+/* Trace the tile [origin, origin + extent) in tile-major order
+ * (VulkanComputeExecutor::dispatch_tile_and_readback). */
+rt_status rt_dispatch_tile(rt_handle* h, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
+                           size_t capacity);
+
+/* Device-resident form: pixels/rays are device pointers, work is enqueued on
+ * `stream` (a cudaStream_t; NULL = the handle's stream) and not waited for. */
+rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
+                             size_t capacity, void* stream);
+
+/* Batched camera bundles of uneven size in one persistent launch.  Bundle b's
+ * rays are written at offset offsets[b] of the (device) outputs, row-major
+ * within the bundle's row window; offsets may be NULL (packed in order).
+ * The launch is captured into a CUDA graph and replayed while the bundle
+ * table's shape is unchanged. */
+rt_status rt_trace_bundles_device(rt_handle* h, const rt_camera* cams, uint32_t n_bundles, const uint64_t* offsets,
+                                  rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity, void* stream);
+
+/* Total rays of a bundle table (sum of the row windows). */
+uint64_t rt_bundle_rays(const rt_camera* cams, uint32_t n_bundles);
+
+/* Launch configuration (the autotuner writes it; zeros select defaults). */
+rt_status rt_set_launch_config(rt_handle* h, const rt_launch_config* cfg);
+rt_status rt_get_launch_config(const rt_handle* h, rt_launch_config* cfg);
+
+/* Counters of the last dispatch; waits for it to finish. */
+rt_status rt_get_stats(rt_handle* h, rt_stats* stats);
+
+/* Wait for the handle's stream with a wall-clock limit (ms); RT_ERR_TIMEOUT
+ * when the limit passes first (the work is not cancelled). */
+rt_status rt_synchronize(rt_handle* h, double timeout_ms);
+
+/* Measured FMA throughput of this device (TFLOP/s, an FMA counted as 2 FLOP),
+ * from a register-resident FMA-chain kernel.  Roofline denominator. */
+rt_status rt_measure_fma_peak(rt_handle* h, double* fp64_tflops, double* fp32_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

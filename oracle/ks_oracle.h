@@ -1,0 +1,126 @@
+/*
+ * ks_oracle.h -- FP64 CPU oracle for the backward null-geodesic tracer.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference
+ * engine's Kerr-Schild null-ray path, used as the checker for the CUDA
+ * kernels.  Only tests/, the smoke check in __graft_entry__.py and the
+ * cpu_baseline leg of bench.py may load it.  No product code path calls it.
+ *
+ * What it restates (reference = Wartets/Relativity-Simulator):
+ *   - Kerr-Schild field and Hamiltonian RHS with p_t = -1
+ *       include/relativistic/core/kerr_schild_null_integrator.hpp:31-44, 72-114
+ *   - BL <-> KS position maps with phi unwrapping  (:47-69)
+ *   - static-observer tetrad and initial null momentum  (:142-194)
+ *   - pinhole camera + tetrad ray generation
+ *       include/relativistic/observer/camera_projections.hpp:27-40
+ *       include/relativistic/render/software_compute_engine.hpp:3838-3938
+ *   - Dormand-Prince 5(4) tableau, max-norm error, accept/reject scaling
+ *       include/relativistic/integrators/rk45_adaptive.hpp:196-311
+ *   - PI30 step controller  include/relativistic/integrators/step_controller.hpp:44-78
+ *   - constraint projection, closest-root quadratic  rk45_adaptive.hpp:91-139
+ *   - ISCO  software_compute_engine.hpp:1052-1061
+ *   - disk redshift  include/relativistic/render/accretion_disk/accretion_disk_model.hpp:205-225
+ *   - Carter constant  include/relativistic/metrics/kerr_invariants.hpp:21-58
+ *   - radial quartic of the Carter classifier
+ *       include/relativistic/optics/carter_ray_classifier.hpp:116-140
+ */
+#ifndef RELSIM_KS_ORACLE_H
+#define RELSIM_KS_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Ray classes (same numbering as the CUDA library's RT_RAY_* codes). */
+enum {
+    ORC_RAY_UNFINISHED = 0, /* step budget exhausted */
+    ORC_RAY_CAPTURED = 1,   /* r_BL < capture_scale * r_+ (or non-finite state) */
+    ORC_RAY_ESCAPED = 2,    /* r_BL > escape_radius */
+    ORC_RAY_DISK = 3        /* first z = 0 crossing with r in [r_in, r_out] */
+};
+enum {
+    ORC_FLAG_NONFINITE = 1u << 0,
+    ORC_FLAG_STEP_UNDERFLOW = 1u << 1,
+    ORC_FLAG_MAX_STEPS = 1u << 2,
+    ORC_FLAG_EARLY_CAPTURE = 1u << 3
+};
+
+/* A ray is declared captured before reaching capture_scale * r_+ when it is
+ * inside the disk's inner edge, moving inwards, and its radial potential has
+ * no turning point outside r_+ by at least this margin (signed distance to the
+ * critical curve, in M). */
+#define ORC_EARLY_CAPTURE_MARGIN 1e-4
+
+typedef struct orc_camera {
+    double observer_position[4]; /* t, r, theta, phi (Boyer-Lindquist) */
+    double tetrad_e1[4];         /* forward  (spatial part in [1..3]) */
+    double tetrad_e2[4];         /* right */
+    double tetrad_e3[4];         /* up */
+    double field_of_view_rad;
+    double metric_mass;
+    double metric_spin;
+    double escape_radius;
+    double capture_scale;        /* captured when r_BL < capture_scale * r_+ */
+    double disk_inner_radius;    /* <= 0 selects r_ISCO(a) */
+    double disk_outer_radius;    /* <= 0 disables the disk */
+    double rtol;
+    double atol;
+    double step_cap_fraction;    /* |h| <= c * max(r_BL - r_+, 0.01 M) */
+    double initial_step_fraction;/* |h0| = f * r_obs */
+    double projection_tol;       /* project when |H| > tol * (1 + |p|^2) */
+    uint32_t screen_width;
+    uint32_t screen_height;
+    uint32_t max_steps;          /* step attempts, accepted + rejected */
+    uint32_t early_capture;      /* 1: stop once capture is certain (Carter test) */
+} orc_camera;
+
+typedef struct orc_ray {
+    uint32_t status;
+    uint32_t flags;
+    uint32_t steps_accepted;
+    uint32_t steps_rejected;
+    double r, theta, phi;        /* final BL position */
+    double r_hit;                /* disk-hit radius, NaN when no hit */
+    double g;                    /* disk redshift factor, 1 when no hit */
+    double lambda;               /* affine parameter at termination */
+    double dH;                   /* max |H| before projection */
+    double dE;                   /* E recomputed from the null condition - 1 */
+    double dLz;                  /* L_z(end) - L_z(start) */
+    double dQ;                   /* Q(end) - Q(start) */
+    double db_shadow;            /* signed distance to the critical curve (M) */
+} orc_ray;
+
+/* --- single-function checks (pinned against the reference) --- */
+void orc_ks_field(const double x[3], double mass, double spin, double* r, double* h, double k[3]);
+void orc_ks_rhs(const double y[6], double mass, double spin, double dy[6]);
+void orc_ks_position_from_bl(double r, double theta, double phi, double spin, double out[3]);
+void orc_bl_from_ks(const double x[3], double spin, double previous_phi, double out[3]);
+void orc_initial_momentum(const double x[3], double mass, double spin, const double outward[3], double p[3]);
+double orc_isco_radius(double mass, double spin);
+double orc_redshift_at(double mass, double spin, double radius, double lz);
+void orc_pinhole_ray(double u, double v, double fov, double n[3]);
+double orc_pi30_factor(double err, double err_prev, int has_history, double order_p1);
+double orc_hamiltonian(const double y[6], double mass, double spin);
+double orc_carter_q(const double y[6], double mass, double spin);
+double orc_shadow_distance(double mass, double spin, double lz, double q);
+
+/* Initial state of pixel (px, py): y0 = (x, p), returns L_z. */
+double orc_ray_initial_state(const orc_camera* cam, uint32_t px, uint32_t py, double y0[6]);
+
+/* One DP45 attempt from y with step h (no control): y_new and the error norm. */
+double orc_dp45_attempt(const orc_camera* cam, const double y[6], double h, double y_new[6]);
+
+/* Trace pixels.  pixel_index == NULL traces the contiguous range
+ * [first, first + count) of row-major pixel indices, else the listed ones.
+ * threads <= 0 uses all online cores. */
+void orc_trace(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
+               orc_ray* out, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,177 @@
+"""ctypes bindings of the CPU checker libraries.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check in
+__graft_entry__.py and by the cpu_baseline / reference legs of bench.py.  The
+product (the CUDA library and its host code) never imports this module.
+
+  liboracle.so           C restatement of the reference's FP64 null-ray path
+                         (ks_oracle.c; see its header for the citations)
+  _ref/libref_oracle.so  the reference's own functions, compiled from its
+                         headers by oracle/Makefile (present where it was built)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libref_oracle.so")
+
+CAMERA_DTYPE = np.dtype([
+    ("observer_position", "f8", 4),
+    ("tetrad_e1", "f8", 4),
+    ("tetrad_e2", "f8", 4),
+    ("tetrad_e3", "f8", 4),
+    ("field_of_view_rad", "f8"),
+    ("metric_mass", "f8"),
+    ("metric_spin", "f8"),
+    ("escape_radius", "f8"),
+    ("capture_scale", "f8"),
+    ("disk_inner_radius", "f8"),
+    ("disk_outer_radius", "f8"),
+    ("rtol", "f8"),
+    ("atol", "f8"),
+    ("step_cap_fraction", "f8"),
+    ("initial_step_fraction", "f8"),
+    ("projection_tol", "f8"),
+    ("screen_width", "u4"),
+    ("screen_height", "u4"),
+    ("max_steps", "u4"),
+    ("early_capture", "u4"),
+])
+
+RAY_DTYPE = np.dtype([
+    ("status", "u4"), ("flags", "u4"), ("steps_accepted", "u4"), ("steps_rejected", "u4"),
+    ("r", "f8"), ("theta", "f8"), ("phi", "f8"), ("r_hit", "f8"), ("g", "f8"), ("lambda", "f8"),
+    ("dH", "f8"), ("dE", "f8"), ("dLz", "f8"), ("dQ", "f8"), ("db_shadow", "f8"),
+])
+
+CAPTURED, ESCAPED, DISK, UNFINISHED = 1, 2, 3, 0
+
+_D = ctypes.POINTER(ctypes.c_double)
+_lib = None
+_ref = None
+
+
+def build(ref: bool = False) -> None:
+    """Compile the checker libraries (the _ref one only where the reference tree exists)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        v = ctypes.c_void_p
+        d = ctypes.c_double
+        L.orc_trace.argtypes = [v, v, ctypes.c_uint64, ctypes.c_uint64, v, ctypes.c_int]
+        L.orc_trace.restype = None
+        L.orc_ray_initial_state.argtypes = [v, ctypes.c_uint32, ctypes.c_uint32, v]
+        L.orc_ray_initial_state.restype = d
+        L.orc_dp45_attempt.argtypes = [v, v, d, v]
+        L.orc_dp45_attempt.restype = d
+        L.orc_ks_field.argtypes = [v, d, d, v, v, v]
+        L.orc_ks_rhs.argtypes = [v, d, d, v]
+        L.orc_ks_position_from_bl.argtypes = [d, d, d, d, v]
+        L.orc_bl_from_ks.argtypes = [v, d, d, v]
+        L.orc_initial_momentum.argtypes = [v, d, d, v, v]
+        L.orc_isco_radius.argtypes = [d, d]
+        L.orc_isco_radius.restype = d
+        L.orc_redshift_at.argtypes = [d, d, d, d]
+        L.orc_redshift_at.restype = d
+        L.orc_pinhole_ray.argtypes = [d, d, d, v]
+        L.orc_pi30_factor.argtypes = [d, d, ctypes.c_int, d]
+        L.orc_pi30_factor.restype = d
+        L.orc_hamiltonian.argtypes = [v, d, d]
+        L.orc_hamiltonian.restype = d
+        L.orc_carter_q.argtypes = [v, d, d]
+        L.orc_carter_q.restype = d
+        L.orc_shadow_distance.argtypes = [d, d, d, d]
+        L.orc_shadow_distance.restype = d
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_PATH)
+
+
+def ref() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise FileNotFoundError(f"{REF_PATH} missing: run `make -C oracle ref` where the reference tree exists")
+        L = ctypes.CDLL(REF_PATH)
+        v = ctypes.c_void_p
+        d = ctypes.c_double
+        u = ctypes.c_uint32
+        L.ref_ks_field.argtypes = [v, d, d, v, v, v]
+        L.ref_ks_rhs.argtypes = [v, d, d, v]
+        L.ref_ks_rk4_step.argtypes = [v, d, d, d]
+        L.ref_ks_position_from_bl.argtypes = [d, d, d, d, v]
+        L.ref_bl_from_ks.argtypes = [v, d, d, v]
+        L.ref_initial_momentum.argtypes = [v, d, d, v, v]
+        L.ref_redshift_at.argtypes = [d, d, d, d]
+        L.ref_redshift_at.restype = d
+        L.ref_isco_radius.argtypes = [d, d]
+        L.ref_isco_radius.restype = d
+        L.ref_pinhole_ray.argtypes = [d, d, d, v]
+        L.ref_pi30_sequence.argtypes = [v, v, ctypes.c_int, v]
+        L.ref_kerr_invariants.argtypes = [v, d, d, v]
+        L.ref_rk45_trace.argtypes = [v, d, d, d, d, d, d, d, d, d, ctypes.c_int, v]
+        L.ref_dispatch_fp64.argtypes = [v, v, v, v, d, d, d, d, d, u, u, u, u, u, v, v, v]
+        L.ref_dispatch_fp64.restype = d
+        _ref = L
+    return _ref
+
+
+def to_camera(cam: dict) -> np.ndarray:
+    """Pack a camera dict (same keys as CAMERA_DTYPE) into the C struct."""
+    c = np.zeros(1, dtype=CAMERA_DTYPE)
+    for name in CAMERA_DTYPE.names:
+        if name in cam:
+            c[name] = cam[name]
+    return c
+
+
+def trace(cam: dict, pixels: np.ndarray | None = None, first: int = 0, count: int | None = None,
+          threads: int = 0) -> np.ndarray:
+    """Trace pixels (row-major indices) through the FP64 oracle."""
+    c = to_camera(cam)
+    if pixels is not None:
+        idx = np.ascontiguousarray(pixels, dtype=np.uint64)
+        n = idx.size
+        out = np.zeros(n, dtype=RAY_DTYPE)
+        lib().orc_trace(_p(c), _p(idx), 0, n, _p(out), threads)
+    else:
+        n = int(cam["screen_width"]) * int(cam["screen_height"]) - first if count is None else count
+        out = np.zeros(n, dtype=RAY_DTYPE)
+        lib().orc_trace(_p(c), None, first, n, _p(out), threads)
+    return out
+
+
+def initial_state(cam: dict, px: int, py: int) -> tuple[np.ndarray, float]:
+    c = to_camera(cam)
+    y = np.zeros(6)
+    lz = lib().orc_ray_initial_state(_p(c), px, py, _p(y))
+    return y, lz
+
+
+def boundary_band(rays: np.ndarray, r_in: float, r_out: float, band: float = 1e-6) -> np.ndarray:
+    """Rays within `band` M of the shadow edge (Kerr critical curve) or of a disk edge."""
+    near_shadow = np.abs(rays["db_shadow"]) < band
+    rh = rays["r_hit"]
+    near_disk = np.isfinite(rh) & ((np.abs(rh - r_in) < band) | (np.abs(rh - r_out) < band))
+    return near_shadow | near_disk

@@ -1,0 +1,531 @@
+// rt_api.cu -- C ABI of the tracer (include/relsim_cuda.h).
+//
+// Host side of the drop-in backend: VulkanComputeExecutor's lifetime,
+// dispatch_and_readback and dispatch_tile_and_readback
+// (vulkan_compute_executor.hpp:983-1464) over the persistent CUDA tracer.
+// Device buffers are owned by the handle and grow on demand
+// (ensure_output_capacity, vulkan_compute_executor.hpp:400); calls on one
+// handle are serialised by the caller.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "relsim_cuda.h"
+#include "rt_internal.h"
+
+namespace relsim {
+template <int BLOCK>
+__global__ void trace_fp64_kernel_t(TraceArgs args);
+void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, cudaStream_t stream);
+int trace_occupancy(uint32_t block, bool mixed);
+double measure_fma_peak(bool fp64, int sm_count, cudaStream_t stream, float* ms_out);
+}  // namespace relsim
+
+using namespace relsim;
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct rt_handle {
+    int device = -1;
+    int sm_count = 0;
+    bool ready = false;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string error;
+    rt_launch_config cfg{};
+    // device scratch
+    DevBuf bundles, queue, stats;
+    DevBuf ray_fields[14];
+    DevBuf pixels;
+    // pinned staging of the bundle table
+    BundleDesc* host_bundles = nullptr;
+    size_t host_bundles_cap = 0;
+    // last launch
+    bool timed = false;
+    // bundle graph cache
+    cudaGraphExec_t graph = nullptr;
+    uint32_t graph_n_bundles = 0;
+    uint64_t graph_total = 0;
+    OutPtrs graph_out{};
+    rt_launch_config graph_cfg{};
+};
+
+namespace {
+
+rt_status fail(rt_handle* h, rt_status st, const std::string& msg) {
+    if (h) h->error = msg;
+    return st;
+}
+
+rt_status cuda_fail(rt_handle* h, cudaError_t e, const char* where) {
+    if (h) {
+        h->error = std::string(where) + ": " + cudaGetErrorString(e);
+        if (e != cudaErrorMemoryAllocation && e != cudaErrorInvalidValue) h->ready = false;
+    }
+    return (e == cudaErrorMemoryAllocation) ? RT_ERR_OOM : RT_ERR_DEVICE;
+}
+
+#define RT_CUDA(h, call)                                          \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_fail((h), e_, #call); \
+    } while (0)
+
+rt_status ensure(rt_handle* h, DevBuf& b, size_t bytes) {
+    if (b.bytes >= bytes) return RT_OK;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    const size_t grow = std::max(bytes, b.bytes + b.bytes / 2);
+    cudaError_t e = cudaMalloc(&b.ptr, grow);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(h, e, "cudaMalloc");
+    }
+    b.bytes = grow;
+    return RT_OK;
+}
+
+void release(DevBuf& b) {
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+}
+
+rt_status ensure_host_bundles(rt_handle* h, size_t n) {
+    if (h->host_bundles_cap >= n) return RT_OK;
+    if (h->host_bundles) cudaFreeHost(h->host_bundles);
+    h->host_bundles = nullptr;
+    h->host_bundles_cap = 0;
+    RT_CUDA(h, cudaMallocHost(&h->host_bundles, n * sizeof(BundleDesc)));
+    h->host_bundles_cap = n;
+    return RT_OK;
+}
+
+bool camera_valid(const rt_camera* c) {
+    return c && c->screen_width > 0 && c->screen_height > 0 && std::isfinite(c->metric_mass) &&
+           std::isfinite(c->metric_spin) && std::isfinite(c->field_of_view_rad) && c->field_of_view_rad > 0.0 &&
+           c->field_of_view_rad < 3.14 && std::isfinite(c->escape_radius) && c->rtol > 0.0 && c->atol >= 0.0 &&
+           c->step_cap_fraction > 0.0 && c->initial_step_fraction > 0.0 && c->capture_scale >= 1.0 &&
+           c->max_integration_steps > 0 && std::isfinite(c->observer_position[1]) &&
+           std::isfinite(c->observer_position[2]) && std::isfinite(c->observer_position[3]) &&
+           (c->precision_mode == RT_PRECISION_FP64 || c->precision_mode == RT_PRECISION_MIXED);
+}
+
+// Row window of the image (vulkan_compute_executor.hpp:1415-1426).
+void row_window(const rt_camera& c, uint32_t& row0, uint32_t& nrows) {
+    row0 = std::min(c.dispatch_row_offset, c.screen_height);
+    nrows = (c.dispatch_row_count == 0) ? (c.screen_height - row0)
+                                        : std::min(c.dispatch_row_count, c.screen_height - row0);
+}
+
+rt_launch_config effective_cfg(const rt_handle* h, bool mixed) {
+    rt_launch_config c = h->cfg;
+    if (c.block_size != 64 && c.block_size != 128 && c.block_size != 256) c.block_size = 128;
+    const int occ = trace_occupancy(c.block_size, mixed);
+    if (c.ctas_per_sm == 0 || static_cast<int>(c.ctas_per_sm) > occ) c.ctas_per_sm = std::max(occ, 1);
+    if (c.refill_threshold == 0 || c.refill_threshold > 32) c.refill_threshold = 8;
+    c.rays_per_claim = 1;
+    return c;
+}
+
+// Launch the tracer over `n` bundles already in h->bundles (device).
+rt_status launch(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs& out, bool mixed, cudaStream_t s) {
+    const rt_launch_config c = effective_cfg(h, mixed);
+    TraceArgs args{};
+    args.bundles = static_cast<const BundleDesc*>(h->bundles.ptr);
+    args.n_bundles = n_bundles;
+    args.refill_threshold = c.refill_threshold;
+    args.total_rays = total;
+    args.queue = static_cast<unsigned long long*>(h->queue.ptr);
+    args.stats = static_cast<unsigned long long*>(h->stats.ptr);
+    args.out = out;
+    RT_CUDA(h, cudaMemsetAsync(h->queue.ptr, 0, sizeof(unsigned long long), s));
+    RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
+    const uint32_t grid = static_cast<uint32_t>(h->sm_count) * c.ctas_per_sm;
+    RT_CUDA(h, cudaEventRecord(h->ev0, s));
+    launch_trace(args, grid, c.block_size, mixed, s);
+    RT_CUDA(h, cudaGetLastError());
+    RT_CUDA(h, cudaEventRecord(h->ev1, s));
+    h->timed = true;
+    return RT_OK;
+}
+
+// Device SoA record in the handle's scratch for `n` rays: only the fields the
+// caller asked for on the host.
+rt_status scratch_rays(rt_handle* h, const rt_ray_out* host, size_t n, rt_ray_out& dev) {
+    std::memset(&dev, 0, sizeof dev);
+    if (!host) return RT_OK;
+    void* const* hp = reinterpret_cast<void* const*>(host);
+    void** dp = reinterpret_cast<void**>(&dev);
+    const size_t elem[14] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
+    for (int f = 0; f < 14; ++f) {
+        if (!hp[f]) continue;
+        rt_status st = ensure(h, h->ray_fields[f], n * elem[f]);
+        if (st != RT_OK) return st;
+        dp[f] = h->ray_fields[f].ptr;
+    }
+    return RT_OK;
+}
+
+rt_status copy_back(rt_handle* h, const rt_ray_out* host, const rt_ray_out& dev, rt_pixel_out* hpix,
+                    const rt_pixel_out* dpix, size_t n, cudaStream_t s) {
+    if (host) {
+        void* const* hp = reinterpret_cast<void* const*>(host);
+        void* const* dp = reinterpret_cast<void* const*>(&dev);
+        const size_t elem[14] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
+        for (int f = 0; f < 14; ++f)
+            if (hp[f]) RT_CUDA(h, cudaMemcpyAsync(hp[f], dp[f], n * elem[f], cudaMemcpyDeviceToHost, s));
+    }
+    if (hpix) RT_CUDA(h, cudaMemcpyAsync(hpix, dpix, n * sizeof(rt_pixel_out), cudaMemcpyDeviceToHost, s));
+    return RT_OK;
+}
+
+rt_status wait_stream(rt_handle* h, cudaStream_t s, double timeout_ms) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(s);
+        if (e == cudaSuccess) return RT_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(h, e, "cudaStreamQuery");
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (timeout_ms > 0.0 && ms > timeout_ms) return fail(h, RT_ERR_TIMEOUT, "stream wait timed out");
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+// One host-buffer dispatch over a window (dispatch_and_readback semantics).
+rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0,
+                          uint32_t nrows, rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity,
+                          const volatile int* cancel) {
+    const size_t n = static_cast<size_t>(ncols) * nrows;
+    if (n == 0) return fail(h, RT_ERR_INVALID_ARG, "empty window");
+    if (capacity < n) return fail(h, RT_ERR_INVALID_ARG, "capacity smaller than the window");
+    rt_status st = ensure_host_bundles(h, 1);
+    if (st != RT_OK) return st;
+    if ((st = ensure(h, h->bundles, sizeof(BundleDesc))) != RT_OK) return st;
+    rt_ray_out dev{};
+    if ((st = scratch_rays(h, rays, n, dev)) != RT_OK) return st;
+    rt_pixel_out* dpix = nullptr;
+    if (pixels) {
+        if ((st = ensure(h, h->pixels, n * sizeof(rt_pixel_out))) != RT_OK) return st;
+        dpix = static_cast<rt_pixel_out*>(h->pixels.ptr);
+    }
+    // bands of at most 2^24 rays; the cancel flag is polled between bands
+    const uint64_t band_rows = std::max<uint64_t>(1, (uint64_t{1} << 24) / ncols);
+    for (uint32_t r = 0; r < nrows; r += static_cast<uint32_t>(band_rows)) {
+        if (cancel && *cancel) return fail(h, RT_ERR_CANCELLED, "cancelled");
+        const uint32_t rows = static_cast<uint32_t>(std::min<uint64_t>(band_rows, nrows - r));
+        const uint64_t offset = static_cast<uint64_t>(r) * ncols;
+        build_bundle(*cam, col0, ncols, row0 + r, rows, 0, offset, h->host_bundles[0]);
+        RT_CUDA(h, cudaMemcpyAsync(h->bundles.ptr, h->host_bundles, sizeof(BundleDesc), cudaMemcpyHostToDevice,
+                                   h->stream));
+        OutPtrs out{dpix, dev};
+        if ((st = launch(h, 1, static_cast<uint64_t>(rows) * ncols, out, cam->precision_mode == RT_PRECISION_MIXED,
+                         h->stream)) != RT_OK)
+            return st;
+        if ((st = wait_stream(h, h->stream, 0.0)) != RT_OK) return st;
+    }
+    if ((st = copy_back(h, rays, dev, pixels, dpix, n, h->stream)) != RT_OK) return st;
+    return wait_stream(h, h->stream, 0.0);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rt_abi_version(void) { return RT_ABI_VERSION; }
+
+int rt_is_platform_supported(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    for (int d = 0; d < n; ++d) {
+        cudaDeviceProp p{};
+        if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10 && p.minor == 0) return 1;
+    }
+    return 0;
+}
+
+rt_status rt_create(rt_handle** out, int device_ordinal) {
+    if (!out) return RT_ERR_INVALID_ARG;
+    *out = nullptr;
+    rt_handle* h = new (std::nothrow) rt_handle();
+    if (!h) return RT_ERR_OOM;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || device_ordinal < 0 || device_ordinal >= n) {
+        cudaGetLastError();
+        delete h;
+        return RT_ERR_DEVICE;
+    }
+    cudaDeviceProp p{};
+    if (cudaGetDeviceProperties(&p, device_ordinal) != cudaSuccess || p.major != 10 || p.minor != 0) {
+        delete h;
+        return RT_ERR_DEVICE;  // built for sm_100a only
+    }
+    h->device = device_ordinal;
+    h->sm_count = p.multiProcessorCount;
+    if (cudaSetDevice(device_ordinal) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+        cudaGetLastError();
+        rt_destroy(h);
+        return RT_ERR_DEVICE;
+    }
+    if (ensure(h, h->queue, 256) != RT_OK || ensure(h, h->stats, 256) != RT_OK) {
+        rt_destroy(h);
+        return RT_ERR_OOM;
+    }
+    h->ready = true;
+    *out = h;
+    return RT_OK;
+}
+
+void rt_destroy(rt_handle* h) {
+    if (!h) return;
+    if (h->device >= 0) cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    release(h->bundles);
+    release(h->queue);
+    release(h->stats);
+    release(h->pixels);
+    for (auto& b : h->ray_fields) release(b);
+    if (h->host_bundles) cudaFreeHost(h->host_bundles);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int rt_is_ready(const rt_handle* h) { return (h && h->ready) ? 1 : 0; }
+
+const char* rt_last_error(const rt_handle* h) { return h ? h->error.c_str() : "null handle"; }
+
+void rt_camera_defaults(rt_camera* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof *c);
+    c->field_of_view_rad = 12.0 * 3.14159265358979323846 / 180.0;
+    c->metric_mass = 1.0;
+    c->metric_spin = 0.94;
+    c->escape_radius = 1000.0;
+    c->capture_scale = 1.01;
+    c->disk_inner_radius = 0.0;
+    c->disk_outer_radius = 20.0;
+    c->rtol = 1e-10;
+    c->atol = 1e-10;
+    c->step_cap_fraction = 0.1;
+    c->initial_step_fraction = 0.01;
+    c->projection_tol = 1e-12;
+    c->mixed_fp64_radius = 0.0;
+    c->screen_width = 2048;
+    c->screen_height = 2048;
+    c->max_integration_steps = 20000;
+    c->early_capture = 1;
+    c->precision_mode = RT_PRECISION_FP64;
+    rt_camera_look_at_hole(c, 100.0, 17.0 * 3.14159265358979323846 / 180.0, 0.0);
+}
+
+void rt_camera_look_at_hole(rt_camera* c, double r, double theta, double phi) {
+    if (!c) return;
+    const double st = std::sin(theta), ct = std::cos(theta), sp = std::sin(phi), cp = std::cos(phi);
+    const double er[3] = {st * cp, st * sp, ct};
+    const double eth[3] = {ct * cp, ct * sp, -st};
+    const double eph[3] = {-sp, cp, 0.0};
+    c->observer_position[0] = 0.0;
+    c->observer_position[1] = r;
+    c->observer_position[2] = theta;
+    c->observer_position[3] = phi;
+    c->tetrad_e1[0] = c->tetrad_e2[0] = c->tetrad_e3[0] = 0.0;
+    for (int i = 0; i < 3; ++i) {
+        c->tetrad_e1[1 + i] = -er[i];
+        c->tetrad_e2[1 + i] = eph[i];
+        c->tetrad_e3[1 + i] = -eth[i];
+    }
+}
+
+rt_status rt_dispatch(rt_handle* h, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
+                      size_t capacity, const volatile int* cancel) {
+    if (!h) return RT_ERR_INVALID_ARG;
+    if (!h->ready) return fail(h, RT_ERR_NOT_READY, "handle not ready");
+    if (!camera_valid(cam)) return fail(h, RT_ERR_INVALID_ARG, "invalid camera");
+    uint32_t row0, nrows;
+    row_window(*cam, row0, nrows);
+    if (nrows == 0) return fail(h, RT_ERR_INVALID_ARG, "empty row window");
+    RT_CUDA(h, cudaSetDevice(h->device));
+    return dispatch_window(h, cam, 0, cam->screen_width, row0, nrows, pixels, rays, capacity, cancel);
+}
+
+rt_status rt_dispatch_tile(rt_handle* h, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
+                           size_t capacity) {
+    if (!h) return RT_ERR_INVALID_ARG;
+    if (!h->ready) return fail(h, RT_ERR_NOT_READY, "handle not ready");
+    if (!camera_valid(cam)) return fail(h, RT_ERR_INVALID_ARG, "invalid camera");
+    // vulkan_compute_executor.hpp:1377-1385
+    if (cam->tile_extent_x == 0 || cam->tile_extent_y == 0) return fail(h, RT_ERR_INVALID_ARG, "empty tile");
+    if (cam->tile_origin_x >= cam->screen_width || cam->tile_origin_y >= cam->screen_height)
+        return fail(h, RT_ERR_INVALID_ARG, "tile origin outside the image");
+    const uint32_t w = std::min(cam->tile_extent_x, cam->screen_width - cam->tile_origin_x);
+    const uint32_t hgt = std::min(cam->tile_extent_y, cam->screen_height - cam->tile_origin_y);
+    RT_CUDA(h, cudaSetDevice(h->device));
+    return dispatch_window(h, cam, cam->tile_origin_x, w, cam->tile_origin_y, hgt, pixels, rays, capacity, nullptr);
+}
+
+rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
+                             size_t capacity, void* stream) {
+    if (!h) return RT_ERR_INVALID_ARG;
+    if (!h->ready) return fail(h, RT_ERR_NOT_READY, "handle not ready");
+    if (!camera_valid(cam)) return fail(h, RT_ERR_INVALID_ARG, "invalid camera");
+    if (pixels && (reinterpret_cast<uintptr_t>(pixels) & 15u)) return fail(h, RT_ERR_INVALID_ARG, "pixels not 16-byte aligned");
+    uint32_t row0, nrows;
+    row_window(*cam, row0, nrows);
+    const uint64_t n = static_cast<uint64_t>(cam->screen_width) * nrows;
+    if (n == 0) return fail(h, RT_ERR_INVALID_ARG, "empty row window");
+    if (capacity < n) return fail(h, RT_ERR_INVALID_ARG, "capacity smaller than the window");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    RT_CUDA(h, cudaSetDevice(h->device));
+    rt_status st = ensure_host_bundles(h, 1);
+    if (st != RT_OK) return st;
+    if ((st = ensure(h, h->bundles, sizeof(BundleDesc))) != RT_OK) return st;
+    // the staging buffer is reused by the next call: wait for the previous upload
+    RT_CUDA(h, cudaStreamSynchronize(s));
+    build_bundle(*cam, 0, cam->screen_width, row0, nrows, 0, 0, h->host_bundles[0]);
+    RT_CUDA(h, cudaMemcpyAsync(h->bundles.ptr, h->host_bundles, sizeof(BundleDesc), cudaMemcpyHostToDevice, s));
+    OutPtrs out{pixels, rays ? *rays : rt_ray_out{}};
+    return launch(h, 1, n, out, cam->precision_mode == RT_PRECISION_MIXED, s);
+}
+
+uint64_t rt_bundle_rays(const rt_camera* cams, uint32_t n) {
+    uint64_t total = 0;
+    for (uint32_t b = 0; cams && b < n; ++b) {
+        uint32_t row0, nrows;
+        row_window(cams[b], row0, nrows);
+        total += static_cast<uint64_t>(cams[b].screen_width) * nrows;
+    }
+    return total;
+}
+
+rt_status rt_trace_bundles_device(rt_handle* h, const rt_camera* cams, uint32_t n_bundles, const uint64_t* offsets,
+                                  rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity, void* stream) {
+    if (!h) return RT_ERR_INVALID_ARG;
+    if (!h->ready) return fail(h, RT_ERR_NOT_READY, "handle not ready");
+    if (!cams || n_bundles == 0) return fail(h, RT_ERR_INVALID_ARG, "no bundles");
+    if (pixels && (reinterpret_cast<uintptr_t>(pixels) & 15u)) return fail(h, RT_ERR_INVALID_ARG, "pixels not 16-byte aligned");
+    bool mixed = cams[0].precision_mode == RT_PRECISION_MIXED;
+    for (uint32_t b = 0; b < n_bundles; ++b) {
+        if (!camera_valid(&cams[b])) return fail(h, RT_ERR_INVALID_ARG, "invalid camera in bundle table");
+        if ((cams[b].precision_mode == RT_PRECISION_MIXED) != mixed)
+            return fail(h, RT_ERR_INVALID_ARG, "one precision mode per bundle launch");
+    }
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    RT_CUDA(h, cudaSetDevice(h->device));
+    rt_status st = ensure_host_bundles(h, n_bundles);
+    if (st != RT_OK) return st;
+    if ((st = ensure(h, h->bundles, sizeof(BundleDesc) * n_bundles)) != RT_OK) return st;
+    RT_CUDA(h, cudaStreamSynchronize(s));
+    uint64_t begin = 0;
+    for (uint32_t b = 0; b < n_bundles; ++b) {
+        uint32_t row0, nrows;
+        row_window(cams[b], row0, nrows);
+        const uint64_t n = static_cast<uint64_t>(cams[b].screen_width) * nrows;
+        const uint64_t off = offsets ? offsets[b] : begin;
+        if (off + n > capacity) return fail(h, RT_ERR_INVALID_ARG, "bundle outputs exceed capacity");
+        build_bundle(cams[b], 0, cams[b].screen_width, row0, nrows, begin, off, h->host_bundles[b]);
+        begin += n;
+    }
+    if (begin == 0) return fail(h, RT_ERR_INVALID_ARG, "empty bundle table");
+    OutPtrs out{pixels, rays ? *rays : rt_ray_out{}};
+    const rt_launch_config c = effective_cfg(h, mixed);
+    const bool same = h->graph && h->graph_n_bundles == n_bundles && h->graph_total == begin &&
+                      std::memcmp(&h->graph_out, &out, sizeof out) == 0 &&
+                      std::memcmp(&h->graph_cfg, &c, sizeof c) == 0;
+    if (!same) {
+        if (h->graph) cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+        cudaGraph_t g = nullptr;
+        RT_CUDA(h, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e1 = cudaMemcpyAsync(h->bundles.ptr, h->host_bundles, sizeof(BundleDesc) * n_bundles,
+                                         cudaMemcpyHostToDevice, s);
+        rt_status ls = (e1 == cudaSuccess) ? launch(h, n_bundles, begin, out, mixed, s) : RT_ERR_DEVICE;
+        cudaError_t e2 = cudaStreamEndCapture(s, &g);
+        if (e1 != cudaSuccess) return cuda_fail(h, e1, "capture memcpy");
+        if (ls != RT_OK) {
+            if (g) cudaGraphDestroy(g);
+            return ls;
+        }
+        if (e2 != cudaSuccess) return cuda_fail(h, e2, "cudaStreamEndCapture");
+        cudaError_t e3 = cudaGraphInstantiate(&h->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) return cuda_fail(h, e3, "cudaGraphInstantiate");
+        h->graph_n_bundles = n_bundles;
+        h->graph_total = begin;
+        h->graph_out = out;
+        h->graph_cfg = c;
+    }
+    RT_CUDA(h, cudaGraphLaunch(h->graph, s));
+    h->timed = true;
+    return RT_OK;
+}
+
+rt_status rt_set_launch_config(rt_handle* h, const rt_launch_config* cfg) {
+    if (!h || !cfg) return RT_ERR_INVALID_ARG;
+    if (cfg->block_size != 0 && cfg->block_size != 64 && cfg->block_size != 128 && cfg->block_size != 256)
+        return fail(h, RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
+    if (cfg->refill_threshold > 32) return fail(h, RT_ERR_INVALID_ARG, "refill_threshold must be <= 32");
+    h->cfg = *cfg;
+    return RT_OK;
+}
+
+rt_status rt_get_launch_config(const rt_handle* h, rt_launch_config* cfg) {
+    if (!h || !cfg) return RT_ERR_INVALID_ARG;
+    *cfg = effective_cfg(h, false);
+    return RT_OK;
+}
+
+rt_status rt_synchronize(rt_handle* h, double timeout_ms) {
+    if (!h) return RT_ERR_INVALID_ARG;
+    return wait_stream(h, h->stream, timeout_ms);
+}
+
+rt_status rt_get_stats(rt_handle* h, rt_stats* out) {
+    if (!h || !out) return RT_ERR_INVALID_ARG;
+    std::memset(out, 0, sizeof *out);
+    RT_CUDA(h, cudaSetDevice(h->device));
+    RT_CUDA(h, cudaEventSynchronize(h->ev1));
+    unsigned long long v[ST_COUNT] = {};
+    RT_CUDA(h, cudaMemcpy(v, h->stats.ptr, sizeof v, cudaMemcpyDeviceToHost));
+    out->rays = v[ST_RAYS];
+    out->attempts = v[ST_ATTEMPTS];
+    out->accepted = v[ST_ACCEPTED];
+    out->rhs_evals = v[ST_RHS];
+    out->fp64_attempts = v[ST_FP64_ATTEMPTS];
+    float ms = 0.0f;
+    if (h->timed) RT_CUDA(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    out->kernel_ms = ms;
+    return RT_OK;
+}
+
+rt_status rt_measure_fma_peak(rt_handle* h, double* fp64_tflops, double* fp32_tflops) {
+    if (!h) return RT_ERR_INVALID_ARG;
+    RT_CUDA(h, cudaSetDevice(h->device));
+    float ms = 0.0f;
+    const double f64 = measure_fma_peak(true, h->sm_count, h->stream, &ms);
+    const double f32 = measure_fma_peak(false, h->sm_count, h->stream, &ms);
+    RT_CUDA(h, cudaGetLastError());
+    if (fp64_tflops) *fp64_tflops = f64;
+    if (fp32_tflops) *fp32_tflops = f32;
+    return RT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+// rt_bundle.cpp -- per-camera constants of the tracer (host, FP64).
+//
+// Everything here is computed once per camera; the per-pixel work runs on the
+// device.  Citations are to the reference source tree.
+#include <algorithm>
+#include <cmath>
+
+#include "rt_internal.h"
+
+namespace relsim {
+
+static double clampd(double v, double lo, double hi) { return (v < lo) ? lo : ((hi < v) ? hi : v); }
+static double maxd(double a, double b) { return (a < b) ? b : a; }
+
+// Bardeen-Press-Teukolsky ISCO, prograde for a >= 0
+// (software_compute_engine.hpp:1052-1061).
+double kerr_isco_radius(double m, double a_spin) {
+    const double a_star = clampd(a_spin / maxd(m, 1e-12), -0.9999999, 0.9999999);
+    const double abs_a = std::fabs(a_star);
+    const double orbit_sign = (a_star >= 0.0) ? -1.0 : 1.0;
+    const double cbrt_term = std::cbrt(maxd(1.0 - abs_a * abs_a, 0.0));
+    const double z1 = 1.0 + cbrt_term * (std::cbrt(1.0 + abs_a) + std::cbrt(1.0 - abs_a));
+    const double z2 = std::sqrt(3.0 * abs_a * abs_a + z1 * z1);
+    return (3.0 + z2 + orbit_sign * std::sqrt(maxd((3.0 - z1) * (3.0 + z1 + 2.0 * z2), 0.0))) * m;
+}
+
+void build_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
+                  uint64_t ray_begin, uint64_t out_offset, BundleDesc& b) {
+    b = BundleDesc{};
+    b.ray_begin = ray_begin;
+    b.out_offset = out_offset;
+    b.width = cam.screen_width;
+    b.height = cam.screen_height;
+    b.col0 = col0;
+    b.ncols = ncols;
+    b.row0 = row0;
+    b.nrows = nrows;
+    b.max_steps = cam.max_integration_steps;
+
+    // mass, spin clamp and outer horizon (software_compute_engine.hpp:3800-3803, 3370)
+    const double m = maxd(cam.metric_mass, 1e-4);
+    const double a = clampd(cam.metric_spin, -0.999 * m, 0.999 * m);
+    const double rh = m + std::sqrt(maxd(m * m - a * a, 0.0));
+    b.m = m;
+    b.a = a;
+    b.rh = rh;
+
+    // observer (software_compute_engine.hpp:3902-3904)
+    const double pi = 3.14159265358979323846;
+    const double r_obs = maxd(cam.observer_position[1], rh * 1.02);
+    const double th = clampd(cam.observer_position[2], 0.001, pi - 0.001);
+    const double ph = cam.observer_position[3];
+    b.st = std::sin(th);
+    b.ct = std::cos(th);
+    b.sp = std::sin(ph);
+    b.cp = std::cos(ph);
+    b.aspect = static_cast<double>(cam.screen_width) / static_cast<double>(cam.screen_height);
+    b.tan_half_fov = std::tan(cam.field_of_view_rad * 0.5);  // camera_projections.hpp:33
+    for (int i = 0; i < 3; ++i) {
+        b.fwd[i] = cam.tetrad_e1[1 + i];
+        b.rgt[i] = cam.tetrad_e2[1 + i];
+        b.up[i] = cam.tetrad_e3[1 + i];
+    }
+
+    // observer KS position (kerr_schild_null_integrator.hpp:47-54)
+    b.x0[0] = (r_obs * std::cos(ph) - a * std::sin(ph)) * std::sin(th);
+    b.x0[1] = (r_obs * std::sin(ph) + a * std::cos(ph)) * std::sin(th);
+    b.x0[2] = r_obs * std::cos(th);
+
+    // field at x0 (kerr_schild_null_integrator.hpp:31-44)
+    const double* x = b.x0;
+    const double a2 = a * a, z2 = x[2] * x[2];
+    const double diff = x[0] * x[0] + x[1] * x[1] + z2 - a2;
+    const double r2 = maxd(0.5 * (diff + std::sqrt(diff * diff + 4.0 * a2 * z2)), 1e-24);
+    const double r = std::sqrt(r2);
+    const double hf = m * r2 * r / (r2 * r2 + a2 * z2);
+    const double rpa = r2 + a2;
+    const double k[3] = {(r * x[0] + a * x[1]) / rpa, (r * x[1] - a * x[0]) / rpa, x[2] / r};
+    const double two_h = 2.0 * hf;
+    b.two_h = two_h;
+    for (int i = 0; i < 3; ++i) b.kf[i] = k[i];
+
+    // static-observer tetrad by Gram-Schmidt under g = eta + 2H l l
+    // (kerr_schild_null_integrator.hpp:154-177)
+    auto inner = [&](const double* A, const double* B) {
+        const double la = A[0] + k[0] * A[1] + k[1] * A[2] + k[2] * A[3];
+        const double lb = B[0] + k[0] * B[1] + k[1] * B[2] + k[2] * B[3];
+        return -A[0] * B[0] + A[1] * B[1] + A[2] * B[2] + A[3] * B[3] + two_h * la * lb;
+    };
+    const double u0 = 1.0 / std::sqrt(maxd(1.0 - two_h, 1e-6));
+    b.u0 = u0;
+    for (int i = 0; i < 3; ++i) {
+        b.e[i][0] = two_h * k[i] * u0 * u0;
+        b.e[i][1] = b.e[i][2] = b.e[i][3] = 0.0;
+        b.e[i][1 + i] = 1.0;
+    }
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < i; ++j) {
+            const double proj = inner(b.e[i], b.e[j]);
+            for (int c = 0; c < 4; ++c) b.e[i][c] -= proj * b.e[j][c];
+        }
+        const double inv_norm = 1.0 / std::sqrt(maxd(inner(b.e[i], b.e[i]), 1e-30));
+        for (int c = 0; c < 4; ++c) b.e[i][c] *= inv_norm;
+    }
+
+    // unwrapped azimuth at the observer (kerr_schild_null_integrator.hpp:61-63)
+    {
+        const double raw = std::atan2(x[1], x[0]) - std::atan2(a, r);
+        const double two_pi = 2.0 * pi;
+        double d = raw - ph;
+        d -= two_pi * std::floor(d / two_pi + 0.5);
+        b.phi_start = ph + d;
+        b.raw_phi0 = raw;
+        b.wind0 = static_cast<int32_t>(std::lround((b.phi_start - raw) / two_pi));
+    }
+
+    // classification and integration
+    b.r_capture = cam.capture_scale * rh;
+    b.r_esc = cam.escape_radius;
+    const bool disk = cam.disk_outer_radius > 0.0;
+    b.r_in = (cam.disk_inner_radius > 0.0) ? cam.disk_inner_radius : kerr_isco_radius(m, a);
+    b.r_out = cam.disk_outer_radius;
+    b.r_early = disk ? b.r_in : 1e300;
+    b.rtol = cam.rtol;
+    b.atol = cam.atol;
+    b.cap_c = cam.step_cap_fraction;
+    b.h0 = cam.initial_step_fraction * r_obs;
+    b.proj_tol = cam.projection_tol;
+    b.fp64_radius = (cam.mixed_fp64_radius > 0.0) ? cam.mixed_fp64_radius : std::max(3.0 * rh, 5.0 * m);
+    b.flags = (disk ? BF_DISK : 0u) | (cam.early_capture ? BF_EARLY_CAPTURE : 0u) |
+              (cam.precision_mode == RT_PRECISION_MIXED ? BF_MIXED : 0u);
+}
+
+}  // namespace relsim

@@ -1,0 +1,121 @@
+// rt_device.cuh -- device math of the backward null-geodesic tracer.
+//
+// Kerr-Schild Hamiltonian with p_t = -1 (kerr_schild_null_integrator.hpp:72-114),
+// rewritten for the GPU: the 9 partial derivatives of the null vector are never
+// formed.  With dk_j/dx_i contracted against p first, the RHS needs one
+// reciprocal each of r, r^2 + a^2 and the Kerr-Schild denominator instead of
+// 12 divisions; one rsqrt gives both r and 1/r.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace relsim {
+
+// Dormand-Prince 5(4) tableau (rk45_adaptive.hpp:196-203).
+struct DP {
+    static constexpr double A21 = 1.0 / 5.0;
+    static constexpr double A31 = 3.0 / 40.0, A32 = 9.0 / 40.0;
+    static constexpr double A41 = 44.0 / 45.0, A42 = -56.0 / 15.0, A43 = 32.0 / 9.0;
+    static constexpr double A51 = 19372.0 / 6561.0, A52 = -25360.0 / 2187.0, A53 = 64448.0 / 6561.0,
+                            A54 = -212.0 / 729.0;
+    static constexpr double A61 = 9017.0 / 3168.0, A62 = -355.0 / 33.0, A63 = 46732.0 / 5247.0,
+                            A64 = 49.0 / 176.0, A65 = -5103.0 / 18656.0;
+    static constexpr double B1 = 35.0 / 384.0, B3 = 500.0 / 1113.0, B4 = 125.0 / 192.0, B5 = -2187.0 / 6784.0,
+                            B6 = 11.0 / 84.0;
+    static constexpr double E1 = 71.0 / 57600.0, E3 = -71.0 / 16695.0, E4 = 71.0 / 1920.0,
+                            E5 = -17253.0 / 339200.0, E6 = 22.0 / 525.0, E7 = -1.0 / 40.0;
+};
+
+template <typename T>
+__device__ __forceinline__ T rt_rsqrt(T v);
+template <>
+__device__ __forceinline__ double rt_rsqrt<double>(double v) { return rsqrt(v); }
+template <>
+__device__ __forceinline__ float rt_rsqrt<float>(float v) { return rsqrtf(v); }
+
+template <typename T>
+__device__ __forceinline__ T rt_rcp(T v);
+template <>
+__device__ __forceinline__ double rt_rcp<double>(double v) { return 1.0 / v; }
+template <>
+__device__ __forceinline__ float rt_rcp<float>(float v) { return __frcp_rn(v); }
+
+template <typename T>
+__device__ __forceinline__ T rt_sqrt(T v);
+template <>
+__device__ __forceinline__ double rt_sqrt<double>(double v) { return sqrt(v); }
+template <>
+__device__ __forceinline__ float rt_sqrt<float>(float v) { return sqrtf(v); }
+
+// Boyer-Lindquist r of a Kerr-Schild point (kerr_schild_null_integrator.hpp:32-36).
+template <typename T>
+__device__ __forceinline__ T bl_r2(T x, T y, T z, T a2) {
+    const T z2 = z * z;
+    const T diff = x * x + y * y + z2 - a2;
+    const T r2 = T(0.5) * (diff + rt_sqrt<T>(diff * diff + T(4) * a2 * z2));
+    return fmax(r2, T(1e-24));
+}
+
+// Hamiltonian RHS.  y = (x, y, z, p_x, p_y, p_z); returns r_BL and, through
+// hf/s, the Kerr-Schild scalar H and s = 1 + k.p at y.
+//   dx/dl = p - 2 H s k
+//   dp/dl = s^2 dH/dx + 2 H s (dk/dx . p)
+// with dk/dx_i . p = dr_i * A + B_i (A, B below) and dH/dx_i = C dr_i (+ D for z).
+template <typename T>
+__device__ __forceinline__ T ks_rhs(const T* __restrict__ y, T M, T a, T* __restrict__ dy, T& hf, T& s) {
+    const T x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
+    const T a2 = a * a;
+    const T z2 = z * z;
+    const T r2 = bl_r2<T>(x, yy, z, a2);
+    const T inv_r = rt_rsqrt<T>(r2);
+    const T r = r2 * inv_r;
+    const T rpa = r2 + a2;
+    const T inv_rpa = rt_rcp<T>(rpa);
+    const T r4 = r2 * r2;
+    const T inv_den = rt_rcp<T>(r4 + a2 * z2);
+    const T r3 = r2 * r;
+    const T H = M * r3 * inv_den;
+    const T k0 = (r * x + a * yy) * inv_rpa;
+    const T k1 = (r * yy - a * x) * inv_rpa;
+    const T k2 = z * inv_r;
+    const T sv = T(1) + k0 * px + k1 * py + k2 * pz;
+    const T two_hs = T(2) * H * sv;
+    dy[0] = px - two_hs * k0;
+    dy[1] = py - two_hs * k1;
+    dy[2] = pz - two_hs * k2;
+    const T r3d = r3 * inv_den;
+    const T dr0 = r3d * x;
+    const T dr1 = r3d * yy;
+    const T dr2 = r * rpa * z * inv_den;
+    const T inv_den2 = inv_den * inv_den;
+    const T C = M * r2 * (T(3) * a2 * z2 - r4) * inv_den2;
+    const T D = T(-2) * M * a2 * r3 * z * inv_den2;
+    const T A = inv_rpa * ((x - T(2) * r * k0) * px + (yy - T(2) * r * k1) * py) - inv_r * k2 * pz;
+    const T B0 = inv_rpa * (r * px - a * py);
+    const T B1 = inv_rpa * (r * py + a * px);
+    const T B2 = inv_r * pz;
+    const T s2 = sv * sv;
+    const T G = s2 * C + two_hs * A;
+    dy[3] = dr0 * G + two_hs * B0;
+    dy[4] = dr1 * G + two_hs * B1;
+    dy[5] = dr2 * G + two_hs * B2 + s2 * D;
+    hf = H;
+    s = sv;
+    return r;
+}
+
+// Kerr-Schild field only (r, H, k) at x.
+__device__ __forceinline__ double ks_field64(const double* x, double M, double a, double* k, double& hf) {
+    const double a2 = a * a;
+    const double r2 = bl_r2<double>(x[0], x[1], x[2], a2);
+    const double r = sqrt(r2);
+    const double rpa = r2 + a2;
+    hf = M * r2 * r / (r2 * r2 + a2 * x[2] * x[2]);
+    k[0] = (r * x[0] + a * x[1]) / rpa;
+    k[1] = (r * x[1] - a * x[0]) / rpa;
+    k[2] = x[2] / r;
+    return r;
+}
+
+}  // namespace relsim

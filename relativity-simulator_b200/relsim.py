@@ -1,0 +1,293 @@
+"""Python binding of the tracer's C ABI (include/relsim_cuda.h).
+
+The product is the CUDA library librelsim_cuda.so; this module loads it with
+ctypes and exposes the same entry points to Python callers (tests, bench,
+serving loop).  There is no CPU path: if the library or the GPU is missing,
+`Tracer()` raises.
+
+    from relsim import Tracer, make_camera
+    tr = Tracer()
+    cam = make_camera(spin=0.94, r_obs=100, incl_deg=17, fov_deg=12, width=2048, height=2048)
+    out = tr.dispatch(cam)            # host arrays: status, r, theta, phi, r_hit, g, ...
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from typing import Iterable
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librelsim_cuda.so")
+
+RT_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "TIMEOUT", 4: "DEVICE", 5: "CANCELLED", 6: "NOT_READY",
+                7: "BUDGET", 8: "AGAIN"}
+RAY_UNFINISHED, RAY_CAPTURED, RAY_ESCAPED, RAY_DISK = 0, 1, 2, 3
+RAYFLAG_NONFINITE, RAYFLAG_STEP_UNDERFLOW, RAYFLAG_MAX_STEPS, RAYFLAG_EARLY_CAPTURE = 1, 2, 4, 8
+PIXEL_HORIZON_ABSORBED, PIXEL_CELESTIAL_HIT, PIXEL_ACCRETION_DISK_HIT = 1, 2, 4
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+_d = ctypes.c_double
+_u32 = ctypes.c_uint32
+
+
+class Camera(ctypes.Structure):
+    _fields_ = [
+        ("observer_position", _d * 4), ("tetrad_e1", _d * 4), ("tetrad_e2", _d * 4), ("tetrad_e3", _d * 4),
+        ("field_of_view_rad", _d), ("metric_mass", _d), ("metric_spin", _d), ("escape_radius", _d),
+        ("capture_scale", _d), ("disk_inner_radius", _d), ("disk_outer_radius", _d), ("rtol", _d), ("atol", _d),
+        ("step_cap_fraction", _d), ("initial_step_fraction", _d), ("projection_tol", _d), ("mixed_fp64_radius", _d),
+        ("screen_width", _u32), ("screen_height", _u32), ("max_integration_steps", _u32), ("early_capture", _u32),
+        ("precision_mode", _u32), ("dispatch_row_offset", _u32), ("dispatch_row_count", _u32),
+        ("tile_origin_x", _u32), ("tile_origin_y", _u32), ("tile_extent_x", _u32), ("tile_extent_y", _u32),
+        ("reserved", _u32),
+    ]
+
+
+class PixelOut(ctypes.Structure):
+    _fields_ = [("r", ctypes.c_float), ("g", ctypes.c_float), ("b", ctypes.c_float), ("a", ctypes.c_float),
+                ("redshift", ctypes.c_float), ("affine_parameter", ctypes.c_float), ("status_flags", _u32),
+                ("iterations_used", _u32)]
+
+
+RAY_FIELDS = [("status", np.uint32), ("flags", np.uint32), ("steps_accepted", np.uint32),
+              ("steps_rejected", np.uint32), ("r", np.float64), ("theta", np.float64), ("phi", np.float64),
+              ("r_hit", np.float64), ("g", np.float64), ("lambda", np.float64), ("dH", np.float64),
+              ("dE", np.float64), ("dLz", np.float64), ("dQ", np.float64)]
+PIXEL_DTYPE = np.dtype([("r", "f4"), ("g", "f4"), ("b", "f4"), ("a", "f4"), ("redshift", "f4"),
+                        ("affine_parameter", "f4"), ("status_flags", "u4"), ("iterations_used", "u4")])
+
+
+class RayOut(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name, _ in RAY_FIELDS]
+
+
+class LaunchConfig(ctypes.Structure):
+    _fields_ = [("block_size", _u32), ("ctas_per_sm", _u32), ("refill_threshold", _u32), ("rays_per_claim", _u32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("rays", ctypes.c_uint64), ("attempts", ctypes.c_uint64), ("accepted", ctypes.c_uint64),
+                ("rhs_evals", ctypes.c_uint64), ("fp64_attempts", ctypes.c_uint64), ("kernel_ms", _d)]
+
+
+_lib: ctypes.CDLL | None = None
+
+EXPORTS = ["rt_create", "rt_destroy", "rt_is_ready", "rt_is_platform_supported", "rt_last_error", "rt_abi_version",
+           "rt_camera_defaults", "rt_camera_look_at_hole", "rt_dispatch", "rt_dispatch_tile", "rt_dispatch_device",
+           "rt_trace_bundles_device", "rt_bundle_rays", "rt_set_launch_config", "rt_get_launch_config",
+           "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak"]
+
+
+def lib() -> ctypes.CDLL:
+    """Load librelsim_cuda.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: run relativity-simulator_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        v, p = ctypes.c_void_p, ctypes.POINTER
+        L.rt_create.argtypes = [p(ctypes.c_void_p), ctypes.c_int]
+        L.rt_destroy.argtypes = [v]
+        L.rt_destroy.restype = None
+        L.rt_is_ready.argtypes = [v]
+        L.rt_last_error.argtypes = [v]
+        L.rt_last_error.restype = ctypes.c_char_p
+        L.rt_camera_defaults.argtypes = [p(Camera)]
+        L.rt_camera_defaults.restype = None
+        L.rt_camera_look_at_hole.argtypes = [p(Camera), _d, _d, _d]
+        L.rt_camera_look_at_hole.restype = None
+        L.rt_dispatch.argtypes = [v, p(Camera), v, p(RayOut), ctypes.c_size_t, v]
+        L.rt_dispatch_tile.argtypes = [v, p(Camera), v, p(RayOut), ctypes.c_size_t]
+        L.rt_dispatch_device.argtypes = [v, p(Camera), v, p(RayOut), ctypes.c_size_t, v]
+        L.rt_trace_bundles_device.argtypes = [v, p(Camera), _u32, v, v, p(RayOut), ctypes.c_size_t, v]
+        L.rt_bundle_rays.argtypes = [p(Camera), _u32]
+        L.rt_bundle_rays.restype = ctypes.c_uint64
+        L.rt_set_launch_config.argtypes = [v, p(LaunchConfig)]
+        L.rt_get_launch_config.argtypes = [v, p(LaunchConfig)]
+        L.rt_get_stats.argtypes = [v, p(Stats)]
+        L.rt_synchronize.argtypes = [v, _d]
+        L.rt_measure_fma_peak.argtypes = [v, p(_d), p(_d)]
+        _lib = L
+    return _lib
+
+
+class RelsimError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def make_camera(*, spin: float = 0.94, mass: float = 1.0, r_obs: float = 100.0, incl_deg: float = 17.0,
+                phi_obs: float = 0.0, fov_deg: float = 12.0, width: int = 2048, height: int = 2048,
+                escape_radius: float = 1000.0, capture_scale: float = 1.01, disk_inner: float = 0.0,
+                disk_outer: float = 20.0, rtol: float = 1e-10, atol: float = 1e-10, max_steps: int = 20000,
+                step_cap: float = 0.1, h0: float = 0.01, projection_tol: float = 1e-12, early_capture: bool = True,
+                precision: int = PRECISION_FP64, mixed_fp64_radius: float = 0.0, row_offset: int = 0,
+                row_count: int = 0) -> Camera:
+    """A camera looking at the hole from (r_obs, incl, phi_obs) with a static-observer tetrad."""
+    c = Camera()
+    c.field_of_view_rad = math.radians(fov_deg)
+    c.metric_mass, c.metric_spin = mass, spin
+    c.escape_radius, c.capture_scale = escape_radius, capture_scale
+    c.disk_inner_radius, c.disk_outer_radius = disk_inner, disk_outer
+    c.rtol, c.atol = rtol, atol
+    c.step_cap_fraction, c.initial_step_fraction, c.projection_tol = step_cap, h0, projection_tol
+    c.mixed_fp64_radius = mixed_fp64_radius
+    c.screen_width, c.screen_height = width, height
+    c.max_integration_steps = max_steps
+    c.early_capture = 1 if early_capture else 0
+    c.precision_mode = precision
+    c.dispatch_row_offset, c.dispatch_row_count = row_offset, row_count
+    th, ph = math.radians(incl_deg), phi_obs
+    st, ct, sp, cp = math.sin(th), math.cos(th), math.sin(ph), math.cos(ph)
+    er, eth, eph = (st * cp, st * sp, ct), (ct * cp, ct * sp, -st), (-sp, cp, 0.0)
+    c.observer_position[:] = [0.0, r_obs, th, ph]
+    c.tetrad_e1[:] = [0.0, -er[0], -er[1], -er[2]]
+    c.tetrad_e2[:] = [0.0, *eph]
+    c.tetrad_e3[:] = [0.0, -eth[0], -eth[1], -eth[2]]
+    return c
+
+
+def camera_dict(c: Camera) -> dict:
+    """The camera as a dict of plain values (the oracle's camera keys)."""
+    d = {}
+    for name, _ in Camera._fields_:
+        v = getattr(c, name)
+        d[name] = list(v) if hasattr(v, "__len__") else v
+    d["max_steps"] = c.max_integration_steps
+    return d
+
+
+def window_rays(c: Camera) -> int:
+    rows = c.screen_height - min(c.dispatch_row_offset, c.screen_height)
+    if c.dispatch_row_count:
+        rows = min(rows, c.dispatch_row_count)
+    return c.screen_width * rows
+
+
+class Tracer:
+    """One device handle (VulkanComputeExecutor's role)."""
+
+    def __init__(self, device: int = 0):
+        L = lib()
+        h = ctypes.c_void_p()
+        st = L.rt_create(ctypes.byref(h), device)
+        if st != RT_OK:
+            raise RelsimError(st, f"rt_create(device={device}) failed (no sm_100 device?)")
+        self._h = h
+        self.lib = L
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.rt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def _check(self, st: int) -> None:
+        if st != RT_OK:
+            raise RelsimError(st, self.lib.rt_last_error(self._h).decode())
+
+    def is_ready(self) -> bool:
+        return bool(self.lib.rt_is_ready(self._h))
+
+    def dispatch(self, cam: Camera, fields: Iterable[str] | None = None, pixels: bool = True,
+                 cancel: ctypes.c_int | None = None, tile: bool = False) -> dict:
+        """Trace on the device, read back into new host arrays (rt_dispatch / rt_dispatch_tile)."""
+        names = [n for n, _ in RAY_FIELDS] if fields is None else list(fields)
+        if tile:
+            n = min(cam.tile_extent_x, cam.screen_width - cam.tile_origin_x) * \
+                min(cam.tile_extent_y, cam.screen_height - cam.tile_origin_y)
+        else:
+            n = window_rays(cam)
+        out = {}
+        ro = RayOut()
+        for name, dt in RAY_FIELDS:
+            if name in names:
+                out[name] = np.empty(n, dtype=dt)
+                setattr(ro, name, out[name].ctypes.data)
+        pix = np.empty(n, dtype=PIXEL_DTYPE) if pixels else None
+        pptr = pix.ctypes.data if pix is not None else None
+        if tile:
+            st = self.lib.rt_dispatch_tile(self._h, ctypes.byref(cam), pptr, ctypes.byref(ro), n)
+        else:
+            st = self.lib.rt_dispatch(self._h, ctypes.byref(cam), pptr, ctypes.byref(ro), n,
+                                      ctypes.byref(cancel) if cancel is not None else None)
+        self._check(st)
+        if pix is not None:
+            out["pixels"] = pix
+        return out
+
+    def dispatch_device(self, cam: Camera, rays: RayOut, pixels_ptr: int | None, capacity: int,
+                        stream: int | None = None) -> None:
+        """Enqueue a trace into device buffers (pointers from torch tensors); no wait."""
+        self._check(self.lib.rt_dispatch_device(self._h, ctypes.byref(cam), pixels_ptr, ctypes.byref(rays),
+                                                capacity, stream))
+
+    def trace_bundles_device(self, cams: list[Camera], rays: RayOut, pixels_ptr: int | None, capacity: int,
+                             offsets: np.ndarray | None = None, stream: int | None = None) -> None:
+        arr = (Camera * len(cams))(*cams)
+        optr = None
+        if offsets is not None:
+            offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+            optr = offsets.ctypes.data
+        self._check(self.lib.rt_trace_bundles_device(self._h, arr, len(cams), optr, pixels_ptr, ctypes.byref(rays),
+                                                     capacity, stream))
+
+    def stats(self) -> Stats:
+        s = Stats()
+        self._check(self.lib.rt_get_stats(self._h, ctypes.byref(s)))
+        return s
+
+    def synchronize(self, timeout_ms: float = 0.0) -> None:
+        self._check(self.lib.rt_synchronize(self._h, timeout_ms))
+
+    def set_launch_config(self, block_size: int = 0, ctas_per_sm: int = 0, refill_threshold: int = 0) -> None:
+        c = LaunchConfig(block_size, ctas_per_sm, refill_threshold, 1)
+        self._check(self.lib.rt_set_launch_config(self._h, ctypes.byref(c)))
+
+    def launch_config(self) -> LaunchConfig:
+        c = LaunchConfig()
+        self._check(self.lib.rt_get_launch_config(self._h, ctypes.byref(c)))
+        return c
+
+    def measure_fma_peak(self) -> tuple[float, float]:
+        f64, f32 = _d(), _d()
+        self._check(self.lib.rt_measure_fma_peak(self._h, ctypes.byref(f64), ctypes.byref(f32)))
+        return f64.value, f32.value
+
+
+def bundle_rays(cams: list[Camera]) -> int:
+    arr = (Camera * len(cams))(*cams)
+    return int(lib().rt_bundle_rays(arr, len(cams)))
+
+
+def device_ray_out(n: int, fields: Iterable[str] | None = None, device: str = "cuda:0"):
+    """Allocate device SoA outputs as torch tensors; returns (RayOut, {name: tensor})."""
+    import torch
+
+    tdt = {np.uint32: torch.int32, np.float64: torch.float64}
+    names = [f for f, _ in RAY_FIELDS] if fields is None else list(fields)
+    ro = RayOut()
+    tensors = {}
+    for name, dt in RAY_FIELDS:
+        if name in names:
+            t = torch.empty(n, dtype=tdt[dt], device=device)
+            tensors[name] = t
+            setattr(ro, name, t.data_ptr())
+    return ro, tensors

@@ -1,0 +1,43 @@
+"""Trace one image on cuda:0 and print a summary (also the profiling driver).
+
+    python relativity-simulator_b200/trace_once.py [--side 512] [--spin 0.94] [--r-obs 100]
+        [--incl 17] [--fov 12] [--precision fp64|mixed] [--repeat 1]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+import numpy as np  # noqa: E402
+
+import relsim  # noqa: E402
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--side", type=int, default=512)
+    ap.add_argument("--spin", type=float, default=0.94)
+    ap.add_argument("--r-obs", type=float, default=100.0)
+    ap.add_argument("--incl", type=float, default=17.0)
+    ap.add_argument("--fov", type=float, default=12.0)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--repeat", type=int, default=1)
+    a = ap.parse_args()
+    cam = relsim.make_camera(spin=a.spin, r_obs=a.r_obs, incl_deg=a.incl, fov_deg=a.fov, width=a.side,
+                             height=a.side,
+                             precision=relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64)
+    with relsim.Tracer(0) as tr:
+        for _ in range(a.repeat):
+            out = tr.dispatch(cam, fields=["status", "steps_accepted", "steps_rejected"], pixels=False)
+            s = tr.stats()
+    print(json.dumps({"rays": int(s.rays), "attempts": int(s.attempts), "accepted": int(s.accepted),
+                      "kernel_ms": s.kernel_ms, "mrays_per_s": s.rays / s.kernel_ms / 1e3,
+                      "classes": np.bincount(out["status"], minlength=4).tolist()}))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,139 @@
+"""Parity of the CUDA FP64 tracer with the FP64 oracle (through the C ABI).
+
+Bars (FP64 mode, same algorithm on both sides):
+  - class identical for every ray outside the 1e-6 M boundary band;
+  - final (r, theta, phi), disk-hit radius and g within 1e-9 relative;
+  - accepted / rejected step counts equal for at least 99.9 % of rays.
+Ulp-level differences (FMA contraction, device vs host libm) grow only along
+near-critical rays; rays that orbit the photon region are excluded from the
+1e-9 position check by |d_b| > 1e-3 M (they stay in the class check).
+"""
+import numpy as np
+import pytest
+
+import relsim
+from cameras import config_cam
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-9
+
+
+def _compare(tr, cam, pixels=None, class_only_band=1e-6, pos_band=1e-3):
+    out = tr.dispatch(cam)
+    ref = O.trace(relsim.camera_dict(cam), pixels=pixels)
+    if pixels is not None:
+        out = {k: v[pixels] for k, v in out.items()}
+    st, rst = out["status"], ref["status"]
+    r_in = O.lib().orc_isco_radius(cam.metric_mass, cam.metric_spin) if cam.disk_inner_radius <= 0 else cam.disk_inner_radius
+    band = O.boundary_band(ref, r_in, cam.disk_outer_radius, class_only_band)
+    mism = (st != rst) & ~band
+    assert not mism.any(), f"{mism.sum()} class mismatches outside the band: idx {np.nonzero(mism)[0][:10]}"
+    same = (st == rst) & (np.abs(ref["db_shadow"]) > pos_band)
+    for f in ("r", "theta"):
+        rel = np.abs(out[f][same] - ref[f][same]) / np.maximum(np.abs(ref[f][same]), 1e-300)
+        assert rel.max() < REL, (f, rel.max())
+    dphi = np.abs(out["phi"][same] - ref["phi"][same]) / np.maximum(np.abs(ref["phi"][same]), 1.0)
+    assert dphi.max() < REL
+    disk = same & (rst == O.DISK)
+    if disk.any():
+        assert np.max(np.abs(out["r_hit"][disk] - ref["r_hit"][disk]) / ref["r_hit"][disk]) < REL
+        assert np.max(np.abs(out["g"][disk] - ref["g"][disk]) / ref["g"][disk]) < REL
+    assert np.all(np.isnan(out["r_hit"][rst != O.DISK]) | (st[rst != O.DISK] == O.DISK))
+    steps_equal = (out["steps_accepted"] == ref["steps_accepted"]) & (out["steps_rejected"] == ref["steps_rejected"])
+    assert steps_equal[same].mean() > 0.999
+    return out, ref
+
+
+@pytest.mark.parametrize("tag,side", [("c1", 64), ("c2", 64), ("c3", 64)])
+def test_fp64_full_image_matches_oracle(tracer, tag, side):
+    cam = config_cam(tag, width=side, height=side)
+    out, ref = _compare(tracer, cam)
+    assert np.all(out["status"] != relsim.RAY_UNFINISHED)
+
+
+def test_fp64_c2_fullsize_sample_matches_oracle(tracer):
+    """2048^2 headline camera: the whole image on the GPU, 3000 random rays on the oracle."""
+    cam = config_cam("c2")
+    rng = np.random.default_rng(7)
+    pix = rng.choice(2048 * 2048, 3000, replace=False)
+    _compare(tracer, cam, pixels=pix)
+
+
+def test_pixel_output_matches_record(tracer):
+    cam = config_cam("c2", width=48, height=48)
+    out = tracer.dispatch(cam)
+    px = out["pixels"]
+    flags = np.select([out["status"] == 1, out["status"] == 2, out["status"] == 3], [1, 2, 4], 0)
+    np.testing.assert_array_equal(px["status_flags"], flags)
+    np.testing.assert_array_equal(px["iterations_used"], out["steps_accepted"])
+    disk = out["status"] == 3
+    np.testing.assert_allclose(px["redshift"][disk], out["g"][disk].astype(np.float32))
+    assert np.all(px["redshift"][~disk] == 1.0)
+    assert np.all(px["a"] == 1.0)
+
+
+def test_row_window_and_tile_match_full_image(tracer):
+    """dispatch_and_readback row window and dispatch_tile_and_readback tile
+    (vulkan_compute_executor.hpp:1372-1426) return the full image's rays."""
+    W = H = 40
+    full = tracer.dispatch(config_cam("c2", width=W, height=H))
+    win = tracer.dispatch(config_cam("c2", width=W, height=H, row_offset=13, row_count=9))
+    for f in ("status", "r", "theta", "phi", "r_hit", "steps_accepted"):
+        np.testing.assert_array_equal(win[f], full[f][13 * W:22 * W])
+    cam = config_cam("c2", width=W, height=H)
+    cam.tile_origin_x, cam.tile_origin_y, cam.tile_extent_x, cam.tile_extent_y = 7, 30, 16, 16
+    tile = tracer.dispatch(cam, tile=True)
+    img = full["r"].reshape(H, W)
+    exp = img[30:40, 7:23].reshape(-1)  # extent clipped to the image
+    np.testing.assert_array_equal(tile["r"], exp)
+
+
+def test_schwarzschild_mirror_symmetry_fullsize(tracer):
+    """a = 0, observer in the x-z plane: the image is mirror-symmetric in u, so
+    pixel x and W-1-x have the same class and r_hit (size-independent check at
+    the full 256^2 c1 size)."""
+    cam = config_cam("c1")
+    out = tracer.dispatch(cam, fields=["status", "r_hit"])
+    st = out["status"].reshape(256, 256)
+    assert np.mean(st == st[:, ::-1]) > 0.9999
+    rh = out["r_hit"].reshape(256, 256)
+    both = (st == 3) & (st[:, ::-1] == 3)
+    assert np.nanmax(np.abs(rh - rh[:, ::-1])[both] / rh[both]) < 1e-9
+
+
+def test_fullsize_c2_invariants_and_classes(tracer):
+    cam = config_cam("c2")
+    out = tracer.dispatch(cam, fields=["status", "flags", "dE", "dLz", "dQ", "r_hit"], pixels=False)
+    st = out["status"]
+    assert st.size == 2048 * 2048
+    assert np.all(st != relsim.RAY_UNFINISHED)
+    counts = np.bincount(st, minlength=4)
+    assert counts[1] > 0 and counts[3] > 0
+    ok = out["flags"] == 0
+    assert np.max(np.abs(out["dE"][ok])) < 1e-8
+    assert np.max(np.abs(out["dLz"][ok])) < 1e-6
+    disk = st == 3
+    r_in = O.lib().orc_isco_radius(1.0, 0.94)
+    assert np.all((out["r_hit"][disk] >= r_in) & (out["r_hit"][disk] <= 20.0))
+
+
+def test_invalid_arguments_are_rejected(tracer):
+    cam = config_cam("c2", width=8, height=8)
+    cam.rtol = -1.0
+    with pytest.raises(relsim.RelsimError) as e:
+        tracer.dispatch(cam)
+    assert e.value.status == 1
+    cam = config_cam("c2", width=8, height=8, row_offset=8)
+    with pytest.raises(relsim.RelsimError):
+        tracer.dispatch(cam)
+    assert tracer.is_ready()
+
+
+def test_repeat_dispatch_is_deterministic(tracer):
+    cam = config_cam("c3", width=48, height=48)
+    a = tracer.dispatch(cam)
+    b = tracer.dispatch(cam)
+    for f in ("status", "r", "theta", "phi", "r_hit", "g", "lambda", "steps_accepted"):
+        np.testing.assert_array_equal(a[f], b[f])
