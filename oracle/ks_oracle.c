@@ -487,6 +487,48 @@ static double disk_root(double m, double a, const double* y, double h, double k1
     return t;
 }
 
+/* Cubic Hermite interpolant of a step from its end points and FSAL slopes:
+ * y(t) = h00 y0 + h10 h f0 + h01 y1 + h11 h f1, t in [0, 1]. */
+static void hermite(const double* y0, const double* f0, const double* y1, const double* f1, double h, double t,
+                    int n, double* out)
+{
+    const double t2 = t * t, t3 = t2 * t;
+    const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
+    const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+    for (int i = 0; i < n; ++i) out[i] = h00 * y0[i] + h10 * h * f0[i] + h01 * y1[i] + h11 * h * f1[i];
+}
+
+/* Fraction t of the step where the interpolated r_BL crosses `target`
+ * (Illinois on r(x(t)) - target; r(0) and r(1) bracket the target). */
+static double crossing_fraction(const double* y0, const double* f0, const double* y1, const double* f1, double h,
+                                double a, double target)
+{
+    double lo = 0.0, hi = 1.0;
+    double flo = bl_radius(y0, a) - target, fhi = bl_radius(y1, a) - target;
+    if (!((flo > 0.0) != (fhi > 0.0))) return 1.0; /* no bracket: keep the step end */
+    int side = 0;
+    double t = 1.0, x[3];
+    for (int it = 0; it < 60; ++it) {
+        t = (lo * fhi - hi * flo) / (fhi - flo);
+        if (!(t > lo && t < hi)) t = 0.5 * (lo + hi);
+        hermite(y0, f0, y1, f1, h, t, 3, x);
+        const double ft = bl_radius(x, a) - target;
+        if (ft == 0.0 || fabs(hi - lo) < 1e-15 || fabs(ft) < 1e-13 * target) break;
+        if ((ft > 0.0) == (fhi > 0.0)) {
+            hi = t;
+            fhi = ft;
+            if (side == -1) flo *= 0.5;
+            side = -1;
+        } else {
+            lo = t;
+            flo = ft;
+            if (side == 1) fhi *= 0.5;
+            side = 1;
+        }
+    }
+    return t;
+}
+
 static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, uint32_t py, orc_ray* out)
 {
     const double m = c->m, a = c->a;
@@ -573,6 +615,42 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
                     }
                 }
             }
+            /* capture / escape / certain capture inside this step: the terminal
+             * point is interpolated to the threshold radius, so it does not
+             * depend on where the step happened to end */
+            {
+                double target = 0.0;
+                uint32_t term = 0, tflag = 0;
+                if (rn < c->r_capture) {
+                    term = ORC_RAY_CAPTURED;
+                    target = c->r_capture;
+                } else if (rn > c->r_esc) {
+                    term = ORC_RAY_ESCAPED;
+                    target = c->r_esc;
+                } else if (can_early && rn < r_early) {
+                    /* dr_BL/dlambda from dx/dlambda (kerr_invariants.hpp:140); the trace
+                     * runs towards decreasing lambda, so dr/dlambda > 0 means inwards. */
+                    const double r2 = rn * rn, z = yn[2];
+                    const double drdl = (r2 * rn * (yn[0] * k[6][0] + yn[1] * k[6][1]) +
+                                         rn * (r2 + a * a) * z * k[6][2]) /
+                                        (r2 * r2 + a * a * z * z);
+                    if (drdl > 0.0) {
+                        term = ORC_RAY_CAPTURED;
+                        tflag = ORC_FLAG_EARLY_CAPTURE;
+                        target = r_early;
+                    }
+                }
+                if (term) {
+                    const double t = crossing_fraction(y, k[0], yn, k[6], h, a, target);
+                    double yt[6];
+                    hermite(y, k[0], yn, k[6], h, t, 6, yt);
+                    memcpy(y, yt, sizeof yt);
+                    lambda += t * h;
+                    status = term;
+                    flags |= tflag;
+                    break;
+                }
+            }
             dH = max_d(dH, project_null(m, a, yn, cam->projection_tol));
             /* phi unwrapping, kerr_schild_null_integrator.hpp:61-63 */
             {
@@ -585,18 +663,6 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
             memcpy(y, yn, sizeof yn);
             memcpy(k[0], k[6], sizeof(double) * 6); /* FSAL */
             r = rn;
-            if (can_early && rn < r_early) {
-                /* dr_BL/dlambda from dx/dlambda (kerr_invariants.hpp:140); the trace
-                 * runs towards decreasing lambda, so dr/dlambda > 0 means inwards. */
-                const double r2 = rn * rn, z = y[2];
-                const double drdl = (r2 * rn * (y[0] * k[0][0] + y[1] * k[0][1]) + rn * (r2 + a * a) * z * k[0][2]) /
-                                    (r2 * r2 + a * a * z * z);
-                if (drdl > 0.0) {
-                    status = ORC_RAY_CAPTURED;
-                    flags |= ORC_FLAG_EARLY_CAPTURE;
-                    break;
-                }
-            }
             double factor;
             if (err == 0.0) {
                 factor = 5.0;

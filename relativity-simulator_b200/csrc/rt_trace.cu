@@ -246,6 +246,47 @@ __device__ void finish_ray(const BundleDesc& B, RayLane& L, uint32_t status, dou
     L.mode = MODE_IDLE;
 }
 
+// Cubic Hermite interpolant of a step from its end points and FSAL slopes.
+__device__ __forceinline__ void hermite(const double* y0, const double* f0, const double* y1, const double* f1,
+                                        double h, double t, int n, double* out) {
+    const double t2 = t * t, t3 = t2 * t;
+    const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
+    const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+    for (int i = 0; i < n; ++i) out[i] = h00 * y0[i] + h10 * h * f0[i] + h01 * y1[i] + h11 * h * f1[i];
+}
+
+// Fraction of the step where the interpolated r_BL crosses `target`
+// (Illinois regula falsi; returns 1 when the end points do not bracket it).
+__device__ double crossing_fraction(const double* y0, const double* f0, const double* y1, const double* f1, double h,
+                                    double a, double target) {
+    const double a2 = a * a;
+    double lo = 0.0, hi = 1.0;
+    double flo = sqrt(bl_r2<double>(y0[0], y0[1], y0[2], a2)) - target;
+    double fhi = sqrt(bl_r2<double>(y1[0], y1[1], y1[2], a2)) - target;
+    if (!((flo > 0.0) != (fhi > 0.0))) return 1.0;
+    int side = 0;
+    double t = 1.0, x[3];
+    for (int it = 0; it < 60; ++it) {
+        t = (lo * fhi - hi * flo) / (fhi - flo);
+        if (!(t > lo && t < hi)) t = 0.5 * (lo + hi);
+        hermite(y0, f0, y1, f1, h, t, 3, x);
+        const double ft = sqrt(bl_r2<double>(x[0], x[1], x[2], a2)) - target;
+        if (ft == 0.0 || fabs(hi - lo) < 1e-15 || fabs(ft) < 1e-13 * target) break;
+        if ((ft > 0.0) == (fhi > 0.0)) {
+            hi = t;
+            fhi = ft;
+            if (side == -1) flo *= 0.5;
+            side = -1;
+        } else {
+            lo = t;
+            flo = ft;
+            if (side == 1) fhi *= 0.5;
+            side = 1;
+        }
+    }
+    return t;
+}
+
 // Stages 2..6 and the 5th-order solution of a step hh from (y, k1)
 // (rk45_adaptive.hpp:210-251).
 __device__ __forceinline__ void dp5_stages(const double* y, const double* k1, double hh, double M, double a,
@@ -454,6 +495,41 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
         // accept, second half (also the REDO of a crossing off the disk)
         L.mode = MODE_STEP;
         {
+            // capture / escape / certain capture inside this step: the terminal point is
+            // interpolated to the threshold radius, independent of where the step ended
+            double target = 0.0;
+            uint32_t term = 0, tflag = 0;
+            if (r5 < B.r_capture) {
+                term = RT_RAY_CAPTURED;
+                target = B.r_capture;
+            } else if (r5 > B.r_esc) {
+                term = RT_RAY_ESCAPED;
+                target = B.r_esc;
+            } else if (L.can_early && r5 < B.r_early) {
+                // dr_BL/dlambda (kerr_invariants.hpp:140); the trace runs towards
+                // decreasing lambda, so dr/dlambda > 0 means inwards
+                const double r2 = r5 * r5, z = y5[2];
+                const double drdl = (r2 * r5 * (y5[0] * k[0][0] + y5[1] * k[0][1]) + r5 * (r2 + a * a) * z * k[0][2]) /
+                                    (r2 * r2 + a * a * z * z);
+                if (drdl > 0.0) {
+                    term = RT_RAY_CAPTURED;
+                    tflag = RT_RAYFLAG_EARLY_CAPTURE;
+                    target = B.r_early;
+                }
+            }
+            if (term) {
+                const double t = crossing_fraction(L.y, L.k1, y5, k[0], hh, a, target);
+                double yt[6];
+                hermite(L.y, L.k1, y5, k[0], hh, t, 6, yt);
+#pragma unroll
+                for (int i = 0; i < 6; ++i) L.y[i] = yt[i];
+                L.lambda += t * hh;
+                L.flags |= tflag;
+                finish_ray(B, L, term, NAN, 1.0, args.out);
+                continue;
+            }
+        }
+        {
             // projection onto H = 0 (closest root, rk45_adaptive.hpp:126-134); n = dx/dl = k7[0..2],
             // k.n and |n|^2 from |k| = 1
             double* p = y5 + 3;
@@ -493,16 +569,6 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
             L.k1[i] = k[0][i];
         }
         L.r = r5;
-        if (L.can_early && r5 < B.r_early) {
-            const double r2 = r5 * r5, z = y5[2];
-            const double drdl = (r2 * r5 * (y5[0] * L.k1[0] + y5[1] * L.k1[1]) + r5 * (r2 + a * a) * z * L.k1[2]) /
-                                (r2 * r2 + a * a * z * z);
-            if (drdl > 0.0) {
-                L.flags |= RT_RAYFLAG_EARLY_CAPTURE;
-                finish_ray(B, L, RT_RAY_CAPTURED, NAN, 1.0, args.out);
-                continue;
-            }
-        }
         double factor = 5.0;
         if (err != 0.0) {
             const double le = log(fmax(err, 1e-12));
