@@ -222,6 +222,9 @@ def ours(args) -> None:
     cam = headline_camera(relsim, precision, args.side)
     n = cam.screen_width * cam.screen_height
     tr = relsim.Tracer(local)
+    from autotune import apply_tuned
+
+    apply_tuned(tr, args.precision)
     fp64_peak, fp32_peak = tr.measure_fma_peak()
     ro, tensors = relsim.device_ray_out(n, RECORD_FIELDS, device=f"cuda:{local}")
     pix = torch.empty(n * 32, dtype=torch.uint8, device=f"cuda:{local}")

@@ -529,6 +529,13 @@ static double crossing_fraction(const double* y0, const double* f0, const double
     return t;
 }
 
+/* The tracer evaluates the PI30 factor (a step-size heuristic) in FP32 from
+ * base-2 logs; the error norm that decides acceptance stays FP64. */
+static inline float pi30f(float le, float lp, float order_p1)
+{
+    return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));
+}
+
 static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, uint32_t py, orc_ray* out)
 {
     const double m = c->m, a = c->a;
@@ -539,7 +546,7 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
     double r = ks_rhs(y, m, a, k[0]);
     double h = -cam->initial_step_fraction * c->r_obs;
     double lambda = 0.0;
-    double ln_prev = 0.0;
+    float ln_prev = 0.0f;
     int has_hist = 0;
     double phi_unwrapped;
     {
@@ -663,12 +670,10 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
             memcpy(y, yn, sizeof yn);
             memcpy(k[0], k[6], sizeof(double) * 6); /* FSAL */
             r = rn;
-            double factor;
-            if (err == 0.0) {
-                factor = 5.0;
-            } else {
-                const double le = log(max_d(err, 1e-12));
-                factor = pi30(le, has_hist ? ln_prev : le, 5.0);
+            float factor = 5.0f;
+            if (err != 0.0) {
+                const float le = log2f(fmaxf((float)err, 1e-12f));
+                factor = pi30f(le, has_hist ? ln_prev : le, 5.0f);
                 ln_prev = le;
                 has_hist = 1;
             }
@@ -678,8 +683,8 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
         } else {
             /* reject (rk45_adaptive.hpp:303-311) */
             ++rej;
-            const double le = log(max_d(err, 1e-12));
-            const double factor = pi30(le, has_hist ? ln_prev : le, 4.0);
+            const float le = log2f(fmaxf((float)err, 1e-12f));
+            const float factor = pi30f(le, has_hist ? ln_prev : le, 4.0f);
             ln_prev = le;
             has_hist = 1;
             h = -fabs(h) * clamp_d(0.9 * factor, 0.1, 0.9);

@@ -71,9 +71,18 @@ __device__ __forceinline__ T ks_rhs(const T* __restrict__ y, T M, T a, T* __rest
     const T inv_r = rt_rsqrt<T>(r2);
     const T r = r2 * inv_r;
     const T rpa = r2 + a2;
-    const T inv_rpa = rt_rcp<T>(rpa);
     const T r4 = r2 * r2;
-    const T inv_den = rt_rcp<T>(r4 + a2 * z2);
+    const T den = r4 + a2 * z2;
+    T inv_rpa, inv_den;
+    if constexpr (sizeof(T) == 8) {
+        // one reciprocal for both denominators (r^6 stays far from overflow in FP64)
+        const T q = rt_rcp<T>(rpa * den);
+        inv_rpa = den * q;
+        inv_den = rpa * q;
+    } else {
+        inv_rpa = rt_rcp<T>(rpa);
+        inv_den = rt_rcp<T>(den);
+    }
     const T r3 = r2 * r;
     const T H = M * r3 * inv_den;
     const T k0 = (r * x + a * yy) * inv_rpa;

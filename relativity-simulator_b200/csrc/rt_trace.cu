@@ -1,24 +1,29 @@
 // rt_trace.cu -- persistent backward null-geodesic tracer for sm_100a.
 //
-// One ray per lane, state in registers.  Warps claim rays from a global work
-// counter; when at least `refill_threshold` lanes of a warp are idle the warp
-// claims that many consecutive rays with one atomic (ballot + popc rank), so
-// lanes whose rays terminated early are refilled instead of idling while the
-// warp's longest ray finishes.
+// One ray per lane.  Warps claim rays from a global work counter; when at
+// least `refill_threshold` lanes of a warp are idle the warp claims that many
+// consecutive rays with one atomic (ballot + popc rank), so lanes whose rays
+// terminated are refilled instead of idling while the warp's longest ray runs.
 //
-// Per ray: Dormand-Prince 5(4) on the Kerr-Schild Hamiltonian state
-// (x, p) with p_t = -1 (kerr_schild_null_integrator.hpp:72-114), PI30 control
-// (step_controller.hpp:51-58, accept/reject scaling rk45_adaptive.hpp:294-310),
+// Per ray: Dormand-Prince 5(4) on the Kerr-Schild Hamiltonian state (x, p)
+// with p_t = -1 (kerr_schild_null_integrator.hpp:72-114), PI30 control
+// (step_controller.hpp:51-58; accept/reject scaling rk45_adaptive.hpp:294-310),
 // FSAL reuse of the last stage, a step cap |h| <= c max(r - r_+, 0.01 M),
 // projection onto H = 0 after each accepted step, and classification:
 // captured (r < capture_scale r_+, software_compute_engine.hpp:1667-1671),
 // escaped (r > escape radius, :1672-1675), disk (first z = 0 crossing on
-// [r_in, r_out], root by Illinois regula falsi on the step fraction), with the
-// Carter certain-capture early-out (carter_ray_classifier.hpp:146-150).
+// [r_in, r_out], root by Illinois regula falsi on the DP5 solution of a step
+// fraction), with the Carter certain-capture early-out
+// (carter_ray_classifier.hpp:146-150).  Terminal points are interpolated to
+// the threshold radius (cubic Hermite on the step's FSAL end points).
 //
-// The disk root solve reuses the main stage code: a lane in ROOT mode runs
-// its next DP5 evaluation at a fraction of the step instead of a full step, so
-// all lanes of a warp share one instruction stream.
+// Layout: the hot state (y, k1, r, h, counters) lives in registers; cold
+// per-lane state (affine parameter, invariants at the start, root bracket) in
+// shared memory as structure of arrays.  Ray set-up, termination and the
+// Carter test are out of line so the step loop stays small in the
+// instruction cache; states cross that boundary through small local arrays.
+// The disk root solve reuses the loop's stage code: a lane in ROOT mode runs
+// its next DP5 evaluation at a fraction of the step instead of a full step.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -37,26 +42,16 @@ constexpr double kEarlyCaptureMargin = 1e-4;  // M, distance to the critical cur
 
 enum LaneMode : int { MODE_IDLE = 0, MODE_STEP = 1, MODE_ROOT = 2, MODE_REDO = 3 };
 
-struct RayLane {
-    double y[6];
-    double k1[6];
-    double r;        // BL radius of y
-    double h;        // next step (negative)
-    double ln_prev;  // log of the previous error (PI30 history)
-    double lambda;
-    double dH;
-    double lz0, q0;
-    // root solve
-    double lo, hi, flo, fhi, troot;
-    uint64_t local;  // ray index inside its bundle
-    uint32_t bidx;
-    uint32_t acc, rej, flags;
-    int mode;
-    int side, rit;
-    int wind;
-    float raw_prev;
-    bool has_hist;
-    bool can_early;
+// Cold per-lane state, structure of arrays indexed by threadIdx.x.
+template <int BLOCK>
+struct Cold {
+    double lambda[BLOCK];
+    double dH[BLOCK];
+    double lz0[BLOCK];
+    double q0[BLOCK];
+    double lo[BLOCK], hi[BLOCK], flo[BLOCK], fhi[BLOCK], troot[BLOCK];
+    uint64_t local[BLOCK];
+    int side[BLOCK], rit[BLOCK];
 };
 
 __device__ __forceinline__ double clampd(double v, double lo, double hi) { return fmin(fmax(v, lo), hi); }
@@ -65,34 +60,33 @@ __device__ __forceinline__ double clampd(double v, double lo, double hi) { retur
 // parameter (units of M): the smallest local minimum R_min of the radial
 // quartic R(r) = r^4 + P r^2 + Qc r - a^2 eta (carter_ray_classifier.hpp:132-135)
 // outside r_+ is moved to zero by d_eta = R_min / Delta.  > 0: no turning point.
-__device__ double shadow_distance(double M, double a, double rh, double xi, double eta) {
+__device__ __noinline__ double shadow_distance(double M, double a, double rh, double xi, double eta) {
     const double a2 = a * a;
     const double P = a2 - xi * xi - eta;
     const double Qc = 2.0 * M * (eta + (xi - a) * (xi - a));
     const double R0 = -a2 * eta;
     const double pp = 0.5 * P, qq = 0.25 * Qc;
-    double roots[3];
-    int n = 0;
-    const double disc = -(4.0 * pp * pp * pp + 27.0 * qq * qq);
-    if (disc > 0.0 && pp < 0.0) {
-        const double m2 = 2.0 * sqrt(-pp / 3.0);
-        const double arg = clampd(3.0 * qq / (pp * m2), -1.0, 1.0);
-        const double th = acos(arg) / 3.0;
-        for (int k = 0; k < 3; ++k) roots[n++] = m2 * cos(th - 2.0 * kPi * k / 3.0);
-    } else {
-        const double sq = sqrt(fmax(qq * qq / 4.0 + pp * pp * pp / 27.0, 0.0));
-        roots[n++] = cbrt(-qq / 2.0 + sq) + cbrt(-qq / 2.0 - sq);
-    }
     double best = INFINITY, best_r = 0.0;
-    for (int i = 0; i < n; ++i) {
-        const double r = roots[i];
-        if (!(r > rh)) continue;
-        if (12.0 * r * r + 2.0 * P <= 0.0) continue;
+    auto consider = [&](double r) {
+        if (!(r > rh)) return;
+        if (12.0 * r * r + 2.0 * P <= 0.0) return;
         const double R = ((r * r + P) * r + Qc) * r + R0;
         if (R < best) {
             best = R;
             best_r = r;
         }
+    };
+    const double disc = -(4.0 * pp * pp * pp + 27.0 * qq * qq);
+    if (disc > 0.0 && pp < 0.0) {
+        const double m2 = 2.0 * sqrt(-pp / 3.0);
+        const double arg = clampd(3.0 * qq / (pp * m2), -1.0, 1.0);
+        const double th = acos(arg) / 3.0;
+        consider(m2 * cos(th));
+        consider(m2 * cos(th - 2.0 * kPi / 3.0));
+        consider(m2 * cos(th - 4.0 * kPi / 3.0));
+    } else {
+        const double sq = sqrt(fmax(qq * qq / 4.0 + pp * pp * pp / 27.0, 0.0));
+        consider(cbrt(-qq / 2.0 + sq) + cbrt(-qq / 2.0 - sq));
     }
     if (!isfinite(best)) return INFINITY;
     const double delta = best_r * best_r - 2.0 * M * best_r + a2;
@@ -113,15 +107,29 @@ __device__ double carter_q(const double* y, double a) {
     return p_theta * p_theta + cos_t * cos_t * (-a * a + lz * lz / sin2);
 }
 
-__device__ __forceinline__ float raw_phi32(const double* y, double a, double r) {
-    return atan2f(static_cast<float>(y[1]), static_cast<float>(y[0])) -
-           atan2f(static_cast<float>(a), static_cast<float>(r));
+// Winding of atan2(y, x) across its branch cut between two points: the
+// azimuth unwrapping of kerr_schild_null_integrator.hpp:61-63 counts a turn
+// exactly when the segment crosses the negative x axis.
+__device__ __forceinline__ int branch_winding(double x0, double y0, double x1, double y1) {
+    if ((y0 < 0.0) == (y1 < 0.0)) return 0;
+    const double xc = x0 + (x1 - x0) * (y0 / (y0 - y1));
+    if (!(xc < 0.0)) return 0;
+    return (y0 < 0.0) ? -1 : 1;
 }
+
+struct InitResult {
+    double r;
+    int can_early;
+};
 
 // Ray generation (software_compute_engine.hpp:3843-3862, :3932-3938, :1637-1650,
 // camera_projections.hpp:27-40) and the initial null covector
-// (kerr_schild_null_integrator.hpp:179-193) from the bundle's precomputed tetrad.
-__device__ void init_ray(const BundleDesc& B, uint64_t local, RayLane& L) {
+// (kerr_schild_null_integrator.hpp:179-193) from the bundle's precomputed
+// tetrad.  Writes y0 and k1 to xch[0..11] (a local array of the caller).
+template <int BLOCK>
+__device__ __noinline__ InitResult init_ray(const BundleDesc* __restrict__ Bp, uint64_t local, Cold<BLOCK>& S,
+                                            int tid, double* __restrict__ xch) {
+    const BundleDesc& B = *Bp;
     const uint32_t row = static_cast<uint32_t>(local / B.ncols);
     const uint32_t col = static_cast<uint32_t>(local - static_cast<uint64_t>(row) * B.ncols);
     const double px = static_cast<double>(B.col0 + col);
@@ -149,26 +157,30 @@ __device__ void init_ray(const BundleDesc& B, uint64_t local, RayLane& L) {
     const double lv = v4[0] + B.kf[0] * v4[1] + B.kf[1] * v4[2] + B.kf[2] * v4[3];
     const double p_t = -v4[0] + B.two_h * lv;
     const double inv_e = 1.0 / fmax(-p_t, 1e-12);
-    L.y[0] = B.x0[0];
-    L.y[1] = B.x0[1];
-    L.y[2] = B.x0[2];
-    L.y[3] = (v4[1] + B.two_h * lv * B.kf[0]) * inv_e;
-    L.y[4] = (v4[2] + B.two_h * lv * B.kf[1]) * inv_e;
-    L.y[5] = (v4[3] + B.two_h * lv * B.kf[2]) * inv_e;
-    L.lz0 = L.y[0] * L.y[4] - L.y[1] * L.y[3];
-    L.q0 = carter_q(L.y, B.a);
-    L.can_early = (B.flags & BF_EARLY_CAPTURE) && shadow_distance(B.m, B.a, B.rh, L.lz0, L.q0) > kEarlyCaptureMargin;
+    double y[6], k1[6];
+    y[0] = B.x0[0];
+    y[1] = B.x0[1];
+    y[2] = B.x0[2];
+    y[3] = (v4[1] + B.two_h * lv * B.kf[0]) * inv_e;
+    y[4] = (v4[2] + B.two_h * lv * B.kf[1]) * inv_e;
+    y[5] = (v4[3] + B.two_h * lv * B.kf[2]) * inv_e;
+    const double lz0 = y[0] * y[4] - y[1] * y[3];
+    const double q0 = carter_q(y, B.a);
     double hf, s;
-    L.r = ks_rhs<double>(L.y, B.m, B.a, L.k1, hf, s);
-    L.h = -B.h0;
-    L.ln_prev = 0.0;
-    L.has_hist = false;
-    L.lambda = 0.0;
-    L.dH = 0.0;
-    L.acc = L.rej = L.flags = 0;
-    L.wind = B.wind0;
-    L.raw_prev = static_cast<float>(B.raw_phi0);
-    L.local = local;
+    InitResult res;
+    res.r = ks_rhs<double>(y, B.m, B.a, k1, hf, s);
+    res.can_early = (B.flags & BF_EARLY_CAPTURE) && shadow_distance(B.m, B.a, B.rh, lz0, q0) > kEarlyCaptureMargin;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        xch[i] = y[i];
+        xch[6 + i] = k1[i];
+    }
+    S.lz0[tid] = lz0;
+    S.q0[tid] = q0;
+    S.lambda[tid] = 0.0;
+    S.dH[tid] = 0.0;
+    S.local[tid] = local;
+    return res;
 }
 
 // Disk redshift of a circular orbit (accretion_disk_model.hpp:205-225).
@@ -185,67 +197,6 @@ __device__ double disk_redshift(double M, double a, double r, double lz) {
     return (fabs(den) > 1e-9) ? clampd(1.0 / den, 0.05, 4.0) : 1.0;
 }
 
-// Write the ray's record and pixel, then free the lane.
-__device__ void finish_ray(const BundleDesc& B, RayLane& L, uint32_t status, double r_hit, double g,
-                           const OutPtrs& out) {
-    const double a = B.a;
-    const double* y = L.y;
-    const double r = sqrt(bl_r2<double>(y[0], y[1], y[2], a * a));
-    const double rho = sqrt(fmax(r * r - y[2] * y[2], 0.0));
-    const double theta = atan2(rho, y[2]);
-    const double raw = atan2(y[1], y[0]) - atan2(a, r);
-    // last winding update against the tracked azimuth (kerr_schild_null_integrator.hpp:61-63)
-    const float raw32 = static_cast<float>(raw);
-    const float dr = raw32 - L.raw_prev;
-    int wind = L.wind;
-    if (dr > static_cast<float>(kPi)) wind -= 1;
-    if (dr < -static_cast<float>(kPi)) wind += 1;
-    const double phi = raw + kTwoPi * static_cast<double>(wind);
-    // invariants at the end
-    double kf[3], hf;
-    ks_field64(y, B.m, a, kf, hf);
-    const double kp = kf[0] * y[3] + kf[1] * y[4] + kf[2] * y[5];
-    const double pp = y[3] * y[3] + y[4] * y[4] + y[5] * y[5];
-    const double qa = 1.0 + 2.0 * hf, qb = 2.0 * hf * kp, qc = pp - 2.0 * hf * kp * kp;
-    const double energy = (-qb + sqrt(fmax(qb * qb + qa * qc, 0.0))) / qa;
-    const double lz = y[0] * y[4] - y[1] * y[3];
-    const double q = carter_q(y, a);
-
-    const uint64_t o = B.out_offset + L.local;
-    const rt_ray_out& R = out.rays;
-    if (R.status) R.status[o] = status;
-    if (R.flags) R.flags[o] = L.flags;
-    if (R.steps_accepted) R.steps_accepted[o] = L.acc;
-    if (R.steps_rejected) R.steps_rejected[o] = L.rej;
-    if (R.r) R.r[o] = r;
-    if (R.theta) R.theta[o] = theta;
-    if (R.phi) R.phi[o] = phi;
-    if (R.r_hit) R.r_hit[o] = r_hit;
-    if (R.g) R.g[o] = g;
-    if (R.lambda) R.lambda[o] = L.lambda;
-    if (R.dH) R.dH[o] = L.dH;
-    if (R.dE) R.dE[o] = energy - 1.0;
-    if (R.dLz) R.dLz[o] = lz - L.lz0;
-    if (R.dQ) R.dQ[o] = q - L.q0;
-    if (out.pixels) {
-        rt_pixel_out px;
-        px.r = px.g = px.b = 0.0f;
-        px.a = 1.0f;
-        px.redshift = static_cast<float>(g);
-        px.affine_parameter = static_cast<float>(-L.lambda);
-        px.status_flags = (status == RT_RAY_CAPTURED)  ? RT_PIXEL_HORIZON_ABSORBED
-                          : (status == RT_RAY_ESCAPED) ? RT_PIXEL_CELESTIAL_HIT
-                          : (status == RT_RAY_DISK)    ? RT_PIXEL_ACCRETION_DISK_HIT
-                                                       : 0u;
-        px.iterations_used = L.acc;
-        reinterpret_cast<float4*>(out.pixels + o)[0] = make_float4(px.r, px.g, px.b, px.a);
-        reinterpret_cast<uint4*>(out.pixels + o)[1] =
-            make_uint4(__float_as_uint(px.redshift), __float_as_uint(px.affine_parameter), px.status_flags,
-                       px.iterations_used);
-    }
-    L.mode = MODE_IDLE;
-}
-
 // Cubic Hermite interpolant of a step from its end points and FSAL slopes.
 __device__ __forceinline__ void hermite(const double* y0, const double* f0, const double* y1, const double* f1,
                                         double h, double t, int n, double* out) {
@@ -256,7 +207,7 @@ __device__ __forceinline__ void hermite(const double* y0, const double* f0, cons
 }
 
 // Fraction of the step where the interpolated r_BL crosses `target`
-// (Illinois regula falsi; returns 1 when the end points do not bracket it).
+// (Illinois regula falsi; 1 when the end points do not bracket it).
 __device__ double crossing_fraction(const double* y0, const double* f0, const double* y1, const double* f1, double h,
                                     double a, double target) {
     const double a2 = a * a;
@@ -285,6 +236,82 @@ __device__ double crossing_fraction(const double* y0, const double* f0, const do
         }
     }
     return t;
+}
+
+// Terminal point, the ray's record and its pixel.  xch (a local array of the
+// caller) holds the last accepted point in [0..5]; with interp_target > 0 it
+// holds the step's y, k1, y5, k7 in [0..23] and the point is interpolated to
+// r_BL = interp_target; for a disk hit the root state is in [12..17].
+template <int BLOCK>
+__device__ __noinline__ void finish_ray(const BundleDesc* __restrict__ Bp, Cold<BLOCK>& S, int tid, uint32_t status,
+                                        uint32_t flags, uint32_t acc, uint32_t rej, int wind, double interp_target,
+                                        double hh, double r_hit, double g, const OutPtrs& out,
+                                        const double* __restrict__ xch) {
+    const BundleDesc& B = *Bp;
+    const double a = B.a;
+    double y[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) y[i] = xch[i];
+    const double y_prev_x = y[0], y_prev_y = y[1];
+    double lambda = S.lambda[tid];
+    if (interp_target > 0.0) {
+        double y0[6], f0[6], y1[6], f1[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            y0[i] = xch[i];
+            f0[i] = xch[6 + i];
+            y1[i] = xch[12 + i];
+            f1[i] = xch[18 + i];
+        }
+        const double t = crossing_fraction(y0, f0, y1, f1, hh, a, interp_target);
+        hermite(y0, f0, y1, f1, hh, t, 6, y);
+        lambda += t * hh;
+    } else if (status == RT_RAY_DISK) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) y[i] = xch[12 + i];
+    }
+    const double r = sqrt(bl_r2<double>(y[0], y[1], y[2], a * a));
+    const double rho = sqrt(fmax(r * r - y[2] * y[2], 0.0));
+    const double theta = atan2(rho, y[2]);
+    wind += branch_winding(y_prev_x, y_prev_y, y[0], y[1]);
+    const double phi = atan2(y[1], y[0]) - atan2(a, r) + kTwoPi * static_cast<double>(wind);
+    // invariants at the end
+    double kf[3], hf;
+    ks_field64(y, B.m, a, kf, hf);
+    const double kp = kf[0] * y[3] + kf[1] * y[4] + kf[2] * y[5];
+    const double pp = y[3] * y[3] + y[4] * y[4] + y[5] * y[5];
+    const double qa = 1.0 + 2.0 * hf, qb = 2.0 * hf * kp, qc = pp - 2.0 * hf * kp * kp;
+    const double energy = (-qb + sqrt(fmax(qb * qb + qa * qc, 0.0))) / qa;
+    const double lz = y[0] * y[4] - y[1] * y[3];
+    const double q = carter_q(y, a);
+
+    const uint64_t o = B.out_offset + S.local[tid];
+    const rt_ray_out& R = out.rays;
+    if (R.status) R.status[o] = status;
+    if (R.flags) R.flags[o] = flags;
+    if (R.steps_accepted) R.steps_accepted[o] = acc;
+    if (R.steps_rejected) R.steps_rejected[o] = rej;
+    if (R.r) R.r[o] = r;
+    if (R.theta) R.theta[o] = theta;
+    if (R.phi) R.phi[o] = phi;
+    if (R.r_hit) R.r_hit[o] = r_hit;
+    if (R.g) R.g[o] = g;
+    if (R.lambda) R.lambda[o] = lambda;
+    if (R.dH) R.dH[o] = S.dH[tid];
+    if (R.dE) R.dE[o] = energy - 1.0;
+    if (R.dLz) R.dLz[o] = lz - S.lz0[tid];
+    if (R.dQ) R.dQ[o] = q - S.q0[tid];
+    if (out.pixels) {
+        // GpuPixelOutput (gpu_types.hpp:1111-1130); shading is not part of this path
+        const uint32_t pflags = (status == RT_RAY_CAPTURED)  ? RT_PIXEL_HORIZON_ABSORBED
+                                : (status == RT_RAY_ESCAPED) ? RT_PIXEL_CELESTIAL_HIT
+                                : (status == RT_RAY_DISK)    ? RT_PIXEL_ACCRETION_DISK_HIT
+                                                             : 0u;
+        float4* p4 = reinterpret_cast<float4*>(out.pixels + o);
+        p4[0] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        reinterpret_cast<uint4*>(p4)[1] = make_uint4(__float_as_uint(static_cast<float>(g)),
+                                                     __float_as_uint(static_cast<float>(-lambda)), pflags, acc);
+    }
 }
 
 // Stages 2..6 and the 5th-order solution of a step hh from (y, k1)
@@ -316,23 +343,37 @@ __device__ __forceinline__ void dp5_stages(const double* y, const double* k1, do
                              DP::B6 * k[5][i]);
 }
 
+// PI30 factor (step_controller.hpp:51-58) from base-2 logs of the errors.
+__device__ __forceinline__ float pi30_factor(float le, float lp, float order_p1) {
+    return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));
+}
+
 }  // namespace
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
+    __shared__ Cold<BLOCK> S;
     const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
 
-    RayLane L;
-    L.mode = MODE_IDLE;
-    L.bidx = 0;
+    // hot lane state
+    double y[6], k1[6];
+    double r = 0.0, h = 0.0;
+    float lnp = 0.0f;  // log2 of the previous error (PI30 history)
+    uint32_t acc = 0, rej = 0, flags = 0, bidx = 0;
+    int mode = MODE_IDLE, wind = 0;
+    bool has_hist = false, can_early = false;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) y[i] = k1[i] = 0.0;
+
     bool queue_open = true;
     unsigned long long n_att = 0, n_acc = 0, n_rays = 0, n_rhs = 0;
 
     for (;;) {
         // ---- refill idle lanes from the global queue ----
-        const unsigned idle = __ballot_sync(FULL, L.mode == MODE_IDLE);
+        const unsigned idle = __ballot_sync(FULL, mode == MODE_IDLE);
         const int n_idle = __popc(idle);
         if (queue_open && n_idle > 0 && (n_idle >= static_cast<int>(args.refill_threshold) || n_idle == 32)) {
             const int leader = __ffs(idle) - 1;
@@ -340,7 +381,7 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
             if (lane == leader) base = atomicAdd(args.queue, static_cast<unsigned long long>(n_idle));
             base = __shfl_sync(FULL, base, leader);
             if (base + static_cast<unsigned long long>(n_idle) >= args.total_rays) queue_open = false;
-            if (L.mode == MODE_IDLE) {
+            if (mode == MODE_IDLE) {
                 const uint64_t rid = base + static_cast<uint64_t>(__popc(idle & lt_mask));
                 if (rid < args.total_rays) {
                     // bundle of this ray: last bundle whose ray_begin <= rid
@@ -349,99 +390,129 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
                         const uint32_t mid = (lo + hi) >> 1;
                         if (args.bundles[mid].ray_begin <= rid) lo = mid; else hi = mid;
                     }
-                    L.bidx = lo;
-                    init_ray(args.bundles[lo], rid - args.bundles[lo].ray_begin, L);
-                    L.mode = MODE_STEP;
+                    bidx = lo;
+                    double xch[12];
+                    const InitResult ir =
+                        init_ray<BLOCK>(args.bundles + lo, rid - args.bundles[lo].ray_begin, S, tid, xch);
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) {
+                        y[i] = xch[i];
+                        k1[i] = xch[6 + i];
+                    }
+                    r = ir.r;
+                    can_early = ir.can_early != 0;
+                    h = -args.bundles[lo].h0;
+                    lnp = 0.0f;
+                    has_hist = false;
+                    acc = rej = flags = 0;
+                    wind = args.bundles[lo].wind0;
+                    mode = MODE_STEP;
                     ++n_rays;
                     ++n_rhs;
                 }
             }
         }
-        if (__ballot_sync(FULL, L.mode != MODE_IDLE) == 0) {
+        if (__ballot_sync(FULL, mode != MODE_IDLE) == 0) {
             if (!queue_open) break;
             continue;
         }
-        if (L.mode == MODE_IDLE) continue;
+        if (mode == MODE_IDLE) continue;
 
-        const BundleDesc& B = args.bundles[L.bidx];
-        const double M = B.m, a = B.a;
-        double hh = L.h;
-        bool attempt = true;
-        if (L.mode == MODE_STEP) {
-            // termination tests at the current point (software_compute_engine.hpp:1667-1675)
-            if (L.r < B.r_capture) {
-                finish_ray(B, L, RT_RAY_CAPTURED, NAN, 1.0, args.out);
-                attempt = false;
-            } else if (L.r > B.r_esc) {
-                finish_ray(B, L, RT_RAY_ESCAPED, NAN, 1.0, args.out);
-                attempt = false;
-            } else if (L.acc + L.rej >= B.max_steps) {
-                L.flags |= RT_RAYFLAG_MAX_STEPS;
-                finish_ray(B, L, RT_RAY_UNFINISHED, NAN, 1.0, args.out);
-                attempt = false;
-            } else {
-                const double cap = B.cap_c * fmax(L.r - B.rh, 0.01 * M);
-                if (fabs(L.h) > cap) L.h = -cap;
-                hh = L.h;
+        const BundleDesc* Bp = args.bundles + bidx;
+        const double M = Bp->m, a = Bp->a;
+        double hh = h;
+        if (mode == MODE_STEP) {
+            // the initial point may already be outside the integration domain
+            uint32_t term = 0;
+            if (r < Bp->r_capture) term = RT_RAY_CAPTURED;
+            else if (r > Bp->r_esc) term = RT_RAY_ESCAPED;
+            else if (acc + rej >= Bp->max_steps) {
+                flags |= RT_RAYFLAG_MAX_STEPS;
+                term = RT_RAY_UNFINISHED + 16;
+            }
+            if (term == 0) {
+                const double cap = Bp->cap_c * fmax(r - Bp->rh, 0.01 * M);
+                if (fabs(h) > cap) h = -cap;
+                hh = h;
                 if (fabs(hh) < 1e-8) {
-                    L.flags |= RT_RAYFLAG_STEP_UNDERFLOW;
-                    finish_ray(B, L, RT_RAY_CAPTURED, NAN, 1.0, args.out);
-                    attempt = false;
+                    flags |= RT_RAYFLAG_STEP_UNDERFLOW;
+                    term = RT_RAY_CAPTURED;
                 }
             }
-        } else if (L.mode == MODE_ROOT) {
-            double t = (L.lo * L.fhi - L.hi * L.flo) / (L.fhi - L.flo);
-            if (!(t > L.lo && t < L.hi)) t = 0.5 * (L.lo + L.hi);
-            L.troot = t;
-            hh = t * L.h;
+            if (term) {
+                double xch[6];
+#pragma unroll
+                for (int i = 0; i < 6; ++i) xch[i] = y[i];
+                finish_ray<BLOCK>(Bp, S, tid, term & 15u, flags, acc, rej, wind, 0.0, 0.0, NAN, 1.0, args.out, xch);
+                mode = MODE_IDLE;
+                continue;
+            }
+        } else if (mode == MODE_ROOT) {
+            const double lo = S.lo[tid], hi = S.hi[tid], flo = S.flo[tid], fhi = S.fhi[tid];
+            double t = (lo * fhi - hi * flo) / (fhi - flo);
+            if (!(t > lo && t < hi)) t = 0.5 * (lo + hi);
+            S.troot[tid] = t;
+            hh = t * h;
         }
-        if (!attempt) continue;
 
         double k[6][6];
         double y5[6];
-        dp5_stages(L.y, L.k1, hh, M, a, k, y5);
+        dp5_stages(y, k1, hh, M, a, k, y5);
         n_rhs += 5;
 
-        if (L.mode == MODE_ROOT) {
+        if (mode == MODE_ROOT) {
             const double ft = y5[2];
-            ++L.rit;
-            const bool done = (ft == 0.0) || (fabs(L.hi - L.lo) < 1e-15) ||
-                              (fabs(ft) < 1e-13 * (1.0 + fabs(y5[0]) + fabs(y5[1]))) || (L.rit >= 60);
+            const int rit = ++S.rit[tid];
+            const double lo = S.lo[tid], hi = S.hi[tid];
+            const bool done = (ft == 0.0) || (fabs(hi - lo) < 1e-15) ||
+                              (fabs(ft) < 1e-13 * (1.0 + fabs(y5[0]) + fabs(y5[1]))) || (rit >= 60);
             if (done) {
                 const double rr = sqrt(bl_r2<double>(y5[0], y5[1], y5[2], a * a));
-                if (rr >= B.r_in && rr <= B.r_out && rr > B.rh * 1.02) {
-                    L.lambda += L.troot * L.h;
-                    for (int i = 0; i < 6; ++i) L.y[i] = y5[i];
-                    finish_ray(B, L, RT_RAY_DISK, rr, disk_redshift(M, a, rr, L.lz0), args.out);
+                if (rr >= Bp->r_in && rr <= Bp->r_out && rr > Bp->rh * 1.02) {
+                    S.lambda[tid] += S.troot[tid] * h;
+                    double xch[18];
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) {
+                        xch[i] = y[i];
+                        xch[12 + i] = y5[i];
+                    }
+                    finish_ray<BLOCK>(Bp, S, tid, RT_RAY_DISK, flags, acc, rej, wind, 0.0, 0.0, rr,
+                                      disk_redshift(M, a, rr, S.lz0[tid]), args.out, xch);
+                    mode = MODE_IDLE;
                 } else {
-                    L.mode = MODE_REDO;  // not on the disk: take the full step again
+                    mode = MODE_REDO;  // not on the disk: take the full step again
                 }
-            } else if ((ft > 0.0) == (L.fhi > 0.0)) {
-                L.hi = L.troot;
-                L.fhi = ft;
-                if (L.side == -1) L.flo *= 0.5;
-                L.side = -1;
             } else {
-                L.lo = L.troot;
-                L.flo = ft;
-                if (L.side == 1) L.fhi *= 0.5;
-                L.side = 1;
+                const double t = S.troot[tid];
+                const int side = S.side[tid];
+                if ((ft > 0.0) == (S.fhi[tid] > 0.0)) {
+                    S.hi[tid] = t;
+                    S.fhi[tid] = ft;
+                    if (side == -1) S.flo[tid] *= 0.5;
+                    S.side[tid] = -1;
+                } else {
+                    S.lo[tid] = t;
+                    S.flo[tid] = ft;
+                    if (side == 1) S.fhi[tid] *= 0.5;
+                    S.side[tid] = 1;
+                }
             }
             continue;
         }
 
-        // full step: last stage (FSAL) and the error norm (rk45_adaptive.hpp:252-261)
+        // full step: last stage (FSAL) and the FP64 error norm (rk45_adaptive.hpp:252-261)
         double hf5, s5;
         const double r5 = ks_rhs<double>(y5, M, a, k[0], hf5, s5);  // k[0] now holds k7
         n_rhs += 1;
         double err;
         {
             double num = 0.0, den = 1.0;
+            const double rtol = Bp->rtol, atol = Bp->atol;
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
-                const double est = fabs(hh) * fabs(DP::E1 * L.k1[i] + DP::E3 * k[2][i] + DP::E4 * k[3][i] +
+                const double est = fabs(hh) * fabs(DP::E1 * k1[i] + DP::E3 * k[2][i] + DP::E4 * k[3][i] +
                                                    DP::E5 * k[4][i] + DP::E6 * k[5][i] + DP::E7 * k[0][i]);
-                const double sc = B.rtol * fmax(fabs(L.y[i]), fabs(y5[i])) + B.atol;
+                const double sc = rtol * fmax(fabs(y[i]), fabs(y5[i])) + atol;
                 if (est * den > num * sc) {
                     num = est;
                     den = sc;
@@ -451,81 +522,88 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
         }
         if (!(err <= 1e300)) err = 1e300;  // non-finite trial: reject with the largest cut
 
-        if (L.mode == MODE_STEP) {
+        if (mode == MODE_STEP) {
             ++n_att;
             if (err > 1.0) {
                 // reject (rk45_adaptive.hpp:303-311)
-                ++L.rej;
-                const double le = log(fmax(err, 1e-12));
-                const double lp = L.has_hist ? L.ln_prev : le;
-                const double factor = exp(-(0.7 / 4.0) * le + (0.3 / 4.0) * (lp - le));
-                L.ln_prev = le;
-                L.has_hist = true;
-                L.h = -fabs(L.h) * clampd(0.9 * factor, 0.1, 0.9);
+                ++rej;
+                const float le = __log2f(fmaxf(static_cast<float>(err), 1e-12f));
+                const float factor = pi30_factor(le, has_hist ? lnp : le, 4.0f);
+                lnp = le;
+                has_hist = true;
+                h = -fabs(h) * clampd(0.9 * static_cast<double>(factor), 0.1, 0.9);
                 continue;
             }
-            ++L.acc;
+            ++acc;
             ++n_acc;
             bool finite = true;
 #pragma unroll
             for (int i = 0; i < 6; ++i) finite = finite && isfinite(y5[i]);
             if (!finite) {
-                L.flags |= RT_RAYFLAG_NONFINITE;
-                finish_ray(B, L, RT_RAY_CAPTURED, NAN, 1.0, args.out);
+                flags |= RT_RAYFLAG_NONFINITE;
+                double xch[6];
+#pragma unroll
+                for (int i = 0; i < 6; ++i) xch[i] = y[i];
+                finish_ray<BLOCK>(Bp, S, tid, RT_RAY_CAPTURED, flags, acc, rej, wind, 0.0, 0.0, NAN, 1.0, args.out,
+                                  xch);
+                mode = MODE_IDLE;
                 continue;
             }
-            if ((B.flags & BF_DISK) && L.y[2] * y5[2] <= 0.0 && L.y[2] != y5[2]) {
-                const double sl = L.y[2] / (L.y[2] - y5[2]);
-                const double xe = L.y[0] + sl * (y5[0] - L.y[0]);
-                const double ye = L.y[1] + sl * (y5[1] - L.y[1]);
+            if ((Bp->flags & BF_DISK) && y[2] * y5[2] <= 0.0 && y[2] != y5[2]) {
+                const double sl = y[2] / (y[2] - y5[2]);
+                const double xe = y[0] + sl * (y5[0] - y[0]);
+                const double ye = y[1] + sl * (y5[1] - y[1]);
                 const double re = sqrt(fmax(xe * xe + ye * ye - a * a, 0.0));
                 const double margin = 0.05 * re + 0.5 * M;
-                if (re >= B.r_in - margin && re <= B.r_out + margin) {
-                    L.mode = MODE_ROOT;
-                    L.lo = 0.0;
-                    L.flo = L.y[2];
-                    L.hi = 1.0;
-                    L.fhi = y5[2];
-                    L.side = 0;
-                    L.rit = 0;
+                if (re >= Bp->r_in - margin && re <= Bp->r_out + margin) {
+                    mode = MODE_ROOT;
+                    S.lo[tid] = 0.0;
+                    S.flo[tid] = y[2];
+                    S.hi[tid] = 1.0;
+                    S.fhi[tid] = y5[2];
+                    S.side[tid] = 0;
+                    S.rit[tid] = 0;
                     continue;
                 }
             }
         }
         // accept, second half (also the REDO of a crossing off the disk)
-        L.mode = MODE_STEP;
+        mode = MODE_STEP;
         {
             // capture / escape / certain capture inside this step: the terminal point is
             // interpolated to the threshold radius, independent of where the step ended
             double target = 0.0;
-            uint32_t term = 0, tflag = 0;
-            if (r5 < B.r_capture) {
+            uint32_t term = 0;
+            if (r5 < Bp->r_capture) {
                 term = RT_RAY_CAPTURED;
-                target = B.r_capture;
-            } else if (r5 > B.r_esc) {
+                target = Bp->r_capture;
+            } else if (r5 > Bp->r_esc) {
                 term = RT_RAY_ESCAPED;
-                target = B.r_esc;
-            } else if (L.can_early && r5 < B.r_early) {
+                target = Bp->r_esc;
+            } else if (can_early && r5 < Bp->r_early) {
                 // dr_BL/dlambda (kerr_invariants.hpp:140); the trace runs towards
                 // decreasing lambda, so dr/dlambda > 0 means inwards
-                const double r2 = r5 * r5, z = y5[2];
-                const double drdl = (r2 * r5 * (y5[0] * k[0][0] + y5[1] * k[0][1]) + r5 * (r2 + a * a) * z * k[0][2]) /
-                                    (r2 * r2 + a * a * z * z);
+                const double rr2 = r5 * r5, z = y5[2];
+                const double drdl =
+                    (rr2 * r5 * (y5[0] * k[0][0] + y5[1] * k[0][1]) + r5 * (rr2 + a * a) * z * k[0][2]) /
+                    (rr2 * rr2 + a * a * z * z);
                 if (drdl > 0.0) {
                     term = RT_RAY_CAPTURED;
-                    tflag = RT_RAYFLAG_EARLY_CAPTURE;
-                    target = B.r_early;
+                    flags |= RT_RAYFLAG_EARLY_CAPTURE;
+                    target = Bp->r_early;
                 }
             }
             if (term) {
-                const double t = crossing_fraction(L.y, L.k1, y5, k[0], hh, a, target);
-                double yt[6];
-                hermite(L.y, L.k1, y5, k[0], hh, t, 6, yt);
+                double xch[24];
 #pragma unroll
-                for (int i = 0; i < 6; ++i) L.y[i] = yt[i];
-                L.lambda += t * hh;
-                L.flags |= tflag;
-                finish_ray(B, L, term, NAN, 1.0, args.out);
+                for (int i = 0; i < 6; ++i) {
+                    xch[i] = y[i];
+                    xch[6 + i] = k1[i];
+                    xch[12 + i] = y5[i];
+                    xch[18 + i] = k[0][i];
+                }
+                finish_ray<BLOCK>(Bp, S, tid, term, flags, acc, rej, wind, target, hh, NAN, 1.0, args.out, xch);
+                mode = MODE_IDLE;
                 continue;
             }
         }
@@ -535,8 +613,8 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
             double* p = y5 + 3;
             const double pp = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
             const double res = 0.5 * (pp - 1.0 - 2.0 * hf5 * s5 * s5);
-            L.dH = fmax(L.dH, fabs(res));
-            if (fabs(res) >= B.proj_tol) {
+            S.dH[tid] = fmax(S.dH[tid], fabs(res));
+            if (fabs(res) >= Bp->proj_tol) {
                 const double hs = hf5 * s5;
                 const double kn = (s5 - 1.0) - 2.0 * hs;
                 const double pn = pp - 2.0 * hs * (s5 - 1.0);
@@ -555,30 +633,23 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
                 }
             }
         }
-        {
-            const float raw = raw_phi32(y5, a, r5);
-            const float d = raw - L.raw_prev;
-            if (d > static_cast<float>(kPi)) L.wind -= 1;
-            if (d < -static_cast<float>(kPi)) L.wind += 1;
-            L.raw_prev = raw;
-        }
-        L.lambda += hh;
+        wind += branch_winding(y[0], y[1], y5[0], y5[1]);
+        S.lambda[tid] += hh;
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
-            L.y[i] = y5[i];
-            L.k1[i] = k[0][i];
+            y[i] = y5[i];
+            k1[i] = k[0][i];
         }
-        L.r = r5;
-        double factor = 5.0;
+        r = r5;
+        float factor = 5.0f;
         if (err != 0.0) {
-            const double le = log(fmax(err, 1e-12));
-            const double lp = L.has_hist ? L.ln_prev : le;
-            factor = exp(-(0.7 / 5.0) * le + (0.3 / 5.0) * (lp - le));
-            L.ln_prev = le;
-            L.has_hist = true;
+            const float le = __log2f(fmaxf(static_cast<float>(err), 1e-12f));
+            factor = pi30_factor(le, has_hist ? lnp : le, 5.0f);
+            lnp = le;
+            has_hist = true;
         }
-        double ah = fabs(L.h) * clampd(0.9 * factor, 0.2, 5.0);
-        L.h = -clampd(ah, 1e-8, 1e13);
+        const double ah = fabs(h) * clampd(0.9 * static_cast<double>(factor), 0.2, 5.0);
+        h = -clampd(ah, 1e-8, 1e13);
     }
 
     // warp-reduced counters
