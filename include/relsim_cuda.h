@@ -142,7 +142,8 @@ typedef struct rt_launch_config {
     uint32_t block_size;       /* threads per CTA: 64, 128, 256 */
     uint32_t ctas_per_sm;      /* persistent CTAs per SM; 0 = occupancy maximum */
     uint32_t refill_threshold; /* idle lanes of a warp before it refills from the queue */
-    uint32_t rays_per_claim;   /* rays a warp claims per lane and refill (1..4) */
+    uint32_t rays_per_thread;  /* consecutive rays claimed per lane with each global atomic:
+                                  a warp claims 32 * rays_per_thread rays at a time (1..64) */
 } rt_launch_config;
 
 /* Counters of the last dispatch (device-side totals). */

@@ -135,7 +135,7 @@ rt_launch_config effective_cfg(const rt_handle* h, bool mixed) {
     const int occ = trace_occupancy(c.block_size, mixed);
     if (c.ctas_per_sm == 0 || static_cast<int>(c.ctas_per_sm) > occ) c.ctas_per_sm = std::max(occ, 1);
     if (c.refill_threshold == 0 || c.refill_threshold > 32) c.refill_threshold = 8;
-    c.rays_per_claim = 1;
+    if (c.rays_per_thread == 0 || c.rays_per_thread > 64) c.rays_per_thread = 4;
     return c;
 }
 
@@ -146,6 +146,7 @@ rt_status launch(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs
     args.bundles = static_cast<const BundleDesc*>(h->bundles.ptr);
     args.n_bundles = n_bundles;
     args.refill_threshold = c.refill_threshold;
+    args.claim = 32u * c.rays_per_thread;
     args.total_rays = total;
     args.queue = static_cast<unsigned long long*>(h->queue.ptr);
     args.stats = static_cast<unsigned long long*>(h->stats.ptr);
@@ -483,6 +484,7 @@ rt_status rt_set_launch_config(rt_handle* h, const rt_launch_config* cfg) {
     if (cfg->block_size != 0 && cfg->block_size != 64 && cfg->block_size != 128 && cfg->block_size != 256)
         return fail(h, RT_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
     if (cfg->refill_threshold > 32) return fail(h, RT_ERR_INVALID_ARG, "refill_threshold must be <= 32");
+    if (cfg->rays_per_thread > 64) return fail(h, RT_ERR_INVALID_ARG, "rays_per_thread must be <= 64");
     h->cfg = *cfg;
     return RT_OK;
 }

@@ -60,6 +60,8 @@ struct TraceArgs {
     const BundleDesc* bundles;
     uint32_t n_bundles;
     uint32_t refill_threshold;
+    uint32_t claim;             // rays a warp claims per global atomic
+    uint32_t pad;
     uint64_t total_rays;
     unsigned long long* queue;  // [0]: next unclaimed ray
     unsigned long long* stats;  // [ST_COUNT]

@@ -119,7 +119,7 @@ __device__ __forceinline__ int branch_winding(double x0, double y0, double x1, d
 
 struct InitResult {
     double r;
-    int can_early;
+    int can_early;  // -1: undecided; the Carter test runs when the ray first needs it
 };
 
 // Ray generation (software_compute_engine.hpp:3843-3862, :3932-3938, :1637-1650,
@@ -169,7 +169,7 @@ __device__ __noinline__ InitResult init_ray(const BundleDesc* __restrict__ Bp, u
     double hf, s;
     InitResult res;
     res.r = ks_rhs<double>(y, B.m, B.a, k1, hf, s);
-    res.can_early = (B.flags & BF_EARLY_CAPTURE) && shadow_distance(B.m, B.a, B.rh, lz0, q0) > kEarlyCaptureMargin;
+    res.can_early = (B.flags & BF_EARLY_CAPTURE) ? -1 : 0;
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         xch[i] = y[i];
@@ -314,35 +314,6 @@ __device__ __noinline__ void finish_ray(const BundleDesc* __restrict__ Bp, Cold<
     }
 }
 
-// Stages 2..6 and the 5th-order solution of a step hh from (y, k1)
-// (rk45_adaptive.hpp:210-251).
-__device__ __forceinline__ void dp5_stages(const double* y, const double* k1, double hh, double M, double a,
-                                           double (&k)[6][6], double* y5) {
-    double s[6], hf, sv;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) s[i] = y[i] + hh * (DP::A21 * k1[i]);
-    ks_rhs<double>(s, M, a, k[1], hf, sv);
-#pragma unroll
-    for (int i = 0; i < 6; ++i) s[i] = y[i] + hh * (DP::A31 * k1[i] + DP::A32 * k[1][i]);
-    ks_rhs<double>(s, M, a, k[2], hf, sv);
-#pragma unroll
-    for (int i = 0; i < 6; ++i) s[i] = y[i] + hh * (DP::A41 * k1[i] + DP::A42 * k[1][i] + DP::A43 * k[2][i]);
-    ks_rhs<double>(s, M, a, k[3], hf, sv);
-#pragma unroll
-    for (int i = 0; i < 6; ++i)
-        s[i] = y[i] + hh * (DP::A51 * k1[i] + DP::A52 * k[1][i] + DP::A53 * k[2][i] + DP::A54 * k[3][i]);
-    ks_rhs<double>(s, M, a, k[4], hf, sv);
-#pragma unroll
-    for (int i = 0; i < 6; ++i)
-        s[i] = y[i] + hh * (DP::A61 * k1[i] + DP::A62 * k[1][i] + DP::A63 * k[2][i] + DP::A64 * k[3][i] +
-                            DP::A65 * k[4][i]);
-    ks_rhs<double>(s, M, a, k[5], hf, sv);
-#pragma unroll
-    for (int i = 0; i < 6; ++i)
-        y5[i] = y[i] + hh * (DP::B1 * k1[i] + DP::B3 * k[2][i] + DP::B4 * k[3][i] + DP::B5 * k[4][i] +
-                             DP::B6 * k[5][i]);
-}
-
 // PI30 factor (step_controller.hpp:51-58) from base-2 logs of the errors.
 __device__ __forceinline__ float pi30_factor(float le, float lp, float order_p1) {
     return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));
@@ -363,26 +334,45 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
     double r = 0.0, h = 0.0;
     float lnp = 0.0f;  // log2 of the previous error (PI30 history)
     uint32_t acc = 0, rej = 0, flags = 0, bidx = 0;
-    int mode = MODE_IDLE, wind = 0;
-    bool has_hist = false, can_early = false;
+    int mode = MODE_IDLE, wind = 0, can_early = 0;
+    bool has_hist = false;
 #pragma unroll
     for (int i = 0; i < 6; ++i) y[i] = k1[i] = 0.0;
 
+    // warp-uniform claim state: rays [chunk_next, chunk_end) belong to this warp
     bool queue_open = true;
+    uint64_t chunk_next = 0, chunk_end = 0;
     unsigned long long n_att = 0, n_acc = 0, n_rays = 0, n_rhs = 0;
 
     for (;;) {
-        // ---- refill idle lanes from the global queue ----
+        // ---- refill idle lanes: from the warp's chunk, then from a new chunk
+        //      of `claim` consecutive rays (one global atomic per chunk) ----
         const unsigned idle = __ballot_sync(FULL, mode == MODE_IDLE);
         const int n_idle = __popc(idle);
-        if (queue_open && n_idle > 0 && (n_idle >= static_cast<int>(args.refill_threshold) || n_idle == 32)) {
-            const int leader = __ffs(idle) - 1;
-            unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(args.queue, static_cast<unsigned long long>(n_idle));
-            base = __shfl_sync(FULL, base, leader);
-            if (base + static_cast<unsigned long long>(n_idle) >= args.total_rays) queue_open = false;
+        if ((queue_open || chunk_next < chunk_end) && n_idle > 0 &&
+            (n_idle >= static_cast<int>(args.refill_threshold) || n_idle == 32)) {
+            const uint64_t avail = chunk_end - chunk_next;
+            uint64_t base2 = 0;
+            bool got2 = false;
+            if (avail < static_cast<uint64_t>(n_idle) && queue_open) {
+                const int leader = __ffs(idle) - 1;
+                unsigned long long b = 0;
+                if (lane == leader) b = atomicAdd(args.queue, static_cast<unsigned long long>(args.claim));
+                b = __shfl_sync(FULL, b, leader);
+                if (b >= args.total_rays) {
+                    queue_open = false;
+                } else {
+                    base2 = b;
+                    got2 = true;
+                    if (b + args.claim >= args.total_rays) queue_open = false;
+                }
+            }
+            const uint64_t used_old = (avail < static_cast<uint64_t>(n_idle)) ? avail : n_idle;
             if (mode == MODE_IDLE) {
-                const uint64_t rid = base + static_cast<uint64_t>(__popc(idle & lt_mask));
+                const uint64_t rank = static_cast<uint64_t>(__popc(idle & lt_mask));
+                uint64_t rid = ~0ull;
+                if (rank < avail) rid = chunk_next + rank;
+                else if (got2) rid = base2 + (rank - avail);
                 if (rid < args.total_rays) {
                     // bundle of this ray: last bundle whose ray_begin <= rid
                     uint32_t lo = 0, hi = args.n_bundles;
@@ -400,7 +390,7 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
                         k1[i] = xch[6 + i];
                     }
                     r = ir.r;
-                    can_early = ir.can_early != 0;
+                    can_early = ir.can_early;
                     h = -args.bundles[lo].h0;
                     lnp = 0.0f;
                     has_hist = false;
@@ -411,9 +401,16 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
                     ++n_rhs;
                 }
             }
+            if (got2) {
+                chunk_next = base2 + (static_cast<uint64_t>(n_idle) - used_old);
+                chunk_end = base2 + args.claim;
+                if (chunk_end > args.total_rays) chunk_end = args.total_rays;
+            } else {
+                chunk_next += used_old;
+            }
         }
         if (__ballot_sync(FULL, mode != MODE_IDLE) == 0) {
-            if (!queue_open) break;
+            if (!queue_open && chunk_next >= chunk_end) break;
             continue;
         }
         if (mode == MODE_IDLE) continue;
@@ -455,12 +452,41 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
             hh = t * h;
         }
 
-        double k[6][6];
-        double y5[6];
-        dp5_stages(y, k1, hh, M, a, k, y5);
-        n_rhs += 5;
+        // ---- Dormand-Prince stages 2..7 (rk45_adaptive.hpp:210-252); stage 7 is
+        //      the FSAL stage at the 5th-order solution y5.  kA holds k2 for
+        //      stages 3..6, then k7. ----
+        double kA[6], k3[6], k4[6], k5[6], k6[6], y5[6];
+        double r5 = 0.0, hf5 = 0.0, s5 = 0.0;
+        const bool root = (mode == MODE_ROOT);
+        {
+            double in[6], hf, sv;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) in[i] = y[i] + hh * (DP::A21 * k1[i]);
+            ks_rhs<double>(in, M, a, kA, hf, sv);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) in[i] = y[i] + hh * (DP::A31 * k1[i] + DP::A32 * kA[i]);
+            ks_rhs<double>(in, M, a, k3, hf, sv);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) in[i] = y[i] + hh * (DP::A41 * k1[i] + DP::A42 * kA[i] + DP::A43 * k3[i]);
+            ks_rhs<double>(in, M, a, k4, hf, sv);
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+                in[i] = y[i] + hh * (DP::A51 * k1[i] + DP::A52 * kA[i] + DP::A53 * k3[i] + DP::A54 * k4[i]);
+            ks_rhs<double>(in, M, a, k5, hf, sv);
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+                in[i] = y[i] + hh * (DP::A61 * k1[i] + DP::A62 * kA[i] + DP::A63 * k3[i] + DP::A64 * k4[i] +
+                                     DP::A65 * k5[i]);
+            ks_rhs<double>(in, M, a, k6, hf, sv);
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+                y5[i] = y[i] + hh * (DP::B1 * k1[i] + DP::B3 * k3[i] + DP::B4 * k4[i] + DP::B5 * k5[i] +
+                                     DP::B6 * k6[i]);
+            if (!root) r5 = ks_rhs<double>(y5, M, a, kA, hf5, s5);
+        }
+        n_rhs += root ? 5 : 6;
 
-        if (mode == MODE_ROOT) {
+        if (root) {
             const double ft = y5[2];
             const int rit = ++S.rit[tid];
             const double lo = S.lo[tid], hi = S.hi[tid];
@@ -500,18 +526,15 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
             continue;
         }
 
-        // full step: last stage (FSAL) and the FP64 error norm (rk45_adaptive.hpp:252-261)
-        double hf5, s5;
-        const double r5 = ks_rhs<double>(y5, M, a, k[0], hf5, s5);  // k[0] now holds k7
-        n_rhs += 1;
+        // FP64 error norm (rk45_adaptive.hpp:254-261); kA holds k7
         double err;
         {
             double num = 0.0, den = 1.0;
             const double rtol = Bp->rtol, atol = Bp->atol;
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
-                const double est = fabs(hh) * fabs(DP::E1 * k1[i] + DP::E3 * k[2][i] + DP::E4 * k[3][i] +
-                                                   DP::E5 * k[4][i] + DP::E6 * k[5][i] + DP::E7 * k[0][i]);
+                const double est = fabs(hh) * fabs(DP::E1 * k1[i] + DP::E3 * k3[i] + DP::E4 * k4[i] +
+                                                   DP::E5 * k5[i] + DP::E6 * k6[i] + DP::E7 * kA[i]);
                 const double sc = rtol * fmax(fabs(y[i]), fabs(y5[i])) + atol;
                 if (est * den > num * sc) {
                     num = est;
@@ -580,14 +603,15 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
             } else if (r5 > Bp->r_esc) {
                 term = RT_RAY_ESCAPED;
                 target = Bp->r_esc;
-            } else if (can_early && r5 < Bp->r_early) {
+            } else if (can_early != 0 && r5 < Bp->r_early) {
+                if (can_early < 0)  // Carter test, once per ray, when first inside r_early
+                    can_early = shadow_distance(M, a, Bp->rh, S.lz0[tid], S.q0[tid]) > kEarlyCaptureMargin;
                 // dr_BL/dlambda (kerr_invariants.hpp:140); the trace runs towards
                 // decreasing lambda, so dr/dlambda > 0 means inwards
                 const double rr2 = r5 * r5, z = y5[2];
-                const double drdl =
-                    (rr2 * r5 * (y5[0] * k[0][0] + y5[1] * k[0][1]) + r5 * (rr2 + a * a) * z * k[0][2]) /
-                    (rr2 * rr2 + a * a * z * z);
-                if (drdl > 0.0) {
+                const double drdl = (rr2 * r5 * (y5[0] * kA[0] + y5[1] * kA[1]) + r5 * (rr2 + a * a) * z * kA[2]) /
+                                    (rr2 * rr2 + a * a * z * z);
+                if (can_early > 0 && drdl > 0.0) {
                     term = RT_RAY_CAPTURED;
                     flags |= RT_RAYFLAG_EARLY_CAPTURE;
                     target = Bp->r_early;
@@ -600,7 +624,7 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
                     xch[i] = y[i];
                     xch[6 + i] = k1[i];
                     xch[12 + i] = y5[i];
-                    xch[18 + i] = k[0][i];
+                    xch[18 + i] = kA[i];
                 }
                 finish_ray<BLOCK>(Bp, S, tid, term, flags, acc, rej, wind, target, hh, NAN, 1.0, args.out, xch);
                 mode = MODE_IDLE;
@@ -626,9 +650,9 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
                     const double q = -0.5 * (qb + copysign(sqrt(disc), qb));
                     if (q != 0.0) {
                         const double alpha = res / q;
-                        p[0] += alpha * k[0][0];
-                        p[1] += alpha * k[0][1];
-                        p[2] += alpha * k[0][2];
+                        p[0] += alpha * kA[0];
+                        p[1] += alpha * kA[1];
+                        p[2] += alpha * kA[2];
                     }
                 }
             }
@@ -638,7 +662,7 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
             y[i] = y5[i];
-            k1[i] = k[0][i];
+            k1[i] = kA[i];
         }
         r = r5;
         float factor = 5.0f;

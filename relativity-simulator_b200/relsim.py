@@ -20,7 +20,7 @@ from typing import Iterable
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "librelsim_cuda.so")
+LIB_PATH = os.environ.get("RELSIM_LIB") or os.path.join(HERE, "librelsim_cuda.so")
 
 RT_OK = 0
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "TIMEOUT", 4: "DEVICE", 5: "CANCELLED", 6: "NOT_READY",
@@ -66,7 +66,7 @@ class RayOut(ctypes.Structure):
 
 
 class LaunchConfig(ctypes.Structure):
-    _fields_ = [("block_size", _u32), ("ctas_per_sm", _u32), ("refill_threshold", _u32), ("rays_per_claim", _u32)]
+    _fields_ = [("block_size", _u32), ("ctas_per_sm", _u32), ("refill_threshold", _u32), ("rays_per_thread", _u32)]
 
 
 class Stats(ctypes.Structure):
@@ -257,8 +257,9 @@ class Tracer:
     def synchronize(self, timeout_ms: float = 0.0) -> None:
         self._check(self.lib.rt_synchronize(self._h, timeout_ms))
 
-    def set_launch_config(self, block_size: int = 0, ctas_per_sm: int = 0, refill_threshold: int = 0) -> None:
-        c = LaunchConfig(block_size, ctas_per_sm, refill_threshold, 1)
+    def set_launch_config(self, block_size: int = 0, ctas_per_sm: int = 0, refill_threshold: int = 0,
+                          rays_per_thread: int = 0) -> None:
+        c = LaunchConfig(block_size, ctas_per_sm, refill_threshold, rays_per_thread)
         self._check(self.lib.rt_set_launch_config(self._h, ctypes.byref(c)))
 
     def launch_config(self) -> LaunchConfig:

@@ -26,11 +26,15 @@ def main() -> None:
     ap.add_argument("--fov", type=float, default=12.0)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--refill", type=int, default=0)
+    ap.add_argument("--rays-per-thread", type=int, default=0)
     a = ap.parse_args()
     cam = relsim.make_camera(spin=a.spin, r_obs=a.r_obs, incl_deg=a.incl, fov_deg=a.fov, width=a.side,
                              height=a.side,
                              precision=relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64)
     with relsim.Tracer(0) as tr:
+        tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread)
         for _ in range(a.repeat):
             out = tr.dispatch(cam, fields=["status", "steps_accepted", "steps_rejected"], pixels=False)
             s = tr.stats()
