@@ -144,6 +144,9 @@ typedef struct rt_launch_config {
     uint32_t refill_threshold; /* idle lanes of a warp before it refills from the queue */
     uint32_t rays_per_thread;  /* consecutive rays claimed per lane with each global atomic:
                                   a warp claims 32 * rays_per_thread rays at a time (1..64) */
+    uint32_t fp64_rolled;      /* FP64 mode: 1 = stage loop rolled around one RHS copy with the
+                                  stage derivatives in shared memory, 0 = straight-line stages
+                                  (the mixed mode always uses the rolled form) */
 } rt_launch_config;
 
 /* Counters of the last dispatch (device-side totals). */

@@ -21,10 +21,10 @@
 #include "rt_internal.h"
 
 namespace relsim {
-template <int BLOCK>
-__global__ void trace_fp64_kernel_t(TraceArgs args);
-void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, cudaStream_t stream);
-int trace_occupancy(uint32_t block, bool mixed);
+void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled,
+                  cudaStream_t stream);
+int trace_occupancy(uint32_t block, bool mixed, bool rolled);
+uint32_t kernel_block(uint32_t block, bool mixed, bool rolled);
 double measure_fma_peak(bool fp64, int sm_count, cudaStream_t stream, float* ms_out);
 }  // namespace relsim
 
@@ -132,10 +132,13 @@ void row_window(const rt_camera& c, uint32_t& row0, uint32_t& nrows) {
 rt_launch_config effective_cfg(const rt_handle* h, bool mixed) {
     rt_launch_config c = h->cfg;
     if (c.block_size != 64 && c.block_size != 128 && c.block_size != 256) c.block_size = 128;
-    const int occ = trace_occupancy(c.block_size, mixed);
+    c.fp64_rolled = c.fp64_rolled ? 1u : 0u;
+    c.block_size = kernel_block(c.block_size, mixed, c.fp64_rolled != 0);
+    const int occ = trace_occupancy(c.block_size, mixed, c.fp64_rolled != 0);
     if (c.ctas_per_sm == 0 || static_cast<int>(c.ctas_per_sm) > occ) c.ctas_per_sm = std::max(occ, 1);
-    if (c.refill_threshold == 0 || c.refill_threshold > 32) c.refill_threshold = 8;
-    if (c.rays_per_thread == 0 || c.rays_per_thread > 64) c.rays_per_thread = 4;
+    // defaults from the autotuner on B200: whole-warp refills of 32 consecutive rays
+    if (c.refill_threshold == 0 || c.refill_threshold > 32) c.refill_threshold = 32;
+    if (c.rays_per_thread == 0 || c.rays_per_thread > 64) c.rays_per_thread = 1;
     return c;
 }
 
@@ -155,7 +158,7 @@ rt_status launch(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs
     RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
     const uint32_t grid = static_cast<uint32_t>(h->sm_count) * c.ctas_per_sm;
     RT_CUDA(h, cudaEventRecord(h->ev0, s));
-    launch_trace(args, grid, c.block_size, mixed, s);
+    launch_trace(args, grid, c.block_size, mixed, c.fp64_rolled != 0, s);
     RT_CUDA(h, cudaGetLastError());
     RT_CUDA(h, cudaEventRecord(h->ev1, s));
     h->timed = true;

@@ -39,14 +39,17 @@ __device__ __forceinline__ T rt_rcp(T v);
 template <>
 __device__ __forceinline__ double rt_rcp<double>(double v) { return 1.0 / v; }
 template <>
-__device__ __forceinline__ float rt_rcp<float>(float v) { return __frcp_rn(v); }
+__device__ __forceinline__ float rt_rcp<float>(float v) { return __fdividef(1.0f, v); }  // MUFU rcp
 
 template <typename T>
 __device__ __forceinline__ T rt_sqrt(T v);
 template <>
 __device__ __forceinline__ double rt_sqrt<double>(double v) { return sqrt(v); }
 template <>
-__device__ __forceinline__ float rt_sqrt<float>(float v) { return sqrtf(v); }
+__device__ __forceinline__ float rt_sqrt<float>(float v) {  // MUFU rsqrt based
+    const float w = fmaxf(v, 1e-30f);
+    return w * rsqrtf(w);
+}
 
 // Boyer-Lindquist r of a Kerr-Schild point (kerr_schild_null_integrator.hpp:32-36).
 template <typename T>
@@ -62,7 +65,9 @@ __device__ __forceinline__ T bl_r2(T x, T y, T z, T a2) {
 //   dx/dl = p - 2 H s k
 //   dp/dl = s^2 dH/dx + 2 H s (dk/dx . p)
 // with dk/dx_i . p = dr_i * A + B_i (A, B below) and dH/dx_i = C dr_i (+ D for z).
-template <typename T>
+// With GRAV = true the position part returns only the gravitational term
+// -2 H s k (the mixed-precision step keeps the free-streaming p in FP64).
+template <typename T, bool GRAV = false>
 __device__ __forceinline__ T ks_rhs(const T* __restrict__ y, T M, T a, T* __restrict__ dy, T& hf, T& s) {
     const T x = y[0], yy = y[1], z = y[2], px = y[3], py = y[4], pz = y[5];
     const T a2 = a * a;
@@ -90,16 +95,24 @@ __device__ __forceinline__ T ks_rhs(const T* __restrict__ y, T M, T a, T* __rest
     const T k2 = z * inv_r;
     const T sv = T(1) + k0 * px + k1 * py + k2 * pz;
     const T two_hs = T(2) * H * sv;
-    dy[0] = px - two_hs * k0;
-    dy[1] = py - two_hs * k1;
-    dy[2] = pz - two_hs * k2;
+    if constexpr (GRAV) {
+        dy[0] = -two_hs * k0;
+        dy[1] = -two_hs * k1;
+        dy[2] = -two_hs * k2;
+    } else {
+        dy[0] = px - two_hs * k0;
+        dy[1] = py - two_hs * k1;
+        dy[2] = pz - two_hs * k2;
+    }
     const T r3d = r3 * inv_den;
     const T dr0 = r3d * x;
     const T dr1 = r3d * yy;
     const T dr2 = r * rpa * z * inv_den;
-    const T inv_den2 = inv_den * inv_den;
-    const T C = M * r2 * (T(3) * a2 * z2 - r4) * inv_den2;
-    const T D = T(-2) * M * a2 * r3 * z * inv_den2;
+    // C = M r^2 (3 a^2 z^2 - r^4) / den^2 and D = -2 M a^2 r^3 z / den^2, grouped so
+    // that FP32 intermediates stay near M / r^2 (no underflow of 1/den^2)
+    const T mr2d = M * r2 * inv_den;
+    const T C = mr2d * ((T(3) * a2 * z2 - r4) * inv_den);
+    const T D = T(-2) * (M * r3 * inv_den) * (a2 * z * inv_den);
     const T A = inv_rpa * ((x - T(2) * r * k0) * px + (yy - T(2) * r * k1) * py) - inv_r * k2 * pz;
     const T B0 = inv_rpa * (r * px - a * py);
     const T B1 = inv_rpa * (r * py + a * px);
@@ -118,12 +131,16 @@ __device__ __forceinline__ T ks_rhs(const T* __restrict__ y, T M, T a, T* __rest
 __device__ __forceinline__ double ks_field64(const double* x, double M, double a, double* k, double& hf) {
     const double a2 = a * a;
     const double r2 = bl_r2<double>(x[0], x[1], x[2], a2);
-    const double r = sqrt(r2);
+    const double inv_r = rsqrt(r2);
+    const double r = r2 * inv_r;
     const double rpa = r2 + a2;
-    hf = M * r2 * r / (r2 * r2 + a2 * x[2] * x[2]);
-    k[0] = (r * x[0] + a * x[1]) / rpa;
-    k[1] = (r * x[1] - a * x[0]) / rpa;
-    k[2] = x[2] / r;
+    const double den = r2 * r2 + a2 * x[2] * x[2];
+    const double q = 1.0 / (rpa * den);
+    const double inv_rpa = den * q;
+    hf = M * r2 * r * (rpa * q);
+    k[0] = (r * x[0] + a * x[1]) * inv_rpa;
+    k[1] = (r * x[1] - a * x[0]) * inv_rpa;
+    k[2] = x[2] * inv_r;
     return r;
 }
 

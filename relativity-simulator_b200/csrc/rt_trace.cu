@@ -314,6 +314,152 @@ __device__ __noinline__ void finish_ray(const BundleDesc* __restrict__ Bp, Cold<
     }
 }
 
+// Largest r_BL at which the FP32 stages are used (keeps r^4 and 1/r^4 in range).
+constexpr double kFp32MaxRadius = 1e6;
+
+// Mixed-precision DP45 step for the far zone.  The state y and the result y5
+// are FP64; the stages run in FP32 on the deviation from free streaming:
+//   x_j = x + h c_j p + h sum_m a_jm dx_m,   dx_m = (p_m - p) - 2 H s k (at stage m)
+//   p_j = p + h sum_m a_jm kp_m,             kp_m = dp/dlambda (at stage m)
+// so the large h p term of every position increment stays FP64 and FP32 only
+// carries the gravitational part.  y5 = y + h p (FP64) + h sum b_j dx_j (FP32).
+// The error estimate uses sum_j e_j = 0: E_x = h sum e_j dx_j.  Outputs k7 in
+// FP64 (FSAL) and |E| per component.
+__device__ __forceinline__ void mixed_stages(const double* __restrict__ y, const double* __restrict__ k1, double hh,
+                                             double M, double a, double* __restrict__ y5, double* __restrict__ k7,
+                                             double* __restrict__ est) {
+    const float h = static_cast<float>(hh);
+    const float Mf = static_cast<float>(M), af = static_cast<float>(a);
+    float x0[3], p0[3];
+    float dx1[3], kp1[3], dx2[3], kp2[3], dx3[3], kp3[3], dx4[3], kp4[3], dx5[3], kp5[3], dx6[3], kp6[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        x0[i] = static_cast<float>(y[i]);
+        p0[i] = static_cast<float>(y[3 + i]);
+        dx1[i] = static_cast<float>(k1[i] - y[3 + i]);
+        kp1[i] = static_cast<float>(k1[3 + i]);
+    }
+    constexpr float C2 = 1.0f / 5.0f, C3 = 3.0f / 10.0f, C4 = 4.0f / 5.0f, C5 = 8.0f / 9.0f;
+    float in[6], g[6], hf, sv;
+#define RT_STAGE(DXO, KPO, CC, SUMX, SUMP)                          \
+    _Pragma("unroll") for (int i = 0; i < 3; ++i) {                 \
+        const float dp = h * (SUMP);                                \
+        in[i] = x0[i] + h * ((CC) * p0[i] + (SUMX));                \
+        in[3 + i] = p0[i] + dp;                                     \
+        g[i] = dp;                                                  \
+    }                                                               \
+    {                                                               \
+        float dpv[3] = {g[0], g[1], g[2]};                          \
+        ks_rhs<float, true>(in, Mf, af, g, hf, sv);                 \
+        _Pragma("unroll") for (int i = 0; i < 3; ++i) {             \
+            DXO[i] = dpv[i] + g[i];                                 \
+            KPO[i] = g[3 + i];                                      \
+        }                                                           \
+    }
+    RT_STAGE(dx2, kp2, C2, float(DP::A21) * dx1[i], float(DP::A21) * kp1[i])
+    RT_STAGE(dx3, kp3, C3, float(DP::A31) * dx1[i] + float(DP::A32) * dx2[i],
+             float(DP::A31) * kp1[i] + float(DP::A32) * kp2[i])
+    RT_STAGE(dx4, kp4, C4, float(DP::A41) * dx1[i] + float(DP::A42) * dx2[i] + float(DP::A43) * dx3[i],
+             float(DP::A41) * kp1[i] + float(DP::A42) * kp2[i] + float(DP::A43) * kp3[i])
+    RT_STAGE(dx5, kp5, C5,
+             float(DP::A51) * dx1[i] + float(DP::A52) * dx2[i] + float(DP::A53) * dx3[i] + float(DP::A54) * dx4[i],
+             float(DP::A51) * kp1[i] + float(DP::A52) * kp2[i] + float(DP::A53) * kp3[i] + float(DP::A54) * kp4[i])
+    RT_STAGE(dx6, kp6, 1.0f,
+             float(DP::A61) * dx1[i] + float(DP::A62) * dx2[i] + float(DP::A63) * dx3[i] + float(DP::A64) * dx4[i] +
+                 float(DP::A65) * dx5[i],
+             float(DP::A61) * kp1[i] + float(DP::A62) * kp2[i] + float(DP::A63) * kp3[i] + float(DP::A64) * kp4[i] +
+                 float(DP::A65) * kp5[i])
+#undef RT_STAGE
+    // 5th-order solution: FP64 accumulation of the FP32 increments
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float sx = float(DP::B1) * dx1[i] + float(DP::B3) * dx3[i] + float(DP::B4) * dx4[i] +
+                         float(DP::B5) * dx5[i] + float(DP::B6) * dx6[i];
+        const float sp = float(DP::B1) * kp1[i] + float(DP::B3) * kp3[i] + float(DP::B4) * kp4[i] +
+                         float(DP::B5) * kp5[i] + float(DP::B6) * kp6[i];
+        y5[i] = y[i] + hh * y[3 + i] + static_cast<double>(h * sx);
+        y5[3 + i] = y[3 + i] + static_cast<double>(h * sp);
+    }
+    // stage 7 (FSAL) at y5
+#pragma unroll
+    for (int i = 0; i < 6; ++i) in[i] = static_cast<float>(y5[i]);
+    ks_rhs<float, true>(in, Mf, af, g, hf, sv);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float dx7 = static_cast<float>(y5[3 + i] - y[3 + i]) + g[i];
+        const float ex = float(DP::E1) * dx1[i] + float(DP::E3) * dx3[i] + float(DP::E4) * dx4[i] +
+                         float(DP::E5) * dx5[i] + float(DP::E6) * dx6[i] + float(DP::E7) * dx7;
+        const float ep = float(DP::E1) * kp1[i] + float(DP::E3) * kp3[i] + float(DP::E4) * kp4[i] +
+                         float(DP::E5) * kp5[i] + float(DP::E6) * kp6[i] + float(DP::E7) * g[3 + i];
+        est[i] = static_cast<double>(fabsf(h * ex));
+        est[3 + i] = static_cast<double>(fabsf(h * ep));
+        k7[i] = y5[3 + i] + static_cast<double>(g[i]);
+        k7[3 + i] = static_cast<double>(g[3 + i]);
+    }
+}
+
+// Dormand-Prince tableau rows for the rolled FP64 step: row s gives the
+// coefficients of k1..k(s+1) in the input of stage s + 2 (row 5 = b, the
+// 5th-order solution); kDpE are the error weights of k1..k7.
+__constant__ double kDpA[6][6] = {
+    {DP::A21, 0, 0, 0, 0, 0},
+    {DP::A31, DP::A32, 0, 0, 0, 0},
+    {DP::A41, DP::A42, DP::A43, 0, 0, 0},
+    {DP::A51, DP::A52, DP::A53, DP::A54, 0, 0},
+    {DP::A61, DP::A62, DP::A63, DP::A64, DP::A65, 0},
+    {DP::B1, 0.0, DP::B3, DP::B4, DP::B5, DP::B6}};
+__constant__ double kDpE[7] = {DP::E1, 0.0, DP::E3, DP::E4, DP::E5, DP::E6, DP::E7};
+
+// Stage derivatives k2..k7 of the rolled FP64 step, per thread in shared memory.
+template <int BLOCK>
+struct KStore {
+    double k[6][6][BLOCK];
+};
+
+// FP64 stages 2..7 as one rolled loop around a single RHS (small in the
+// instruction cache; used where FP64 steps are a minority, e.g. the near zone
+// of the mixed mode).  Same arithmetic as the straight-line form.
+template <int BLOCK>
+__device__ __forceinline__ void fp64_stages_rolled(const double* __restrict__ y, const double* __restrict__ k1,
+                                                   double hh, double M, double a, KStore<BLOCK>& K, int tid,
+                                                   bool root, double* __restrict__ y5, double* __restrict__ k7,
+                                                   double* __restrict__ est, double& r5, double& hf5, double& s5) {
+#pragma unroll 1
+    for (int st = 0; st < 6; ++st) {
+        double in[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            double acc = kDpA[st][0] * k1[i];
+#pragma unroll 1
+            for (int j = 1; j <= st; ++j) acc += kDpA[st][j] * K.k[j - 1][i][tid];
+            in[i] = y[i] + hh * acc;
+        }
+        if (st == 5) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) y5[i] = in[i];
+            if (root) return;
+        }
+        double out[6], hf, sv;
+        const double rr = ks_rhs<double>(in, M, a, out, hf, sv);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) K.k[st][i][tid] = out[i];
+        if (st == 5) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) k7[i] = out[i];
+            r5 = rr;
+            hf5 = hf;
+            s5 = sv;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double acc = kDpE[0] * k1[i];
+#pragma unroll 1
+        for (int j = 2; j < 7; ++j) acc += kDpE[j] * K.k[j - 1][i][tid];
+        est[i] = fabs(hh) * fabs(acc);
+    }
+}
+
 // PI30 factor (step_controller.hpp:51-58) from base-2 logs of the errors.
 __device__ __forceinline__ float pi30_factor(float le, float lp, float order_p1) {
     return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));
@@ -321,9 +467,12 @@ __device__ __forceinline__ float pi30_factor(float le, float lp, float order_p1)
 
 }  // namespace
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
+// 384 / BLOCK resident CTAs per SM caps the kernel at 168 registers per thread
+// (12 warps per SM).
+template <int BLOCK, bool MIXED, bool ROLLED>
+__global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs args) {
     __shared__ Cold<BLOCK> S;
+    __shared__ KStore<ROLLED ? BLOCK : 1> K;
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -336,13 +485,15 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
     uint32_t acc = 0, rej = 0, flags = 0, bidx = 0;
     int mode = MODE_IDLE, wind = 0, can_early = 0;
     bool has_hist = false;
+    bool k1_fp32 = false;  // k1 came from an FP32 far-zone stage (mixed mode)
+    uint32_t guard = 0;    // loop iterations spent on the current ray
 #pragma unroll
     for (int i = 0; i < 6; ++i) y[i] = k1[i] = 0.0;
 
     // warp-uniform claim state: rays [chunk_next, chunk_end) belong to this warp
     bool queue_open = true;
     uint64_t chunk_next = 0, chunk_end = 0;
-    unsigned long long n_att = 0, n_acc = 0, n_rays = 0, n_rhs = 0;
+    unsigned long long n_att = 0, n_acc = 0, n_rays = 0, n_rhs = 0, n_far = 0;
 
     for (;;) {
         // ---- refill idle lanes: from the warp's chunk, then from a new chunk
@@ -396,6 +547,8 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
                     has_hist = false;
                     acc = rej = flags = 0;
                     wind = args.bundles[lo].wind0;
+                    k1_fp32 = false;
+                    guard = 0;
                     mode = MODE_STEP;
                     ++n_rays;
                     ++n_rhs;
@@ -413,10 +566,33 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
             if (!queue_open && chunk_next >= chunk_end) break;
             continue;
         }
+        // mixed mode: the warp takes an FP32 far-zone step only when no stepping
+        // lane is inside the FP64 zone (one instruction stream per iteration;
+        // lanes in a root solve always run FP64)
+        bool far = false;
+        if constexpr (MIXED) {
+            const bool stepping = (mode == MODE_STEP || mode == MODE_REDO);
+            const BundleDesc* Bz = args.bundles + bidx;
+            const bool lane_far = stepping && r >= Bz->fp64_radius && r < kFp32MaxRadius;
+            // every lane executes the ballot (no short-circuit around a full-mask sync)
+            const unsigned near_lanes = __ballot_sync(FULL, stepping && !lane_far);
+            far = lane_far && near_lanes == 0u;
+        }
         if (mode == MODE_IDLE) continue;
 
         const BundleDesc* Bp = args.bundles + bidx;
         const double M = Bp->m, a = Bp->a;
+        // backstop: a ray needs at most 62 iterations per attempt (attempt, <= 60
+        // root iterations, redo); past that bound it is ended as unfinished
+        if (++guard > 64u * Bp->max_steps + 64u) {
+            flags |= RT_RAYFLAG_MAX_STEPS;
+            double xch[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) xch[i] = y[i];
+            finish_ray<BLOCK>(Bp, S, tid, RT_RAY_UNFINISHED, flags, acc, rej, wind, 0.0, 0.0, NAN, 1.0, args.out, xch);
+            mode = MODE_IDLE;
+            continue;
+        }
         double hh = h;
         if (mode == MODE_STEP) {
             // the initial point may already be outside the integration domain
@@ -454,35 +630,61 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
 
         // ---- Dormand-Prince stages 2..7 (rk45_adaptive.hpp:210-252); stage 7 is
         //      the FSAL stage at the 5th-order solution y5.  kA holds k2 for
-        //      stages 3..6, then k7. ----
-        double kA[6], k3[6], k4[6], k5[6], k6[6], y5[6];
+        //      stages 3..6, then k7; est holds |h| |sum_j e_j k_j| per component. ----
+        double kA[6], y5[6], est[6];
         double r5 = 0.0, hf5 = 0.0, s5 = 0.0;
         const bool root = (mode == MODE_ROOT);
-        {
-            double in[6], hf, sv;
+        if (far) {
+            mixed_stages(y, k1, hh, M, a, y5, kA, est);
+            double kf[3];
+            r5 = ks_field64(y5, M, a, kf, hf5);
+            s5 = 1.0 + kf[0] * y5[3] + kf[1] * y5[4] + kf[2] * y5[5];
+            if (mode == MODE_STEP) ++n_far;
+        } else {
+            if constexpr (MIXED) {
+                if (k1_fp32) {  // entering the FP64 zone: first stage again in FP64
+                    double hf, sv;
+                    ks_rhs<double>(y, M, a, k1, hf, sv);
+                    k1_fp32 = false;
+                    ++n_rhs;
+                }
+            }
+            if constexpr (ROLLED) {
+                fp64_stages_rolled<BLOCK>(y, k1, hh, M, a, K, tid, root, y5, kA, est, r5, hf5, s5);
+            } else {
+                double k3[6], k4[6], k5[6], k6[6];
+                double in[6], hf, sv;
 #pragma unroll
-            for (int i = 0; i < 6; ++i) in[i] = y[i] + hh * (DP::A21 * k1[i]);
-            ks_rhs<double>(in, M, a, kA, hf, sv);
+                for (int i = 0; i < 6; ++i) in[i] = y[i] + hh * (DP::A21 * k1[i]);
+                ks_rhs<double>(in, M, a, kA, hf, sv);
 #pragma unroll
-            for (int i = 0; i < 6; ++i) in[i] = y[i] + hh * (DP::A31 * k1[i] + DP::A32 * kA[i]);
-            ks_rhs<double>(in, M, a, k3, hf, sv);
+                for (int i = 0; i < 6; ++i) in[i] = y[i] + hh * (DP::A31 * k1[i] + DP::A32 * kA[i]);
+                ks_rhs<double>(in, M, a, k3, hf, sv);
 #pragma unroll
-            for (int i = 0; i < 6; ++i) in[i] = y[i] + hh * (DP::A41 * k1[i] + DP::A42 * kA[i] + DP::A43 * k3[i]);
-            ks_rhs<double>(in, M, a, k4, hf, sv);
+                for (int i = 0; i < 6; ++i)
+                    in[i] = y[i] + hh * (DP::A41 * k1[i] + DP::A42 * kA[i] + DP::A43 * k3[i]);
+                ks_rhs<double>(in, M, a, k4, hf, sv);
 #pragma unroll
-            for (int i = 0; i < 6; ++i)
-                in[i] = y[i] + hh * (DP::A51 * k1[i] + DP::A52 * kA[i] + DP::A53 * k3[i] + DP::A54 * k4[i]);
-            ks_rhs<double>(in, M, a, k5, hf, sv);
+                for (int i = 0; i < 6; ++i)
+                    in[i] = y[i] + hh * (DP::A51 * k1[i] + DP::A52 * kA[i] + DP::A53 * k3[i] + DP::A54 * k4[i]);
+                ks_rhs<double>(in, M, a, k5, hf, sv);
 #pragma unroll
-            for (int i = 0; i < 6; ++i)
-                in[i] = y[i] + hh * (DP::A61 * k1[i] + DP::A62 * kA[i] + DP::A63 * k3[i] + DP::A64 * k4[i] +
-                                     DP::A65 * k5[i]);
-            ks_rhs<double>(in, M, a, k6, hf, sv);
+                for (int i = 0; i < 6; ++i)
+                    in[i] = y[i] + hh * (DP::A61 * k1[i] + DP::A62 * kA[i] + DP::A63 * k3[i] + DP::A64 * k4[i] +
+                                         DP::A65 * k5[i]);
+                ks_rhs<double>(in, M, a, k6, hf, sv);
 #pragma unroll
-            for (int i = 0; i < 6; ++i)
-                y5[i] = y[i] + hh * (DP::B1 * k1[i] + DP::B3 * k3[i] + DP::B4 * k4[i] + DP::B5 * k5[i] +
-                                     DP::B6 * k6[i]);
-            if (!root) r5 = ks_rhs<double>(y5, M, a, kA, hf5, s5);
+                for (int i = 0; i < 6; ++i)
+                    y5[i] = y[i] + hh * (DP::B1 * k1[i] + DP::B3 * k3[i] + DP::B4 * k4[i] + DP::B5 * k5[i] +
+                                         DP::B6 * k6[i]);
+                if (!root) {
+                    r5 = ks_rhs<double>(y5, M, a, kA, hf5, s5);
+#pragma unroll
+                    for (int i = 0; i < 6; ++i)
+                        est[i] = fabs(hh) * fabs(DP::E1 * k1[i] + DP::E3 * k3[i] + DP::E4 * k4[i] +
+                                                 DP::E5 * k5[i] + DP::E6 * k6[i] + DP::E7 * kA[i]);
+                }
+            }
         }
         n_rhs += root ? 5 : 6;
 
@@ -533,11 +735,9 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
             const double rtol = Bp->rtol, atol = Bp->atol;
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
-                const double est = fabs(hh) * fabs(DP::E1 * k1[i] + DP::E3 * k3[i] + DP::E4 * k4[i] +
-                                                   DP::E5 * k5[i] + DP::E6 * k6[i] + DP::E7 * kA[i]);
                 const double sc = rtol * fmax(fabs(y[i]), fabs(y5[i])) + atol;
-                if (est * den > num * sc) {
-                    num = est;
+                if (est[i] * den > num * sc) {
+                    num = est[i];
                     den = sc;
                 }
             }
@@ -665,6 +865,7 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
             k1[i] = kA[i];
         }
         r = r5;
+        if constexpr (MIXED) k1_fp32 = far;
         float factor = 5.0f;
         if (err != 0.0) {
             const float le = __log2f(fmaxf(static_cast<float>(err), 1e-12f));
@@ -682,34 +883,55 @@ __global__ void __launch_bounds__(BLOCK) trace_fp64_kernel_t(TraceArgs args) {
         n_acc += __shfl_down_sync(FULL, n_acc, off);
         n_rays += __shfl_down_sync(FULL, n_rays, off);
         n_rhs += __shfl_down_sync(FULL, n_rhs, off);
+        n_far += __shfl_down_sync(FULL, n_far, off);
     }
     if (lane == 0) {
         atomicAdd(args.stats + ST_RAYS, n_rays);
         atomicAdd(args.stats + ST_ATTEMPTS, n_att);
         atomicAdd(args.stats + ST_ACCEPTED, n_acc);
         atomicAdd(args.stats + ST_RHS, n_rhs);
-        atomicAdd(args.stats + ST_FP64_ATTEMPTS, n_att);
+        atomicAdd(args.stats + ST_FP64_ATTEMPTS, n_att - n_far);
     }
 }
 
-template __global__ void trace_fp64_kernel_t<64>(TraceArgs);
-template __global__ void trace_fp64_kernel_t<128>(TraceArgs);
-template __global__ void trace_fp64_kernel_t<256>(TraceArgs);
+template __global__ void trace_kernel_t<64, false, false>(TraceArgs);
+template __global__ void trace_kernel_t<128, false, false>(TraceArgs);
+template __global__ void trace_kernel_t<256, false, false>(TraceArgs);
+template __global__ void trace_kernel_t<64, false, true>(TraceArgs);
+template __global__ void trace_kernel_t<128, false, true>(TraceArgs);
+template __global__ void trace_kernel_t<64, true, true>(TraceArgs);
+template __global__ void trace_kernel_t<128, true, true>(TraceArgs);
 
 namespace {
-const void* kernel_for(uint32_t block, bool mixed) {
-    (void)mixed;
+// Mixed precision always uses the rolled FP64 step (its FP64 steps are a
+// minority; the rolled form keeps the loop small).  Rolled kernels exist for
+// 64- and 128-thread blocks (their stage store is 36 KB of shared memory at 128).
+const void* kernel_for(uint32_t block, bool mixed, bool rolled) {
+    if (mixed) {
+        return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, true, true>)
+                             : reinterpret_cast<const void*>(&trace_kernel_t<128, true, true>);
+    }
+    if (rolled) {
+        return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, false, true>)
+                             : reinterpret_cast<const void*>(&trace_kernel_t<128, false, true>);
+    }
     switch (block) {
-        case 64: return reinterpret_cast<const void*>(&trace_fp64_kernel_t<64>);
-        case 256: return reinterpret_cast<const void*>(&trace_fp64_kernel_t<256>);
-        default: return reinterpret_cast<const void*>(&trace_fp64_kernel_t<128>);
+        case 64: return reinterpret_cast<const void*>(&trace_kernel_t<64, false, false>);
+        case 256: return reinterpret_cast<const void*>(&trace_kernel_t<256, false, false>);
+        default: return reinterpret_cast<const void*>(&trace_kernel_t<128, false, false>);
     }
 }
 }  // namespace
 
-int trace_occupancy(uint32_t block, bool mixed) {
+uint32_t kernel_block(uint32_t block, bool mixed, bool rolled) {
+    if ((mixed || rolled) && block > 128) return 128;
+    return block;
+}
+
+int trace_occupancy(uint32_t block, bool mixed, bool rolled) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_for(block, mixed), static_cast<int>(block), 0) !=
+    block = kernel_block(block, mixed, rolled);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_for(block, mixed, rolled), static_cast<int>(block), 0) !=
         cudaSuccess) {
         cudaGetLastError();
         return 1;
@@ -717,9 +939,11 @@ int trace_occupancy(uint32_t block, bool mixed) {
     return n;
 }
 
-void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, cudaStream_t stream) {
+void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled,
+                  cudaStream_t stream) {
     void* params[] = {const_cast<TraceArgs*>(&args)};
-    cudaLaunchKernel(kernel_for(block, mixed), dim3(grid), dim3(block), params, 0, stream);
+    block = kernel_block(block, mixed, rolled);
+    cudaLaunchKernel(kernel_for(block, mixed, rolled), dim3(grid), dim3(block), params, 0, stream);
 }
 
 }  // namespace relsim

@@ -29,6 +29,7 @@ RAY_UNFINISHED, RAY_CAPTURED, RAY_ESCAPED, RAY_DISK = 0, 1, 2, 3
 RAYFLAG_NONFINITE, RAYFLAG_STEP_UNDERFLOW, RAYFLAG_MAX_STEPS, RAYFLAG_EARLY_CAPTURE = 1, 2, 4, 8
 PIXEL_HORIZON_ABSORBED, PIXEL_CELESTIAL_HIT, PIXEL_ACCRETION_DISK_HIT = 1, 2, 4
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+MIXED_RTOL = 1e-8  # DP45 tolerance of the mixed-precision mode
 
 _d = ctypes.c_double
 _u32 = ctypes.c_uint32
@@ -66,7 +67,8 @@ class RayOut(ctypes.Structure):
 
 
 class LaunchConfig(ctypes.Structure):
-    _fields_ = [("block_size", _u32), ("ctas_per_sm", _u32), ("refill_threshold", _u32), ("rays_per_thread", _u32)]
+    _fields_ = [("block_size", _u32), ("ctas_per_sm", _u32), ("refill_threshold", _u32), ("rays_per_thread", _u32),
+                ("fp64_rolled", _u32)]
 
 
 class Stats(ctypes.Structure):
@@ -124,11 +126,19 @@ class RelsimError(RuntimeError):
 def make_camera(*, spin: float = 0.94, mass: float = 1.0, r_obs: float = 100.0, incl_deg: float = 17.0,
                 phi_obs: float = 0.0, fov_deg: float = 12.0, width: int = 2048, height: int = 2048,
                 escape_radius: float = 1000.0, capture_scale: float = 1.01, disk_inner: float = 0.0,
-                disk_outer: float = 20.0, rtol: float = 1e-10, atol: float = 1e-10, max_steps: int = 20000,
+                disk_outer: float = 20.0, rtol: float | None = None, atol: float | None = None,
+                max_steps: int = 20000,
                 step_cap: float = 0.1, h0: float = 0.01, projection_tol: float = 1e-12, early_capture: bool = True,
                 precision: int = PRECISION_FP64, mixed_fp64_radius: float = 0.0, row_offset: int = 0,
                 row_count: int = 0) -> Camera:
-    """A camera looking at the hole from (r_obs, incl, phi_obs) with a static-observer tetrad."""
+    """A camera looking at the hole from (r_obs, incl, phi_obs) with a static-observer tetrad.
+
+    Tolerances default to rtol = atol = 1e-10 for FP64 and 1e-8 for the mixed
+    precision mode (whose FP32 stages carry ~1e-7 relative increments)."""
+    if rtol is None:
+        rtol = MIXED_RTOL if precision == PRECISION_MIXED else 1e-10
+    if atol is None:
+        atol = rtol
     c = Camera()
     c.field_of_view_rad = math.radians(fov_deg)
     c.metric_mass, c.metric_spin = mass, spin
@@ -258,8 +268,8 @@ class Tracer:
         self._check(self.lib.rt_synchronize(self._h, timeout_ms))
 
     def set_launch_config(self, block_size: int = 0, ctas_per_sm: int = 0, refill_threshold: int = 0,
-                          rays_per_thread: int = 0) -> None:
-        c = LaunchConfig(block_size, ctas_per_sm, refill_threshold, rays_per_thread)
+                          rays_per_thread: int = 0, fp64_rolled: int = 0) -> None:
+        c = LaunchConfig(block_size, ctas_per_sm, refill_threshold, rays_per_thread, fp64_rolled)
         self._check(self.lib.rt_set_launch_config(self._h, ctypes.byref(c)))
 
     def launch_config(self) -> LaunchConfig:

@@ -29,16 +29,21 @@ def main() -> None:
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--refill", type=int, default=0)
     ap.add_argument("--rays-per-thread", type=int, default=0)
+    ap.add_argument("--fp64-rolled", type=int, default=0)
+    ap.add_argument("--rtol", type=float, default=None)
+    ap.add_argument("--fp64-radius", type=float, default=0.0)
     a = ap.parse_args()
     cam = relsim.make_camera(spin=a.spin, r_obs=a.r_obs, incl_deg=a.incl, fov_deg=a.fov, width=a.side,
                              height=a.side,
-                             precision=relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64)
+                             precision=relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64,
+                             rtol=a.rtol, mixed_fp64_radius=a.fp64_radius)
     with relsim.Tracer(0) as tr:
-        tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread)
+        tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread, a.fp64_rolled)
         for _ in range(a.repeat):
             out = tr.dispatch(cam, fields=["status", "steps_accepted", "steps_rejected"], pixels=False)
             s = tr.stats()
     print(json.dumps({"rays": int(s.rays), "attempts": int(s.attempts), "accepted": int(s.accepted),
+                      "fp64_attempts": int(s.fp64_attempts),
                       "kernel_ms": s.kernel_ms, "mrays_per_s": s.rays / s.kernel_ms / 1e3,
                       "classes": np.bincount(out["status"], minlength=4).tolist()}))
 
