@@ -219,6 +219,42 @@ rt_status rt_synchronize(rt_handle* h, double timeout_ms);
  * from a register-resident FMA-chain kernel.  Roofline denominator. */
 rt_status rt_measure_fma_peak(rt_handle* h, double* fp64_tflops, double* fp32_tflops);
 
+/* Allocation-free bundle trace.  No counterpart in the reference: its compute
+ * executor always owns its device buffers and grows them on demand.
+ *
+ * For callers that cannot allocate device memory at dispatch time: a host
+ * that has reserved the whole device for its own pool allocator (a serving
+ * process or an ML framework's caching allocator, where an outside cudaMalloc
+ * fails or fragments the pool), a frame loop for which the implicit device
+ * synchronisation of cudaFree is too costly, or a plugin with no
+ * initialise/shutdown hooks to own an rt_handle.  The call needs no handle and
+ * calls no cudaMalloc, cudaFree or other allocating routine.
+ *
+ * Scratch: one static device array per device, RT_NOALLOC_SCRATCH_BYTES
+ * (15,104) bytes: the ray-queue counter and the launch counters (256 bytes,
+ * zeroed on `stream` by every call before its launch) and a table of at most
+ * RT_NOALLOC_MAX_BUNDLES bundle descriptors (written by every call).  A longer
+ * table is rejected with RT_ERR_INVALID_ARG.  The outputs need no clearing:
+ * every ray of the table is written.
+ *
+ * The first call on a device does its set-up (scratch address lookup, kernel
+ * loading); make it before any stream capture that is to contain this call.
+ * Calls that overlap in time on one device share the one scratch array and
+ * race: serialise them (one stream, or events between streams).
+ *
+ * cams / n_bundles / offsets / pixels / rays / capacity: as
+ * rt_trace_bundles_device (device output pointers).  cfg: launch shape, NULL
+ * for the defaults.  stream: a cudaStream_t, NULL = the legacy default stream;
+ * the work is enqueued and not waited for (the bundle table is read from
+ * host memory before the call returns).  error (optional): receives a
+ * NUL-terminated message of at most error_len bytes on failure. */
+#define RT_NOALLOC_MAX_BUNDLES 32
+#define RT_NOALLOC_SCRATCH_BYTES 15104
+rt_status rt_trace_bundles_noalloc(int device_ordinal, const rt_camera* cams, uint32_t n_bundles,
+                                   const uint64_t* offsets, rt_pixel_out* pixels, const rt_ray_out* rays,
+                                   size_t capacity, const rt_launch_config* cfg, void* stream, char* error,
+                                   size_t error_len);
+
 #ifdef __cplusplus
 }
 #endif

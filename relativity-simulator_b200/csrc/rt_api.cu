@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -534,3 +535,154 @@ rt_status rt_measure_fma_peak(rt_handle* h, double* fp64_tflops, double* fp32_tf
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free bundle trace (rt_trace_bundles_noalloc).
+//
+// The scratch of the persistent launch (ray-queue counter, launch counters,
+// bundle table) lives in one static device array per device instead of
+// handle-owned cudaMalloc buffers; the kernel is the same one the handle
+// entry points launch.
+
+namespace {
+
+constexpr size_t kNoAllocCounterBytes = 256;  // queue counter at byte 0, launch counters at byte 64
+constexpr size_t kNoAllocStatsOffset = 64;
+constexpr size_t kNoAllocScratchBytes = kNoAllocCounterBytes + RT_NOALLOC_MAX_BUNDLES * sizeof(BundleDesc);
+static_assert(kNoAllocScratchBytes == RT_NOALLOC_SCRATCH_BYTES, "header states the scratch size");
+static_assert(kNoAllocStatsOffset + ST_COUNT * sizeof(unsigned long long) <= kNoAllocCounterBytes,
+              "launch counters fit the zeroed block");
+
+}  // namespace
+
+// Bytes [0, 256): counters, zeroed by every call; bytes [256, ...): bundle table.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+
+struct NoAllocDevice {
+    unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch on this device
+    int sm_count = 0;
+};
+
+std::mutex g_noalloc_mutex;
+NoAllocDevice g_noalloc_devices[kNoAllocMaxDevices];
+
+rt_status noalloc_fail(char* buf, size_t len, rt_status st, const char* msg, const char* detail = nullptr) {
+    if (buf && len > 0) std::snprintf(buf, len, "%s%s%s", msg, detail ? ": " : "", detail ? detail : "");
+    return st;
+}
+
+rt_status noalloc_cuda_fail(char* buf, size_t len, cudaError_t e, const char* where) {
+    cudaGetLastError();
+    return noalloc_fail(buf, len, e == cudaErrorMemoryAllocation ? RT_ERR_OOM : RT_ERR_DEVICE, where,
+                        cudaGetErrorString(e));
+}
+
+// Per-device set-up, once: device check, scratch address, kernel loading.
+// The caller has made `dev` current.
+rt_status noalloc_setup(int dev, NoAllocDevice& out, char* err, size_t len) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoAllocDevice& d = g_noalloc_devices[dev];
+    if (!d.scratch) {
+        int major = 0, minor = 0, sms = 0;
+        cudaError_t e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return noalloc_cuda_fail(err, len, e, "cudaDeviceGetAttribute");
+        if (major != 10 || minor != 0) return noalloc_fail(err, len, RT_ERR_DEVICE, "device is not sm_100");
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return noalloc_cuda_fail(err, len, e, "cudaGetSymbolAddress");
+        // load every tracer kernel now (occupancy queries load them), not inside a later call
+        for (uint32_t block : {64u, 128u, 256u})
+            for (bool mixed : {false, true})
+                for (bool rolled : {false, true}) trace_occupancy(kernel_block(block, mixed, rolled), mixed, rolled);
+        if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_cuda_fail(err, len, e, "kernel set-up");
+        d.scratch = static_cast<unsigned char*>(p);
+        d.sm_count = sms;
+    }
+    out = d;
+    return RT_OK;
+}
+
+}  // namespace
+
+extern "C" rt_status rt_trace_bundles_noalloc(int device_ordinal, const rt_camera* cams, uint32_t n_bundles,
+                                              const uint64_t* offsets, rt_pixel_out* pixels, const rt_ray_out* rays,
+                                              size_t capacity, const rt_launch_config* cfg, void* stream,
+                                              char* error, size_t error_len) {
+    if (error && error_len > 0) error[0] = '\0';
+    if (!cams || n_bundles == 0) return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "no bundles");
+    if (n_bundles > RT_NOALLOC_MAX_BUNDLES) {
+        char detail[96];
+        std::snprintf(detail, sizeof detail, "%u bundles requested, the static scratch holds at most %d",
+                      n_bundles, RT_NOALLOC_MAX_BUNDLES);
+        return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "bundle table too long", detail);
+    }
+    if (pixels && (reinterpret_cast<uintptr_t>(pixels) & 15u))
+        return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "pixels not 16-byte aligned");
+    if (cfg && ((cfg->block_size != 0 && cfg->block_size != 64 && cfg->block_size != 128 && cfg->block_size != 256) ||
+                cfg->refill_threshold > 32 || cfg->rays_per_thread > 64))
+        return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "invalid launch config");
+    const bool mixed = cams[0].precision_mode == RT_PRECISION_MIXED;
+    for (uint32_t b = 0; b < n_bundles; ++b) {
+        if (!camera_valid(&cams[b]))
+            return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "invalid camera in bundle table");
+        if ((cams[b].precision_mode == RT_PRECISION_MIXED) != mixed)
+            return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "one precision mode per bundle launch");
+    }
+    // bundle table on the host stack
+    BundleDesc table[RT_NOALLOC_MAX_BUNDLES];
+    uint64_t begin = 0;
+    for (uint32_t b = 0; b < n_bundles; ++b) {
+        uint32_t row0, nrows;
+        row_window(cams[b], row0, nrows);
+        const uint64_t n = static_cast<uint64_t>(cams[b].screen_width) * nrows;
+        const uint64_t off = offsets ? offsets[b] : begin;
+        if (off + n > capacity)
+            return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "bundle outputs exceed capacity");
+        build_bundle(cams[b], 0, cams[b].screen_width, row0, nrows, begin, off, table[b]);
+        begin += n;
+    }
+    if (begin == 0) return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "empty bundle table");
+
+    int n_dev = 0;
+    cudaError_t e = cudaGetDeviceCount(&n_dev);
+    if (e != cudaSuccess) return noalloc_cuda_fail(error, error_len, e, "cudaGetDeviceCount");
+    if (device_ordinal < 0 || device_ordinal >= n_dev || device_ordinal >= kNoAllocMaxDevices)
+        return noalloc_fail(error, error_len, RT_ERR_DEVICE, "no such device");
+    if ((e = cudaSetDevice(device_ordinal)) != cudaSuccess) return noalloc_cuda_fail(error, error_len, e, "cudaSetDevice");
+    NoAllocDevice dev;
+    rt_status st = noalloc_setup(device_ordinal, dev, error, error_len);
+    if (st != RT_OK) return st;
+
+    // effective_cfg reads only the handle's launch config
+    rt_handle shape;
+    if (cfg) shape.cfg = *cfg;
+    const rt_launch_config c = effective_cfg(&shape, mixed);
+
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* table_dev = dev.scratch + kNoAllocCounterBytes;
+    // pageable source: the copy is staged before the call returns, after the stream's earlier work
+    if ((e = cudaMemcpyAsync(table_dev, table, sizeof(BundleDesc) * n_bundles, cudaMemcpyHostToDevice, s)) !=
+        cudaSuccess)
+        return noalloc_cuda_fail(error, error_len, e, "bundle table upload");
+    if ((e = cudaMemsetAsync(dev.scratch, 0, kNoAllocCounterBytes, s)) != cudaSuccess)
+        return noalloc_cuda_fail(error, error_len, e, "counter reset");
+    TraceArgs args{};
+    args.bundles = reinterpret_cast<const BundleDesc*>(table_dev);
+    args.n_bundles = n_bundles;
+    args.refill_threshold = c.refill_threshold;
+    args.claim = 32u * c.rays_per_thread;
+    args.total_rays = begin;
+    args.queue = reinterpret_cast<unsigned long long*>(dev.scratch);
+    args.stats = reinterpret_cast<unsigned long long*>(dev.scratch + kNoAllocStatsOffset);
+    args.out = OutPtrs{pixels, rays ? *rays : rt_ray_out{}};
+    const uint32_t grid = static_cast<uint32_t>(dev.sm_count) * c.ctas_per_sm;
+    launch_trace(args, grid, c.block_size, mixed, c.fp64_rolled != 0, s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_cuda_fail(error, error_len, e, "tracer launch");
+    return RT_OK;
+}

@@ -81,7 +81,8 @@ _lib: ctypes.CDLL | None = None
 EXPORTS = ["rt_create", "rt_destroy", "rt_is_ready", "rt_is_platform_supported", "rt_last_error", "rt_abi_version",
            "rt_camera_defaults", "rt_camera_look_at_hole", "rt_dispatch", "rt_dispatch_tile", "rt_dispatch_device",
            "rt_trace_bundles_device", "rt_bundle_rays", "rt_set_launch_config", "rt_get_launch_config",
-           "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak"]
+           "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc"]
+NOALLOC_MAX_BUNDLES = 32  # RT_NOALLOC_MAX_BUNDLES
 
 
 def lib() -> ctypes.CDLL:
@@ -113,6 +114,8 @@ def lib() -> ctypes.CDLL:
         L.rt_get_stats.argtypes = [v, p(Stats)]
         L.rt_synchronize.argtypes = [v, _d]
         L.rt_measure_fma_peak.argtypes = [v, p(_d), p(_d)]
+        L.rt_trace_bundles_noalloc.argtypes = [ctypes.c_int, p(Camera), _u32, v, v, p(RayOut), ctypes.c_size_t,
+                                               p(LaunchConfig), v, ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
     return _lib
 
@@ -281,6 +284,23 @@ class Tracer:
         f64, f32 = _d(), _d()
         self._check(self.lib.rt_measure_fma_peak(self._h, ctypes.byref(f64), ctypes.byref(f32)))
         return f64.value, f32.value
+
+
+def trace_bundles_noalloc(cams: list[Camera], rays: RayOut, pixels_ptr: int | None, capacity: int,
+                          offsets: np.ndarray | None = None, device: int = 0, launch: LaunchConfig | None = None,
+                          stream: int | None = None) -> None:
+    """rt_trace_bundles_noalloc: the bundle trace without a handle and without
+    device allocation (scratch in a static device array); enqueued, no wait."""
+    arr = (Camera * len(cams))(*cams)
+    optr = None
+    if offsets is not None:
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        optr = offsets.ctypes.data
+    err = ctypes.create_string_buffer(256)
+    st = lib().rt_trace_bundles_noalloc(device, arr, len(cams), optr, pixels_ptr, ctypes.byref(rays), capacity,
+                                        ctypes.byref(launch) if launch is not None else None, stream, err, len(err))
+    if st != RT_OK:
+        raise RelsimError(st, err.value.decode())
 
 
 def bundle_rays(cams: list[Camera]) -> int:
