@@ -324,10 +324,11 @@ constexpr double kFp32MaxRadius = 1e6;
 // so the large h p term of every position increment stays FP64 and FP32 only
 // carries the gravitational part.  y5 = y + h p (FP64) + h sum b_j dx_j (FP32).
 // The error estimate uses sum_j e_j = 0: E_x = h sum e_j dx_j.  Outputs k7 in
-// FP64 (FSAL) and |E| per component.
+// FP64 (FSAL), |E| per component, and the FP32 BL radius, H and s of the FSAL
+// stage at y5 (the step's bookkeeping: step cap, termination, projection).
 __device__ __forceinline__ void mixed_stages(const double* __restrict__ y, const double* __restrict__ k1, double hh,
                                              double M, double a, double* __restrict__ y5, double* __restrict__ k7,
-                                             double* __restrict__ est) {
+                                             double* __restrict__ est, float& r7, float& hf7, float& s7) {
     const float h = static_cast<float>(hh);
     const float Mf = static_cast<float>(M), af = static_cast<float>(a);
     float x0[3], p0[3];
@@ -383,7 +384,9 @@ __device__ __forceinline__ void mixed_stages(const double* __restrict__ y, const
     // stage 7 (FSAL) at y5
 #pragma unroll
     for (int i = 0; i < 6; ++i) in[i] = static_cast<float>(y5[i]);
-    ks_rhs<float, true>(in, Mf, af, g, hf, sv);
+    r7 = ks_rhs<float, true>(in, Mf, af, g, hf, sv);
+    hf7 = hf;
+    s7 = sv;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         const float dx7 = static_cast<float>(y5[3 + i] - y[3 + i]) + g[i];
@@ -635,10 +638,13 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
         double r5 = 0.0, hf5 = 0.0, s5 = 0.0;
         const bool root = (mode == MODE_ROOT);
         if (far) {
-            mixed_stages(y, k1, hh, M, a, y5, kA, est);
-            double kf[3];
-            r5 = ks_field64(y5, M, a, kf, hf5);
-            s5 = 1.0 + kf[0] * y5[3] + kf[1] * y5[4] + kf[2] * y5[5];
+            // FP32 radius, H and s of the FSAL stage: the projection then holds
+            // H = 0 to the FP32 stages' own accuracy
+            float r7, hf7, s7;
+            mixed_stages(y, k1, hh, M, a, y5, kA, est, r7, hf7, s7);
+            r5 = r7;
+            hf5 = hf7;
+            s5 = s7;
             if (mode == MODE_STEP) ++n_far;
         } else {
             if constexpr (MIXED) {
@@ -728,9 +734,23 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
             continue;
         }
 
-        // FP64 error norm (rk45_adaptive.hpp:254-261); kA holds k7
+        // error norm (rk45_adaptive.hpp:254-261); kA holds k7.  FP64 in the FP64
+        // mode; FP32 in the mixed mode, whose estimate carries FP32 stages
         double err;
-        {
+        if constexpr (MIXED) {
+            float num = 0.0f, den = 1.0f;
+            const float rtol = static_cast<float>(Bp->rtol), atol = static_cast<float>(Bp->atol);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const float sc = rtol * static_cast<float>(fmax(fabs(y[i]), fabs(y5[i]))) + atol;
+                const float e = static_cast<float>(est[i]);
+                if (e * den > num * sc) {
+                    num = e;
+                    den = sc;
+                }
+            }
+            err = static_cast<double>(num / den);
+        } else {
             double num = 0.0, den = 1.0;
             const double rtol = Bp->rtol, atol = Bp->atol;
 #pragma unroll
