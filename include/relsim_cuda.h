@@ -219,6 +219,67 @@ rt_status rt_synchronize(rt_handle* h, double timeout_ms);
  * from a register-resident FMA-chain kernel.  Roofline denominator. */
 rt_status rt_measure_fma_peak(rt_handle* h, double* fp64_tflops, double* fp32_tflops);
 
+/* ---- Continuous-batching request server ----
+ * Replaces the reference's frame-at-a-time render worker
+ * (GeodesicComputePipeline, geodesic_compute_pipeline.hpp:505-529, which
+ * serialises whole frames on one executor under gpu_mutex_) for a stream of
+ * render requests.  Requests are admitted in arrival order while their output
+ * records fit memory_budget_bytes of device memory, and traced in epochs: one
+ * persistent launch over row chunks taken round-robin from every admitted
+ * request, so a request arriving while others are on the GPU joins the next
+ * epoch.  Records stay on the device until a request's last chunk is done,
+ * then go to the caller's host buffers.  A scheduler thread owned by the server
+ * does all device work; submit and poll may be called from any thread. */
+typedef struct rt_server rt_server;
+
+typedef struct rt_server_config {
+    uint64_t memory_budget_bytes;  /* device bytes for in-flight output records (admission budget) */
+    uint32_t max_requests;         /* waiting + admitted requests; more: RT_ERR_AGAIN */
+    uint32_t chunk_rays;           /* rays a request contributes to one epoch (whole rows, >= 1 row) */
+    uint32_t epoch_rays;           /* rays per epoch launch */
+    uint32_t max_epoch_bundles;    /* row chunks per epoch launch */
+    uint32_t record_mask;          /* bit f: rt_ray_out field f (declaration order) is recorded;
+                                      bit 14: the 32-byte pixels */
+    uint32_t reserved;
+    rt_launch_config launch_fp64;  /* launch shapes; zeros select the defaults */
+    rt_launch_config launch_mixed;
+} rt_server_config;
+
+typedef struct rt_request_done {
+    uint64_t id;
+    uint64_t rays;
+    double latency_ms;  /* submit to records in the caller's host buffers */
+    double queue_ms;    /* submit to the first epoch launch that traces it */
+    rt_status status;
+    uint32_t reserved;
+} rt_request_done;
+
+typedef struct rt_server_stats {
+    uint64_t requests_submitted, requests_done, rays_done;
+    uint64_t epochs, bundles;                  /* launches and row chunks traced */
+    uint64_t bytes_in_use, peak_bytes_in_use;  /* admitted requests' records */
+    uint64_t budget_bytes;                     /* usable budget (whole rays) */
+    uint32_t pending;                          /* waiting + admitted, not yet polled as done */
+    uint32_t peak_active;                      /* most requests admitted at once */
+} rt_server_stats;
+
+/* Defaults: 1 GiB budget, 4096 requests, 2^18-ray chunks, 2^22-ray epochs,
+ * records status, r, theta, phi, r_hit, g and the pixels. */
+void rt_server_config_defaults(rt_server_config* cfg);
+rt_status rt_server_create(rt_server** out, int device_ordinal, const rt_server_config* cfg);
+/* Stops the scheduler; requests not yet done are dropped. */
+void rt_server_destroy(rt_server* s);
+/* Queue one request.  Host buffers (pinned memory overlaps best) must stay valid
+ * until the request is polled as done and may only name recorded fields.
+ * RT_ERR_AGAIN: max_requests reached; RT_ERR_BUDGET: larger than the whole budget. */
+rt_status rt_server_submit(rt_server* s, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
+                           size_t capacity, uint64_t* id);
+/* Up to max_done finished requests, waiting at most timeout_ms for the first. */
+rt_status rt_server_poll(rt_server* s, rt_request_done* done, uint32_t max_done, uint32_t* n_done,
+                         double timeout_ms);
+rt_status rt_server_get_stats(rt_server* s, rt_server_stats* stats);
+const char* rt_server_last_error(const rt_server* s);
+
 /* Allocation-free bundle trace.  No counterpart in the reference: its compute
  * executor always owns its device buffers and grows them on demand.
  *

@@ -22,10 +22,6 @@
 #include "rt_internal.h"
 
 namespace relsim {
-void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled,
-                  cudaStream_t stream);
-int trace_occupancy(uint32_t block, bool mixed, bool rolled);
-uint32_t kernel_block(uint32_t block, bool mixed, bool rolled);
 double measure_fma_peak(bool fp64, int sm_count, cudaStream_t stream, float* ms_out);
 }  // namespace relsim
 
@@ -69,6 +65,7 @@ rt_status fail(rt_handle* h, rt_status st, const std::string& msg) {
 }
 
 rt_status cuda_fail(rt_handle* h, cudaError_t e, const char* where) {
+    cudaGetLastError();  // clear it: a later cudaGetLastError() must not report this call again
     if (h) {
         h->error = std::string(where) + ": " + cudaGetErrorString(e);
         if (e != cudaErrorMemoryAllocation && e != cudaErrorInvalidValue) h->ready = false;
@@ -123,28 +120,14 @@ bool camera_valid(const rt_camera* c) {
            (c->precision_mode == RT_PRECISION_FP64 || c->precision_mode == RT_PRECISION_MIXED);
 }
 
-// Row window of the image (vulkan_compute_executor.hpp:1415-1426).
-void row_window(const rt_camera& c, uint32_t& row0, uint32_t& nrows) {
-    row0 = std::min(c.dispatch_row_offset, c.screen_height);
-    nrows = (c.dispatch_row_count == 0) ? (c.screen_height - row0)
-                                        : std::min(c.dispatch_row_count, c.screen_height - row0);
-}
+rt_launch_config effective_cfg(const rt_handle* h, bool mixed) { return resolve_launch_config(h->cfg, mixed); }
 
-rt_launch_config effective_cfg(const rt_handle* h, bool mixed) {
-    rt_launch_config c = h->cfg;
-    if (c.block_size != 64 && c.block_size != 128 && c.block_size != 256) c.block_size = 128;
-    c.fp64_rolled = c.fp64_rolled ? 1u : 0u;
-    c.block_size = kernel_block(c.block_size, mixed, c.fp64_rolled != 0);
-    const int occ = trace_occupancy(c.block_size, mixed, c.fp64_rolled != 0);
-    if (c.ctas_per_sm == 0 || static_cast<int>(c.ctas_per_sm) > occ) c.ctas_per_sm = std::max(occ, 1);
-    // defaults from the autotuner on B200: whole-warp refills of 32 consecutive rays
-    if (c.refill_threshold == 0 || c.refill_threshold > 32) c.refill_threshold = 32;
-    if (c.rays_per_thread == 0 || c.rays_per_thread > 64) c.rays_per_thread = 1;
-    return c;
-}
-
-// Launch the tracer over `n` bundles already in h->bundles (device).
-rt_status launch(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs& out, bool mixed, cudaStream_t s) {
+// Launch the tracer over `n` bundles already in h->bundles (device).  The
+// timing events bracket the launch unless it is being captured into a graph
+// (an event recorded on a capturing stream only orders the capture; the graph
+// launch is bracketed instead).
+rt_status launch(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs& out, bool mixed, cudaStream_t s,
+                 bool capturing = false) {
     const rt_launch_config c = effective_cfg(h, mixed);
     TraceArgs args{};
     args.bundles = static_cast<const BundleDesc*>(h->bundles.ptr);
@@ -158,11 +141,13 @@ rt_status launch(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs
     RT_CUDA(h, cudaMemsetAsync(h->queue.ptr, 0, sizeof(unsigned long long), s));
     RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
     const uint32_t grid = static_cast<uint32_t>(h->sm_count) * c.ctas_per_sm;
-    RT_CUDA(h, cudaEventRecord(h->ev0, s));
+    if (!capturing) RT_CUDA(h, cudaEventRecord(h->ev0, s));
     launch_trace(args, grid, c.block_size, mixed, c.fp64_rolled != 0, s);
     RT_CUDA(h, cudaGetLastError());
-    RT_CUDA(h, cudaEventRecord(h->ev1, s));
-    h->timed = true;
+    if (!capturing) {
+        RT_CUDA(h, cudaEventRecord(h->ev1, s));
+        h->timed = true;
+    }
     return RT_OK;
 }
 
@@ -462,7 +447,7 @@ rt_status rt_trace_bundles_device(rt_handle* h, const rt_camera* cams, uint32_t 
         RT_CUDA(h, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         cudaError_t e1 = cudaMemcpyAsync(h->bundles.ptr, h->host_bundles, sizeof(BundleDesc) * n_bundles,
                                          cudaMemcpyHostToDevice, s);
-        rt_status ls = (e1 == cudaSuccess) ? launch(h, n_bundles, begin, out, mixed, s) : RT_ERR_DEVICE;
+        rt_status ls = (e1 == cudaSuccess) ? launch(h, n_bundles, begin, out, mixed, s, true) : RT_ERR_DEVICE;
         cudaError_t e2 = cudaStreamEndCapture(s, &g);
         if (e1 != cudaSuccess) return cuda_fail(h, e1, "capture memcpy");
         if (ls != RT_OK) {
@@ -478,7 +463,9 @@ rt_status rt_trace_bundles_device(rt_handle* h, const rt_camera* cams, uint32_t 
         h->graph_out = out;
         h->graph_cfg = c;
     }
+    RT_CUDA(h, cudaEventRecord(h->ev0, s));
     RT_CUDA(h, cudaGraphLaunch(h->graph, s));
+    RT_CUDA(h, cudaEventRecord(h->ev1, s));
     h->timed = true;
     return RT_OK;
 }

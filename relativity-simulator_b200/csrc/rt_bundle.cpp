@@ -131,4 +131,10 @@ void build_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t 
               (cam.precision_mode == RT_PRECISION_MIXED ? BF_MIXED : 0u);
 }
 
+void row_window(const rt_camera& c, uint32_t& row0, uint32_t& nrows) {
+    row0 = std::min(c.dispatch_row_offset, c.screen_height);
+    nrows = (c.dispatch_row_count == 0) ? (c.screen_height - row0)
+                                        : std::min(c.dispatch_row_count, c.screen_height - row0);
+}
+
 }  // namespace relsim

@@ -72,5 +72,15 @@ struct TraceArgs {
 void build_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
                   uint64_t ray_begin, uint64_t out_offset, BundleDesc& b);
 double kerr_isco_radius(double m, double a);
+// Row window of a camera (vulkan_compute_executor.hpp:1415-1426): first row and
+// row count; count 0 in the camera means every row from the offset on.
+void row_window(const rt_camera& c, uint32_t& row0, uint32_t& nrows);
+
+// Tracer launch helpers implemented in rt_trace.cu.
+void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled, void* stream);
+int trace_occupancy(uint32_t block, bool mixed, bool rolled);
+uint32_t kernel_block(uint32_t block, bool mixed, bool rolled);
+// Launch shape with defaults filled in and limits applied for one precision.
+rt_launch_config resolve_launch_config(rt_launch_config c, bool mixed);
 
 }  // namespace relsim

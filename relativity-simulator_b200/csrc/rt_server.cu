@@ -1,0 +1,558 @@
+// rt_server.cu -- continuous-batching request server (include/relsim_cuda.h, rt_server_*).
+//
+// Render requests (one camera each) are admitted in arrival order while their
+// output records fit a device-memory budget, and are traced in "epochs": one
+// persistent tracer launch over a bundle table of row chunks taken round-robin
+// from every admitted request with rows left, so a request that arrives while
+// others are on the GPU joins the next epoch instead of waiting for them to
+// finish.  Two epoch slots on separate streams keep the GPU busy while the
+// scheduler retires one epoch and builds the next (the tail of one launch
+// overlaps the start of the other).  Output records stay on the device, in a
+// budget-sized arena, until a request's last chunk is done; then they are copied
+// to the caller's host buffers on a copy stream and the arena range is freed.
+//
+// Reference counterpart: the render worker of GeodesicComputePipeline
+// (geodesic_compute_pipeline.hpp:505-529) serialises whole frames on one
+// executor; there is no request admission or batching in the reference.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "relsim_cuda.h"
+#include "rt_internal.h"
+
+using namespace relsim;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+constexpr int kFields = 14;                                          // rt_ray_out fields
+constexpr size_t kFieldBytes[kFields] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
+constexpr uint32_t kPixelBit = 1u << 14;                             // record_mask bit of the pixels
+constexpr int kSlots = 2;                                            // epochs in flight
+
+// First-fit allocator over ray slots [0, capacity) of the output arena.
+class RangeAllocator {
+public:
+    explicit RangeAllocator(uint64_t capacity = 0) { reset(capacity); }
+    void reset(uint64_t capacity) {
+        free_.clear();
+        if (capacity) free_[0] = capacity;
+        used_ = 0;
+    }
+    bool alloc(uint64_t n, uint64_t& base) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < n) continue;
+            base = it->first;
+            const uint64_t rest = it->second - n;
+            free_.erase(it);
+            if (rest) free_[base + n] = rest;
+            used_ += n;
+            return true;
+        }
+        return false;
+    }
+    void release(uint64_t base, uint64_t n) {
+        used_ -= n;
+        auto it = free_.emplace(base, n).first;
+        auto next = std::next(it);
+        if (next != free_.end() && it->first + it->second == next->first) {
+            it->second += next->second;
+            free_.erase(next);
+        }
+        if (it != free_.begin()) {
+            auto prev = std::prev(it);
+            if (prev->first + prev->second == it->first) {
+                prev->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    uint64_t used() const { return used_; }
+
+private:
+    std::map<uint64_t, uint64_t> free_;  // base -> length
+    uint64_t used_ = 0;
+};
+
+enum class ReqState { Waiting, Active, Copying, Done };
+
+struct Request {
+    uint64_t id = 0;
+    rt_camera cam{};
+    uint32_t row0 = 0, nrows = 0, width = 0;
+    uint64_t rays = 0;
+    rt_pixel_out* host_pixels = nullptr;
+    rt_ray_out host_rays{};
+    ReqState state = ReqState::Waiting;
+    uint64_t base = 0;            // arena ray slot of the request's first ray
+    uint32_t rows_issued = 0;     // rows put into an epoch
+    uint64_t rays_done = 0;       // rays of finished epochs
+    cudaEvent_t copy_done = nullptr;
+    Clock::time_point t_submit, t_admit, t_first_launch, t_done;
+    bool launched = false;
+    bool admitted = false;        // holds an arena range
+    rt_status status = RT_OK;
+};
+
+struct Chunk {
+    Request* req;
+    uint64_t rays;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    BundleDesc* host_table = nullptr;   // pinned staging of the bundle table
+    BundleDesc* dev_table = nullptr;
+    unsigned long long* counters = nullptr;  // [0] queue, [8..] stats
+    std::vector<Chunk> chunks;
+    bool busy = false;
+};
+
+}  // namespace
+
+struct rt_server {
+    int device = 0;
+    int sm_count = 0;
+    rt_server_config cfg{};
+    uint32_t bytes_per_ray = 0;
+    uint64_t arena_rays = 0;
+    void* arena = nullptr;
+    void* field_base[kFields] = {};
+    rt_pixel_out* pixel_base = nullptr;
+    RangeAllocator alloc;
+    Slot slots[kSlots];
+    cudaStream_t copy_stream = nullptr;
+
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> waiting;
+    std::vector<Request*> active;           // admitted, not yet done
+    std::deque<rt_request_done> completed;  // not yet polled
+    uint64_t next_id = 1;
+    bool stop = false;
+    bool failed = false;
+    std::string error;
+    rt_server_stats stats{};
+    std::thread worker;
+    size_t rr = 0;  // round-robin start in `active`
+};
+
+namespace {
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+void fail_server(rt_server* s, const char* where, cudaError_t e) {
+    s->failed = true;
+    s->error = std::string(where) + ": " + cudaGetErrorString(e);
+}
+
+// Finish a request (lock held): record, free its arena range, publish.
+void complete(rt_server* s, Request* r, rt_status st) {
+    r->t_done = Clock::now();
+    r->state = ReqState::Done;
+    r->status = st;
+    if (r->copy_done) cudaEventDestroy(r->copy_done);
+    r->copy_done = nullptr;
+    if (r->admitted) s->alloc.release(r->base, r->rays);
+    rt_request_done d{};
+    d.id = r->id;
+    d.status = st;
+    d.rays = r->rays;
+    d.queue_ms = ms_between(r->t_submit, r->launched ? r->t_first_launch : r->t_done);
+    d.latency_ms = ms_between(r->t_submit, r->t_done);
+    s->completed.push_back(d);
+    ++s->stats.requests_done;
+    s->stats.rays_done += r->rays;
+    s->active.erase(std::remove(s->active.begin(), s->active.end(), r), s->active.end());
+    delete r;
+    s->cv_done.notify_all();
+}
+
+// Admit waiting requests in arrival order while the arena has room (lock held).
+void admit(rt_server* s) {
+    while (!s->waiting.empty()) {
+        Request* r = s->waiting.front();
+        uint64_t base = 0;
+        if (!s->alloc.alloc(r->rays, base)) break;  // FIFO: later requests wait behind it
+        s->waiting.pop_front();
+        r->base = base;
+        r->admitted = true;
+        r->state = ReqState::Active;
+        r->t_admit = Clock::now();
+        s->active.push_back(r);
+        const uint64_t used = s->alloc.used() * s->bytes_per_ray;
+        s->stats.peak_bytes_in_use = std::max<uint64_t>(s->stats.peak_bytes_in_use, used);
+        s->stats.peak_active = std::max<uint32_t>(s->stats.peak_active, static_cast<uint32_t>(s->active.size()));
+    }
+}
+
+// Copy a finished request's records to the caller's host buffers (lock held).
+bool start_copy(rt_server* s, Request* r) {
+    cudaStream_t cs = s->copy_stream;
+    void* const* hp = reinterpret_cast<void* const*>(&r->host_rays);
+    for (int f = 0; f < kFields; ++f) {
+        if (!hp[f]) continue;
+        const char* src = static_cast<const char*>(s->field_base[f]) + r->base * kFieldBytes[f];
+        cudaError_t e = cudaMemcpyAsync(hp[f], src, r->rays * kFieldBytes[f], cudaMemcpyDeviceToHost, cs);
+        if (e != cudaSuccess) return fail_server(s, "cudaMemcpyAsync", e), false;
+    }
+    if (r->host_pixels) {
+        cudaError_t e = cudaMemcpyAsync(r->host_pixels, s->pixel_base + r->base, r->rays * sizeof(rt_pixel_out),
+                                        cudaMemcpyDeviceToHost, cs);
+        if (e != cudaSuccess) return fail_server(s, "cudaMemcpyAsync", e), false;
+    }
+    cudaError_t e = cudaEventCreateWithFlags(&r->copy_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(r->copy_done, cs);
+    if (e != cudaSuccess) return fail_server(s, "cudaEventRecord", e), false;
+    r->state = ReqState::Copying;
+    return true;
+}
+
+// Build and launch one epoch into a free slot (lock held).  Returns false when
+// there is nothing to trace.
+bool launch_epoch(rt_server* s, Slot& slot) {
+    // precision of this epoch: that of the oldest active request with rows left
+    int precision = -1;
+    for (Request* r : s->active)
+        if (r->state == ReqState::Active && r->rows_issued < r->nrows) {
+            precision = static_cast<int>(r->cam.precision_mode);
+            break;
+        }
+    if (precision < 0) return false;
+    const bool mixed = precision == RT_PRECISION_MIXED;
+    slot.chunks.clear();
+    uint64_t total = 0;
+    uint32_t nb = 0;
+    const size_t n_active = s->active.size();
+    // round robin over active requests: each gets up to chunk_rays per epoch
+    bool progress = true;
+    while (progress && total < s->cfg.epoch_rays && nb < s->cfg.max_epoch_bundles) {
+        progress = false;
+        for (size_t k = 0; k < n_active && total < s->cfg.epoch_rays && nb < s->cfg.max_epoch_bundles; ++k) {
+            Request* r = s->active[(s->rr + k) % n_active];
+            if (r->state != ReqState::Active || r->rows_issued >= r->nrows) continue;
+            if (static_cast<int>(r->cam.precision_mode) != precision) continue;
+            const uint64_t budget = std::min<uint64_t>(s->cfg.chunk_rays, s->cfg.epoch_rays - total);
+            uint32_t rows = static_cast<uint32_t>(std::max<uint64_t>(1, budget / r->width));
+            rows = std::min(rows, r->nrows - r->rows_issued);
+            const uint64_t n = static_cast<uint64_t>(rows) * r->width;
+            build_bundle(r->cam, 0, r->width, r->row0 + r->rows_issued, rows, total,
+                         r->base + static_cast<uint64_t>(r->rows_issued) * r->width, slot.host_table[nb]);
+            if (!r->launched) {
+                r->launched = true;
+                r->t_first_launch = Clock::now();
+            }
+            r->rows_issued += rows;
+            slot.chunks.push_back({r, n});
+            total += n;
+            ++nb;
+            progress = true;
+        }
+    }
+    s->rr = n_active ? (s->rr + 1) % n_active : 0;
+    if (nb == 0) return false;
+    cudaStream_t st = slot.stream;
+    // the staging table was last read by this slot's previous epoch, which is retired
+    cudaError_t e = cudaMemcpyAsync(slot.dev_table, slot.host_table, sizeof(BundleDesc) * nb,
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(slot.counters, 0, 256, st);
+    if (e != cudaSuccess) return fail_server(s, "epoch upload", e), false;
+    const rt_launch_config c = resolve_launch_config(mixed ? s->cfg.launch_mixed : s->cfg.launch_fp64, mixed);
+    TraceArgs args{};
+    args.bundles = slot.dev_table;
+    args.n_bundles = nb;
+    args.refill_threshold = c.refill_threshold;
+    args.claim = 32u * c.rays_per_thread;
+    args.total_rays = total;
+    args.queue = slot.counters;
+    args.stats = slot.counters + 8;
+    rt_ray_out rays{};
+    void** dp = reinterpret_cast<void**>(&rays);
+    for (int f = 0; f < kFields; ++f)
+        if (s->cfg.record_mask & (1u << f)) dp[f] = s->field_base[f];
+    args.out = OutPtrs{(s->cfg.record_mask & kPixelBit) ? s->pixel_base : nullptr, rays};
+    launch_trace(args, static_cast<uint32_t>(s->sm_count) * c.ctas_per_sm, c.block_size, mixed,
+                 c.fp64_rolled != 0, st);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(slot.done, st);
+    if (e != cudaSuccess) return fail_server(s, "epoch launch", e), false;
+    slot.busy = true;
+    ++s->stats.epochs;
+    s->stats.bundles += nb;
+    return true;
+}
+
+void worker_main(rt_server* s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stop) {
+        bool did = false;
+        if (!s->failed) {
+            admit(s);
+            // retire finished epochs
+            for (Slot& slot : s->slots) {
+                if (!slot.busy) continue;
+                const cudaError_t q = cudaEventQuery(slot.done);
+                if (q == cudaErrorNotReady) continue;
+                if (q != cudaSuccess) {
+                    fail_server(s, "epoch", q);
+                    break;
+                }
+                slot.busy = false;
+                did = true;
+                for (const Chunk& c : slot.chunks) {
+                    c.req->rays_done += c.rays;
+                    if (c.req->rays_done == c.req->rays && c.req->state == ReqState::Active) start_copy(s, c.req);
+                }
+                slot.chunks.clear();
+            }
+            // retire finished copies
+            for (size_t i = 0; i < s->active.size();) {
+                Request* r = s->active[i];
+                if (r->state == ReqState::Copying) {
+                    const cudaError_t q = cudaEventQuery(r->copy_done);
+                    if (q == cudaSuccess) {
+                        complete(s, r, RT_OK);
+                        did = true;
+                        continue;
+                    }
+                    if (q != cudaErrorNotReady) {
+                        fail_server(s, "copy", q);
+                        break;
+                    }
+                }
+                ++i;
+            }
+            admit(s);
+            for (Slot& slot : s->slots)
+                if (!slot.busy && !s->failed && launch_epoch(s, slot)) did = true;
+        }
+        if (s->failed) {
+            // end every request with the device error; the server stays failed
+            while (!s->waiting.empty()) {
+                Request* r = s->waiting.front();
+                s->waiting.pop_front();
+                s->active.push_back(r);
+                r->state = ReqState::Active;
+            }
+            while (!s->active.empty()) complete(s, s->active.front(), RT_ERR_DEVICE);
+            s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            continue;
+        }
+        if (!did) {
+            bool busy = false;
+            for (const Slot& slot : s->slots) busy = busy || slot.busy;
+            for (Request* r : s->active) busy = busy || r->state == ReqState::Copying;
+            // short waits while the GPU works; sleep until a submission when idle
+            if (busy) s->cv_work.wait_for(lk, std::chrono::microseconds(100));
+            else s->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+        }
+    }
+}
+
+bool record_fields_ok(const rt_server* s, const rt_ray_out* rays, const rt_pixel_out* pixels) {
+    if (pixels && !(s->cfg.record_mask & kPixelBit)) return false;
+    if (!rays) return true;
+    void* const* hp = reinterpret_cast<void* const*>(rays);
+    for (int f = 0; f < kFields; ++f)
+        if (hp[f] && !(s->cfg.record_mask & (1u << f))) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void rt_server_config_defaults(rt_server_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof *c);
+    c->memory_budget_bytes = uint64_t{1} << 30;
+    c->max_requests = 4096;
+    c->chunk_rays = 1u << 18;
+    c->epoch_rays = 1u << 22;
+    c->max_epoch_bundles = 4096;
+    // class, final position, disk radius and g, plus the 32-byte pixels
+    c->record_mask = (1u << 0) | (1u << 4) | (1u << 5) | (1u << 6) | (1u << 7) | (1u << 8) | kPixelBit;
+}
+
+rt_status rt_server_create(rt_server** out, int device_ordinal, const rt_server_config* cfg) {
+    if (!out || !cfg) return RT_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (cfg->chunk_rays == 0 || cfg->epoch_rays == 0 || cfg->max_epoch_bundles == 0 || cfg->max_requests == 0 ||
+        (cfg->record_mask & ~((kPixelBit << 1) - 1u)) != 0)
+        return RT_ERR_INVALID_ARG;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device_ordinal < 0 || device_ordinal >= n) {
+        cudaGetLastError();
+        return RT_ERR_DEVICE;
+    }
+    cudaDeviceProp p{};
+    if (cudaGetDeviceProperties(&p, device_ordinal) != cudaSuccess || p.major != 10 || p.minor != 0)
+        return RT_ERR_DEVICE;
+    if (cudaSetDevice(device_ordinal) != cudaSuccess) return RT_ERR_DEVICE;
+    rt_server* s = new (std::nothrow) rt_server();
+    if (!s) return RT_ERR_OOM;
+    s->device = device_ordinal;
+    s->sm_count = p.multiProcessorCount;
+    s->cfg = *cfg;
+    uint32_t bpr = (cfg->record_mask & kPixelBit) ? sizeof(rt_pixel_out) : 0;
+    for (int f = 0; f < kFields; ++f)
+        if (cfg->record_mask & (1u << f)) bpr += static_cast<uint32_t>(kFieldBytes[f]);
+    s->bytes_per_ray = std::max<uint32_t>(bpr, 1);
+    // arena: one allocation, one SoA array per recorded field, each 256-byte aligned
+    s->arena_rays = cfg->memory_budget_bytes / s->bytes_per_ray;
+    if (s->arena_rays < 32) {
+        delete s;
+        return RT_ERR_BUDGET;
+    }
+    s->arena_rays &= ~uint64_t{31};
+    size_t bytes = 0;
+    size_t offs[kFields + 1] = {};
+    for (int f = 0; f <= kFields; ++f) {
+        const bool on = (f < kFields) ? (cfg->record_mask & (1u << f)) != 0 : (cfg->record_mask & kPixelBit) != 0;
+        offs[f] = bytes;
+        if (on) bytes += ((s->arena_rays * ((f < kFields) ? kFieldBytes[f] : sizeof(rt_pixel_out)) + 255) / 256) * 256;
+    }
+    cudaError_t e = cudaMalloc(&s->arena, std::max<size_t>(bytes, 256));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return RT_ERR_OOM;
+    }
+    for (int f = 0; f < kFields; ++f)
+        if (cfg->record_mask & (1u << f)) s->field_base[f] = static_cast<char*>(s->arena) + offs[f];
+    if (cfg->record_mask & kPixelBit) s->pixel_base = reinterpret_cast<rt_pixel_out*>(static_cast<char*>(s->arena) + offs[kFields]);
+    s->alloc.reset(s->arena_rays);
+    bool ok = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) == cudaSuccess;
+    for (Slot& slot : s->slots) {
+        ok = ok && cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking) == cudaSuccess;
+        ok = ok && cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming) == cudaSuccess;
+        ok = ok && cudaMallocHost(&slot.host_table, sizeof(BundleDesc) * cfg->max_epoch_bundles) == cudaSuccess;
+        ok = ok && cudaMalloc(&slot.dev_table, sizeof(BundleDesc) * cfg->max_epoch_bundles) == cudaSuccess;
+        ok = ok && cudaMalloc(&slot.counters, 256) == cudaSuccess;
+    }
+    if (!ok) {
+        cudaGetLastError();
+        rt_server_destroy(s);
+        return RT_ERR_DEVICE;
+    }
+    s->worker = std::thread(worker_main, s);
+    *out = s;
+    return RT_OK;
+}
+
+void rt_server_destroy(rt_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->device);
+    for (Slot& slot : s->slots) {
+        if (slot.stream) cudaStreamSynchronize(slot.stream);
+        if (slot.done) cudaEventDestroy(slot.done);
+        if (slot.host_table) cudaFreeHost(slot.host_table);
+        if (slot.dev_table) cudaFree(slot.dev_table);
+        if (slot.counters) cudaFree(slot.counters);
+        if (slot.stream) cudaStreamDestroy(slot.stream);
+    }
+    if (s->copy_stream) {
+        cudaStreamSynchronize(s->copy_stream);
+        cudaStreamDestroy(s->copy_stream);
+    }
+    for (Request* r : s->waiting) delete r;
+    for (Request* r : s->active) {
+        if (r->copy_done) cudaEventDestroy(r->copy_done);
+        delete r;
+    }
+    if (s->arena) cudaFree(s->arena);
+    delete s;
+}
+
+rt_status rt_server_submit(rt_server* s, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
+                           size_t capacity, uint64_t* id) {
+    if (!s || !cam || !id) return RT_ERR_INVALID_ARG;
+    *id = 0;
+    if (cam->screen_width == 0 || cam->screen_height == 0 || cam->rtol <= 0.0 ||
+        (cam->precision_mode != RT_PRECISION_FP64 && cam->precision_mode != RT_PRECISION_MIXED))
+        return RT_ERR_INVALID_ARG;
+    if (!record_fields_ok(s, rays, pixels)) return RT_ERR_INVALID_ARG;
+    uint32_t row0, nrows;
+    row_window(*cam, row0, nrows);
+    const uint64_t n = static_cast<uint64_t>(cam->screen_width) * nrows;
+    if (n == 0 || capacity < n) return RT_ERR_INVALID_ARG;
+    if (n > s->arena_rays) return RT_ERR_BUDGET;  // could never be admitted
+    Request* r = new (std::nothrow) Request();
+    if (!r) return RT_ERR_OOM;
+    r->cam = *cam;
+    r->row0 = row0;
+    r->nrows = nrows;
+    r->width = cam->screen_width;
+    r->rays = n;
+    r->host_pixels = pixels;
+    if (rays) r->host_rays = *rays;
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->failed) {
+            delete r;
+            return RT_ERR_DEVICE;
+        }
+        if (s->waiting.size() + s->active.size() >= s->cfg.max_requests) {
+            delete r;
+            return RT_ERR_AGAIN;
+        }
+        r->id = s->next_id++;
+        *id = r->id;
+        s->waiting.push_back(r);
+        ++s->stats.requests_submitted;
+    }
+    s->cv_work.notify_all();
+    return RT_OK;
+}
+
+rt_status rt_server_poll(rt_server* s, rt_request_done* done, uint32_t max_done, uint32_t* n_done,
+                         double timeout_ms) {
+    if (!s || !n_done || (max_done > 0 && !done)) return RT_ERR_INVALID_ARG;
+    *n_done = 0;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->completed.empty() && timeout_ms > 0.0)
+        s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms),
+                            [s] { return !s->completed.empty(); });
+    while (*n_done < max_done && !s->completed.empty()) {
+        done[(*n_done)++] = s->completed.front();
+        s->completed.pop_front();
+    }
+    return RT_OK;
+}
+
+rt_status rt_server_get_stats(rt_server* s, rt_server_stats* out) {
+    if (!s || !out) return RT_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    *out = s->stats;
+    out->pending = static_cast<uint32_t>(s->waiting.size() + s->active.size());
+    out->bytes_in_use = s->alloc.used() * s->bytes_per_ray;
+    out->budget_bytes = s->arena_rays * s->bytes_per_ray;
+    return RT_OK;
+}
+
+const char* rt_server_last_error(const rt_server* s) { return s ? s->error.c_str() : "null server"; }
+
+}  // extern "C"

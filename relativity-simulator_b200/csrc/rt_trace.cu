@@ -959,11 +959,23 @@ int trace_occupancy(uint32_t block, bool mixed, bool rolled) {
     return n;
 }
 
-void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled,
-                  cudaStream_t stream) {
+void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled, void* stream) {
     void* params[] = {const_cast<TraceArgs*>(&args)};
     block = kernel_block(block, mixed, rolled);
-    cudaLaunchKernel(kernel_for(block, mixed, rolled), dim3(grid), dim3(block), params, 0, stream);
+    cudaLaunchKernel(kernel_for(block, mixed, rolled), dim3(grid), dim3(block), params, 0,
+                     static_cast<cudaStream_t>(stream));
+}
+
+rt_launch_config resolve_launch_config(rt_launch_config c, bool mixed) {
+    if (c.block_size != 64 && c.block_size != 128 && c.block_size != 256) c.block_size = 128;
+    c.fp64_rolled = c.fp64_rolled ? 1u : 0u;
+    c.block_size = kernel_block(c.block_size, mixed, c.fp64_rolled != 0);
+    const int occ = trace_occupancy(c.block_size, mixed, c.fp64_rolled != 0);
+    if (c.ctas_per_sm == 0 || static_cast<int>(c.ctas_per_sm) > occ) c.ctas_per_sm = occ > 1 ? occ : 1;
+    // defaults from the autotuner on B200: whole-warp refills of 32 consecutive rays
+    if (c.refill_threshold == 0 || c.refill_threshold > 32) c.refill_threshold = 32;
+    if (c.rays_per_thread == 0 || c.rays_per_thread > 64) c.rays_per_thread = 1;
+    return c;
 }
 
 }  // namespace relsim

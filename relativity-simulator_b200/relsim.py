@@ -76,12 +76,38 @@ class Stats(ctypes.Structure):
                 ("rhs_evals", ctypes.c_uint64), ("fp64_attempts", ctypes.c_uint64), ("kernel_ms", _d)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("memory_budget_bytes", ctypes.c_uint64), ("max_requests", _u32), ("chunk_rays", _u32),
+                ("epoch_rays", _u32), ("max_epoch_bundles", _u32), ("record_mask", _u32), ("reserved", _u32),
+                ("launch_fp64", LaunchConfig), ("launch_mixed", LaunchConfig)]
+
+
+class RequestDone(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("rays", ctypes.c_uint64), ("latency_ms", _d), ("queue_ms", _d),
+                ("status", ctypes.c_int), ("reserved", _u32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("requests_submitted", ctypes.c_uint64), ("requests_done", ctypes.c_uint64),
+                ("rays_done", ctypes.c_uint64), ("epochs", ctypes.c_uint64), ("bundles", ctypes.c_uint64),
+                ("bytes_in_use", ctypes.c_uint64), ("peak_bytes_in_use", ctypes.c_uint64),
+                ("budget_bytes", ctypes.c_uint64), ("pending", _u32), ("peak_active", _u32)]
+
+
+# record_mask bits: rt_ray_out fields in declaration order, then the pixels
+RECORD_BIT = {name: 1 << i for i, (name, _) in enumerate(
+    [("status", 0), ("flags", 0), ("steps_accepted", 0), ("steps_rejected", 0), ("r", 0), ("theta", 0),
+     ("phi", 0), ("r_hit", 0), ("g", 0), ("lambda", 0), ("dH", 0), ("dE", 0), ("dLz", 0), ("dQ", 0)])}
+RECORD_BIT["pixels"] = 1 << 14
+
 _lib: ctypes.CDLL | None = None
 
 EXPORTS = ["rt_create", "rt_destroy", "rt_is_ready", "rt_is_platform_supported", "rt_last_error", "rt_abi_version",
            "rt_camera_defaults", "rt_camera_look_at_hole", "rt_dispatch", "rt_dispatch_tile", "rt_dispatch_device",
            "rt_trace_bundles_device", "rt_bundle_rays", "rt_set_launch_config", "rt_get_launch_config",
-           "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc"]
+           "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc",
+           "rt_server_config_defaults", "rt_server_create", "rt_server_destroy", "rt_server_submit",
+           "rt_server_poll", "rt_server_get_stats", "rt_server_last_error"]
 NOALLOC_MAX_BUNDLES = 32  # RT_NOALLOC_MAX_BUNDLES
 
 
@@ -114,6 +140,16 @@ def lib() -> ctypes.CDLL:
         L.rt_get_stats.argtypes = [v, p(Stats)]
         L.rt_synchronize.argtypes = [v, _d]
         L.rt_measure_fma_peak.argtypes = [v, p(_d), p(_d)]
+        L.rt_server_config_defaults.argtypes = [p(ServerConfig)]
+        L.rt_server_config_defaults.restype = None
+        L.rt_server_create.argtypes = [p(ctypes.c_void_p), ctypes.c_int, p(ServerConfig)]
+        L.rt_server_destroy.argtypes = [v]
+        L.rt_server_destroy.restype = None
+        L.rt_server_submit.argtypes = [v, p(Camera), v, p(RayOut), ctypes.c_size_t, p(ctypes.c_uint64)]
+        L.rt_server_poll.argtypes = [v, p(RequestDone), _u32, p(_u32), _d]
+        L.rt_server_get_stats.argtypes = [v, p(ServerStats)]
+        L.rt_server_last_error.argtypes = [v]
+        L.rt_server_last_error.restype = ctypes.c_char_p
         L.rt_trace_bundles_noalloc.argtypes = [ctypes.c_int, p(Camera), _u32, v, v, p(RayOut), ctypes.c_size_t,
                                                p(LaunchConfig), v, ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
@@ -301,6 +337,104 @@ def trace_bundles_noalloc(cams: list[Camera], rays: RayOut, pixels_ptr: int | No
                                         ctypes.byref(launch) if launch is not None else None, stream, err, len(err))
     if st != RT_OK:
         raise RelsimError(st, err.value.decode())
+
+
+def server_config(budget_bytes: int | None = None, record: Iterable[str] | None = None, **kw) -> ServerConfig:
+    """rt_server_config with the library defaults, overridden by keyword (field names)."""
+    c = ServerConfig()
+    lib().rt_server_config_defaults(ctypes.byref(c))
+    if budget_bytes is not None:
+        c.memory_budget_bytes = int(budget_bytes)
+    if record is not None:
+        c.record_mask = sum(RECORD_BIT[f] for f in set(record))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+class Server:
+    """Continuous-batching request server (rt_server_*): submit cameras with host
+    output buffers, poll finished requests.  The host buffers are kept alive here
+    until their request is polled as done."""
+
+    def __init__(self, device: int = 0, config: ServerConfig | None = None):
+        L = lib()
+        self.lib = L
+        self.config = config if config is not None else server_config()
+        h = ctypes.c_void_p()
+        st = L.rt_server_create(ctypes.byref(h), device, ctypes.byref(self.config))
+        if st != RT_OK:
+            raise RelsimError(st, f"rt_server_create(device={device}) failed")
+        self._h = h
+        self._keep: dict[int, dict] = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.rt_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, cam: Camera, fields: Iterable[str] = ("status", "r_hit", "g"), pixels: bool = False,
+               out: dict | None = None) -> tuple[int, dict]:
+        """Queue a request; returns (id, host arrays that receive the records).
+        Raises RelsimError with status AGAIN when the queue is full."""
+        n = window_rays(cam)
+        if out is None:
+            out = {name: np.empty(n, dtype=dt) for name, dt in RAY_FIELDS if name in set(fields)}
+            if pixels:
+                out["pixels"] = np.empty(n, dtype=PIXEL_DTYPE)
+        ro = RayOut()
+        for name, arr in out.items():
+            if name != "pixels":
+                setattr(ro, name, arr.ctypes.data)
+        pptr = out["pixels"].ctypes.data if "pixels" in out else None
+        rid = ctypes.c_uint64()
+        st = self.lib.rt_server_submit(self._h, ctypes.byref(cam), pptr, ctypes.byref(ro), n, ctypes.byref(rid))
+        if st != RT_OK:
+            raise RelsimError(st, self.lib.rt_server_last_error(self._h).decode() or "rt_server_submit")
+        self._keep[rid.value] = out
+        return rid.value, out
+
+    def poll(self, timeout_ms: float = 0.0, max_done: int = 256) -> list[RequestDone]:
+        buf = (RequestDone * max_done)()
+        n = _u32()
+        st = self.lib.rt_server_poll(self._h, buf, max_done, ctypes.byref(n), timeout_ms)
+        if st != RT_OK:
+            raise RelsimError(st, "rt_server_poll")
+        done = [buf[i] for i in range(n.value)]
+        for d in done:
+            self._keep.pop(d.id, None)
+        return done
+
+    def stats(self) -> ServerStats:
+        s = ServerStats()
+        st = self.lib.rt_server_get_stats(self._h, ctypes.byref(s))
+        if st != RT_OK:
+            raise RelsimError(st, "rt_server_get_stats")
+        return s
+
+    def wait(self, ids: Iterable[int], timeout_s: float = 60.0) -> dict[int, RequestDone]:
+        """Poll until every id is done (or raise TimeoutError)."""
+        import time
+
+        want = set(ids)
+        got: dict[int, RequestDone] = {}
+        t_end = time.monotonic() + timeout_s
+        while want - set(got):
+            if time.monotonic() > t_end:
+                raise TimeoutError(f"{len(want - set(got))} requests not done")
+            for d in self.poll(timeout_ms=50.0):
+                got[d.id] = d
+        return got
 
 
 def bundle_rays(cams: list[Camera]) -> int:

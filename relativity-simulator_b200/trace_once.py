@@ -32,6 +32,9 @@ def main() -> None:
     ap.add_argument("--fp64-rolled", type=int, default=0)
     ap.add_argument("--rtol", type=float, default=None)
     ap.add_argument("--fp64-radius", type=float, default=0.0)
+    ap.add_argument("--record", choices=["minimal", "bench"], default="minimal",
+                    help="outputs written: class and step counts, or the bench's record (class, r, theta, "
+                         "phi, r_hit, g) plus the 32-byte pixels")
     a = ap.parse_args()
     cam = relsim.make_camera(spin=a.spin, r_obs=a.r_obs, incl_deg=a.incl, fov_deg=a.fov, width=a.side,
                              height=a.side,
@@ -40,7 +43,10 @@ def main() -> None:
     with relsim.Tracer(0) as tr:
         tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread, a.fp64_rolled)
         for _ in range(a.repeat):
-            out = tr.dispatch(cam, fields=["status", "steps_accepted", "steps_rejected"], pixels=False)
+            if a.record == "bench":
+                out = tr.dispatch(cam, fields=["status", "r", "theta", "phi", "r_hit", "g"], pixels=True)
+            else:
+                out = tr.dispatch(cam, fields=["status", "steps_accepted", "steps_rejected"], pixels=False)
             s = tr.stats()
     print(json.dumps({"rays": int(s.rays), "attempts": int(s.attempts), "accepted": int(s.accepted),
                       "fp64_attempts": int(s.fp64_attempts),

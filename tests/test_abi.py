@@ -48,6 +48,32 @@ def test_layouts_match_header(tmp_path):
     assert relsim.PIXEL_DTYPE.itemsize == 32
 
 
+def test_server_layouts_match_header(tmp_path):
+    prog = tmp_path / "srv.c"
+    prog.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "relsim_cuda.h"\nint main(void){'
+                    'printf("%zu %zu %zu %zu %zu\\n", sizeof(rt_server_config), sizeof(rt_request_done),'
+                    ' sizeof(rt_server_stats), offsetof(rt_server_config, launch_mixed),'
+                    ' offsetof(rt_request_done, status)); return 0;}\n')
+    exe = tmp_path / "srv"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    exp = [ctypes.sizeof(relsim.ServerConfig), ctypes.sizeof(relsim.RequestDone), ctypes.sizeof(relsim.ServerStats),
+           relsim.ServerConfig.launch_mixed.offset, relsim.RequestDone.status.offset]
+    assert got == exp
+
+
+def test_server_config_defaults_and_no_device():
+    c = relsim.server_config()
+    assert c.memory_budget_bytes == 1 << 30 and c.chunk_rays == 1 << 18 and c.epoch_rays == 1 << 22
+    assert c.record_mask == sum(relsim.RECORD_BIT[f] for f in ("status", "r", "theta", "phi", "r_hit", "g", "pixels"))
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(relsim.RelsimError) as e:
+        relsim.Server(0, c)
+    assert e.value.status == 4  # DEVICE: no CPU fallback
+
+
 def test_host_only_entry_points():
     L = relsim.lib()
     assert L.rt_abi_version() == 1

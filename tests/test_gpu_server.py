@@ -1,0 +1,130 @@
+"""Continuous-batching request server (rt_server_*) on the GPU.
+
+  - records equal a direct trace of the same camera (rt_dispatch);
+  - a request's records are the same alone and inside a mix of concurrent
+    requests of other sizes and both precisions (rays never share a warp with
+    another request's rays: row chunks of widths that are multiples of 32 start
+    on warp boundaries, so even the mixed mode's warp-uniform precision choice
+    repeats; bit-identical);
+  - admission holds the device-memory budget (peak records in use <= budget,
+    requests wait until room frees up, then all complete);
+  - a request larger than the budget is refused (BUDGET), a full queue answers
+    AGAIN;
+  - a short replay of the seeded request stream serves every single-source
+    request, with sampled rays within the mixed mode's stated error.
+"""
+import numpy as np
+import pytest
+
+import relsim
+import scenes
+from cameras import config_cam
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("status", "r", "theta", "phi", "r_hit", "g")
+
+
+def same(a, b) -> bool:
+    return np.array_equal(a, b, equal_nan=(a.dtype.kind == "f"))
+
+
+def _server(budget=1 << 28, **kw):
+    return relsim.Server(0, relsim.server_config(budget, record=FIELDS + ("pixels",), **kw))
+
+
+def test_server_matches_direct_trace(tracer):
+    cams = [config_cam("c2", width=256, height=192, precision=relsim.PRECISION_MIXED),
+            config_cam("c3", width=160, height=96),
+            config_cam("c1", width=100, height=60),  # width not a multiple of 32
+            config_cam("c2", width=64, height=64, row_offset=10, row_count=20)]
+    tracer.set_launch_config()
+    with _server() as srv:
+        subs = [srv.submit(c, FIELDS, pixels=True) for c in cams]
+        got = srv.wait([rid for rid, _ in subs])
+        assert all(d.status == 0 for d in got.values())
+    for cam, (rid, out) in zip(cams, subs):
+        ref = tracer.dispatch(cam, fields=list(FIELDS), pixels=True)
+        for k in FIELDS:
+            assert same(out[k], ref[k]), k
+        assert np.array_equal(out["pixels"], ref["pixels"])
+
+
+@pytest.mark.parametrize("precision", [relsim.PRECISION_FP64, relsim.PRECISION_MIXED])
+def test_request_same_alone_and_in_the_mix(precision):
+    target = config_cam("c2", width=512, height=384, precision=precision)
+    with _server(chunk_rays=1 << 15) as srv:
+        rid, alone = srv.submit(target, FIELDS)
+        srv.wait([rid])
+    others = [d.camera(relsim.PRECISION_MIXED if i % 2 else relsim.PRECISION_FP64)
+              for i, d in enumerate(scenes.bundle_table(24, 11)) if d.side <= 512]
+    with _server(chunk_rays=1 << 15) as srv:
+        ids = [srv.submit(c, FIELDS)[0] for c in others[:8]]
+        rid, mixed_in = srv.submit(target, FIELDS)
+        ids += [srv.submit(c, FIELDS)[0] for c in others[8:]]
+        got = srv.wait(ids + [rid])
+        st = srv.stats()
+    assert all(d.status == 0 for d in got.values())
+    assert st.peak_active > 1 and st.epochs > 1
+    for k in FIELDS:
+        assert same(mixed_in[k], alone[k]), k
+
+
+def test_admission_holds_the_budget():
+    cam = config_cam("c2", width=256, height=256)
+    per_request = 256 * 256 * (4 + 5 * 8 + 32)
+    budget = int(2.5 * per_request)
+    with _server(budget) as srv:
+        subs = [srv.submit(cam, FIELDS, pixels=True) for _ in range(8)]
+        got = srv.wait([rid for rid, _ in subs])
+        st = srv.stats()
+    assert all(d.status == 0 for d in got.values())
+    assert st.peak_bytes_in_use <= st.budget_bytes <= budget
+    assert st.peak_active <= 2
+    for _, out in subs[1:]:
+        assert same(out["r_hit"], subs[0][1]["r_hit"])
+    # later requests queued behind the budget: their latency includes the wait
+    lat = sorted(d.latency_ms for d in got.values())
+    assert lat[-1] > lat[0]
+
+
+def test_oversized_request_and_full_queue():
+    with _server(1 << 20) as srv:  # about 13 k rays of records
+        with pytest.raises(relsim.RelsimError) as e:
+            srv.submit(config_cam("c2", width=256, height=256), FIELDS)
+        assert e.value.status == 7  # BUDGET
+    with _server(1 << 30, max_requests=2) as srv:
+        big = config_cam("c2", width=1024, height=1024)
+        a, _ = srv.submit(big, FIELDS)
+        b, _ = srv.submit(big, FIELDS)
+        with pytest.raises(relsim.RelsimError) as e:
+            srv.submit(big, FIELDS)
+        assert e.value.status == 8  # AGAIN
+        srv.wait([a, b])
+
+
+def test_stream_replay_serves_every_request():
+    import serve_stream
+
+    reqs = scenes.request_stream(80)
+    keep = {r.index for r in reqs[:40] if not r.multi_source}
+    keep = set(sorted(keep)[:4])
+    cfg = relsim.server_config(8 << 30, record=serve_stream.FIELDS)
+    with relsim.Server(0, cfg) as srv:
+        res = serve_stream.replay(srv, reqs, relsim.PRECISION_MIXED, speed=4.0, keep=keep)
+    assert res["failed"] == 0
+    assert res["served"] + res["skipped_multi_source"] == len(reqs)
+    assert res["latency_ms_p99"] >= res["latency_ms_p50"] > 0.0
+    from oracle import oracle as O
+    rng = np.random.default_rng(4)
+    for idx, (r, out) in sorted(res["kept"].items()):
+        cam = r.bundle.camera(relsim.PRECISION_FP64)
+        pix = rng.choice(r.rays, min(r.rays, 60), replace=False)
+        ref = O.trace(relsim.camera_dict(cam), pixels=pix.astype(np.uint64))
+        st = out["status"][pix].astype(np.uint32)
+        band = O.boundary_band(ref, O.lib().orc_isco_radius(1.0, cam.metric_spin), cam.disk_outer_radius, 1e-6)
+        assert not ((st != ref["status"]) & ~band).any(), idx
+        both = (st == O.DISK) & (ref["status"] == O.DISK)
+        if both.any():
+            assert np.max(np.abs(out["r_hit"][pix][both] - ref["r_hit"][both]) / ref["r_hit"][both]) < 1e-5
+            assert np.max(np.abs(out["g"][pix][both] - ref["g"][both]) / ref["g"][both]) < 1e-5
