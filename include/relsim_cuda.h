@@ -169,6 +169,10 @@ int rt_is_platform_supported(void);
 const char* rt_last_error(const rt_handle* h);
 int rt_abi_version(void);
 
+/* Prograde/retrograde ISCO radius by the sign of the spin
+ * (SoftwareComputeEngine::kerr_isco_radius, software_compute_engine.hpp:1052-1061). */
+double rt_kerr_isco_radius(double mass, double spin);
+
 /* Defaults: r=100, i=17 deg, FOV 12 deg, a=0.94, 2048^2, disk [r_ISCO, 20],
  * rtol=atol=1e-10, cap 0.1, h0 = 0.01 r_obs, 20000 attempts, FP64. */
 void rt_camera_defaults(rt_camera* cam);

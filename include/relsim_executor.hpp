@@ -1,0 +1,179 @@
+// relsim_executor.hpp -- C++ adapter with the method names and semantics of
+// Render::VulkanComputeExecutor (include/relativistic/render/vulkan_compute_executor.hpp:29)
+// over the tracer's C ABI (relsim_cuda.h).  Header only; link librelsim_cuda.so.
+//
+//   reference                                        here
+//   initialize(VulkanContext&)            :983       initialize(int device)
+//   is_ready() const                      :1257      is_ready()
+//   shutdown()                            :1272      shutdown()
+//   dispatch_and_readback(params, out, bodies, cancel)  :1399-1464
+//                                                    dispatch_and_readback(camera, out, cancel)
+//   dispatch_tile_and_readback(params, out, bodies)     :1372-1391
+//                                                    dispatch_tile_and_readback(camera, out)
+//   static is_platform_supported()        :1634      is_platform_supported()
+//
+// Semantics kept from the reference: bool returns and no exceptions across the
+// boundary; the output vector is resized by the callee (row window x width, or
+// tile extent); the cancel flag is polled between bands and a cancelled
+// dispatch returns false; a device error clears is_ready(), after which the
+// caller falls back as GeodesicComputePipeline does
+// (geodesic_compute_pipeline.hpp:508-524).  Calls on one executor are
+// serialised by the caller (gpu_mutex_ in the reference).  Scene bodies are not
+// part of this path (the pipeline's eligibility gate sends body scenes
+// elsewhere).
+#ifndef RELSIM_EXECUTOR_HPP
+#define RELSIM_EXECUTOR_HPP
+
+#include <algorithm>
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "relsim_cuda.h"
+
+namespace relsim {
+
+// Integration settings of the tracer that GpuCameraPushConstants does not carry.
+struct TraceSettings {
+    double rtol = 1e-10;
+    double atol = 1e-10;
+    double capture_scale = 1.01;    // captured when r_BL < capture_scale * r_+
+    uint32_t precision = RT_PRECISION_FP64;
+    uint32_t early_capture = 1;
+};
+
+// rt_camera from the reference's push constants (gpu_types.hpp:966-1109): the
+// observer, tetrad, field of view, metric mass and spin, escape radius, image
+// size, step budget, row window and tile, and the primary disk
+// (inner = inner_radius_scale x r_ISCO(a), outer = outer_radius_mass_units x M).
+// A template so that this header does not depend on the reference's headers.
+template <class PushConstants>
+rt_camera camera_from_push_constants(const PushConstants& p, const TraceSettings& s = {}) {
+    rt_camera c;
+    rt_camera_defaults(&c);
+    for (int i = 0; i < 4; ++i) {
+        c.observer_position[i] = p.observer_position[i];
+        c.tetrad_e1[i] = p.tetrad_e1[i];
+        c.tetrad_e2[i] = p.tetrad_e2[i];
+        c.tetrad_e3[i] = p.tetrad_e3[i];
+    }
+    c.field_of_view_rad = p.field_of_view_rad;
+    c.metric_mass = std::max(p.metric_mass, 1e-4);
+    c.metric_spin = std::clamp(p.metric_spin, -0.999 * c.metric_mass, 0.999 * c.metric_mass);
+    c.escape_radius = p.escape_radius;
+    c.screen_width = p.screen_width;
+    c.screen_height = p.screen_height;
+    c.max_integration_steps = p.max_integration_steps;
+    c.dispatch_row_offset = p.dispatch_row_offset;
+    c.dispatch_row_count = p.dispatch_row_count;
+    c.tile_origin_x = p.tile_origin_x;
+    c.tile_origin_y = p.tile_origin_y;
+    c.tile_extent_x = p.tile_extent_x;
+    c.tile_extent_y = p.tile_extent_y;
+    const double scale = static_cast<double>(p.primary_disk.inner_radius_scale);
+    c.disk_inner_radius = (scale == 1.0) ? 0.0 : scale * rt_kerr_isco_radius(c.metric_mass, c.metric_spin);
+    c.disk_outer_radius = static_cast<double>(p.primary_disk.outer_radius_mass_units) * c.metric_mass;
+    c.rtol = s.rtol;
+    c.atol = s.atol;
+    c.capture_scale = s.capture_scale;
+    c.precision_mode = s.precision;
+    c.early_capture = s.early_capture;
+    return c;
+}
+
+class CudaComputeExecutor {
+public:
+    CudaComputeExecutor() = default;
+    CudaComputeExecutor(const CudaComputeExecutor&) = delete;
+    CudaComputeExecutor& operator=(const CudaComputeExecutor&) = delete;
+    ~CudaComputeExecutor() { shutdown(); }
+
+    [[nodiscard]] static bool is_platform_supported() { return rt_is_platform_supported() != 0; }
+
+    [[nodiscard]] bool initialize(int device = 0) {
+        shutdown();
+        const rt_status st = rt_create(&h_, device);
+        if (st != RT_OK) {
+            error_ = "rt_create failed (no sm_100 device?)";
+            h_ = nullptr;
+            return false;
+        }
+        return true;
+    }
+
+    [[nodiscard]] bool is_ready() const noexcept { return h_ != nullptr && rt_is_ready(h_) != 0; }
+
+    void shutdown() noexcept {
+        if (h_) rt_destroy(h_);
+        h_ = nullptr;
+    }
+
+    const std::string& last_error() const noexcept { return error_; }
+    rt_handle* handle() noexcept { return h_; }
+
+    // Row window of the image, banded so that `cancel` is polled between bands.
+    [[nodiscard]] bool dispatch_and_readback(const rt_camera& camera, std::vector<rt_pixel_out>& output,
+                                             const std::atomic<bool>* cancel = nullptr,
+                                             const rt_ray_out* rays = nullptr) {
+        if (!is_ready() || camera.screen_width == 0 || camera.screen_height == 0) return false;
+        const uint32_t first = std::min(camera.dispatch_row_offset, camera.screen_height);
+        const uint32_t rows = (camera.dispatch_row_count == 0)
+                                  ? camera.screen_height - first
+                                  : std::min(camera.dispatch_row_count, camera.screen_height - first);
+        if (rows == 0) return false;
+        const size_t width = camera.screen_width;
+        if (output.size() != width * rows) output.resize(width * rows);
+        const uint32_t band = static_cast<uint32_t>(std::max<size_t>(1, kBandRays / width));
+        for (uint32_t r = 0; r < rows; r += band) {
+            if (cancel && cancel->load(std::memory_order_relaxed)) return false;
+            rt_camera c = camera;
+            c.dispatch_row_offset = first + r;
+            c.dispatch_row_count = std::min(band, rows - r);
+            const size_t offset = static_cast<size_t>(r) * width;
+            rt_ray_out part{};
+            if (rays) part = offset_rays(*rays, offset);
+            if (!check(rt_dispatch(h_, &c, output.data() + offset, rays ? &part : nullptr,
+                                   width * c.dispatch_row_count, nullptr)))
+                return false;
+        }
+        return true;
+    }
+
+    // Tile [origin, origin + extent), tile-major; output resized to the extent.
+    [[nodiscard]] bool dispatch_tile_and_readback(const rt_camera& camera, std::vector<rt_pixel_out>& output) {
+        if (!is_ready() || camera.tile_extent_x == 0 || camera.tile_extent_y == 0) return false;
+        if (camera.tile_origin_x >= camera.screen_width || camera.tile_origin_y >= camera.screen_height) return false;
+        const size_t n = static_cast<size_t>(camera.tile_extent_x) * camera.tile_extent_y;
+        if (output.size() != n) output.resize(n);
+        return check(rt_dispatch_tile(h_, &camera, output.data(), nullptr, n));
+    }
+
+private:
+    static constexpr size_t kBandRays = size_t{1} << 22;
+
+    static rt_ray_out offset_rays(const rt_ray_out& r, size_t k) {
+        rt_ray_out o = r;
+        auto adv = [k](auto*& p) {
+            if (p) p += k;
+        };
+        adv(o.status), adv(o.flags), adv(o.steps_accepted), adv(o.steps_rejected);
+        adv(o.r), adv(o.theta), adv(o.phi), adv(o.r_hit), adv(o.g), adv(o.lambda);
+        adv(o.dH), adv(o.dE), adv(o.dLz), adv(o.dQ);
+        return o;
+    }
+
+    bool check(rt_status st) {
+        if (st == RT_OK) return true;
+        error_ = rt_last_error(h_);
+        return false;
+    }
+
+    rt_handle* h_ = nullptr;
+    std::string error_;
+};
+
+}  // namespace relsim
+
+#endif

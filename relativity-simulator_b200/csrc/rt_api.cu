@@ -235,6 +235,8 @@ extern "C" {
 
 int rt_abi_version(void) { return RT_ABI_VERSION; }
 
+double rt_kerr_isco_radius(double mass, double spin) { return kerr_isco_radius(mass, spin); }
+
 int rt_is_platform_supported(void) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) {

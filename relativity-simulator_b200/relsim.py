@@ -105,7 +105,7 @@ _lib: ctypes.CDLL | None = None
 EXPORTS = ["rt_create", "rt_destroy", "rt_is_ready", "rt_is_platform_supported", "rt_last_error", "rt_abi_version",
            "rt_camera_defaults", "rt_camera_look_at_hole", "rt_dispatch", "rt_dispatch_tile", "rt_dispatch_device",
            "rt_trace_bundles_device", "rt_bundle_rays", "rt_set_launch_config", "rt_get_launch_config",
-           "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc",
+           "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc", "rt_kerr_isco_radius",
            "rt_server_config_defaults", "rt_server_create", "rt_server_destroy", "rt_server_submit",
            "rt_server_poll", "rt_server_get_stats", "rt_server_last_error"]
 NOALLOC_MAX_BUNDLES = 32  # RT_NOALLOC_MAX_BUNDLES
@@ -140,6 +140,8 @@ def lib() -> ctypes.CDLL:
         L.rt_get_stats.argtypes = [v, p(Stats)]
         L.rt_synchronize.argtypes = [v, _d]
         L.rt_measure_fma_peak.argtypes = [v, p(_d), p(_d)]
+        L.rt_kerr_isco_radius.argtypes = [_d, _d]
+        L.rt_kerr_isco_radius.restype = _d
         L.rt_server_config_defaults.argtypes = [p(ServerConfig)]
         L.rt_server_config_defaults.restype = None
         L.rt_server_create.argtypes = [p(ctypes.c_void_p), ctypes.c_int, p(ServerConfig)]

@@ -1,0 +1,92 @@
+// Drives relsim::CudaComputeExecutor (include/relsim_executor.hpp) the way the
+// reference's pipeline drives VulkanComputeExecutor.  Used by tests/test_adapter.py.
+//   adapter_main map                 print the mapped camera of a push-constant struct
+//   adapter_main cpu                 platform/initialise answers without a device
+//   adapter_main gpu <out.bin>       dispatch_and_readback of a 96x64 image -> raw pixels; cancel check
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#ifdef RELSIM_WITH_REFERENCE_TYPES
+#include "relativistic/render/gpu_types.hpp"
+using Push = Relativistic::Render::GpuCameraPushConstants;
+#else
+#include <array>
+struct DiskProfile {
+    float inner_radius_scale = 1.0f;
+    float outer_radius_mass_units = 24.0f;
+};
+struct Push {  // the fields of GpuCameraPushConstants the tracer reads (gpu_types.hpp:966-1109)
+    std::array<double, 4> observer_position{}, tetrad_e1{}, tetrad_e2{}, tetrad_e3{};
+    double field_of_view_rad = 1.0471975511965976, metric_mass = 1.0, metric_spin = 0.0, escape_radius = 100.0;
+    uint32_t screen_width = 3840, screen_height = 2160, max_integration_steps = 2048;
+    uint32_t dispatch_row_offset = 0, dispatch_row_count = 0;
+    uint32_t tile_origin_x = 0, tile_origin_y = 0, tile_extent_x = 0, tile_extent_y = 0;
+    DiskProfile primary_disk{};
+};
+#endif
+#include "relsim_executor.hpp"
+
+static Push headline_push(uint32_t w, uint32_t h) {
+    rt_camera d;
+    rt_camera_defaults(&d);  // r=100, i=17 deg, FOV 12 deg, a=0.94
+    Push p{};
+    for (int i = 0; i < 4; ++i) {
+        p.observer_position[i] = d.observer_position[i];
+        p.tetrad_e1[i] = d.tetrad_e1[i];
+        p.tetrad_e2[i] = d.tetrad_e2[i];
+        p.tetrad_e3[i] = d.tetrad_e3[i];
+    }
+    p.field_of_view_rad = d.field_of_view_rad;
+    p.metric_mass = 1.0;
+    p.metric_spin = 0.94;
+    p.escape_radius = 1000.0;
+    p.screen_width = w;
+    p.screen_height = h;
+    p.max_integration_steps = 20000;
+    p.primary_disk.inner_radius_scale = 1.0f;
+    p.primary_disk.outer_radius_mass_units = 20.0f;
+    return p;
+}
+
+int main(int argc, char** argv) {
+    const char* mode = argc > 1 ? argv[1] : "map";
+    if (!std::strcmp(mode, "map")) {
+        Push p = headline_push(96, 64);
+        p.metric_spin = 1.5;  // clamped to 0.999 M
+        p.primary_disk.inner_radius_scale = 1.5f;
+        const rt_camera c = relsim::camera_from_push_constants(p);
+        std::printf("%.17g %.17g %.17g %.17g %u %u %u %.17g\n", c.metric_spin, c.disk_inner_radius,
+                    c.disk_outer_radius, c.escape_radius, c.screen_width, c.screen_height, c.max_integration_steps,
+                    rt_kerr_isco_radius(1.0, 0.999));
+        return 0;
+    }
+    if (!std::strcmp(mode, "cpu")) {
+        relsim::CudaComputeExecutor ex;
+        const bool sup = relsim::CudaComputeExecutor::is_platform_supported();
+        const bool init = ex.initialize(0);
+        std::vector<rt_pixel_out> out;
+        const rt_camera c = relsim::camera_from_push_constants(headline_push(32, 32));
+        const bool disp = ex.dispatch_and_readback(c, out);
+        std::printf("%d %d %d %d\n", sup, init, ex.is_ready(), disp);
+        return 0;
+    }
+    if (!std::strcmp(mode, "gpu") && argc > 2) {
+        relsim::CudaComputeExecutor ex;
+        if (!ex.initialize(0)) return 2;
+        const rt_camera c = relsim::camera_from_push_constants(headline_push(96, 64));
+        std::vector<rt_pixel_out> out;
+        if (!ex.dispatch_and_readback(c, out)) return 3;
+        FILE* f = std::fopen(argv[2], "wb");
+        if (!f) return 4;
+        std::fwrite(out.data(), sizeof(rt_pixel_out), out.size(), f);
+        std::fclose(f);
+        std::atomic<bool> cancel{true};
+        std::vector<rt_pixel_out> out2;
+        const bool cancelled_ok = !ex.dispatch_and_readback(c, out2, &cancel);
+        std::printf("%zu %d %d\n", out.size(), cancelled_ok, ex.is_ready());
+        return 0;
+    }
+    return 1;
+}
