@@ -29,6 +29,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "relsim_cuda.h"
@@ -114,9 +115,14 @@ public:
     rt_handle* handle() noexcept { return h_; }
 
     // Row window of the image, banded so that `cancel` is polled between bands.
-    [[nodiscard]] bool dispatch_and_readback(const rt_camera& camera, std::vector<rt_pixel_out>& output,
+    // Pixel: rt_pixel_out or any 32-byte standard-layout type of the same layout
+    // (the reference's GpuPixelOutput).
+    template <class Pixel = rt_pixel_out>
+    [[nodiscard]] bool dispatch_and_readback(const rt_camera& camera, std::vector<Pixel>& output,
                                              const std::atomic<bool>* cancel = nullptr,
                                              const rt_ray_out* rays = nullptr) {
+        static_assert(sizeof(Pixel) == sizeof(rt_pixel_out) && std::is_standard_layout_v<Pixel>,
+                      "pixel type must have the 32-byte GpuPixelOutput layout");
         if (!is_ready() || camera.screen_width == 0 || camera.screen_height == 0) return false;
         const uint32_t first = std::min(camera.dispatch_row_offset, camera.screen_height);
         const uint32_t rows = (camera.dispatch_row_count == 0)
@@ -134,7 +140,8 @@ public:
             const size_t offset = static_cast<size_t>(r) * width;
             rt_ray_out part{};
             if (rays) part = offset_rays(*rays, offset);
-            if (!check(rt_dispatch(h_, &c, output.data() + offset, rays ? &part : nullptr,
+            if (!check(rt_dispatch(h_, &c, reinterpret_cast<rt_pixel_out*>(output.data() + offset),
+                                   rays ? &part : nullptr,
                                    width * c.dispatch_row_count, nullptr)))
                 return false;
         }
@@ -142,12 +149,15 @@ public:
     }
 
     // Tile [origin, origin + extent), tile-major; output resized to the extent.
-    [[nodiscard]] bool dispatch_tile_and_readback(const rt_camera& camera, std::vector<rt_pixel_out>& output) {
+    template <class Pixel = rt_pixel_out>
+    [[nodiscard]] bool dispatch_tile_and_readback(const rt_camera& camera, std::vector<Pixel>& output) {
+        static_assert(sizeof(Pixel) == sizeof(rt_pixel_out) && std::is_standard_layout_v<Pixel>,
+                      "pixel type must have the 32-byte GpuPixelOutput layout");
         if (!is_ready() || camera.tile_extent_x == 0 || camera.tile_extent_y == 0) return false;
         if (camera.tile_origin_x >= camera.screen_width || camera.tile_origin_y >= camera.screen_height) return false;
         const size_t n = static_cast<size_t>(camera.tile_extent_x) * camera.tile_extent_y;
         if (output.size() != n) output.resize(n);
-        return check(rt_dispatch_tile(h_, &camera, output.data(), nullptr, n));
+        return check(rt_dispatch_tile(h_, &camera, reinterpret_cast<rt_pixel_out*>(output.data()), nullptr, n));
     }
 
 private:

@@ -57,6 +57,12 @@ int main(int argc, char** argv) {
         p.metric_spin = 1.5;  // clamped to 0.999 M
         p.primary_disk.inner_radius_scale = 1.5f;
         const rt_camera c = relsim::camera_from_push_constants(p);
+#ifdef RELSIM_WITH_REFERENCE_TYPES
+        // the executor takes the reference's own pixel vector (compile-time layout check)
+        std::vector<Relativistic::Render::GpuPixelOutput> ref_pixels;
+        relsim::CudaComputeExecutor unused;
+        if (argc > 99) (void)unused.dispatch_and_readback(c, ref_pixels);
+#endif
         std::printf("%.17g %.17g %.17g %.17g %u %u %u %.17g\n", c.metric_spin, c.disk_inner_radius,
                     c.disk_outer_radius, c.escape_radius, c.screen_width, c.screen_height, c.max_integration_steps,
                     rt_kerr_isco_radius(1.0, 0.999));
