@@ -145,8 +145,11 @@ typedef struct rt_launch_config {
     uint32_t rays_per_thread;  /* consecutive rays claimed per lane with each global atomic:
                                   a warp claims 32 * rays_per_thread rays at a time (1..64) */
     uint32_t fp64_rolled;      /* FP64 mode: 1 = stage loop rolled around one RHS copy with the
-                                  stage derivatives in shared memory, 0 = straight-line stages
-                                  (the mixed mode always uses the rolled form) */
+                                  stage derivatives in shared memory, 0 = straight-line stages */
+    uint32_t mixed_single_kernel; /* MIXED mode: 0 = two passes per round, an FP32 far-zone kernel and
+                                  an FP64 near-zone kernel exchanging parked rays through HBM (the
+                                  default); 1 = one kernel, FP64 steps for a whole warp whenever one
+                                  of its rays is in the FP64 zone (rolled FP64 step) */
 } rt_launch_config;
 
 /* Counters of the last dispatch (device-side totals). */
@@ -232,7 +235,9 @@ rt_status rt_measure_fma_peak(rt_handle* h, double* fp64_tflops, double* fp32_tf
  * persistent launch over row chunks taken round-robin from every admitted
  * request, so a request arriving while others are on the GPU joins the next
  * epoch.  Records stay on the device until a request's last chunk is done,
- * then go to the caller's host buffers.  A scheduler thread owned by the server
+ * then go to the caller's host buffers.  Besides the budget, the server holds
+ * two epochs' ray state for the two-pass mixed tracer (124 bytes per epoch ray
+ * per slot: about 1 GB at the default 2^22-ray epochs).  A scheduler thread owned by the server
  * does all device work; submit and poll may be called from any thread. */
 typedef struct rt_server rt_server;
 
@@ -286,6 +291,8 @@ const char* rt_server_last_error(const rt_server* s);
 
 /* Allocation-free bundle trace.  No counterpart in the reference: its compute
  * executor always owns its device buffers and grows them on demand.
+ * Mixed-precision tables run the single-kernel form (mixed_single_kernel = 1):
+ * the two-pass form needs buffers for parked rays.
  *
  * For callers that cannot allocate device memory at dispatch time: a host
  * that has reserved the whole device for its own pool allocator (a serving

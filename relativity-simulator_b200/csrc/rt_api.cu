@@ -42,6 +42,7 @@ struct rt_handle {
     rt_launch_config cfg{};
     // device scratch
     DevBuf bundles, queue, stats;
+    DevBuf park_d, park_u, pass_queues;  // two-pass mixed tracer: parked state, far/near queues
     DevBuf ray_fields[14];
     DevBuf pixels;
     // pinned staging of the bundle table
@@ -81,7 +82,12 @@ rt_status cuda_fail(rt_handle* h, cudaError_t e, const char* where) {
 
 rt_status ensure(rt_handle* h, DevBuf& b, size_t bytes) {
     if (b.bytes >= bytes) return RT_OK;
-    if (b.ptr) cudaFree(b.ptr);
+    if (b.ptr) {
+        cudaFree(b.ptr);  // waits for the device: no launch still reads the old buffer
+        // a captured bundle graph may hold the old address
+        if (h->graph) cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
     b.ptr = nullptr;
     b.bytes = 0;
     const size_t grow = std::max(bytes, b.bytes + b.bytes / 2);
@@ -102,7 +108,11 @@ void release(DevBuf& b) {
 
 rt_status ensure_host_bundles(rt_handle* h, size_t n) {
     if (h->host_bundles_cap >= n) return RT_OK;
-    if (h->host_bundles) cudaFreeHost(h->host_bundles);
+    if (h->host_bundles) {
+        cudaFreeHost(h->host_bundles);
+        if (h->graph) cudaGraphExecDestroy(h->graph);  // its upload node read the old staging buffer
+        h->graph = nullptr;
+    }
     h->host_bundles = nullptr;
     h->host_bundles_cap = 0;
     RT_CUDA(h, cudaMallocHost(&h->host_bundles, n * sizeof(BundleDesc)));
@@ -122,6 +132,52 @@ bool camera_valid(const rt_camera* c) {
 
 rt_launch_config effective_cfg(const rt_handle* h, bool mixed) { return resolve_launch_config(h->cfg, mixed); }
 
+// Parked-state and queue buffers of the two-pass tracer for `total` rays
+// (allocated before any graph capture: allocation is not capturable).
+rt_status ensure_two_pass(rt_handle* h, uint64_t total) {
+    rt_status st;
+    if ((st = ensure(h, h->park_d, sizeof(double) * PD_COUNT * total)) != RT_OK) return st;
+    if ((st = ensure(h, h->park_u, sizeof(uint32_t) * PU_COUNT * total)) != RT_OK) return st;
+    return ensure(h, h->pass_queues, sizeof(uint32_t) * 3 * total);
+}
+
+bool uses_two_pass(const rt_launch_config& c, bool mixed, uint64_t total) {
+    return mixed && c.mixed_single_kernel == 0 && total <= 0xffffffffull;
+}
+
+rt_status launch_two_pass(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs& out,
+                          const rt_launch_config& c, cudaStream_t s, bool capturing) {
+    if (!capturing) {
+        const rt_status st = ensure_two_pass(h, total);
+        if (st != RT_OK) return st;
+    } else if (h->park_d.bytes < sizeof(double) * PD_COUNT * total ||
+               h->park_u.bytes < sizeof(uint32_t) * PU_COUNT * total ||
+               h->pass_queues.bytes < sizeof(uint32_t) * 3 * total) {
+        return fail(h, RT_ERR_INVALID_ARG, "two-pass buffers not reserved before capture");
+    }
+    TraceArgs args{};
+    args.bundles = static_cast<const BundleDesc*>(h->bundles.ptr);
+    args.n_bundles = n_bundles;
+    args.refill_threshold = c.refill_threshold;
+    args.claim = 32u * c.rays_per_thread;
+    args.total_rays = total;
+    args.stats = static_cast<unsigned long long*>(h->stats.ptr);
+    args.out = out;
+    TwoPassBuffers buf{};
+    buf.park = ParkBuf{static_cast<double*>(h->park_d.ptr), static_cast<uint32_t*>(h->park_u.ptr), total};
+    buf.queues = static_cast<uint32_t*>(h->pass_queues.ptr);
+    buf.counters = static_cast<char*>(h->queue.ptr);
+    RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
+    if (!capturing) RT_CUDA(h, cudaEventRecord(h->ev0, s));
+    RT_CUDA(h, static_cast<cudaError_t>(
+                   enqueue_two_pass(args, buf, h->sm_count, c.block_size, s, nullptr, nullptr, nullptr, 1)));
+    if (!capturing) {
+        RT_CUDA(h, cudaEventRecord(h->ev1, s));
+        h->timed = true;
+    }
+    return RT_OK;
+}
+
 // Launch the tracer over `n` bundles already in h->bundles (device).  The
 // timing events bracket the launch unless it is being captured into a graph
 // (an event recorded on a capturing stream only orders the capture; the graph
@@ -129,6 +185,7 @@ rt_launch_config effective_cfg(const rt_handle* h, bool mixed) { return resolve_
 rt_status launch(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs& out, bool mixed, cudaStream_t s,
                  bool capturing = false) {
     const rt_launch_config c = effective_cfg(h, mixed);
+    if (uses_two_pass(c, mixed, total)) return launch_two_pass(h, n_bundles, total, out, c, s, capturing);
     TraceArgs args{};
     args.bundles = static_cast<const BundleDesc*>(h->bundles.ptr);
     args.n_bundles = n_bundles;
@@ -290,6 +347,9 @@ void rt_destroy(rt_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     release(h->bundles);
+    release(h->park_d);
+    release(h->park_u);
+    release(h->pass_queues);
     release(h->queue);
     release(h->stats);
     release(h->pixels);
@@ -439,6 +499,7 @@ rt_status rt_trace_bundles_device(rt_handle* h, const rt_camera* cams, uint32_t 
     if (begin == 0) return fail(h, RT_ERR_INVALID_ARG, "empty bundle table");
     OutPtrs out{pixels, rays ? *rays : rt_ray_out{}};
     const rt_launch_config c = effective_cfg(h, mixed);
+    if (uses_two_pass(c, mixed, begin) && (st = ensure_two_pass(h, begin)) != RT_OK) return st;
     const bool same = h->graph && h->graph_n_bundles == n_bundles && h->graph_total == begin &&
                       std::memcmp(&h->graph_out, &out, sizeof out) == 0 &&
                       std::memcmp(&h->graph_cfg, &c, sizeof c) == 0;

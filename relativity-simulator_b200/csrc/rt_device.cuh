@@ -25,6 +25,13 @@ struct DP {
                             B6 = 11.0 / 84.0;
     static constexpr double E1 = 71.0 / 57600.0, E3 = -71.0 / 16695.0, E4 = 71.0 / 1920.0,
                             E5 = -17253.0 / 339200.0, E6 = 22.0 / 525.0, E7 = -1.0 / 40.0;
+    // Continuous extension of order 4 (Shampine's dense output for this pair, as
+    // in Hairer, Norsett & Wanner, Solving ODEs I, sec. II.6): with
+    // d = y1 - y0, b = h k1 - d, c = d - h k7 - b and e = h sum_j D_j k_j,
+    // y(t) = y0 + t (d + (1 - t) (b + t (c + (1 - t) e))), t in [0, 1].
+    static constexpr double D1 = -12715105075.0 / 11282082432.0, D3 = 87487479700.0 / 32700410799.0,
+                            D4 = -10690763975.0 / 1880347072.0, D5 = 701980252875.0 / 199316789632.0,
+                            D6 = -1453857185.0 / 822651844.0, D7 = 69997945.0 / 29380423.0;
 };
 
 template <typename T>

@@ -56,6 +56,27 @@ struct OutPtrs {
 // Device counters of one launch.
 enum StatIndex { ST_RAYS = 0, ST_ATTEMPTS, ST_ACCEPTED, ST_RHS, ST_FP64_ATTEMPTS, ST_COUNT };
 
+// Parked ray state of the two-pass mixed tracer: structure of arrays with one
+// slot per ray of the launch, indexed by the ray's launch index.
+enum ParkD : int { PD_Y = 0, PD_H = 6, PD_LAMBDA, PD_DH, PD_LZ0, PD_Q0, PD_COUNT };
+enum ParkU : int { PU_ACC = 0, PU_REJ, PU_FLAGS, PU_GUARD, PU_WIND, PU_MISC, PU_LNP, PU_COUNT };
+// PU_MISC bits
+enum : uint32_t {
+    PM_HAS_HIST = 1u,    // bit 0: PI30 history present
+    PM_EARLY_SHIFT = 2u  // bits 2..3: Carter early-capture state + 1
+};
+
+struct ParkBuf {
+    double* d;    // [PD_COUNT][n]
+    uint32_t* u;  // [PU_COUNT][n]
+    uint64_t n;   // slots
+};
+
+// Passes of the launch.  PASS_SINGLE: one kernel traces every ray to the end.
+// The two-pass mixed tracer alternates an FP32 far-zone pass and an FP64
+// near-zone pass; rays move between them through queues of launch indices.
+enum TracePass : int { PASS_SINGLE = 0, PASS_FAR = 1, PASS_NEAR = 2 };
+
 struct TraceArgs {
     const BundleDesc* bundles;
     uint32_t n_bundles;
@@ -63,9 +84,20 @@ struct TraceArgs {
     uint32_t claim;             // rays a warp claims per global atomic
     uint32_t pad;
     uint64_t total_rays;
-    unsigned long long* queue;  // [0]: next unclaimed ray
+    unsigned long long* queue;  // [0]: next unclaimed ray (or queue entry)
     unsigned long long* stats;  // [ST_COUNT]
     OutPtrs out;
+    // two-pass mixed tracer (zero for PASS_SINGLE launches)
+    uint64_t ray_base;          // far pass from pixels: launch index of this band's first ray
+    uint32_t from_pixels;       // far pass: rays start at their pixels
+    uint32_t allow_exit;        // near pass: rays leaving the near zone go back to the far pass
+    const uint32_t* in_queue;   // launch indices of the rays to resume
+    const uint32_t* in_count;
+    uint32_t* out_queue;        // launch indices parked for the other pass
+    uint32_t* out_count;
+    uint32_t* finish_queue;     // disk hits parked with their root point for the finish pass
+    uint32_t* finish_count;
+    ParkBuf park;
 };
 
 // Host-side helpers implemented in rt_bundle.cpp.
@@ -78,6 +110,29 @@ void row_window(const rt_camera& c, uint32_t& row0, uint32_t& nrows);
 
 // Tracer launch helpers implemented in rt_trace.cu.
 void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled, void* stream);
+// One pass of the two-pass mixed tracer (PASS_FAR or PASS_NEAR).
+void launch_trace_pass(const TraceArgs& args, int pass, uint32_t grid, uint32_t block, void* stream);
+int trace_pass_occupancy(int pass, uint32_t block);
+
+// Device buffers of the two-pass mixed tracer for n rays.
+struct TwoPassBuffers {
+    ParkBuf park;       // parked state, n slots
+    uint32_t* queues;   // 3n entries: per band near, far and finish queues
+    char* counters;     // 32 bytes per band (up to kMaxBands): claim counters and queue counts
+};
+constexpr uint32_t kMaxBands = 8;
+// Bytes of park.d, park.u and queues for n rays.
+uint64_t two_pass_state_bytes(uint64_t n);
+// Enqueue the rounds of the two-pass mixed tracer (memsets, launches and event
+// records only, so it can be captured into a graph).  `base` carries the
+// bundles, outputs, zeroed stats, the far pass's refill threshold and claim,
+// and total_rays.  The rays are split into `bands` contiguous ranges traced
+// alternately on `stream` and `stream2`, so that one band's near-pass tail
+// overlaps the next band's far pass; fork and join (events created by the
+// caller) bring stream2 into and out of the sequence.  bands = 1 uses
+// `stream` alone.  Returns a cudaError_t value.
+int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_count, uint32_t far_block,
+                     void* stream, void* stream2, void* fork, void* join, uint32_t bands);
 int trace_occupancy(uint32_t block, bool mixed, bool rolled);
 uint32_t kernel_block(uint32_t block, bool mixed, bool rolled);
 // Launch shape with defaults filled in and limits applied for one precision.

@@ -117,6 +117,8 @@ struct Slot {
     BundleDesc* host_table = nullptr;   // pinned staging of the bundle table
     BundleDesc* dev_table = nullptr;
     unsigned long long* counters = nullptr;  // [0] queue, [8..] stats
+    void* pass_state = nullptr;              // two-pass mixed tracer: parked state and queues
+    char* pass_counters = nullptr;           // its queue counters
     std::vector<Chunk> chunks;
     bool busy = false;
 };
@@ -286,9 +288,22 @@ bool launch_epoch(rt_server* s, Slot& slot) {
     for (int f = 0; f < kFields; ++f)
         if (s->cfg.record_mask & (1u << f)) dp[f] = s->field_base[f];
     args.out = OutPtrs{(s->cfg.record_mask & kPixelBit) ? s->pixel_base : nullptr, rays};
-    launch_trace(args, static_cast<uint32_t>(s->sm_count) * c.ctas_per_sm, c.block_size, mixed,
-                 c.fp64_rolled != 0, st);
-    e = cudaGetLastError();
+    if (mixed && c.mixed_single_kernel == 0) {
+        // parked state of the epoch's rays: SoA with `total` slots in the slot's buffer
+        TwoPassBuffers buf{};
+        double* pd = static_cast<double*>(slot.pass_state);
+        uint32_t* pu = reinterpret_cast<uint32_t*>(pd + PD_COUNT * total);
+        buf.park = ParkBuf{pd, pu, total};
+        buf.queues = pu + PU_COUNT * total;
+        buf.counters = slot.pass_counters;
+        // one band per epoch: the two epoch slots already overlap each other's tails
+        e = static_cast<cudaError_t>(
+            enqueue_two_pass(args, buf, s->sm_count, c.block_size, st, nullptr, nullptr, nullptr, 1));
+    } else {
+        launch_trace(args, static_cast<uint32_t>(s->sm_count) * c.ctas_per_sm, c.block_size, mixed,
+                     c.fp64_rolled != 0, st);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaEventRecord(slot.done, st);
     if (e != cudaSuccess) return fail_server(s, "epoch launch", e), false;
     slot.busy = true;
@@ -445,6 +460,8 @@ rt_status rt_server_create(rt_server** out, int device_ordinal, const rt_server_
         ok = ok && cudaMallocHost(&slot.host_table, sizeof(BundleDesc) * cfg->max_epoch_bundles) == cudaSuccess;
         ok = ok && cudaMalloc(&slot.dev_table, sizeof(BundleDesc) * cfg->max_epoch_bundles) == cudaSuccess;
         ok = ok && cudaMalloc(&slot.counters, 256) == cudaSuccess;
+        ok = ok && cudaMalloc(&slot.pass_state, two_pass_state_bytes(cfg->epoch_rays)) == cudaSuccess;
+        ok = ok && cudaMalloc(&slot.pass_counters, 256) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();
@@ -471,6 +488,8 @@ void rt_server_destroy(rt_server* s) {
         if (slot.host_table) cudaFreeHost(slot.host_table);
         if (slot.dev_table) cudaFree(slot.dev_table);
         if (slot.counters) cudaFree(slot.counters);
+        if (slot.pass_state) cudaFree(slot.pass_state);
+        if (slot.pass_counters) cudaFree(slot.pass_counters);
         if (slot.stream) cudaStreamDestroy(slot.stream);
     }
     if (s->copy_stream) {

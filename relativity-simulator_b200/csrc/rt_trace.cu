@@ -24,6 +24,14 @@
 // instruction cache; states cross that boundary through small local arrays.
 // The disk root solve reuses the loop's stage code: a lane in ROOT mode runs
 // its next DP5 evaluation at a fraction of the step instead of a full step.
+//
+// The mixed-precision mode runs as two passes (PASS_FAR, PASS_NEAR) instead:
+// an FP32-stage kernel for the far zone and an FP64 kernel for the zone near
+// the hole, rays moving between them through queues with their state parked
+// in HBM, disk crossings solved on the step's dense output, and disk hits
+// written by a finish kernel.  Splitting the code this way keeps each loop
+// small in the instruction cache (the single mixed kernel, which holds both
+// step forms, is instruction-fetch bound).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -40,7 +48,7 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr double kTwoPi = 2.0 * kPi;
 constexpr double kEarlyCaptureMargin = 1e-4;  // M, distance to the critical curve
 
-enum LaneMode : int { MODE_IDLE = 0, MODE_STEP = 1, MODE_ROOT = 2, MODE_REDO = 3 };
+enum LaneMode : int { MODE_IDLE = 0, MODE_STEP = 1, MODE_ROOT = 2, MODE_REDO = 3, MODE_PARK = 4, MODE_FINISHQ = 5 };
 
 // Cold per-lane state, structure of arrays indexed by threadIdx.x.
 template <int BLOCK>
@@ -314,6 +322,97 @@ __device__ __noinline__ void finish_ray(const BundleDesc* __restrict__ Bp, Cold<
     }
 }
 
+// Resume a parked ray (two-pass tracer): its state from the park buffer, the
+// cold per-lane state into shared memory, and the FSAL stage k1 = f(y) in FP64
+// (one RHS per transition between passes).  Writes y, k1 to xch[0..11], h to
+// xch[12], the parked words to uch[]; returns r_BL.
+template <int BLOCK>
+__device__ __noinline__ double resume_ray(const BundleDesc* __restrict__ Bp, const ParkBuf pb, uint64_t ray,
+                                          uint64_t local, Cold<BLOCK>& S, int tid, double* __restrict__ xch,
+                                          uint32_t* __restrict__ uch) {
+    const uint64_t n = pb.n;
+    double y[6], k1[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) y[i] = pb.d[(PD_Y + i) * n + ray];
+    xch[12] = pb.d[PD_H * n + ray];
+    S.lambda[tid] = pb.d[PD_LAMBDA * n + ray];
+    S.dH[tid] = pb.d[PD_DH * n + ray];
+    S.lz0[tid] = pb.d[PD_LZ0 * n + ray];
+    S.q0[tid] = pb.d[PD_Q0 * n + ray];
+    S.local[tid] = local;
+#pragma unroll
+    for (int j = 0; j < PU_COUNT; ++j) uch[j] = pb.u[j * n + ray];
+    double hf, sv;
+    const double r = ks_rhs<double>(y, Bp->m, Bp->a, k1, hf, sv);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        xch[i] = y[i];
+        xch[6 + i] = k1[i];
+    }
+    return r;
+}
+
+// Park a ray for the other pass: y and h from xch[0..6], the words in uch[].
+template <int BLOCK>
+__device__ __noinline__ void park_ray(const ParkBuf pb, uint64_t ray, const Cold<BLOCK>& S, int tid,
+                                      const double* __restrict__ xch, const uint32_t* __restrict__ uch) {
+    const uint64_t n = pb.n;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) pb.d[(PD_Y + i) * n + ray] = xch[i];
+    pb.d[PD_H * n + ray] = xch[6];
+    pb.d[PD_LAMBDA * n + ray] = S.lambda[tid];
+    pb.d[PD_DH * n + ray] = S.dH[tid];
+    pb.d[PD_LZ0 * n + ray] = S.lz0[tid];
+    pb.d[PD_Q0 * n + ray] = S.q0[tid];
+#pragma unroll
+    for (int j = 0; j < PU_COUNT; ++j) pb.u[j * n + ray] = uch[j];
+}
+
+// Disk crossing on the continuous extension of an accepted step (near pass of
+// the two-pass mixed tracer): Illinois regula falsi on z(t) of the 4th-order
+// dense output, which needs no RHS evaluation (the DP5-fraction root of the
+// FP64 tracer costs five per iteration).  y0, k1: step start; y1, k7: step
+// end; e = h sum_j D_j k_j.  Writes the point at the root to out[0..5] and
+// returns t.
+__device__ __noinline__ double dense_disk_root(const double* __restrict__ y0, const double* __restrict__ k1,
+                                               const double* __restrict__ y1, const double* __restrict__ k7,
+                                               const double* __restrict__ e, double h, double* __restrict__ out) {
+    double d[6], b[6], c[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        d[i] = y1[i] - y0[i];
+        b[i] = h * k1[i] - d[i];
+        c[i] = d[i] - h * k7[i] - b[i];
+    }
+    auto z_at = [&](double t) { return y0[2] + t * (d[2] + (1.0 - t) * (b[2] + t * (c[2] + (1.0 - t) * e[2]))); };
+    double lo = 0.0, hi = 1.0, flo = y0[2], fhi = y1[2], t = 1.0;
+    int side = 0;
+    for (int it = 0; it < 60; ++it) {
+        t = (lo * fhi - hi * flo) / (fhi - flo);
+        if (!(t > lo && t < hi)) t = 0.5 * (lo + hi);
+        const double ft = z_at(t);
+        if (ft == 0.0 || fabs(hi - lo) < 1e-15 || fabs(ft) < 1e-13 * (1.0 + fabs(y0[0]) + fabs(y0[1]))) break;
+        if ((ft > 0.0) == (fhi > 0.0)) {
+            hi = t;
+            fhi = ft;
+            if (side == -1) flo *= 0.5;
+            side = -1;
+        } else {
+            lo = t;
+            flo = ft;
+            if (side == 1) fhi *= 0.5;
+            side = 1;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) out[i] = y0[i] + t * (d[i] + (1.0 - t) * (b[i] + t * (c[i] + (1.0 - t) * e[i])));
+    return t;
+}
+
+// A ray in the near pass returns to the far pass once r_BL exceeds this
+// multiple of the FP64 radius (hysteresis against ping-pong at the boundary).
+constexpr double kNearExitFactor = 1.25;
+
 // Largest r_BL at which the FP32 stages are used (keeps r^4 and 1/r^4 in range).
 constexpr double kFp32MaxRadius = 1e6;
 
@@ -326,9 +425,13 @@ constexpr double kFp32MaxRadius = 1e6;
 // The error estimate uses sum_j e_j = 0: E_x = h sum e_j dx_j.  Outputs k7 in
 // FP64 (FSAL), |E| per component, and the FP32 BL radius, H and s of the FSAL
 // stage at y5 (the step's bookkeeping: step cap, termination, projection).
+// When the step crosses z = 0 it also writes the dense-output term
+// e = h sum_j D_j k_j; sum_j D_j = 0 makes its position part h sum_j D_j dx_j,
+// so it too comes from the FP32 deviations.
 __device__ __forceinline__ void mixed_stages(const double* __restrict__ y, const double* __restrict__ k1, double hh,
                                              double M, double a, double* __restrict__ y5, double* __restrict__ k7,
-                                             double* __restrict__ est, float& r7, float& hf7, float& s7) {
+                                             double* __restrict__ est, float& r7, float& hf7, float& s7,
+                                             double* __restrict__ dense_e) {
     const float h = static_cast<float>(hh);
     const float Mf = static_cast<float>(M), af = static_cast<float>(a);
     float x0[3], p0[3];
@@ -398,6 +501,18 @@ __device__ __forceinline__ void mixed_stages(const double* __restrict__ y, const
         est[3 + i] = static_cast<double>(fabsf(h * ep));
         k7[i] = y5[3 + i] + static_cast<double>(g[i]);
         k7[3 + i] = static_cast<double>(g[3 + i]);
+    }
+    if (y[2] * y5[2] <= 0.0) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float dx7 = static_cast<float>(y5[3 + i] - y[3 + i]) + g[i];
+            const float sx = float(DP::D1) * dx1[i] + float(DP::D3) * dx3[i] + float(DP::D4) * dx4[i] +
+                             float(DP::D5) * dx5[i] + float(DP::D6) * dx6[i] + float(DP::D7) * dx7;
+            const float sp = float(DP::D1) * kp1[i] + float(DP::D3) * kp3[i] + float(DP::D4) * kp4[i] +
+                             float(DP::D5) * kp5[i] + float(DP::D6) * kp6[i] + float(DP::D7) * g[3 + i];
+            dense_e[i] = static_cast<double>(h * sx);
+            dense_e[3 + i] = static_cast<double>(h * sp);
+        }
     }
 }
 
@@ -472,7 +587,16 @@ __device__ __forceinline__ float pi30_factor(float le, float lp, float order_p1)
 
 // 384 / BLOCK resident CTAs per SM caps the kernel at 168 registers per thread
 // (12 warps per SM).
-template <int BLOCK, bool MIXED, bool ROLLED>
+//
+// PASS selects the single-kernel tracer or one pass of the two-pass mixed
+// tracer.  The far pass (FP32 stages only) parks a ray when it enters the FP64
+// zone; the near pass (FP64 stages) parks it back when it leaves the zone
+// again.  Both passes solve disk crossings on the step's dense output.  Parked
+// rays resume from their saved state, so a ray's arithmetic does not depend on
+// which rays share its warp.
+// Every form runs 12 warps per SM (168 registers); the pass kernels spill a
+// little there, which measured faster than 8 warps without spills.
+template <int BLOCK, bool MIXED, bool ROLLED, int PASS = PASS_SINGLE>
 __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs args) {
     __shared__ Cold<BLOCK> S;
     __shared__ KStore<ROLLED ? BLOCK : 1> K;
@@ -480,6 +604,13 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
+    constexpr bool FAR_PASS = (PASS == PASS_FAR);
+    constexpr bool NEAR_PASS = (PASS == PASS_NEAR);
+    static_assert(!FAR_PASS || MIXED, "the far pass runs the FP32 stages");
+    static_assert(!NEAR_PASS || !MIXED, "the near pass runs FP64 stages");
+    // rays of this launch: pixels (single kernel, first far pass) or queue entries
+    const bool from_queue = (PASS != PASS_SINGLE) && !(FAR_PASS && args.from_pixels != 0);
+    const uint64_t total = from_queue ? static_cast<uint64_t>(*args.in_count) : args.total_rays;
 
     // hot lane state
     double y[6], k1[6];
@@ -490,6 +621,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     bool has_hist = false;
     bool k1_fp32 = false;  // k1 came from an FP32 far-zone stage (mixed mode)
     uint32_t guard = 0;    // loop iterations spent on the current ray
+    uint64_t ray = 0;        // launch index of the lane's ray
 #pragma unroll
     for (int i = 0; i < 6; ++i) y[i] = k1[i] = 0.0;
 
@@ -499,6 +631,42 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     unsigned long long n_att = 0, n_acc = 0, n_rays = 0, n_rhs = 0, n_far = 0;
 
     for (;;) {
+        if constexpr (PASS != PASS_SINGLE) {
+            // park the lanes whose rays go to the other pass, and the disk hits for
+            // the finish pass (one atomic per warp and queue)
+            const unsigned pmask = __ballot_sync(FULL, mode == MODE_PARK);
+            const unsigned fmask = __ballot_sync(FULL, mode == MODE_FINISHQ);
+            if (pmask | fmask) {
+                uint32_t pbase = 0, fbase = 0;
+                if (pmask) {
+                    const int leader = __ffs(pmask) - 1;
+                    if (lane == leader) pbase = atomicAdd(args.out_count, static_cast<uint32_t>(__popc(pmask)));
+                    pbase = __shfl_sync(FULL, pbase, leader);
+                }
+                if (fmask) {
+                    const int leader = __ffs(fmask) - 1;
+                    if (lane == leader) fbase = atomicAdd(args.finish_count, static_cast<uint32_t>(__popc(fmask)));
+                    fbase = __shfl_sync(FULL, fbase, leader);
+                }
+                if (mode == MODE_PARK || mode == MODE_FINISHQ) {
+                    if (mode == MODE_PARK)
+                        args.out_queue[pbase + static_cast<uint32_t>(__popc(pmask & lt_mask))] = static_cast<uint32_t>(ray);
+                    else
+                        args.finish_queue[fbase + static_cast<uint32_t>(__popc(fmask & lt_mask))] =
+                            static_cast<uint32_t>(ray);
+                    double xch[7];
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) xch[i] = y[i];
+                    xch[6] = h;
+                    const uint32_t misc =
+                        (has_hist ? PM_HAS_HIST : 0u) | (static_cast<uint32_t>(can_early + 1) << PM_EARLY_SHIFT);
+                    const uint32_t uch[PU_COUNT] = {acc, rej, flags, guard, static_cast<uint32_t>(wind), misc,
+                                                    __float_as_uint(lnp)};
+                    park_ray<BLOCK>(args.park, ray, S, tid, xch, uch);
+                    mode = MODE_IDLE;
+                }
+            }
+        }
         // ---- refill idle lanes: from the warp's chunk, then from a new chunk
         //      of `claim` consecutive rays (one global atomic per chunk) ----
         const unsigned idle = __ballot_sync(FULL, mode == MODE_IDLE);
@@ -513,12 +681,12 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 unsigned long long b = 0;
                 if (lane == leader) b = atomicAdd(args.queue, static_cast<unsigned long long>(args.claim));
                 b = __shfl_sync(FULL, b, leader);
-                if (b >= args.total_rays) {
+                if (b >= total) {
                     queue_open = false;
                 } else {
                     base2 = b;
                     got2 = true;
-                    if (b + args.claim >= args.total_rays) queue_open = false;
+                    if (b + args.claim >= total) queue_open = false;
                 }
             }
             const uint64_t used_old = (avail < static_cast<uint64_t>(n_idle)) ? avail : n_idle;
@@ -527,40 +695,74 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 uint64_t rid = ~0ull;
                 if (rank < avail) rid = chunk_next + rank;
                 else if (got2) rid = base2 + (rank - avail);
-                if (rid < args.total_rays) {
-                    // bundle of this ray: last bundle whose ray_begin <= rid
+                if (rid < total) {
+                    uint64_t rix = rid;
+                    if constexpr (PASS != PASS_SINGLE) {
+                        rix = from_queue ? static_cast<uint64_t>(args.in_queue[rid]) : args.ray_base + rid;
+                    }
+                    // bundle of this ray: last bundle whose ray_begin <= rix
                     uint32_t lo = 0, hi = args.n_bundles;
                     while (hi - lo > 1) {
                         const uint32_t mid = (lo + hi) >> 1;
-                        if (args.bundles[mid].ray_begin <= rid) lo = mid; else hi = mid;
+                        if (args.bundles[mid].ray_begin <= rix) lo = mid; else hi = mid;
                     }
                     bidx = lo;
-                    double xch[12];
-                    const InitResult ir =
-                        init_ray<BLOCK>(args.bundles + lo, rid - args.bundles[lo].ray_begin, S, tid, xch);
+                    ray = rix;
+                    bool resumed = false;
+                    if constexpr (PASS != PASS_SINGLE) {
+                        if (from_queue) {
+                            double xch[13];
+                            uint32_t uch[PU_COUNT];
+                            r = resume_ray<BLOCK>(args.bundles + lo, args.park, rix, rix - args.bundles[lo].ray_begin,
+                                                  S, tid, xch, uch);
 #pragma unroll
-                    for (int i = 0; i < 6; ++i) {
-                        y[i] = xch[i];
-                        k1[i] = xch[6 + i];
+                            for (int i = 0; i < 6; ++i) {
+                                y[i] = xch[i];
+                                k1[i] = xch[6 + i];
+                            }
+                            h = xch[12];
+                            acc = uch[PU_ACC];
+                            rej = uch[PU_REJ];
+                            flags = uch[PU_FLAGS];
+                            guard = uch[PU_GUARD];
+                            wind = static_cast<int>(uch[PU_WIND]);
+                            has_hist = (uch[PU_MISC] & PM_HAS_HIST) != 0u;
+                            can_early = static_cast<int>((uch[PU_MISC] >> PM_EARLY_SHIFT) & 3u) - 1;
+                            lnp = __uint_as_float(uch[PU_LNP]);
+                            k1_fp32 = false;
+                            mode = MODE_STEP;
+                            ++n_rhs;
+                            resumed = true;
+                        }
                     }
-                    r = ir.r;
-                    can_early = ir.can_early;
-                    h = -args.bundles[lo].h0;
-                    lnp = 0.0f;
-                    has_hist = false;
-                    acc = rej = flags = 0;
-                    wind = args.bundles[lo].wind0;
-                    k1_fp32 = false;
-                    guard = 0;
-                    mode = MODE_STEP;
-                    ++n_rays;
-                    ++n_rhs;
+                    if (!resumed) {
+                        double xch[12];
+                        const InitResult ir =
+                            init_ray<BLOCK>(args.bundles + lo, rix - args.bundles[lo].ray_begin, S, tid, xch);
+#pragma unroll
+                        for (int i = 0; i < 6; ++i) {
+                            y[i] = xch[i];
+                            k1[i] = xch[6 + i];
+                        }
+                        r = ir.r;
+                        can_early = ir.can_early;
+                        h = -args.bundles[lo].h0;
+                        lnp = 0.0f;
+                        has_hist = false;
+                        acc = rej = flags = 0;
+                        wind = args.bundles[lo].wind0;
+                        k1_fp32 = false;
+                        guard = 0;
+                        mode = MODE_STEP;
+                        ++n_rays;
+                        ++n_rhs;
+                    }
                 }
             }
             if (got2) {
                 chunk_next = base2 + (static_cast<uint64_t>(n_idle) - used_old);
                 chunk_end = base2 + args.claim;
-                if (chunk_end > args.total_rays) chunk_end = args.total_rays;
+                if (chunk_end > total) chunk_end = total;
             } else {
                 chunk_next += used_old;
             }
@@ -573,7 +775,9 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
         // lane is inside the FP64 zone (one instruction stream per iteration;
         // lanes in a root solve always run FP64)
         bool far = false;
-        if constexpr (MIXED) {
+        if constexpr (FAR_PASS) {
+            far = true;  // near-zone rays were parked for the near pass
+        } else if constexpr (MIXED) {
             const bool stepping = (mode == MODE_STEP || mode == MODE_REDO);
             const BundleDesc* Bz = args.bundles + bidx;
             const bool lane_far = stepping && r >= Bz->fp64_radius && r < kFp32MaxRadius;
@@ -623,6 +827,19 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 mode = MODE_IDLE;
                 continue;
             }
+            if constexpr (FAR_PASS) {
+                if (r < Bp->fp64_radius || r >= kFp32MaxRadius) {  // into the FP64 zone
+                    mode = MODE_PARK;
+                    continue;
+                }
+            }
+            if constexpr (NEAR_PASS) {
+                if (args.allow_exit != 0u && r >= kNearExitFactor * Bp->fp64_radius &&
+                    r < kFp32MaxRadius) {  // back out of the FP64 zone
+                    mode = MODE_PARK;
+                    continue;
+                }
+            }
         } else if (mode == MODE_ROOT) {
             const double lo = S.lo[tid], hi = S.hi[tid], flo = S.flo[tid], fhi = S.fhi[tid];
             double t = (lo * fhi - hi * flo) / (fhi - flo);
@@ -634,6 +851,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
         // ---- Dormand-Prince stages 2..7 (rk45_adaptive.hpp:210-252); stage 7 is
         //      the FSAL stage at the 5th-order solution y5.  kA holds k2 for
         //      stages 3..6, then k7; est holds |h| |sum_j e_j k_j| per component. ----
+        double dense5[6];  // h sum_j D_j k_j of a step that crosses z = 0 (two-pass tracer)
         double kA[6], y5[6], est[6];
         double r5 = 0.0, hf5 = 0.0, s5 = 0.0;
         const bool root = (mode == MODE_ROOT);
@@ -641,12 +859,12 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
             // FP32 radius, H and s of the FSAL stage: the projection then holds
             // H = 0 to the FP32 stages' own accuracy
             float r7, hf7, s7;
-            mixed_stages(y, k1, hh, M, a, y5, kA, est, r7, hf7, s7);
+            mixed_stages(y, k1, hh, M, a, y5, kA, est, r7, hf7, s7, dense5);
             r5 = r7;
             hf5 = hf7;
             s5 = s7;
             if (mode == MODE_STEP) ++n_far;
-        } else {
+        } else if constexpr (!FAR_PASS) {
             if constexpr (MIXED) {
                 if (k1_fp32) {  // entering the FP64 zone: first stage again in FP64
                     double hf, sv;
@@ -657,6 +875,14 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
             }
             if constexpr (ROLLED) {
                 fp64_stages_rolled<BLOCK>(y, k1, hh, M, a, K, tid, root, y5, kA, est, r5, hf5, s5);
+                if constexpr (NEAR_PASS) {
+                    if (y[2] * y5[2] <= 0.0) {  // dense-output term; K holds k2..k7
+#pragma unroll
+                        for (int i = 0; i < 6; ++i)
+                            dense5[i] = hh * (DP::D1 * k1[i] + DP::D3 * K.k[1][i][tid] + DP::D4 * K.k[2][i][tid] +
+                                              DP::D5 * K.k[3][i][tid] + DP::D6 * K.k[4][i][tid] + DP::D7 * kA[i]);
+                    }
+                }
             } else {
                 double k3[6], k4[6], k5[6], k6[6];
                 double in[6], hf, sv;
@@ -689,12 +915,20 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                     for (int i = 0; i < 6; ++i)
                         est[i] = fabs(hh) * fabs(DP::E1 * k1[i] + DP::E3 * k3[i] + DP::E4 * k4[i] +
                                                  DP::E5 * k5[i] + DP::E6 * k6[i] + DP::E7 * kA[i]);
+                    if constexpr (NEAR_PASS) {
+                        if (y[2] * y5[2] <= 0.0) {
+#pragma unroll
+                            for (int i = 0; i < 6; ++i)
+                                dense5[i] = hh * (DP::D1 * k1[i] + DP::D3 * k3[i] + DP::D4 * k4[i] +
+                                                  DP::D5 * k5[i] + DP::D6 * k6[i] + DP::D7 * kA[i]);
+                        }
+                    }
                 }
             }
         }
         n_rhs += root ? 5 : 6;
 
-        if (root) {
+        if (PASS == PASS_SINGLE && root) {
             const double ft = y5[2];
             const int rit = ++S.rit[tid];
             const double lo = S.lo[tid], hi = S.hi[tid];
@@ -799,14 +1033,34 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 const double re = sqrt(fmax(xe * xe + ye * ye - a * a, 0.0));
                 const double margin = 0.05 * re + 0.5 * M;
                 if (re >= Bp->r_in - margin && re <= Bp->r_out + margin) {
-                    mode = MODE_ROOT;
-                    S.lo[tid] = 0.0;
-                    S.flo[tid] = y[2];
-                    S.hi[tid] = 1.0;
-                    S.fhi[tid] = y5[2];
-                    S.side[tid] = 0;
-                    S.rit[tid] = 0;
-                    continue;
+                    if constexpr (PASS != PASS_SINGLE) {
+                        // FP64 root on the step's dense output (its correction term from
+                        // this step's stages: FP32 in the far pass, FP64 in the near
+                        // pass); off the disk the step is accepted as it is
+                        double xr[18];
+                        const double t = dense_disk_root(y, k1, y5, kA, dense5, hh, xr + 12);
+                        const double rr = sqrt(bl_r2<double>(xr[12], xr[13], xr[14], a * a));
+                        if (rr >= Bp->r_in && rr <= Bp->r_out && rr > Bp->rh * 1.02) {
+                            // a disk hit: park the root point (r_hit in the step slot) for
+                            // the finish pass, which writes the record in lockstep
+                            S.lambda[tid] += t * hh;
+                            wind += branch_winding(y[0], y[1], xr[12], xr[13]);
+#pragma unroll
+                            for (int i = 0; i < 6; ++i) y[i] = xr[12 + i];
+                            h = rr;
+                            mode = MODE_FINISHQ;
+                            continue;
+                        }
+                    } else {
+                        mode = MODE_ROOT;
+                        S.lo[tid] = 0.0;
+                        S.flo[tid] = y[2];
+                        S.hi[tid] = 1.0;
+                        S.fhi[tid] = y5[2];
+                        S.side[tid] = 0;
+                        S.rit[tid] = 0;
+                        continue;
+                    }
                 }
             }
         }
@@ -921,6 +1175,10 @@ template __global__ void trace_kernel_t<64, false, true>(TraceArgs);
 template __global__ void trace_kernel_t<128, false, true>(TraceArgs);
 template __global__ void trace_kernel_t<64, true, true>(TraceArgs);
 template __global__ void trace_kernel_t<128, true, true>(TraceArgs);
+template __global__ void trace_kernel_t<64, true, false, PASS_FAR>(TraceArgs);
+template __global__ void trace_kernel_t<128, true, false, PASS_FAR>(TraceArgs);
+template __global__ void trace_kernel_t<64, false, false, PASS_NEAR>(TraceArgs);
+template __global__ void trace_kernel_t<128, false, false, PASS_NEAR>(TraceArgs);
 
 namespace {
 // Mixed precision always uses the rolled FP64 step (its FP64 steps are a
@@ -959,6 +1217,167 @@ int trace_occupancy(uint32_t block, bool mixed, bool rolled) {
     return n;
 }
 
+// Finish pass of the two-pass mixed tracer: the record and pixel of every disk
+// hit parked by the far and near passes (root point, r_hit in the step slot).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) finish_kernel_t(TraceArgs args) {
+    __shared__ Cold<BLOCK> S;
+    const int tid = threadIdx.x;
+    const uint64_t count = *args.in_count;
+    const uint64_t n = args.park.n;
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * BLOCK + tid; j < count;
+         j += static_cast<uint64_t>(gridDim.x) * BLOCK) {
+        const uint64_t ray = args.in_queue[j];
+        uint32_t lo = 0, hi = args.n_bundles;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (args.bundles[mid].ray_begin <= ray) lo = mid; else hi = mid;
+        }
+        const BundleDesc* Bp = args.bundles + lo;
+        double xch[18];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) xch[i] = xch[12 + i] = args.park.d[(PD_Y + i) * n + ray];
+        const double r_hit = args.park.d[PD_H * n + ray];
+        S.lambda[tid] = args.park.d[PD_LAMBDA * n + ray];
+        S.dH[tid] = args.park.d[PD_DH * n + ray];
+        S.lz0[tid] = args.park.d[PD_LZ0 * n + ray];
+        S.q0[tid] = args.park.d[PD_Q0 * n + ray];
+        S.local[tid] = ray - Bp->ray_begin;
+        finish_ray<BLOCK>(Bp, S, tid, RT_RAY_DISK, args.park.u[PU_FLAGS * n + ray], args.park.u[PU_ACC * n + ray],
+                          args.park.u[PU_REJ * n + ray], static_cast<int>(args.park.u[PU_WIND * n + ray]), 0.0, 0.0,
+                          r_hit, disk_redshift(Bp->m, Bp->a, r_hit, S.lz0[tid]), args.out, xch);
+    }
+}
+template __global__ void finish_kernel_t<128>(TraceArgs);
+
+namespace {
+const void* pass_kernel(int pass, uint32_t block) {
+    if (pass == PASS_FAR)
+        return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, true, false, PASS_FAR>)
+                             : reinterpret_cast<const void*>(&trace_kernel_t<128, true, false, PASS_FAR>);
+    return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, false, false, PASS_NEAR>)
+                         : reinterpret_cast<const void*>(&trace_kernel_t<128, false, false, PASS_NEAR>);
+}
+}  // namespace
+
+int trace_pass_occupancy(int pass, uint32_t block) {
+    int n = 0;
+    block = (block == 64) ? 64u : 128u;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pass_kernel(pass, block), static_cast<int>(block), 0) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n;
+}
+
+void launch_trace_pass(const TraceArgs& args, int pass, uint32_t grid, uint32_t block, void* stream) {
+    void* params[] = {const_cast<TraceArgs*>(&args)};
+    block = (block == 64) ? 64u : 128u;
+    cudaLaunchKernel(pass_kernel(pass, block), dim3(grid), dim3(block), params, 0, static_cast<cudaStream_t>(stream));
+}
+
+// Rounds of the two-pass mixed tracer: far pass (FP32) then near pass (FP64),
+// the last near pass keeping every ray to its end.  A ray typically needs one
+// round (in to a disk crossing or the near zone, and out); rays left after the
+// last far pass finish in FP64.
+constexpr int kMixedRounds = 4;
+// Refill threshold of the near pass: its rays resume from parked state (a few
+// loads and one RHS), so refilling a partly idle warp is cheap, while the
+// near-zone work per ray (disk root, photon-region orbits) varies widely.
+constexpr uint32_t kNearRefill = 16;  // measured best of 1, 4, 8, 16, 32
+
+uint64_t two_pass_state_bytes(uint64_t n) {
+    return n * (sizeof(double) * PD_COUNT + sizeof(uint32_t) * PU_COUNT + 3 * sizeof(uint32_t));
+}
+
+// Per-band queue counters (32 bytes): [0] far-pass claim (u64), [8] near queue
+// count (u32), [12] far queue count (u32), [16] near-pass claim (u64), zeroed
+// pairwise before each pass; [24] finish queue count (u32), zeroed once.
+namespace {
+cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t begin, uint64_t count, char* qb,
+                         uint32_t far_grid, uint32_t far_block, uint32_t near_grid, uint32_t finish_grid,
+                         cudaStream_t s) {
+    uint32_t* near_q = buf.queues + 3 * begin;
+    uint32_t* far_q = near_q + count;
+    args.park = buf.park;
+    args.total_rays = count;
+    args.ray_base = begin;
+    args.finish_queue = far_q + count;
+    args.finish_count = reinterpret_cast<uint32_t*>(qb + 24);
+    const uint32_t far_refill = args.refill_threshold;
+    cudaError_t e = cudaMemsetAsync(qb + 24, 0, 8, s);
+    for (int round = 0; e == cudaSuccess && round < kMixedRounds; ++round) {
+        // far pass: pixels (first round) or the far queue -> near queue
+        if ((e = cudaMemsetAsync(qb, 0, 12, s)) != cudaSuccess) break;
+        args.queue = reinterpret_cast<unsigned long long*>(qb);
+        args.refill_threshold = far_refill;
+        args.from_pixels = (round == 0) ? 1u : 0u;
+        args.allow_exit = 0;
+        args.in_queue = far_q;
+        args.in_count = reinterpret_cast<const uint32_t*>(qb + 12);
+        args.out_queue = near_q;
+        args.out_count = reinterpret_cast<uint32_t*>(qb + 8);
+        launch_trace_pass(args, PASS_FAR, far_grid, far_block, s);
+        if ((e = cudaGetLastError()) != cudaSuccess) break;
+        // near pass: near queue -> far queue (the last one keeps its rays)
+        if ((e = cudaMemsetAsync(qb + 12, 0, 12, s)) != cudaSuccess) break;
+        args.queue = reinterpret_cast<unsigned long long*>(qb + 16);
+        args.refill_threshold = far_refill < kNearRefill ? far_refill : kNearRefill;
+        args.from_pixels = 0;
+        args.allow_exit = (round + 1 < kMixedRounds) ? 1u : 0u;
+        args.in_queue = near_q;
+        args.in_count = reinterpret_cast<const uint32_t*>(qb + 8);
+        args.out_queue = far_q;
+        args.out_count = reinterpret_cast<uint32_t*>(qb + 12);
+        launch_trace_pass(args, PASS_NEAR, near_grid, 128, s);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return e;
+    // finish pass over the band's parked disk hits
+    args.in_queue = args.finish_queue;
+    args.in_count = args.finish_count;
+    finish_kernel_t<128><<<finish_grid, 128, 0, s>>>(args);
+    return cudaGetLastError();
+}
+}  // namespace
+
+int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_count, uint32_t far_block,
+                     void* stream, void* stream2, void* fork, void* join, uint32_t bands) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStream_t s2 = static_cast<cudaStream_t>(stream2);
+    const uint64_t n = base.total_rays;
+    if (!s2 || !fork || !join) bands = 1;
+    bands = bands < 1 ? 1 : (bands > kMaxBands ? kMaxBands : bands);
+    if (static_cast<uint64_t>(bands) > n) bands = static_cast<uint32_t>(n > 0 ? n : 1);
+    far_block = (far_block == 64) ? 64u : 128u;
+    const int far_occ = trace_pass_occupancy(PASS_FAR, far_block);
+    const int near_occ = trace_pass_occupancy(PASS_NEAR, 128);
+    const uint32_t far_grid = static_cast<uint32_t>(sm_count) * static_cast<uint32_t>(far_occ > 1 ? far_occ : 1);
+    const uint32_t near_grid = static_cast<uint32_t>(sm_count) * static_cast<uint32_t>(near_occ > 1 ? near_occ : 1);
+    const uint32_t finish_grid = static_cast<uint32_t>(sm_count) * 8u;
+    cudaError_t e = cudaSuccess;
+    if (bands > 1) {
+        if ((e = cudaEventRecord(static_cast<cudaEvent_t>(fork), s)) != cudaSuccess) return static_cast<int>(e);
+        if ((e = cudaStreamWaitEvent(s2, static_cast<cudaEvent_t>(fork), 0)) != cudaSuccess) return static_cast<int>(e);
+    }
+    // bands of whole warps' worth of rays (multiples of 32)
+    const uint64_t per = ((n + bands - 1) / bands + 31) / 32 * 32;
+    uint64_t begin = 0;
+    for (uint32_t b = 0; b < bands && begin < n && e == cudaSuccess; ++b) {
+        const uint64_t count = (n - begin < per) ? n - begin : per;
+        e = enqueue_band(base, buf, begin, count, buf.counters + 32 * b, far_grid, far_block, near_grid, finish_grid,
+                         (b & 1u) ? s2 : s);
+        begin += count;
+    }
+    if (e != cudaSuccess) return static_cast<int>(e);
+    if (bands > 1) {
+        if ((e = cudaEventRecord(static_cast<cudaEvent_t>(join), s2)) != cudaSuccess) return static_cast<int>(e);
+        e = cudaStreamWaitEvent(s, static_cast<cudaEvent_t>(join), 0);
+    }
+    return static_cast<int>(e);
+}
+
 void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled, void* stream) {
     void* params[] = {const_cast<TraceArgs*>(&args)};
     block = kernel_block(block, mixed, rolled);
@@ -969,6 +1388,7 @@ void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mix
 rt_launch_config resolve_launch_config(rt_launch_config c, bool mixed) {
     if (c.block_size != 64 && c.block_size != 128 && c.block_size != 256) c.block_size = 128;
     c.fp64_rolled = c.fp64_rolled ? 1u : 0u;
+    c.mixed_single_kernel = c.mixed_single_kernel ? 1u : 0u;
     c.block_size = kernel_block(c.block_size, mixed, c.fp64_rolled != 0);
     const int occ = trace_occupancy(c.block_size, mixed, c.fp64_rolled != 0);
     if (c.ctas_per_sm == 0 || static_cast<int>(c.ctas_per_sm) > occ) c.ctas_per_sm = occ > 1 ? occ : 1;

@@ -68,7 +68,7 @@ class RayOut(ctypes.Structure):
 
 class LaunchConfig(ctypes.Structure):
     _fields_ = [("block_size", _u32), ("ctas_per_sm", _u32), ("refill_threshold", _u32), ("rays_per_thread", _u32),
-                ("fp64_rolled", _u32)]
+                ("fp64_rolled", _u32), ("mixed_single_kernel", _u32)]
 
 
 class Stats(ctypes.Structure):
@@ -309,8 +309,8 @@ class Tracer:
         self._check(self.lib.rt_synchronize(self._h, timeout_ms))
 
     def set_launch_config(self, block_size: int = 0, ctas_per_sm: int = 0, refill_threshold: int = 0,
-                          rays_per_thread: int = 0, fp64_rolled: int = 0) -> None:
-        c = LaunchConfig(block_size, ctas_per_sm, refill_threshold, rays_per_thread, fp64_rolled)
+                          rays_per_thread: int = 0, fp64_rolled: int = 0, mixed_single_kernel: int = 0) -> None:
+        c = LaunchConfig(block_size, ctas_per_sm, refill_threshold, rays_per_thread, fp64_rolled, mixed_single_kernel)
         self._check(self.lib.rt_set_launch_config(self._h, ctypes.byref(c)))
 
     def launch_config(self) -> LaunchConfig:

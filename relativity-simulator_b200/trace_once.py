@@ -32,6 +32,8 @@ def main() -> None:
     ap.add_argument("--fp64-rolled", type=int, default=0)
     ap.add_argument("--rtol", type=float, default=None)
     ap.add_argument("--fp64-radius", type=float, default=0.0)
+    ap.add_argument("--mixed-single", type=int, default=0,
+                    help="mixed precision: 1 = the single-kernel form instead of far/near passes")
     ap.add_argument("--record", choices=["minimal", "bench"], default="minimal",
                     help="outputs written: class and step counts, or the bench's record (class, r, theta, "
                          "phi, r_hit, g) plus the 32-byte pixels")
@@ -41,7 +43,7 @@ def main() -> None:
                              precision=relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64,
                              rtol=a.rtol, mixed_fp64_radius=a.fp64_radius)
     with relsim.Tracer(0) as tr:
-        tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread, a.fp64_rolled)
+        tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread, a.fp64_rolled, a.mixed_single)
         for _ in range(a.repeat):
             if a.record == "bench":
                 out = tr.dispatch(cam, fields=["status", "r", "theta", "phi", "r_hit", "g"], pixels=True)
@@ -49,7 +51,7 @@ def main() -> None:
                 out = tr.dispatch(cam, fields=["status", "steps_accepted", "steps_rejected"], pixels=False)
             s = tr.stats()
     print(json.dumps({"rays": int(s.rays), "attempts": int(s.attempts), "accepted": int(s.accepted),
-                      "fp64_attempts": int(s.fp64_attempts),
+                      "fp64_attempts": int(s.fp64_attempts), "rhs_evals": int(s.rhs_evals),
                       "kernel_ms": s.kernel_ms, "mrays_per_s": s.rays / s.kernel_ms / 1e3,
                       "classes": np.bincount(out["status"], minlength=4).tolist()}))
 

@@ -71,6 +71,8 @@ def test_noalloc_matches_the_handle_entry_point_twice(precision):
     cams = _cams(precision)
     n = relsim.bundle_rays(cams)
     with relsim.Tracer(0) as tr:
+        # the allocation-free call runs the single-kernel tracer (no buffers for parked rays)
+        tr.set_launch_config(mixed_single_kernel=1)
         ro, t, pix = _outputs(n)
         tr.trace_bundles_device(cams, ro, pix.data_ptr(), n)
         ref = _host(t, pix)
