@@ -69,6 +69,7 @@ enum {
     RT_RAYFLAG_STEP_UNDERFLOW = 1u << 1,
     RT_RAYFLAG_MAX_STEPS = 1u << 2,
     RT_RAYFLAG_EARLY_CAPTURE = 1u << 3
+    /* bit 4: RT_RAYFLAG_DIVERGED (multi-source, below) */
 };
 /* PixelFlags (gpu_types.hpp:1123-1130). */
 #define RT_PIXEL_HORIZON_ABSORBED (1u << 0)
@@ -171,6 +172,42 @@ int rt_is_ready(const rt_handle* h);
 int rt_is_platform_supported(void);
 const char* rt_last_error(const rt_handle* h);
 int rt_abi_version(void);
+
+/* ---- Multi-source Kerr-Schild superposition ----
+ * SoftwareComputeEngine's multi-source path (software_compute_engine.hpp:
+ * 2708-3252, trace_multi_source): the camera's hole at the origin plus black-
+ * hole bodies (GpuBodyData with preset 8), each with its own mass, spin axis
+ * and thin disk; the ray equations sum every source's Kerr-Schild terms in its
+ * local frame.  Traced in FP64 with the DP45 machinery of the single-hole
+ * tracer: projection onto H = 0 of the superposed Hamiltonian, step cap from
+ * the nearest source, captured inside capture_scale * r_+ of any source (or,
+ * flag RT_RAYFLAG_DIVERGED, when the momentum exceeds 1000: a horizon-like
+ * region of the summed fields), escaped at |x| > escape_radius, disk hit at a
+ * source's first equatorial crossing on its disk (g from that source's disk).
+ * The record's r, theta, phi are spherical about the origin; dE, dLz, dQ are
+ * NaN (no Kerr invariants for the superposition). */
+#define RT_MAX_SOURCES 16        /* the camera's hole and up to 15 sources */
+#define RT_RAYFLAG_DIVERGED (1u << 4)
+
+/* A black-hole body (GpuBodyData, gpu_types.hpp:1213-1307, preset 8). */
+typedef struct rt_source {
+    double position[3];
+    double mass;
+    double spin_parameter;  /* a / m, clamped to [-0.9999, 0.9999] */
+    double axis[3];         /* spin axis (normalised here; zero selects +z) */
+    double disk_enabled;    /* > 0.5: thin disk */
+    double disk_inner_scale;/* inner radius = max(scale, 1) * r_ISCO of the source */
+    double disk_outer_units;/* outer radius = max(units * mass, 1.05 * inner) */
+} rt_source;
+
+/* Trace the row window of a multi-source scene (host buffers, as rt_dispatch).
+ * The camera's metric_mass / metric_spin / disk describe the hole at the
+ * origin; n_sources <= RT_MAX_SOURCES - 1 more.  FP64 only. */
+rt_status rt_dispatch_multi(rt_handle* h, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
+                            rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity);
+/* Device-resident form: device outputs, enqueued on `stream` (NULL: the handle's). */
+rt_status rt_dispatch_multi_device(rt_handle* h, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
+                                   rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity, void* stream);
 
 /* Prograde/retrograde ISCO radius by the sign of the spin
  * (SoftwareComputeEngine::kerr_isco_radius, software_compute_engine.hpp:1052-1061). */
@@ -283,6 +320,9 @@ void rt_server_destroy(rt_server* s);
  * RT_ERR_AGAIN: max_requests reached; RT_ERR_BUDGET: larger than the whole budget. */
 rt_status rt_server_submit(rt_server* s, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
                            size_t capacity, uint64_t* id);
+/* Queue a multi-source scene (see rt_dispatch_multi; traced in FP64). */
+rt_status rt_server_submit_multi(rt_server* s, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
+                                 rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity, uint64_t* id);
 /* Up to max_done finished requests, waiting at most timeout_ms for the first. */
 rt_status rt_server_poll(rt_server* s, rt_request_done* done, uint32_t max_done, uint32_t* n_done,
                          double timeout_ms);

@@ -45,7 +45,8 @@ enum {
     ORC_FLAG_NONFINITE = 1u << 0,
     ORC_FLAG_STEP_UNDERFLOW = 1u << 1,
     ORC_FLAG_MAX_STEPS = 1u << 2,
-    ORC_FLAG_EARLY_CAPTURE = 1u << 3
+    ORC_FLAG_EARLY_CAPTURE = 1u << 3,
+    ORC_FLAG_DIVERGED = 1u << 4 /* multi-source: |p| above ORC_MS_MAX_MOMENTUM */
 };
 
 /* A ray is declared captured before reaching capture_scale * r_+ when it is
@@ -118,6 +119,49 @@ double orc_dp45_attempt(const orc_camera* cam, const double y[6], double h, doub
  * threads <= 0 uses all online cores. */
 void orc_trace(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
                orc_ray* out, int threads);
+
+/* --- multi-source Kerr-Schild superposition (ms_oracle.c) --- */
+#define ORC_MS_MAX_SOURCES 16
+/* A multi-source ray whose momentum exceeds this (E = 1 units) is inside a
+ * horizon-like region of the superposed field, where the sum of the sources'
+ * fields traps it without reaching any single source's horizon: it is
+ * captured, with ORC_FLAG_DIVERGED. */
+#define ORC_MS_MAX_MOMENTUM 1e3
+
+/* A black-hole body beside the camera's own hole (GpuBodyData with preset 8). */
+typedef struct orc_source {
+    double position[3];
+    double mass;
+    double spin_parameter;   /* a / m, clamped to [-0.9999, 0.9999] */
+    double axis[3];          /* spin axis (normalised; zero selects +z) */
+    double disk_enabled;     /* > 0.5: thin disk */
+    double disk_inner_scale; /* inner radius = max(scale, 1) * r_ISCO */
+    double disk_outer_units; /* outer radius = max(units * m, 1.05 * inner) */
+} orc_source;
+
+/* Source table with local frames; source 0 is the camera's hole at the origin. */
+typedef struct orc_ms_table {
+    uint32_t count;
+    double pos[ORC_MS_MAX_SOURCES][3];
+    double mass[ORC_MS_MAX_SOURCES];
+    double axis[ORC_MS_MAX_SOURCES][3];
+    double spin[ORC_MS_MAX_SOURCES];
+    double fx[ORC_MS_MAX_SOURCES][3];
+    double rh[ORC_MS_MAX_SOURCES];
+    double fy[ORC_MS_MAX_SOURCES][3];
+    double req[ORC_MS_MAX_SOURCES];
+    double disk_in[ORC_MS_MAX_SOURCES];  /* < 0: no disk */
+    double disk_out[ORC_MS_MAX_SOURCES];
+} orc_ms_table;
+
+void orc_ms_build(const orc_camera* cam, const orc_source* src, uint32_t n, orc_ms_table* t);
+void orc_ms_rhs(const orc_ms_table* t, const double y[6], double dy[6]);
+double orc_ms_hamiltonian(const orc_ms_table* t, const double y[6]);
+void orc_ms_initial_momentum(const orc_ms_table* t, const double x[3], const double outward[3], double p[3]);
+int orc_ms_inside_horizon(const orc_ms_table* t, const double x[3]);
+void orc_ms_initial_state(const orc_camera* cam, const orc_ms_table* t, uint32_t px, uint32_t py, double y0[6]);
+void orc_ms_trace(const orc_camera* cam, const orc_ms_table* t, const uint64_t* pixel_index, uint64_t first,
+                  uint64_t count, orc_ray* out, int threads);
 
 #ifdef __cplusplus
 }

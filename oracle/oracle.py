@@ -52,6 +52,18 @@ RAY_DTYPE = np.dtype([
 
 CAPTURED, ESCAPED, DISK, UNFINISHED = 1, 2, 3, 0
 
+# orc_source: a black-hole body beside the camera's hole (ms_oracle.c)
+SOURCE_DTYPE = np.dtype([
+    ("position", "f8", 3), ("mass", "f8"), ("spin_parameter", "f8"), ("axis", "f8", 3),
+    ("disk_enabled", "f8"), ("disk_inner_scale", "f8"), ("disk_outer_units", "f8"),
+])
+MS_MAX_SOURCES = 16
+MS_TABLE_DTYPE = np.dtype([
+    ("count", "u4"), ("pad", "u4"), ("pos", "f8", (16, 3)), ("mass", "f8", 16), ("axis", "f8", (16, 3)),
+    ("spin", "f8", 16), ("fx", "f8", (16, 3)), ("rh", "f8", 16), ("fy", "f8", (16, 3)), ("req", "f8", 16),
+    ("disk_in", "f8", 16), ("disk_out", "f8", 16),
+])
+
 _D = ctypes.POINTER(ctypes.c_double)
 _lib = None
 _ref = None
@@ -100,6 +112,15 @@ def lib() -> ctypes.CDLL:
         L.orc_carter_q.restype = d
         L.orc_shadow_distance.argtypes = [d, d, d, d]
         L.orc_shadow_distance.restype = d
+        L.orc_ms_build.argtypes = [v, v, ctypes.c_uint32, v]
+        L.orc_ms_rhs.argtypes = [v, v, v]
+        L.orc_ms_hamiltonian.argtypes = [v, v]
+        L.orc_ms_hamiltonian.restype = d
+        L.orc_ms_initial_momentum.argtypes = [v, v, v, v]
+        L.orc_ms_inside_horizon.argtypes = [v, v]
+        L.orc_ms_initial_state.argtypes = [v, v, ctypes.c_uint32, ctypes.c_uint32, v]
+        L.orc_ms_trace.argtypes = [v, v, v, ctypes.c_uint64, ctypes.c_uint64, v, ctypes.c_int]
+        L.orc_ms_trace.restype = None
         _lib = L
     return _lib
 
@@ -133,6 +154,8 @@ def ref() -> ctypes.CDLL:
         L.ref_rk45_trace.argtypes = [v, d, d, d, d, d, d, d, d, d, ctypes.c_int, v]
         L.ref_dispatch_fp64.argtypes = [v, v, v, v, d, d, d, d, d, u, u, u, u, u, v, v, v]
         L.ref_dispatch_fp64.restype = d
+        L.ref_ms_case.argtypes = [v, u, v, v, v, v, v, v, v, v]
+        L.ref_ms_case.restype = u
         _ref = L
     return _ref
 
@@ -175,3 +198,36 @@ def boundary_band(rays: np.ndarray, r_in: float, r_out: float, band: float = 1e-
     rh = rays["r_hit"]
     near_disk = np.isfinite(rh) & ((np.abs(rh - r_in) < band) | (np.abs(rh - r_out) < band))
     return near_shadow | near_disk
+
+
+def sources_array(sources) -> np.ndarray:
+    """Pack source dicts (SOURCE_DTYPE keys) into orc_source structs."""
+    arr = np.zeros(len(sources), dtype=SOURCE_DTYPE)
+    for i, src in enumerate(sources):
+        for k in SOURCE_DTYPE.names:
+            arr[i][k] = src[k]
+    return arr
+
+
+def ms_table(cam: dict, sources) -> np.ndarray:
+    """The oracle's source table (camera hole + bodies)."""
+    c = to_camera(cam)
+    src = sources_array(sources)
+    t = np.zeros(1, dtype=MS_TABLE_DTYPE)
+    lib().orc_ms_build(_p(c), _p(src) if len(src) else None, len(src), _p(t))
+    return t
+
+
+def ms_trace(cam: dict, sources, pixels: np.ndarray | None = None, threads: int = 0) -> np.ndarray:
+    """Trace pixels (row-major indices) of a multi-source scene through the FP64 oracle."""
+    c = to_camera(cam)
+    t = ms_table(cam, sources)
+    if pixels is None:
+        n = int(cam["screen_width"]) * int(cam["screen_height"])
+        out = np.zeros(n, dtype=RAY_DTYPE)
+        lib().orc_ms_trace(_p(c), _p(t), None, 0, n, _p(out), threads)
+    else:
+        idx = np.ascontiguousarray(pixels, dtype=np.uint64)
+        out = np.zeros(idx.size, dtype=RAY_DTYPE)
+        lib().orc_ms_trace(_p(c), _p(t), _p(idx), 0, idx.size, _p(out), threads)
+    return out

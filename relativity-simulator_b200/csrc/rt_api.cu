@@ -43,6 +43,7 @@ struct rt_handle {
     // device scratch
     DevBuf bundles, queue, stats;
     DevBuf park_d, park_u, pass_queues;  // two-pass mixed tracer: parked state, far/near queues
+    DevBuf ms_desc, ms_sources;          // multi-source camera and source table
     DevBuf ray_fields[14];
     DevBuf pixels;
     // pinned staging of the bundle table
@@ -286,11 +287,95 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
     return wait_stream(h, h->stream, 0.0);
 }
 
+// Enqueue a multi-source trace of the camera's row window (outputs: device).
+rt_status ms_launch(rt_handle* h, const rt_camera* cam, const rt_source* src, uint32_t n_src, uint32_t row0,
+                    uint32_t nrows, const OutPtrs& out, cudaStream_t s) {
+    MsSource table[kMaxSources];
+    const uint32_t count = build_ms_sources(*cam, src, n_src, table);
+    MsDesc d;
+    build_ms_bundle(*cam, 0, cam->screen_width, row0, nrows, 0, 0, 0, count, d);
+    rt_status st;
+    if ((st = ensure(h, h->ms_desc, sizeof(MsDesc))) != RT_OK) return st;
+    if ((st = ensure(h, h->ms_sources, sizeof(table))) != RT_OK) return st;
+    // pageable sources: each copy is staged before the call returns
+    RT_CUDA(h, cudaMemcpyAsync(h->ms_desc.ptr, &d, sizeof d, cudaMemcpyHostToDevice, s));
+    RT_CUDA(h, cudaMemcpyAsync(h->ms_sources.ptr, table, sizeof(MsSource) * count, cudaMemcpyHostToDevice, s));
+    RT_CUDA(h, cudaMemsetAsync(h->queue.ptr, 0, sizeof(unsigned long long), s));
+    RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
+    MsArgs args{};
+    args.bundles = static_cast<const MsDesc*>(h->ms_desc.ptr);
+    args.sources = static_cast<const MsSource*>(h->ms_sources.ptr);
+    args.n_bundles = 1;
+    args.refill_threshold = 32;
+    args.claim = 32;
+    args.total_rays = static_cast<uint64_t>(cam->screen_width) * nrows;
+    args.queue = static_cast<unsigned long long*>(h->queue.ptr);
+    args.stats = static_cast<unsigned long long*>(h->stats.ptr);
+    args.out = out;
+    RT_CUDA(h, cudaEventRecord(h->ev0, s));
+    launch_ms_trace(args, ms_trace_grid(h->sm_count), s);
+    RT_CUDA(h, cudaGetLastError());
+    RT_CUDA(h, cudaEventRecord(h->ev1, s));
+    h->timed = true;
+    return RT_OK;
+}
+
+rt_status ms_check(rt_handle* h, const rt_camera* cam, const rt_source* src, uint32_t n_src) {
+    if (!h->ready) return fail(h, RT_ERR_NOT_READY, "handle not ready");
+    if (!camera_valid(cam)) return fail(h, RT_ERR_INVALID_ARG, "invalid camera");
+    if (n_src > RT_MAX_SOURCES - 1) return fail(h, RT_ERR_INVALID_ARG, "at most 15 sources beside the camera's hole");
+    if (n_src > 0 && !src) return fail(h, RT_ERR_INVALID_ARG, "null source table");
+    for (uint32_t i = 0; i < n_src; ++i)
+        if (!std::isfinite(src[i].mass) || !(src[i].mass > 0.0) || !std::isfinite(src[i].position[0]) ||
+            !std::isfinite(src[i].position[1]) || !std::isfinite(src[i].position[2]))
+            return fail(h, RT_ERR_INVALID_ARG, "invalid source");
+    return RT_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
 int rt_abi_version(void) { return RT_ABI_VERSION; }
+
+rt_status rt_dispatch_multi(rt_handle* h, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
+                            rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity) {
+    if (!h) return RT_ERR_INVALID_ARG;
+    rt_status st = ms_check(h, cam, sources, n_sources);
+    if (st != RT_OK) return st;
+    uint32_t row0, nrows;
+    row_window(*cam, row0, nrows);
+    const size_t n = static_cast<size_t>(cam->screen_width) * nrows;
+    if (n == 0) return fail(h, RT_ERR_INVALID_ARG, "empty row window");
+    if (capacity < n) return fail(h, RT_ERR_INVALID_ARG, "capacity smaller than the window");
+    RT_CUDA(h, cudaSetDevice(h->device));
+    rt_ray_out dev{};
+    if ((st = scratch_rays(h, rays, n, dev)) != RT_OK) return st;
+    rt_pixel_out* dpix = nullptr;
+    if (pixels) {
+        if ((st = ensure(h, h->pixels, n * sizeof(rt_pixel_out))) != RT_OK) return st;
+        dpix = static_cast<rt_pixel_out*>(h->pixels.ptr);
+    }
+    if ((st = ms_launch(h, cam, sources, n_sources, row0, nrows, OutPtrs{dpix, dev}, h->stream)) != RT_OK) return st;
+    if ((st = copy_back(h, rays, dev, pixels, dpix, n, h->stream)) != RT_OK) return st;
+    return wait_stream(h, h->stream, 0.0);
+}
+
+rt_status rt_dispatch_multi_device(rt_handle* h, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
+                                   rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity, void* stream) {
+    if (!h) return RT_ERR_INVALID_ARG;
+    rt_status st = ms_check(h, cam, sources, n_sources);
+    if (st != RT_OK) return st;
+    if (pixels && (reinterpret_cast<uintptr_t>(pixels) & 15u)) return fail(h, RT_ERR_INVALID_ARG, "pixels not 16-byte aligned");
+    uint32_t row0, nrows;
+    row_window(*cam, row0, nrows);
+    const size_t n = static_cast<size_t>(cam->screen_width) * nrows;
+    if (n == 0) return fail(h, RT_ERR_INVALID_ARG, "empty row window");
+    if (capacity < n) return fail(h, RT_ERR_INVALID_ARG, "capacity smaller than the window");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    RT_CUDA(h, cudaSetDevice(h->device));
+    return ms_launch(h, cam, sources, n_sources, row0, nrows, OutPtrs{pixels, rays ? *rays : rt_ray_out{}}, s);
+}
 
 double rt_kerr_isco_radius(double mass, double spin) { return kerr_isco_radius(mass, spin); }
 
@@ -347,6 +432,8 @@ void rt_destroy(rt_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     release(h->bundles);
+    release(h->ms_desc);
+    release(h->ms_sources);
     release(h->park_d);
     release(h->park_u);
     release(h->pass_queues);

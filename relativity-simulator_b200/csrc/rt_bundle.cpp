@@ -131,6 +131,111 @@ void build_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t 
               (cam.precision_mode == RT_PRECISION_MIXED ? BF_MIXED : 0u);
 }
 
+// Source table of a multi-source scene (software_compute_engine.hpp:2738-2798):
+// the camera's hole at the origin, then each body with its spin axis
+// normalised and a local frame from a helper axis (z unless the spin axis is
+// near z, then x).  The camera's disk radii are absolute (inner <= 0: r_ISCO),
+// a body's are scaled as in the reference.
+uint32_t build_ms_sources(const rt_camera& cam, const rt_source* src, uint32_t n, MsSource* out) {
+    const double m = maxd(cam.metric_mass, 1e-4);
+    const double a = clampd(cam.metric_spin, -0.999 * m, 0.999 * m);
+    const double rh = m + std::sqrt(maxd(m * m - a * a, 0.0));
+    MsSource p{};
+    p.m = m;
+    p.a = a;
+    p.axis[2] = 1.0;
+    p.fx[0] = 1.0;
+    p.fy[1] = 1.0;
+    p.rh = rh;
+    p.req = std::sqrt(rh * rh + a * a);
+    if (cam.disk_outer_radius > 0.0) {
+        p.disk_in = (cam.disk_inner_radius > 0.0) ? cam.disk_inner_radius : kerr_isco_radius(m, a);
+        p.disk_out = cam.disk_outer_radius;
+    } else {
+        p.disk_in = p.disk_out = -1.0;
+    }
+    out[0] = p;
+    uint32_t count = 1;
+    for (uint32_t b = 0; b < n && count < kMaxSources; ++b) {
+        const rt_source& s = src[b];
+        MsSource q{};
+        const double mb = maxd(s.mass, 1e-9);
+        const double ab = clampd(s.spin_parameter, -0.9999, 0.9999) * mb;
+        const double rhb = mb + std::sqrt(maxd(mb * mb - ab * ab, 0.0));
+        const double len = std::sqrt(s.axis[0] * s.axis[0] + s.axis[1] * s.axis[1] + s.axis[2] * s.axis[2]);
+        double ax[3] = {0.0, 0.0, 1.0};
+        if (len > 1e-12)
+            for (int k = 0; k < 3; ++k) ax[k] = s.axis[k] / len;
+        const bool near_z = !(std::fabs(ax[2]) < 0.9);
+        const double hp[3] = {near_z ? 1.0 : 0.0, 0.0, near_z ? 0.0 : 1.0};
+        double fx[3] = {hp[1] * ax[2] - hp[2] * ax[1], hp[2] * ax[0] - hp[0] * ax[2], hp[0] * ax[1] - hp[1] * ax[0]};
+        const double fl = std::sqrt(fx[0] * fx[0] + fx[1] * fx[1] + fx[2] * fx[2]);
+        for (double& v : fx) v /= fl;
+        const double fy[3] = {ax[1] * fx[2] - ax[2] * fx[1], ax[2] * fx[0] - ax[0] * fx[2],
+                              ax[0] * fx[1] - ax[1] * fx[0]};
+        for (int k = 0; k < 3; ++k) {
+            q.pos[k] = s.position[k];
+            q.axis[k] = ax[k];
+            q.fx[k] = fx[k];
+            q.fy[k] = fy[k];
+        }
+        q.m = mb;
+        q.a = ab;
+        q.rh = rhb;
+        q.req = std::sqrt(rhb * rhb + ab * ab);
+        if (s.disk_enabled > 0.5) {
+            const double inner = kerr_isco_radius(mb, ab) * maxd(s.disk_inner_scale, 1.0);
+            q.disk_in = inner;
+            q.disk_out = maxd(s.disk_outer_units * mb, inner * 1.05);
+        } else {
+            q.disk_in = q.disk_out = -1.0;
+        }
+        out[count++] = q;
+    }
+    return count;
+}
+
+// Per-camera constants of a multi-source bundle: the observer at the Cartesian
+// point of (r, theta, phi) and the tetrad directions (trace_multi_source,
+// software_compute_engine.hpp:3049-3068).
+void build_ms_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
+                     uint64_t ray_begin, uint64_t out_offset, uint32_t src_begin, uint32_t src_count, MsDesc& b) {
+    b = MsDesc{};
+    b.ray_begin = ray_begin;
+    b.out_offset = out_offset;
+    b.width = cam.screen_width;
+    b.height = cam.screen_height;
+    b.col0 = col0;
+    b.ncols = ncols;
+    b.row0 = row0;
+    b.nrows = nrows;
+    b.max_steps = cam.max_integration_steps;
+    b.src_begin = src_begin;
+    b.src_count = src_count;
+    const double pi = 3.14159265358979323846;
+    const double r = cam.observer_position[1];
+    const double th = clampd(cam.observer_position[2], 0.001, pi - 0.001);
+    const double ph = cam.observer_position[3];
+    b.x0[0] = r * std::sin(th) * std::cos(ph);
+    b.x0[1] = r * std::sin(th) * std::sin(ph);
+    b.x0[2] = r * std::cos(th);
+    b.phi0 = std::atan2(b.x0[1], b.x0[0]);
+    b.aspect = static_cast<double>(cam.screen_width) / static_cast<double>(cam.screen_height);
+    b.tan_half_fov = std::tan(cam.field_of_view_rad * 0.5);
+    for (int i = 0; i < 3; ++i) {
+        b.fwd[i] = cam.tetrad_e1[1 + i];
+        b.rgt[i] = cam.tetrad_e2[1 + i];
+        b.up[i] = cam.tetrad_e3[1 + i];
+    }
+    b.rtol = cam.rtol;
+    b.atol = cam.atol;
+    b.cap_c = cam.step_cap_fraction;
+    b.h0 = cam.initial_step_fraction * r;
+    b.proj_tol = cam.projection_tol;
+    b.r_esc = cam.escape_radius;
+    b.capture_scale = cam.capture_scale;
+}
+
 void row_window(const rt_camera& c, uint32_t& row0, uint32_t& nrows) {
     row0 = std::min(c.dispatch_row_offset, c.screen_height);
     nrows = (c.dispatch_row_count == 0) ? (c.screen_height - row0)

@@ -134,6 +134,37 @@ __device__ __forceinline__ T ks_rhs(const T* __restrict__ y, T M, T a, T* __rest
     return r;
 }
 
+__device__ __forceinline__ double clampd(double v, double lo, double hi) { return fmin(fmax(v, lo), hi); }
+
+// Disk redshift of a circular orbit (accretion_disk_model.hpp:205-225).
+__device__ inline double disk_redshift(double M, double a, double r, double lz) {
+    const double am = fabs(a);
+    const double sm = sqrt(fmax(M, 1e-12));
+    const double sr = sqrt(fmax(r, 1e-12));
+    const double r15 = r * sr;
+    const double ang = sm / (r15 + am * sm);
+    const double bracket = fmax(r15 - 3.0 * M * sr + 2.0 * am * sm, 1e-9);
+    const double omega = (a < 0.0) ? -ang : ang;
+    const double ut = (r15 + am * sm) / (sqrt(r15) * sqrt(bracket));
+    const double den = ut * (1.0 - omega * lz);
+    return (fabs(den) > 1e-9) ? clampd(1.0 / den, 0.05, 4.0) : 1.0;
+}
+
+// Cubic Hermite interpolant of a step from its end points and FSAL slopes.
+__device__ __forceinline__ void hermite(const double* y0, const double* f0, const double* y1, const double* f1,
+                                        double h, double t, int n, double* out) {
+    const double t2 = t * t, t3 = t2 * t;
+    const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
+    const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+    for (int i = 0; i < n; ++i) out[i] = h00 * y0[i] + h10 * h * f0[i] + h01 * y1[i] + h11 * h * f1[i];
+}
+
+// PI30 factor (step_controller.hpp:51-58) from base-2 logs of the errors.
+__device__ __forceinline__ float pi30_factor(float le, float lp, float order_p1) {
+    return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));
+}
+
+
 // Kerr-Schild field only (r, H, k) at x.
 __device__ __forceinline__ double ks_field64(const double* x, double M, double a, double* k, double& hf) {
     const double a2 = a * a;

@@ -100,7 +100,50 @@ struct TraceArgs {
     ParkBuf park;
 };
 
+// Multi-source Kerr-Schild superposition: per-source frame (source 0 is the
+// camera's hole at the origin), as build_multi_source_data
+// (software_compute_engine.hpp:2738-2798) builds it.
+constexpr uint32_t kMaxSources = 16;
+struct alignas(16) MsSource {
+    double pos[3], m;
+    double axis[3], a;
+    double fx[3], rh;
+    double fy[3], req;
+    double disk_in, disk_out;  // disk_in < 0: no disk
+    double pad0, pad1;
+};
+
+// Per-camera constants of a multi-source bundle.
+struct alignas(16) MsDesc {
+    uint64_t ray_begin, out_offset;
+    uint32_t width, height, col0, ncols, row0, nrows;
+    uint32_t max_steps, src_begin, src_count, pad0;
+    double aspect, tan_half_fov;
+    double fwd[3], rgt[3], up[3];
+    double x0[3];     // observer, Cartesian point of (r, theta, phi)
+    double phi0;      // atan2(y0, x0)
+    double rtol, atol, cap_c, h0, proj_tol, r_esc, capture_scale;
+};
+
+struct MsArgs {
+    const MsDesc* bundles;
+    const MsSource* sources;
+    uint32_t n_bundles;
+    uint32_t refill_threshold;
+    uint32_t claim;
+    uint32_t pad;
+    uint64_t total_rays;
+    unsigned long long* queue;
+    unsigned long long* stats;
+    OutPtrs out;
+};
+
 // Host-side helpers implemented in rt_bundle.cpp.
+// Source table of a multi-source camera: the camera's hole and up to 15
+// sources; returns the count.
+uint32_t build_ms_sources(const rt_camera& cam, const rt_source* src, uint32_t n, MsSource* out);
+void build_ms_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
+                     uint64_t ray_begin, uint64_t out_offset, uint32_t src_begin, uint32_t src_count, MsDesc& b);
 void build_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
                   uint64_t ray_begin, uint64_t out_offset, BundleDesc& b);
 double kerr_isco_radius(double m, double a);
@@ -137,5 +180,9 @@ int trace_occupancy(uint32_t block, bool mixed, bool rolled);
 uint32_t kernel_block(uint32_t block, bool mixed, bool rolled);
 // Launch shape with defaults filled in and limits applied for one precision.
 rt_launch_config resolve_launch_config(rt_launch_config c, bool mixed);
+
+// Multi-source tracer (rt_multi.cu).
+void launch_ms_trace(const MsArgs& args, uint32_t grid, void* stream);
+uint32_t ms_trace_grid(int sm_count);
 
 }  // namespace relsim

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -104,6 +105,10 @@ struct Request {
     bool launched = false;
     bool admitted = false;        // holds an arena range
     rt_status status = RT_OK;
+    uint32_t n_sources = 0;       // multi-source scene: its source table (0: single hole)
+    MsSource sources[kMaxSources];
+    // epochs trace one kind of request: FP64, mixed precision, or multi-source
+    int kind() const { return n_sources ? 2 : static_cast<int>(cam.precision_mode); }
 };
 
 struct Chunk {
@@ -119,6 +124,10 @@ struct Slot {
     unsigned long long* counters = nullptr;  // [0] queue, [8..] stats
     void* pass_state = nullptr;              // two-pass mixed tracer: parked state and queues
     char* pass_counters = nullptr;           // its queue counters
+    MsDesc* host_ms = nullptr;               // multi-source epochs: camera table (pinned) and sources
+    MsDesc* dev_ms = nullptr;
+    MsSource* host_src = nullptr;
+    MsSource* dev_src = nullptr;
     std::vector<Chunk> chunks;
     bool busy = false;
 };
@@ -149,7 +158,8 @@ struct rt_server {
     std::string error;
     rt_server_stats stats{};
     std::thread worker;
-    size_t rr = 0;  // round-robin start in `active`
+    size_t rr = 0;       // round-robin start in `active`
+    int last_kind = -1;  // kind of the last epoch launched
 };
 
 namespace {
@@ -228,15 +238,22 @@ bool start_copy(rt_server* s, Request* r) {
 // Build and launch one epoch into a free slot (lock held).  Returns false when
 // there is nothing to trace.
 bool launch_epoch(rt_server* s, Slot& slot) {
-    // precision of this epoch: that of the oldest active request with rows left
-    int precision = -1;
-    for (Request* r : s->active)
-        if (r->state == ReqState::Active && r->rows_issued < r->nrows) {
-            precision = static_cast<int>(r->cam.precision_mode);
-            break;
-        }
-    if (precision < 0) return false;
-    const bool mixed = precision == RT_PRECISION_MIXED;
+    // kind of this epoch: that of the oldest active request with rows left,
+    // alternating with the other kinds when they have rows waiting too, so
+    // that a stream of one kind does not hold back requests of another
+    int kind = -1, other = -1;
+    for (Request* r : s->active) {
+        if (r->state != ReqState::Active || r->rows_issued >= r->nrows) continue;
+        if (kind < 0) kind = r->kind();
+        if (other < 0 && r->kind() != s->last_kind) other = r->kind();
+    }
+    if (kind < 0) return false;
+    if (other >= 0) kind = other;
+    s->last_kind = kind;
+    const bool mixed = kind == RT_PRECISION_MIXED;
+    const bool multi = kind == 2;
+    uint32_t n_src = 0;               // sources copied into this epoch's table
+    std::vector<std::pair<Request*, uint32_t>> src_at;  // request -> its first source in the table
     slot.chunks.clear();
     uint64_t total = 0;
     uint32_t nb = 0;
@@ -248,13 +265,27 @@ bool launch_epoch(rt_server* s, Slot& slot) {
         for (size_t k = 0; k < n_active && total < s->cfg.epoch_rays && nb < s->cfg.max_epoch_bundles; ++k) {
             Request* r = s->active[(s->rr + k) % n_active];
             if (r->state != ReqState::Active || r->rows_issued >= r->nrows) continue;
-            if (static_cast<int>(r->cam.precision_mode) != precision) continue;
+            if (r->kind() != kind) continue;
             const uint64_t budget = std::min<uint64_t>(s->cfg.chunk_rays, s->cfg.epoch_rays - total);
             uint32_t rows = static_cast<uint32_t>(std::max<uint64_t>(1, budget / r->width));
             rows = std::min(rows, r->nrows - r->rows_issued);
             const uint64_t n = static_cast<uint64_t>(rows) * r->width;
-            build_bundle(r->cam, 0, r->width, r->row0 + r->rows_issued, rows, total,
-                         r->base + static_cast<uint64_t>(r->rows_issued) * r->width, slot.host_table[nb]);
+            if (multi) {
+                uint32_t begin = UINT32_MAX;
+                for (const auto& q : src_at)
+                    if (q.first == r) begin = q.second;
+                if (begin == UINT32_MAX) {
+                    begin = n_src;
+                    for (uint32_t j = 0; j < r->n_sources; ++j) slot.host_src[n_src++] = r->sources[j];
+                    src_at.emplace_back(r, begin);
+                }
+                build_ms_bundle(r->cam, 0, r->width, r->row0 + r->rows_issued, rows, total,
+                                r->base + static_cast<uint64_t>(r->rows_issued) * r->width, begin, r->n_sources,
+                                slot.host_ms[nb]);
+            } else {
+                build_bundle(r->cam, 0, r->width, r->row0 + r->rows_issued, rows, total,
+                             r->base + static_cast<uint64_t>(r->rows_issued) * r->width, slot.host_table[nb]);
+            }
             if (!r->launched) {
                 r->launched = true;
                 r->t_first_launch = Clock::now();
@@ -269,9 +300,15 @@ bool launch_epoch(rt_server* s, Slot& slot) {
     s->rr = n_active ? (s->rr + 1) % n_active : 0;
     if (nb == 0) return false;
     cudaStream_t st = slot.stream;
-    // the staging table was last read by this slot's previous epoch, which is retired
-    cudaError_t e = cudaMemcpyAsync(slot.dev_table, slot.host_table, sizeof(BundleDesc) * nb,
-                                    cudaMemcpyHostToDevice, st);
+    // the staging tables were last read by this slot's previous epoch, which is retired
+    cudaError_t e;
+    if (multi) {
+        e = cudaMemcpyAsync(slot.dev_ms, slot.host_ms, sizeof(MsDesc) * nb, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(slot.dev_src, slot.host_src, sizeof(MsSource) * n_src, cudaMemcpyHostToDevice, st);
+    } else {
+        e = cudaMemcpyAsync(slot.dev_table, slot.host_table, sizeof(BundleDesc) * nb, cudaMemcpyHostToDevice, st);
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(slot.counters, 0, 256, st);
     if (e != cudaSuccess) return fail_server(s, "epoch upload", e), false;
     const rt_launch_config c = resolve_launch_config(mixed ? s->cfg.launch_mixed : s->cfg.launch_fp64, mixed);
@@ -288,7 +325,20 @@ bool launch_epoch(rt_server* s, Slot& slot) {
     for (int f = 0; f < kFields; ++f)
         if (s->cfg.record_mask & (1u << f)) dp[f] = s->field_base[f];
     args.out = OutPtrs{(s->cfg.record_mask & kPixelBit) ? s->pixel_base : nullptr, rays};
-    if (mixed && c.mixed_single_kernel == 0) {
+    if (multi) {
+        MsArgs ma{};
+        ma.bundles = slot.dev_ms;
+        ma.sources = slot.dev_src;
+        ma.n_bundles = nb;
+        ma.refill_threshold = 32;
+        ma.claim = 32;
+        ma.total_rays = total;
+        ma.queue = slot.counters;
+        ma.stats = slot.counters + 8;
+        ma.out = args.out;
+        launch_ms_trace(ma, ms_trace_grid(s->sm_count), st);
+        e = cudaGetLastError();
+    } else if (mixed && c.mixed_single_kernel == 0) {
         // parked state of the epoch's rays: SoA with `total` slots in the slot's buffer
         TwoPassBuffers buf{};
         double* pd = static_cast<double*>(slot.pass_state);
@@ -462,6 +512,11 @@ rt_status rt_server_create(rt_server** out, int device_ordinal, const rt_server_
         ok = ok && cudaMalloc(&slot.counters, 256) == cudaSuccess;
         ok = ok && cudaMalloc(&slot.pass_state, two_pass_state_bytes(cfg->epoch_rays)) == cudaSuccess;
         ok = ok && cudaMalloc(&slot.pass_counters, 256) == cudaSuccess;
+        ok = ok && cudaMallocHost(&slot.host_ms, sizeof(MsDesc) * cfg->max_epoch_bundles) == cudaSuccess;
+        ok = ok && cudaMalloc(&slot.dev_ms, sizeof(MsDesc) * cfg->max_epoch_bundles) == cudaSuccess;
+        ok = ok && cudaMallocHost(&slot.host_src, sizeof(MsSource) * kMaxSources * cfg->max_epoch_bundles) ==
+                       cudaSuccess;
+        ok = ok && cudaMalloc(&slot.dev_src, sizeof(MsSource) * kMaxSources * cfg->max_epoch_bundles) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();
@@ -490,6 +545,10 @@ void rt_server_destroy(rt_server* s) {
         if (slot.counters) cudaFree(slot.counters);
         if (slot.pass_state) cudaFree(slot.pass_state);
         if (slot.pass_counters) cudaFree(slot.pass_counters);
+        if (slot.host_ms) cudaFreeHost(slot.host_ms);
+        if (slot.dev_ms) cudaFree(slot.dev_ms);
+        if (slot.host_src) cudaFreeHost(slot.host_src);
+        if (slot.dev_src) cudaFree(slot.dev_src);
         if (slot.stream) cudaStreamDestroy(slot.stream);
     }
     if (s->copy_stream) {
@@ -505,13 +564,23 @@ void rt_server_destroy(rt_server* s) {
     delete s;
 }
 
-rt_status rt_server_submit(rt_server* s, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
-                           size_t capacity, uint64_t* id) {
+}  // extern "C"
+
+namespace {
+rt_status submit_request(rt_server* s, const rt_camera* cam, const rt_source* src, uint32_t n_src, bool multi,
+                         rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity, uint64_t* id) {
     if (!s || !cam || !id) return RT_ERR_INVALID_ARG;
     *id = 0;
     if (cam->screen_width == 0 || cam->screen_height == 0 || cam->rtol <= 0.0 ||
         (cam->precision_mode != RT_PRECISION_FP64 && cam->precision_mode != RT_PRECISION_MIXED))
         return RT_ERR_INVALID_ARG;
+    if (multi) {
+        if (n_src > RT_MAX_SOURCES - 1 || (n_src > 0 && !src)) return RT_ERR_INVALID_ARG;
+        for (uint32_t i = 0; i < n_src; ++i)
+            if (!(src[i].mass > 0.0) || !std::isfinite(src[i].mass) || !std::isfinite(src[i].position[0]) ||
+                !std::isfinite(src[i].position[1]) || !std::isfinite(src[i].position[2]))
+                return RT_ERR_INVALID_ARG;
+    }
     if (!record_fields_ok(s, rays, pixels)) return RT_ERR_INVALID_ARG;
     uint32_t row0, nrows;
     row_window(*cam, row0, nrows);
@@ -521,6 +590,10 @@ rt_status rt_server_submit(rt_server* s, const rt_camera* cam, rt_pixel_out* pix
     Request* r = new (std::nothrow) Request();
     if (!r) return RT_ERR_OOM;
     r->cam = *cam;
+    if (multi) {
+        r->cam.precision_mode = RT_PRECISION_FP64;  // the multi-source tracer is FP64
+        r->n_sources = build_ms_sources(*cam, src, n_src, r->sources);
+    }
     r->row0 = row0;
     r->nrows = nrows;
     r->width = cam->screen_width;
@@ -545,6 +618,19 @@ rt_status rt_server_submit(rt_server* s, const rt_camera* cam, rt_pixel_out* pix
     }
     s->cv_work.notify_all();
     return RT_OK;
+}
+}  // namespace
+
+extern "C" {
+
+rt_status rt_server_submit(rt_server* s, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
+                           size_t capacity, uint64_t* id) {
+    return submit_request(s, cam, nullptr, 0, false, pixels, rays, capacity, id);
+}
+
+rt_status rt_server_submit_multi(rt_server* s, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
+                                 rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity, uint64_t* id) {
+    return submit_request(s, cam, sources, n_sources, true, pixels, rays, capacity, id);
 }
 
 rt_status rt_server_poll(rt_server* s, rt_request_done* done, uint32_t max_done, uint32_t* n_done,

@@ -62,7 +62,7 @@ struct Cold {
     int side[BLOCK], rit[BLOCK];
 };
 
-__device__ __forceinline__ double clampd(double v, double lo, double hi) { return fmin(fmax(v, lo), hi); }
+
 
 // Signed distance of (xi, eta) from the Kerr critical curve in impact
 // parameter (units of M): the smallest local minimum R_min of the radial
@@ -189,29 +189,6 @@ __device__ __noinline__ InitResult init_ray(const BundleDesc* __restrict__ Bp, u
     S.dH[tid] = 0.0;
     S.local[tid] = local;
     return res;
-}
-
-// Disk redshift of a circular orbit (accretion_disk_model.hpp:205-225).
-__device__ double disk_redshift(double M, double a, double r, double lz) {
-    const double am = fabs(a);
-    const double sm = sqrt(fmax(M, 1e-12));
-    const double sr = sqrt(fmax(r, 1e-12));
-    const double r15 = r * sr;
-    const double ang = sm / (r15 + am * sm);
-    const double bracket = fmax(r15 - 3.0 * M * sr + 2.0 * am * sm, 1e-9);
-    const double omega = (a < 0.0) ? -ang : ang;
-    const double ut = (r15 + am * sm) / (sqrt(r15) * sqrt(bracket));
-    const double den = ut * (1.0 - omega * lz);
-    return (fabs(den) > 1e-9) ? clampd(1.0 / den, 0.05, 4.0) : 1.0;
-}
-
-// Cubic Hermite interpolant of a step from its end points and FSAL slopes.
-__device__ __forceinline__ void hermite(const double* y0, const double* f0, const double* y1, const double* f1,
-                                        double h, double t, int n, double* out) {
-    const double t2 = t * t, t3 = t2 * t;
-    const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
-    const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
-    for (int i = 0; i < n; ++i) out[i] = h00 * y0[i] + h10 * h * f0[i] + h01 * y1[i] + h11 * h * f1[i];
 }
 
 // Fraction of the step where the interpolated r_BL crosses `target`
@@ -576,11 +553,6 @@ __device__ __forceinline__ void fp64_stages_rolled(const double* __restrict__ y,
         for (int j = 2; j < 7; ++j) acc += kDpE[j] * K.k[j - 1][i][tid];
         est[i] = fabs(hh) * fabs(acc);
     }
-}
-
-// PI30 factor (step_controller.hpp:51-58) from base-2 logs of the errors.
-__device__ __forceinline__ float pi30_factor(float le, float lp, float order_p1) {
-    return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));
 }
 
 }  // namespace

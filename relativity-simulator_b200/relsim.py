@@ -76,6 +76,22 @@ class Stats(ctypes.Structure):
                 ("rhs_evals", ctypes.c_uint64), ("fp64_attempts", ctypes.c_uint64), ("kernel_ms", _d)]
 
 
+class Source(ctypes.Structure):
+    """rt_source: a black-hole body beside the camera's hole (multi-source scenes)."""
+    _fields_ = [("position", _d * 3), ("mass", _d), ("spin_parameter", _d), ("axis", _d * 3), ("disk_enabled", _d),
+                ("disk_inner_scale", _d), ("disk_outer_units", _d)]
+
+
+MAX_SOURCES = 16  # RT_MAX_SOURCES: the camera's hole and up to 15 sources
+RAYFLAG_DIVERGED = 16
+
+
+def make_source(position, mass: float = 1.0, spin_parameter: float = 0.0, axis=(0.0, 0.0, 1.0), disk: bool = True,
+                disk_inner_scale: float = 1.0, disk_outer_units: float = 20.0) -> Source:
+    return Source((_d * 3)(*position), mass, spin_parameter, (_d * 3)(*axis), 1.0 if disk else 0.0, disk_inner_scale,
+                  disk_outer_units)
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [("memory_budget_bytes", ctypes.c_uint64), ("max_requests", _u32), ("chunk_rays", _u32),
                 ("epoch_rays", _u32), ("max_epoch_bundles", _u32), ("record_mask", _u32), ("reserved", _u32),
@@ -105,9 +121,9 @@ _lib: ctypes.CDLL | None = None
 EXPORTS = ["rt_create", "rt_destroy", "rt_is_ready", "rt_is_platform_supported", "rt_last_error", "rt_abi_version",
            "rt_camera_defaults", "rt_camera_look_at_hole", "rt_dispatch", "rt_dispatch_tile", "rt_dispatch_device",
            "rt_trace_bundles_device", "rt_bundle_rays", "rt_set_launch_config", "rt_get_launch_config",
-           "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc", "rt_kerr_isco_radius",
+           "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc", "rt_kerr_isco_radius", "rt_dispatch_multi", "rt_dispatch_multi_device",
            "rt_server_config_defaults", "rt_server_create", "rt_server_destroy", "rt_server_submit",
-           "rt_server_poll", "rt_server_get_stats", "rt_server_last_error"]
+           "rt_server_poll", "rt_server_get_stats", "rt_server_last_error", "rt_server_submit_multi"]
 NOALLOC_MAX_BUNDLES = 32  # RT_NOALLOC_MAX_BUNDLES
 
 
@@ -140,6 +156,8 @@ def lib() -> ctypes.CDLL:
         L.rt_get_stats.argtypes = [v, p(Stats)]
         L.rt_synchronize.argtypes = [v, _d]
         L.rt_measure_fma_peak.argtypes = [v, p(_d), p(_d)]
+        L.rt_dispatch_multi.argtypes = [v, p(Camera), p(Source), _u32, v, p(RayOut), ctypes.c_size_t]
+        L.rt_dispatch_multi_device.argtypes = [v, p(Camera), p(Source), _u32, v, p(RayOut), ctypes.c_size_t, v]
         L.rt_kerr_isco_radius.argtypes = [_d, _d]
         L.rt_kerr_isco_radius.restype = _d
         L.rt_server_config_defaults.argtypes = [p(ServerConfig)]
@@ -148,6 +166,8 @@ def lib() -> ctypes.CDLL:
         L.rt_server_destroy.argtypes = [v]
         L.rt_server_destroy.restype = None
         L.rt_server_submit.argtypes = [v, p(Camera), v, p(RayOut), ctypes.c_size_t, p(ctypes.c_uint64)]
+        L.rt_server_submit_multi.argtypes = [v, p(Camera), p(Source), _u32, v, p(RayOut), ctypes.c_size_t,
+                                             p(ctypes.c_uint64)]
         L.rt_server_poll.argtypes = [v, p(RequestDone), _u32, p(_u32), _d]
         L.rt_server_get_stats.argtypes = [v, p(ServerStats)]
         L.rt_server_last_error.argtypes = [v]
@@ -284,6 +304,31 @@ class Tracer:
             out["pixels"] = pix
         return out
 
+    def dispatch_multi(self, cam: Camera, sources: list[Source], fields: Iterable[str] | None = None,
+                       pixels: bool = True) -> dict:
+        """Trace a multi-source scene (the camera's hole plus `sources`) into new host arrays."""
+        names = [n for n, _ in RAY_FIELDS] if fields is None else list(fields)
+        n = window_rays(cam)
+        out = {}
+        ro = RayOut()
+        for name, dt in RAY_FIELDS:
+            if name in names:
+                out[name] = np.empty(n, dtype=dt)
+                setattr(ro, name, out[name].ctypes.data)
+        pix = np.empty(n, dtype=PIXEL_DTYPE) if pixels else None
+        arr = (Source * max(len(sources), 1))(*sources)
+        self._check(self.lib.rt_dispatch_multi(self._h, ctypes.byref(cam), arr, len(sources),
+                                               pix.ctypes.data if pix is not None else None, ctypes.byref(ro), n))
+        if pix is not None:
+            out["pixels"] = pix
+        return out
+
+    def dispatch_multi_device(self, cam: Camera, sources: list[Source], rays: RayOut, pixels_ptr: int | None,
+                              capacity: int, stream: int | None = None) -> None:
+        arr = (Source * max(len(sources), 1))(*sources)
+        self._check(self.lib.rt_dispatch_multi_device(self._h, ctypes.byref(cam), arr, len(sources), pixels_ptr,
+                                                      ctypes.byref(rays), capacity, stream))
+
     def dispatch_device(self, cam: Camera, rays: RayOut, pixels_ptr: int | None, capacity: int,
                         stream: int | None = None) -> None:
         """Enqueue a trace into device buffers (pointers from torch tensors); no wait."""
@@ -386,9 +431,10 @@ class Server:
         self.close()
 
     def submit(self, cam: Camera, fields: Iterable[str] = ("status", "r_hit", "g"), pixels: bool = False,
-               out: dict | None = None) -> tuple[int, dict]:
-        """Queue a request; returns (id, host arrays that receive the records).
-        Raises RelsimError with status AGAIN when the queue is full."""
+               out: dict | None = None, sources: list[Source] | None = None) -> tuple[int, dict]:
+        """Queue a request (a multi-source scene when `sources` is given); returns
+        (id, host arrays that receive the records).  Raises RelsimError with
+        status AGAIN when the queue is full."""
         n = window_rays(cam)
         if out is None:
             out = {name: np.empty(n, dtype=dt) for name, dt in RAY_FIELDS if name in set(fields)}
@@ -400,7 +446,12 @@ class Server:
                 setattr(ro, name, arr.ctypes.data)
         pptr = out["pixels"].ctypes.data if "pixels" in out else None
         rid = ctypes.c_uint64()
-        st = self.lib.rt_server_submit(self._h, ctypes.byref(cam), pptr, ctypes.byref(ro), n, ctypes.byref(rid))
+        if sources is None:
+            st = self.lib.rt_server_submit(self._h, ctypes.byref(cam), pptr, ctypes.byref(ro), n, ctypes.byref(rid))
+        else:
+            arr = (Source * max(len(sources), 1))(*sources)
+            st = self.lib.rt_server_submit_multi(self._h, ctypes.byref(cam), arr, len(sources), pptr,
+                                                 ctypes.byref(ro), n, ctypes.byref(rid))
         if st != RT_OK:
             raise RelsimError(st, self.lib.rt_server_last_error(self._h).decode() or "rt_server_submit")
         self._keep[rid.value] = out

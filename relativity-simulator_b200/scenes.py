@@ -11,10 +11,11 @@ Disk [r_ISCO(a), 20 M]; M = 1; mixed precision unless asked otherwise.
 
 Request stream (2000 requests, seed 1): Poisson arrivals at 200 requests/s;
 each request draws its camera as a bundle above; 10 % of the requests are
-multi-source Kerr-Schild superpositions of N ~ U{2..16} holes (mass
-U[0.2, 1] M, spin U[0, 0.9] x mass about an isotropic axis, position
-U[-30, 30]^3 M, placements rejected inside another hole's horizon scale or
-within 2 M of the observer's line of sight origin).
+multi-source Kerr-Schild superpositions of N ~ U{2..16} holes: the camera's
+own hole at the origin (M = 1, spin a of the bundle) and N - 1 more, each with
+mass U[0.2, 1] M, spin parameter U[0, 0.9] about an isotropic axis and
+position U[-30, 30]^3 M.  A placement is drawn again when it lies within
+2 (m_i + m_j) of another hole or within 5 + 2 m of the observer.
 """
 from __future__ import annotations
 
@@ -65,9 +66,14 @@ def bundle_cameras(n: int = 512, seed: int = 0, precision: int = relsim.PRECISIO
 @dataclass
 class Source:
     mass: float
-    spin: float
+    spin_parameter: float  # a / m
     axis: tuple[float, float, float]
     position: tuple[float, float, float]
+
+
+def rt_sources(sources: list[Source]) -> list[relsim.Source]:
+    """The tracer's source records (each hole carries a disk [r_ISCO, 20 m])."""
+    return [relsim.make_source(s.position, s.mass, s.spin_parameter, s.axis) for s in sources]
 
 
 @dataclass
@@ -93,19 +99,24 @@ def _isotropic_axis(rng: np.random.Generator) -> tuple[float, float, float]:
     return (s * math.cos(ph), s * math.sin(ph), z)
 
 
-def _draw_sources(rng: np.random.Generator, r_obs: float) -> list[Source]:
-    n = int(rng.integers(2, 17))
+def _draw_sources(rng: np.random.Generator, b: BundleDraw) -> list[Source]:
+    """The N - 1 holes beside the camera's own (N ~ U{2..16} in total)."""
+    n = int(rng.integers(2, 17)) - 1
+    th = math.radians(b.incl_deg)
+    observer = (b.r_obs * math.sin(th), 0.0, b.r_obs * math.cos(th))
+    placed = [((0.0, 0.0, 0.0), 1.0)]  # the camera's hole
     out: list[Source] = []
     while len(out) < n:
         m = rng.uniform(0.2, 1.0)
-        a = rng.uniform(0.0, 0.9) * m
+        chi = rng.uniform(0.0, 0.9)
         axis = _isotropic_axis(rng)
         pos = tuple(float(v) for v in rng.uniform(-30.0, 30.0, 3))
-        ok = math.dist(pos, (0.0, 0.0, r_obs)) > 2.0 + 2.0 * m
-        for s in out:
-            ok = ok and math.dist(pos, s.position) > 2.0 * (m + s.mass)
+        ok = math.dist(pos, observer) > 5.0 + 2.0 * m
+        for q, mq in placed:
+            ok = ok and math.dist(pos, q) > 2.0 * (m + mq)
         if ok:
-            out.append(Source(m, a, axis, pos))
+            out.append(Source(m, chi, axis, pos))
+            placed.append((pos, m))
     return out
 
 
@@ -121,6 +132,6 @@ def request_stream(n: int = 2000, rate_hz: float = 200.0, seed: int = 1, multi_f
         t += rng.exponential(1.0 / rate_hz)
         b = _draw_bundle(rng)
         multi = rng.uniform() < multi_fraction
-        srcs = _draw_sources(rng, b.r_obs) if multi else []
+        srcs = _draw_sources(rng, b) if multi else []
         out.append(Request(i, t, b, srcs))
     return out

@@ -13,11 +13,16 @@ committed so that the pins run without the reference tree:
   ref_image_path.npz  per-pixel status/iterations of the reference's CPU image
                       path (SoftwareComputeEngine::dispatch_fp64) on a 32x32
                       Kerr-Schild camera
+  ref_multi_source.npz  multi-source scenes: the reference's source table
+                      (build_multi_source_data), superposed RHS (ms_rhs),
+                      initial momentum (ms_initial_momentum) and inside-horizon
+                      answer (ms_inside_horizon) at random points
 
-Usage:  python tests/golden/make_golden.py
+Usage:  python tests/golden/make_golden.py [name ...]   (default: every file)
 """
 from __future__ import annotations
 
+import ctypes
 import os
 import sys
 
@@ -177,12 +182,70 @@ def image_path() -> dict:
     return {"status_flags": st, "iterations": it, "redshift": z, "width": np.array(W), "height": np.array(H)}
 
 
+def multi_source(rng: np.random.Generator, cases: int = 40) -> dict:
+    """Random scenes of 1..15 bodies beside a camera hole; per scene one point."""
+    R = O.ref()
+    spins, bodies, counts, xs, ps, outs = [], [], [], [], [], []
+    tables, rhs, p0, inside = [], [], [], []
+    for c in range(cases):
+        a = rng.uniform(0.0, 0.99)
+        n = int(rng.integers(1, 16))
+        b = np.zeros((15, 11))
+        for i in range(n):
+            b[i, 0:3] = rng.uniform(-30.0, 30.0, 3)
+            b[i, 3] = rng.uniform(0.2, 1.0)
+            b[i, 4] = rng.uniform(-0.95, 0.95)
+            ax = rng.normal(size=3)
+            b[i, 5:8] = ax / np.linalg.norm(ax) * rng.uniform(0.5, 2.0)  # not normalised: the reference normalises
+            b[i, 8] = 1.0 if rng.uniform() < 0.7 else 0.0
+            b[i, 9] = rng.uniform(1.0, 1.5)
+            b[i, 10] = rng.uniform(8.0, 24.0)
+        if c % 5 == 0:
+            b[0, 5:8] = [0.0, 0.0, 2.0]  # an axis near +z takes the other helper vector
+        # a point away from the holes, or (every 4th case) inside one
+        x = rng.uniform(-40.0, 40.0, 3)
+        if c % 4 == 3:
+            x = b[0, 0:3] + 0.3 * b[0, 3] * rng.normal(size=3) / np.sqrt(3)
+        pd = rng.normal(size=3)
+        pd /= np.linalg.norm(pd)
+        ow = rng.normal(size=3)
+        ow /= np.linalg.norm(ow)
+        prim = np.array([1.0, a, 1.0, 20.0])
+        tab = np.zeros((16, 20))
+        r6 = np.zeros(6)
+        m0 = np.zeros(3)
+        ins = ctypes.c_int(0)
+        cnt = R.ref_ms_case(_p(prim), n, _p(b), _p(x), _p(pd), _p(ow), _p(tab), _p(r6), _p(m0), ctypes.byref(ins))
+        spins.append(a)
+        bodies.append(b)
+        counts.append(cnt)
+        xs.append(x)
+        ps.append(pd)
+        outs.append(ow)
+        tables.append(tab)
+        rhs.append(r6)
+        p0.append(m0)
+        inside.append(ins.value)
+    return {"spin": np.array(spins), "bodies": np.array(bodies), "n_bodies": np.array([int(np.count_nonzero(bb[:, 3])) for bb in bodies]),
+            "count": np.array(counts), "x": np.array(xs), "p": np.array(ps), "outward": np.array(outs),
+            "table": np.array(tables), "rhs": np.array(rhs), "p0": np.array(p0), "inside": np.array(inside)}
+
+
 def main() -> None:
     O.build(ref=True)
     rng = np.random.default_rng(20261203)
-    np.savez_compressed(os.path.join(HERE, "ref_functions.npz"), **functions(rng))
-    np.savez_compressed(os.path.join(HERE, "ref_rk45_rays.npz"), **rk45_rays(rng))
-    np.savez_compressed(os.path.join(HERE, "ref_image_path.npz"), **image_path())
+    makers = {
+        "ref_functions": lambda: functions(rng),
+        "ref_rk45_rays": lambda: rk45_rays(rng),
+        "ref_image_path": image_path,
+        "ref_multi_source": lambda: multi_source(np.random.default_rng(12)),
+    }
+    wanted = sys.argv[1:] or list(makers)
+    for name in makers:  # in this order: the first two share one generator
+        if name in wanted or (name == "ref_functions" and "ref_rk45_rays" in wanted):
+            data = makers[name]()
+            if name in wanted:
+                np.savez_compressed(os.path.join(HERE, name + ".npz"), **data)
     print("wrote golden vectors to", HERE)
 
 
