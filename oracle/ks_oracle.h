@@ -163,6 +163,26 @@ void orc_ms_initial_state(const orc_camera* cam, const orc_ms_table* t, uint32_t
 void orc_ms_trace(const orc_camera* cam, const orc_ms_table* t, const uint64_t* pixel_index, uint64_t first,
                   uint64_t count, orc_ray* out, int threads);
 
+/* --- Boyer-Lindquist Kerr-Newman form (bl_oracle.c) ---
+ * State y = (r, theta, phi, u^t, u^r, u^theta, u^phi), u future-directed and
+ * traced with steps h < 0.  Metric components in the order
+ * (g_tt, g_tphi, g_rr, g_thth, g_phiphi).  In orc_ray: dE = E / E0 - 1,
+ * dLz = (L - L0) / E0, dQ = (Q - Q0) / E0^2, db_shadow from the Kerr-Newman
+ * radial potential. */
+double orc_kn_horizon(double mass, double spin, double charge);
+void orc_kn_metric(double mass, double spin, double charge, double r, double theta, double g[5]);
+void orc_kn_metric_derivs(double mass, double spin, double charge, double r, double theta, double dr[5],
+                          double dth[5]);
+void orc_bl_rhs(double mass, double spin, double charge, const double y[7], double dy[7]);
+double orc_bl_null_residual(double mass, double spin, double charge, const double y[7]);
+void orc_bl_invariants(double mass, double spin, double charge, const double y[7], double out[3]);
+double orc_kn_shadow_distance(double mass, double spin, double charge, double xi, double eta);
+void orc_bl_zamo_ray(double mass, double spin, double charge, double r, double theta, double n_r, double n_th,
+                     double n_ph, double u[4]);
+void orc_bl_initial_state(const orc_camera* cam, double charge, uint32_t px, uint32_t py, double y0[7]);
+void orc_bl_trace(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first, uint64_t count,
+                  orc_ray* out, int threads);
+
 #ifdef __cplusplus
 }
 #endif

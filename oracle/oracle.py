@@ -4,8 +4,10 @@ TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check in
 __graft_entry__.py and by the cpu_baseline / reference legs of bench.py.  The
 product (the CUDA library and its host code) never imports this module.
 
-  liboracle.so           C restatement of the reference's FP64 null-ray path
-                         (ks_oracle.c; see its header for the citations)
+  liboracle.so           C restatement of the reference's FP64 null-ray paths
+                         (ks_oracle.c Kerr-Schild, ms_oracle.c multi-source,
+                         bl_oracle.c Boyer-Lindquist Kerr-Newman; see their
+                         headers for the citations)
   _ref/libref_oracle.so  the reference's own functions, compiled from its
                          headers by oracle/Makefile (present where it was built)
 """
@@ -121,6 +123,20 @@ def lib() -> ctypes.CDLL:
         L.orc_ms_initial_state.argtypes = [v, v, ctypes.c_uint32, ctypes.c_uint32, v]
         L.orc_ms_trace.argtypes = [v, v, v, ctypes.c_uint64, ctypes.c_uint64, v, ctypes.c_int]
         L.orc_ms_trace.restype = None
+        L.orc_kn_horizon.argtypes = [d, d, d]
+        L.orc_kn_horizon.restype = d
+        L.orc_kn_metric.argtypes = [d, d, d, d, d, v]
+        L.orc_kn_metric_derivs.argtypes = [d, d, d, d, d, v, v]
+        L.orc_bl_rhs.argtypes = [d, d, d, v, v]
+        L.orc_bl_null_residual.argtypes = [d, d, d, v]
+        L.orc_bl_null_residual.restype = d
+        L.orc_bl_invariants.argtypes = [d, d, d, v, v]
+        L.orc_kn_shadow_distance.argtypes = [d, d, d, d, d]
+        L.orc_kn_shadow_distance.restype = d
+        L.orc_bl_zamo_ray.argtypes = [d, d, d, d, d, d, d, d, v]
+        L.orc_bl_initial_state.argtypes = [v, d, ctypes.c_uint32, ctypes.c_uint32, v]
+        L.orc_bl_trace.argtypes = [v, d, v, ctypes.c_uint64, ctypes.c_uint64, v, ctypes.c_int]
+        L.orc_bl_trace.restype = None
         _lib = L
     return _lib
 
@@ -156,6 +172,14 @@ def ref() -> ctypes.CDLL:
         L.ref_dispatch_fp64.restype = d
         L.ref_ms_case.argtypes = [v, u, v, v, v, v, v, v, v, v]
         L.ref_ms_case.restype = u
+        L.ref_kn_metric.argtypes = [d, d, d, v, v]
+        L.ref_kerr_bl_metric.argtypes = [d, d, v, v]
+        L.ref_kn_christoffel.argtypes = [d, d, d, v, v, v, v]
+        L.ref_kerr_bl_christoffel.argtypes = [d, d, v, v, v, v]
+        L.ref_kn_horizon.argtypes = [d, d, d]
+        L.ref_kn_horizon.restype = d
+        L.ref_kn_zamo_ray.argtypes = [d, d, d, d, d, d, d, d, d, v]
+        L.ref_kn_rk45_trace.argtypes = [v, d, d, d, d, d, d, d, d, d, d, ctypes.c_int, v]
         _ref = L
     return _ref
 
@@ -230,4 +254,26 @@ def ms_trace(cam: dict, sources, pixels: np.ndarray | None = None, threads: int 
         idx = np.ascontiguousarray(pixels, dtype=np.uint64)
         out = np.zeros(idx.size, dtype=RAY_DTYPE)
         lib().orc_ms_trace(_p(c), _p(t), _p(idx), 0, idx.size, _p(out), threads)
+    return out
+
+
+def bl_initial_state(cam: dict, charge: float, px: int, py: int) -> np.ndarray:
+    """Boyer-Lindquist initial state (r, theta, phi, u^t, u^r, u^theta, u^phi) of a pixel."""
+    c = to_camera(cam)
+    y = np.zeros(7)
+    lib().orc_bl_initial_state(_p(c), charge, px, py, _p(y))
+    return y
+
+
+def bl_trace(cam: dict, charge: float, pixels: np.ndarray | None = None, threads: int = 0) -> np.ndarray:
+    """Trace pixels (row-major indices) through the Boyer-Lindquist Kerr-Newman oracle."""
+    c = to_camera(cam)
+    if pixels is None:
+        n = int(cam["screen_width"]) * int(cam["screen_height"])
+        out = np.zeros(n, dtype=RAY_DTYPE)
+        lib().orc_bl_trace(_p(c), charge, None, 0, n, _p(out), threads)
+    else:
+        idx = np.ascontiguousarray(pixels, dtype=np.uint64)
+        out = np.zeros(idx.size, dtype=RAY_DTYPE)
+        lib().orc_bl_trace(_p(c), charge, _p(idx), 0, idx.size, _p(out), threads)
     return out

@@ -17,6 +17,12 @@ committed so that the pins run without the reference tree:
                       (build_multi_source_data), superposed RHS (ms_rhs),
                       initial momentum (ms_initial_momentum) and inside-horizon
                       answer (ms_inside_horizon) at random points
+  ref_boyer_lindquist.npz  Boyer-Lindquist Kerr-Newman form: the reference's
+                      metric tensor, analytic Christoffel symbols and their
+                      contraction -Gamma u u (KerrNewmanMetric and KerrMetric),
+                      outer horizon and ZAMO light ray at random points, and
+                      rays traced by RK45AdaptiveIntegrator<KerrNewmanMetric>
+                      from the C restatement's initial states
 
 Usage:  python tests/golden/make_golden.py [name ...]   (default: every file)
 """
@@ -231,6 +237,70 @@ def multi_source(rng: np.random.Generator, cases: int = 40) -> dict:
             "table": np.array(tables), "rhs": np.array(rhs), "p0": np.array(p0), "inside": np.array(inside)}
 
 
+BL_CAMERAS = {
+    # tag: (spin, charge, camera keywords)
+    "kn": (0.9, 0.3, dict(r_obs=50.0, incl_deg=75.0, fov_deg=30.0)),
+    "kerr": (0.94, 0.0, dict(r_obs=100.0, incl_deg=17.0, fov_deg=12.0)),
+    "schw": (0.0, 0.0, dict(r_obs=50.0, incl_deg=60.0, fov_deg=30.0, disk_inner=6.0)),
+    "kn_hi_q": (0.5, 0.7, dict(r_obs=50.0, incl_deg=85.0, fov_deg=30.0)),
+}
+
+
+def boyer_lindquist(rng: np.random.Generator) -> dict:
+    """Function-level vectors at random points and reference RK45 rays."""
+    import relsim
+
+    R = O.ref()
+    n = 256
+    out: dict[str, np.ndarray] = {}
+    m = rng.uniform(0.5, 2.0, n)
+    m[:8] = 1.0
+    a = rng.uniform(-0.99, 0.99, n) * m
+    q = rng.uniform(0.0, 1.0, n) * np.sqrt(np.maximum(m * m - a * a, 0.0)) * 0.99
+    q[::3] = 0.0
+    rh = np.array([R.ref_kn_horizon(m[i], a[i], q[i]) for i in range(n)])
+    r = rh * 1.01 + rng.exponential(10.0, n) * m
+    th = rng.uniform(0.01, np.pi - 0.01, n)
+    th[:4] = [np.pi / 2, 0.02, np.pi - 0.02, 1.0]
+    ph = rng.uniform(-np.pi, np.pi, n)
+    u = rng.normal(size=(n, 4))
+    nd = rng.normal(size=(n, 3))
+    nd /= np.linalg.norm(nd, axis=1, keepdims=True)
+    g = np.zeros((n, 16))
+    gam = np.zeros((n, 64))
+    acc = np.zeros((n, 4))
+    acc_kerr = np.full((n, 4), np.nan)
+    zamo = np.zeros((n, 4))
+    for i in range(n):
+        x = np.array([0.0, r[i], th[i], ph[i]])
+        R.ref_kn_metric(m[i], a[i], q[i], _p(x), _p(g[i]))
+        ui = np.ascontiguousarray(u[i])
+        R.ref_kn_christoffel(m[i], a[i], q[i], _p(x), _p(ui), _p(gam[i]), _p(acc[i]))
+        if q[i] == 0.0:
+            R.ref_kerr_bl_christoffel(m[i], a[i], _p(x), _p(ui), None, _p(acc_kerr[i]))
+        R.ref_kn_zamo_ray(m[i], a[i], q[i], r[i], th[i], ph[i], nd[i, 0], nd[i, 1], nd[i, 2], _p(zamo[i]))
+    out.update(mass=m, spin=a, charge=q, rh=rh, r=r, theta=th, phi=ph, u=u, n=nd, metric=g, gamma=gam, acc=acc,
+               acc_kerr=acc_kerr, zamo=zamo)
+    L = O.lib()
+    for tag, (spin, charge, kw) in BL_CAMERAS.items():
+        side = 32
+        cam = relsim.camera_dict(relsim.make_camera(spin=spin, width=side, height=side, **kw))
+        k = 40
+        pix = rng.choice(side * side, k, replace=False).astype(np.uint64)
+        y0 = np.zeros((k, 7))
+        res = np.zeros((k, 7))
+        r_in = cam["disk_inner_radius"] if cam["disk_inner_radius"] > 0 else L.orc_isco_radius(1.0, spin)
+        for i, pq in enumerate(pix):
+            y0[i] = O.bl_initial_state(cam, charge, int(pq % side), int(pq // side))
+            R.ref_kn_rk45_trace(_p(y0[i]), 1.0, spin, charge, 1e-11, 1e-12, cam["step_cap_fraction"],
+                                cam["capture_scale"], cam["escape_radius"], r_in, cam["disk_outer_radius"], 200000,
+                                _p(res[i]))
+        out[f"{tag}_pixels"] = pix
+        out[f"{tag}_y0"] = y0
+        out[f"{tag}_res"] = res
+    return out
+
+
 def main() -> None:
     O.build(ref=True)
     rng = np.random.default_rng(20261203)
@@ -239,6 +309,7 @@ def main() -> None:
         "ref_rk45_rays": lambda: rk45_rays(rng),
         "ref_image_path": image_path,
         "ref_multi_source": lambda: multi_source(np.random.default_rng(12)),
+        "ref_boyer_lindquist": lambda: boyer_lindquist(np.random.default_rng(5)),
     }
     wanted = sys.argv[1:] or list(makers)
     for name in makers:  # in this order: the first two share one generator

@@ -1,0 +1,198 @@
+"""Pin the Boyer-Lindquist Kerr-Newman restatement (oracle/bl_oracle.c)
+against the reference's own functions, on the golden vectors of
+tests/golden/ref_boyer_lindquist.npz (made by tests/golden/make_golden.py from
+oracle/_ref).  Runs on the CPU without the reference tree.
+
+(1) Function level: KerrNewmanMetric::metric_tensor, the contraction of its
+    analytic Christoffel symbols -Gamma^mu_ab u^a u^b (and KerrMetric's for
+    Q = 0), the outer horizon, and the ZAMO light ray of trace_exact_photon.
+(2) Whole rays: class and disk radius against RK45AdaptiveIntegrator
+    <KerrNewmanMetric> integrated from the oracle's initial states.
+(3) Physical checks: null initial rays, invariant drift, the Kerr-Newman
+    shadow (captured exactly when the radial potential has no turning point),
+    the Schwarzschild shadow edge, mirror symmetry.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import relsim
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_boyer_lindquist.npz")
+
+# tag: (spin, charge, camera keywords) -- the cameras of make_golden.BL_CAMERAS
+BL_CAMERAS = {
+    "kn": (0.9, 0.3, dict(r_obs=50.0, incl_deg=75.0, fov_deg=30.0)),
+    "kerr": (0.94, 0.0, dict(r_obs=100.0, incl_deg=17.0, fov_deg=12.0)),
+    "schw": (0.0, 0.0, dict(r_obs=50.0, incl_deg=60.0, fov_deg=30.0, disk_inner=6.0)),
+    "kn_hi_q": (0.5, 0.7, dict(r_obs=50.0, incl_deg=85.0, fov_deg=30.0)),
+}
+
+
+@pytest.fixture(scope="module")
+def fx():
+    return np.load(GOLDEN)
+
+
+def _p(a):
+    return O._p(a)
+
+
+def test_metric_matches_reference(fx):
+    L = O.lib()
+    for i in range(len(fx["mass"])):
+        g = np.zeros(5)
+        L.orc_kn_metric(fx["mass"][i], fx["spin"][i], fx["charge"][i], fx["r"][i], fx["theta"][i], _p(g))
+        G = fx["metric"][i].reshape(4, 4)
+        ref = np.array([G[0, 0], G[0, 3], G[1, 1], G[2, 2], G[3, 3]])
+        np.testing.assert_allclose(g, ref, rtol=1e-13, atol=0)
+        # the other components vanish
+        assert G[0, 1] == G[0, 2] == G[1, 2] == G[1, 3] == G[2, 3] == 0.0
+
+
+def test_horizon_matches_reference(fx):
+    L = O.lib()
+    for i in range(len(fx["mass"])):
+        assert abs(L.orc_kn_horizon(fx["mass"][i], fx["spin"][i], fx["charge"][i]) - fx["rh"][i]) <= 1e-15 * fx["rh"][i]
+
+
+def test_factored_contraction_matches_christoffel(fx):
+    """-Gamma^mu_ab u^a u^b: the oracle contracts dg/dr and dg/dtheta directly;
+    the reference forms the 64 symbols analytically.  Tolerance relative to the
+    sum of |Gamma u u| terms."""
+    L = O.lib()
+    for i in range(len(fx["mass"])):
+        m, a, q = fx["mass"][i], fx["spin"][i], fx["charge"][i]
+        u = fx["u"][i]
+        y = np.array([fx["r"][i], fx["theta"][i], fx["phi"][i], *u])
+        dy = np.zeros(7)
+        L.orc_bl_rhs(m, a, q, _p(y), _p(dy))
+        np.testing.assert_array_equal(dy[[0, 1, 2]], u[[1, 2, 3]])
+        scale = np.abs(fx["gamma"][i].reshape(4, 16)) @ np.abs(np.outer(u, u)).ravel()
+        assert np.all(np.abs(dy[[3, 4, 5, 6]] - fx["acc"][i]) <= 1e-11 * scale), i
+        if q == 0.0:  # KerrMetric is the Q = 0 case
+            assert np.all(np.abs(dy[[3, 4, 5, 6]] - fx["acc_kerr"][i]) <= 1e-11 * scale), i
+
+
+def test_zamo_ray_matches_reference(fx):
+    L = O.lib()
+    for i in range(len(fx["mass"])):
+        u = np.zeros(4)
+        n = fx["n"][i]
+        L.orc_bl_zamo_ray(fx["mass"][i], fx["spin"][i], fx["charge"][i], fx["r"][i], fx["theta"][i], n[0], n[1], n[2],
+                          _p(u))
+        ref = fx["zamo"][i]
+        np.testing.assert_allclose(u, ref, rtol=0, atol=1e-13 * np.abs(ref).max())
+        # a null vector
+        y = np.array([fx["r"][i], fx["theta"][i], 0.0, *u])
+        res = L.orc_bl_null_residual(fx["mass"][i], fx["spin"][i], fx["charge"][i], _p(y))
+        assert abs(res) < 1e-13 * (u @ u)
+
+
+def _camera(tag, side=32, **over):
+    spin, charge, kw = BL_CAMERAS[tag]
+    kw = dict(kw)
+    kw.update(over)
+    return relsim.camera_dict(relsim.make_camera(spin=spin, width=side, height=side, **kw)), charge
+
+
+@pytest.mark.parametrize("tag", list(BL_CAMERAS))
+def test_matches_reference_rk45_integrator(fx, tag):
+    cam, charge = _camera(tag, rtol=1e-11, atol=1e-12)
+    pix = fx[f"{tag}_pixels"]
+    res = fx[f"{tag}_res"]
+    for q, y0 in zip(pix[:6], fx[f"{tag}_y0"][:6]):
+        np.testing.assert_array_equal(O.bl_initial_state(cam, charge, int(q % 32), int(q // 32)), y0)
+    rays = O.bl_trace(cam, charge, pixels=pix)
+    np.testing.assert_array_equal(rays["status"], res[:, 0].astype(np.uint32))
+    disk = rays["status"] == O.DISK
+    assert np.all(np.abs(rays["r_hit"][disk] - res[disk, 4]) <= 1e-8 * res[disk, 4])
+
+
+@pytest.mark.parametrize("tag", list(BL_CAMERAS))
+def test_invariant_drift_small(tag):
+    cam, charge = _camera(tag, side=24)
+    rays = O.bl_trace(cam, charge)
+    assert np.all(rays["status"] != O.UNFINISHED)
+    ok = rays["flags"] == 0
+    assert np.max(np.abs(rays["dE"][ok])) < 1e-9
+    assert np.max(rays["dH"]) < 1e-10
+    # near the hole (disk hits): rtol governs every component
+    near = ok & (rays["status"] == O.DISK)
+    if near.any():
+        assert np.max(np.abs(rays["dLz"][near])) < 1e-8
+        assert np.max(np.abs(rays["dQ"][near])) < 1e-6
+    # escaped rays: atol = 1e-10 on u^theta, u^phi ~ 1/r^2 far out lets L = r^2 sin^2 u^phi
+    # and Q drift by up to r^2 atol per step; the bound is a few 1e-7 / 1e-6
+    far = ok & (rays["status"] == O.ESCAPED)
+    if far.any():
+        assert np.max(np.abs(rays["dLz"][far])) < 1e-6
+        assert np.max(np.abs(rays["dQ"][far])) < 2e-5
+
+
+@pytest.mark.parametrize("tag", list(BL_CAMERAS))
+def test_capture_matches_radial_potential(tag):
+    """Without a disk a ray is captured exactly when its Kerr-Newman radial
+    potential has no turning point outside r_+ (db_shadow > 0), outside a
+    1e-6 M band around the critical curve.  The early capture is off, so every
+    captured ray is integrated down to capture_scale r_+."""
+    cam, charge = _camera(tag, side=40, disk_outer=0.0, early_capture=False)
+    rays = O.bl_trace(cam, charge)
+    band = np.abs(rays["db_shadow"]) < 1e-6
+    cap = rays["status"] == O.CAPTURED
+    assert cap.sum() > 20 and (~cap).sum() > 20
+    np.testing.assert_array_equal(cap[~band], rays["db_shadow"][~band] > 0)
+
+
+def test_early_capture_does_not_change_classes():
+    cam, charge = _camera("kn", side=32)
+    on = O.bl_trace(cam, charge)
+    cam["early_capture"] = 0
+    off = O.bl_trace(cam, charge)
+    np.testing.assert_array_equal(on["status"], off["status"])
+    disk = on["status"] == O.DISK
+    np.testing.assert_array_equal(on["r_hit"][disk], off["r_hit"][disk])
+    assert np.any(on["flags"] & 8)
+
+
+def test_schwarzschild_shadow_edge():
+    """The shadow edge of a = Q = 0 at r = 50 lies within 5 % of
+    asin(3 sqrt(3) M sqrt(1 - 2M/r) / r) (test_schwarzschild_shadow_render.cpp:24-86)."""
+    r_obs, W = 50.0, 257
+    cam = relsim.camera_dict(relsim.make_camera(spin=0.0, r_obs=r_obs, incl_deg=90.0, fov_deg=40.0, width=W,
+                                                height=W, disk_outer=0.0))
+    row = W // 2
+    rays = O.bl_trace(cam, 0.0, pixels=np.arange(row * W, (row + 1) * W, dtype=np.uint64))
+    captured = rays["status"] == O.CAPTURED
+    u = (np.arange(W) + 0.5) / W * 2 - 1
+    ang = np.arctan(np.abs(u) * np.tan(np.radians(40.0) / 2))
+    edge = ang[captured].max()
+    expected = math.asin(3 * math.sqrt(3) * math.sqrt(1 - 2 / r_obs) / r_obs)
+    assert abs(edge - expected) < 0.05 * expected
+
+
+def test_reissner_nordstrom_shadow_shrinks_with_charge():
+    """The photon sphere of a = 0 moves in with Q (r_ph = (3M + sqrt(9M^2 - 8Q^2)) / 2),
+    so fewer pixels of the same camera are captured."""
+    counts = []
+    for q in (0.0, 0.5, 0.9):
+        cam = relsim.camera_dict(relsim.make_camera(spin=0.0, r_obs=50.0, incl_deg=90.0, fov_deg=30.0, width=48,
+                                                    height=48, disk_outer=0.0))
+        counts.append(int(np.sum(O.bl_trace(cam, q)["status"] == O.CAPTURED)))
+    assert counts[0] > counts[1] > counts[2] > 0
+
+
+def test_mirror_symmetry_equatorial_observer():
+    """An equatorial observer sees the image mirrored top-bottom (theta -> pi - theta)."""
+    W = 24
+    cam = relsim.camera_dict(relsim.make_camera(spin=0.7, r_obs=40.0, incl_deg=90.0, fov_deg=30.0, width=W,
+                                                height=W))
+    rays = O.bl_trace(cam, 0.4)
+    st = rays["status"].reshape(W, W)
+    np.testing.assert_array_equal(st, st[::-1])
+    rh = rays["r_hit"].reshape(W, W)
+    both = np.isfinite(rh) & np.isfinite(rh[::-1])
+    np.testing.assert_allclose(rh[both], rh[::-1][both], rtol=1e-8)  # mirrored step sequences differ in rounding
