@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define RT_ABI_VERSION 1
+#define RT_ABI_VERSION 2
 
 typedef enum rt_status {
     RT_OK = 0,
@@ -76,6 +76,20 @@ enum {
 #define RT_PIXEL_CELESTIAL_HIT (1u << 1)
 #define RT_PIXEL_ACCRETION_DISK_HIT (1u << 2)
 
+/* Coordinate form of the traced metric (rt_camera.metric_form). */
+typedef enum rt_metric_form {
+    /* Kerr: Kerr-Schild Hamiltonian tracer (metric types 2 and 3 of the
+     * reference, trace_kerr_schild_photon, software_compute_engine.hpp:3370) */
+    RT_METRIC_KERR_SCHILD = 0,
+    /* Kerr-Newman in Boyer-Lindquist coordinates with charge metric_charge:
+     * geodesic equation -Gamma u u from the ZAMO ray (metric type 5,
+     * KerrNewmanMetric; with charge 0 the KerrMetric default route; with
+     * spin and charge 0 Schwarzschild, metric type 1) -- trace_exact_photon,
+     * software_compute_engine.hpp:1334-1622, routed at :3364-3391.  FP64
+     * always (precision_mode is not used); a^2 + Q^2 < M^2 required. */
+    RT_METRIC_BOYER_LINDQUIST = 1
+} rt_metric_form;
+
 /* Camera and integration parameters of one image (one "bundle"). */
 typedef struct rt_camera {
     double observer_position[4]; /* t, r, theta, phi (Boyer-Lindquist), as GpuCameraPushConstants */
@@ -95,6 +109,7 @@ typedef struct rt_camera {
     double initial_step_fraction;/* |h0| = f * r_obs */
     double projection_tol;       /* project onto H = 0 when |H| >= tol */
     double mixed_fp64_radius;    /* MIXED: FP64 stages inside this r_BL (<= 0: max(3 r_+, 5 M)) */
+    double metric_charge;        /* Q (G = c = k_e = 1), RT_METRIC_BOYER_LINDQUIST only */
     uint32_t screen_width;
     uint32_t screen_height;
     uint32_t max_integration_steps; /* step attempts per ray, accepted + rejected */
@@ -106,7 +121,7 @@ typedef struct rt_camera {
     uint32_t tile_origin_y;
     uint32_t tile_extent_x;
     uint32_t tile_extent_y;
-    uint32_t reserved;
+    uint32_t metric_form;        /* rt_metric_form */
 } rt_camera;
 
 /* GpuPixelOutput (gpu_types.hpp:1111-1121): 32 bytes. */

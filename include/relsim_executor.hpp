@@ -45,9 +45,17 @@ struct TraceSettings {
     uint32_t early_capture = 1;
 };
 
+// Metric types of GpuCameraPushConstants this backend traces
+// (trace_exact_photon_dispatch, software_compute_engine.hpp:3316-3392):
+// 2 and 3 Kerr-Schild Kerr; 5 Kerr-Newman and 1 Schwarzschild in
+// Boyer-Lindquist coordinates.
+inline bool metric_type_supported(uint32_t metric_type) {
+    return metric_type == 1u || metric_type == 2u || metric_type == 3u || metric_type == 5u;
+}
+
 // rt_camera from the reference's push constants (gpu_types.hpp:966-1109): the
-// observer, tetrad, field of view, metric mass and spin, escape radius, image
-// size, step budget, row window and tile, and the primary disk
+// observer, tetrad, field of view, metric (type, mass, spin, charge), escape
+// radius, image size, step budget, row window and tile, and the primary disk
 // (inner = inner_radius_scale x r_ISCO(a), outer = outer_radius_mass_units x M).
 // A template so that this header does not depend on the reference's headers.
 template <class PushConstants>
@@ -63,6 +71,14 @@ rt_camera camera_from_push_constants(const PushConstants& p, const TraceSettings
     c.field_of_view_rad = p.field_of_view_rad;
     c.metric_mass = std::max(p.metric_mass, 1e-4);
     c.metric_spin = std::clamp(p.metric_spin, -0.999 * c.metric_mass, 0.999 * c.metric_mass);
+    if (p.metric_type == 5u) {  // KerrNewmanMetric (:3364-3368)
+        c.metric_form = RT_METRIC_BOYER_LINDQUIST;
+        c.metric_charge = p.metric_charge;
+    } else if (p.metric_type == 1u) {  // Schwarzschild: spin and charge unused
+        c.metric_form = RT_METRIC_BOYER_LINDQUIST;
+        c.metric_spin = 0.0;
+        c.metric_charge = 0.0;
+    }
     c.escape_radius = p.escape_radius;
     c.screen_width = p.screen_width;
     c.screen_height = p.screen_height;

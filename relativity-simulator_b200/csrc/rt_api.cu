@@ -44,6 +44,7 @@ struct rt_handle {
     DevBuf bundles, queue, stats;
     DevBuf park_d, park_u, pass_queues;  // two-pass mixed tracer: parked state, far/near queues
     DevBuf ms_desc, ms_sources;          // multi-source camera and source table
+    DevBuf bl_desc;                      // Boyer-Lindquist camera
     DevBuf ray_fields[14];
     DevBuf pixels;
     // pinned staging of the bundle table
@@ -121,8 +122,21 @@ rt_status ensure_host_bundles(rt_handle* h, size_t n) {
     return RT_OK;
 }
 
+// Boyer-Lindquist form: a finite charge and a horizon, a^2 + Q^2 < M^2 after
+// the spin clamp (the reference traces larger charges with r_+ = M, a radius
+// that is no horizon).
+bool bl_camera_valid(const rt_camera* c) {
+    if (!std::isfinite(c->metric_charge)) return false;
+    const double m = std::max(c->metric_mass, 1e-4);
+    const double a = std::min(std::max(c->metric_spin, -0.999 * m), 0.999 * m);
+    return m * m - a * a - c->metric_charge * c->metric_charge > 0.0;
+}
+
+bool is_bl(const rt_camera* c) { return c->metric_form == RT_METRIC_BOYER_LINDQUIST; }
+
 bool camera_valid(const rt_camera* c) {
     return c && c->screen_width > 0 && c->screen_height > 0 && std::isfinite(c->metric_mass) &&
+           (c->metric_form == RT_METRIC_KERR_SCHILD || (c->metric_form == RT_METRIC_BOYER_LINDQUIST && bl_camera_valid(c))) &&
            std::isfinite(c->metric_spin) && std::isfinite(c->field_of_view_rad) && c->field_of_view_rad > 0.0 &&
            c->field_of_view_rad < 3.14 && std::isfinite(c->escape_radius) && c->rtol > 0.0 && c->atol >= 0.0 &&
            c->step_cap_fraction > 0.0 && c->initial_step_fraction > 0.0 && c->capture_scale >= 1.0 &&
@@ -251,6 +265,9 @@ rt_status wait_stream(rt_handle* h, cudaStream_t s, double timeout_ms) {
     }
 }
 
+rt_status bl_launch(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
+                    uint64_t out_offset, const OutPtrs& out, cudaStream_t s);
+
 // One host-buffer dispatch over a window (dispatch_and_readback semantics).
 rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0,
                           uint32_t nrows, rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity,
@@ -274,6 +291,12 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
         if (cancel && *cancel) return fail(h, RT_ERR_CANCELLED, "cancelled");
         const uint32_t rows = static_cast<uint32_t>(std::min<uint64_t>(band_rows, nrows - r));
         const uint64_t offset = static_cast<uint64_t>(r) * ncols;
+        if (is_bl(cam)) {
+            if ((st = bl_launch(h, cam, col0, ncols, row0 + r, rows, offset, OutPtrs{dpix, dev}, h->stream)) != RT_OK)
+                return st;
+            if ((st = wait_stream(h, h->stream, 0.0)) != RT_OK) return st;
+            continue;
+        }
         build_bundle(*cam, col0, ncols, row0 + r, rows, 0, offset, h->host_bundles[0]);
         RT_CUDA(h, cudaMemcpyAsync(h->bundles.ptr, h->host_bundles, sizeof(BundleDesc), cudaMemcpyHostToDevice,
                                    h->stream));
@@ -329,6 +352,36 @@ rt_status ms_check(rt_handle* h, const rt_camera* cam, const rt_source* src, uin
         if (!std::isfinite(src[i].mass) || !(src[i].mass > 0.0) || !std::isfinite(src[i].position[0]) ||
             !std::isfinite(src[i].position[1]) || !std::isfinite(src[i].position[2]))
             return fail(h, RT_ERR_INVALID_ARG, "invalid source");
+    return RT_OK;
+}
+
+// Enqueue a Boyer-Lindquist trace of a camera window, its first ray written at
+// element out_offset of the (device) outputs.
+rt_status bl_launch(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
+                    uint64_t out_offset, const OutPtrs& out, cudaStream_t s) {
+    BlDesc d;
+    build_bl_bundle(*cam, col0, ncols, row0, nrows, 0, out_offset, d);
+    rt_status st;
+    if ((st = ensure(h, h->bl_desc, sizeof(BlDesc))) != RT_OK) return st;
+    // pageable descriptor: the copy is staged before the call returns
+    RT_CUDA(h, cudaMemcpyAsync(h->bl_desc.ptr, &d, sizeof d, cudaMemcpyHostToDevice, s));
+    RT_CUDA(h, cudaMemsetAsync(h->queue.ptr, 0, sizeof(unsigned long long), s));
+    RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
+    const rt_launch_config c = effective_cfg(h, false);
+    BlArgs args{};
+    args.bundles = static_cast<const BlDesc*>(h->bl_desc.ptr);
+    args.n_bundles = 1;
+    args.refill_threshold = c.refill_threshold;
+    args.claim = 32u * c.rays_per_thread;
+    args.total_rays = static_cast<uint64_t>(ncols) * nrows;
+    args.queue = static_cast<unsigned long long*>(h->queue.ptr);
+    args.stats = static_cast<unsigned long long*>(h->stats.ptr);
+    args.out = out;
+    RT_CUDA(h, cudaEventRecord(h->ev0, s));
+    launch_bl_trace(args, bl_trace_grid(h->sm_count), s);
+    RT_CUDA(h, cudaGetLastError());
+    RT_CUDA(h, cudaEventRecord(h->ev1, s));
+    h->timed = true;
     return RT_OK;
 }
 
@@ -434,6 +487,7 @@ void rt_destroy(rt_handle* h) {
     release(h->bundles);
     release(h->ms_desc);
     release(h->ms_sources);
+    release(h->bl_desc);
     release(h->park_d);
     release(h->park_u);
     release(h->pass_queues);
@@ -534,6 +588,8 @@ rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* p
     if (capacity < n) return fail(h, RT_ERR_INVALID_ARG, "capacity smaller than the window");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
     RT_CUDA(h, cudaSetDevice(h->device));
+    if (is_bl(cam))
+        return bl_launch(h, cam, 0, cam->screen_width, row0, nrows, 0, OutPtrs{pixels, rays ? *rays : rt_ray_out{}}, s);
     rt_status st = ensure_host_bundles(h, 1);
     if (st != RT_OK) return st;
     if ((st = ensure(h, h->bundles, sizeof(BundleDesc))) != RT_OK) return st;
@@ -564,6 +620,8 @@ rt_status rt_trace_bundles_device(rt_handle* h, const rt_camera* cams, uint32_t 
     bool mixed = cams[0].precision_mode == RT_PRECISION_MIXED;
     for (uint32_t b = 0; b < n_bundles; ++b) {
         if (!camera_valid(&cams[b])) return fail(h, RT_ERR_INVALID_ARG, "invalid camera in bundle table");
+        if (is_bl(&cams[b]))
+            return fail(h, RT_ERR_INVALID_ARG, "Boyer-Lindquist cameras trace through rt_dispatch* (not bundles)");
         if ((cams[b].precision_mode == RT_PRECISION_MIXED) != mixed)
             return fail(h, RT_ERR_INVALID_ARG, "one precision mode per bundle launch");
     }
@@ -768,6 +826,8 @@ extern "C" rt_status rt_trace_bundles_noalloc(int device_ordinal, const rt_camer
     for (uint32_t b = 0; b < n_bundles; ++b) {
         if (!camera_valid(&cams[b]))
             return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "invalid camera in bundle table");
+        if (is_bl(&cams[b]))
+            return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "Boyer-Lindquist cameras are not bundle cameras");
         if ((cams[b].precision_mode == RT_PRECISION_MIXED) != mixed)
             return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "one precision mode per bundle launch");
     }

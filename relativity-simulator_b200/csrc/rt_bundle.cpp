@@ -131,6 +131,89 @@ void build_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t 
               (cam.precision_mode == RT_PRECISION_MIXED ? BF_MIXED : 0u);
 }
 
+double kn_horizon(double m, double a, double q) {
+    const double diff = m * m - a * a - q * q;  // kerr_newman.hpp:95-101
+    return (diff < 0.0) ? m : m + std::sqrt(diff);
+}
+
+// Boyer-Lindquist Kerr-Newman camera (trace_exact_photon_dispatch,
+// software_compute_engine.hpp:3364-3368 and :3388-3391): r_+ of the
+// Kerr-Newman metric, ISCO and disk from the Kerr formula, and the ZAMO tetrad
+// at the observer (observer_tetrad.hpp:82-100): omega = -g_tphi / g_phiphi,
+// alpha^2 = -(g_tt + omega g_tphi), e0 = (1, 0, 0, omega) / alpha and the unit
+// coordinate vectors (orthonormal already; the reference's Gram-Schmidt pass
+// moves them only by rounding).
+void build_bl_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
+                     uint64_t ray_begin, uint64_t out_offset, BlDesc& b) {
+    b = BlDesc{};
+    b.ray_begin = ray_begin;
+    b.out_offset = out_offset;
+    b.width = cam.screen_width;
+    b.height = cam.screen_height;
+    b.col0 = col0;
+    b.ncols = ncols;
+    b.row0 = row0;
+    b.nrows = nrows;
+    b.max_steps = cam.max_integration_steps;
+
+    const double m = maxd(cam.metric_mass, 1e-4);
+    const double a = clampd(cam.metric_spin, -0.999 * m, 0.999 * m);
+    const double q = cam.metric_charge;
+    const double rh = kn_horizon(m, a, q);
+    b.m = m;
+    b.a = a;
+    b.q2 = q * q;
+    b.rh = rh;
+
+    const double pi = 3.14159265358979323846;
+    const double r_obs = maxd(cam.observer_position[1], rh * 1.02);
+    const double th = clampd(cam.observer_position[2], 0.001, pi - 0.001);
+    const double ph = cam.observer_position[3];
+    b.r_obs = r_obs;
+    b.th_obs = th;
+    b.ph_obs = ph;
+    b.st = std::sin(th);
+    b.ct = std::cos(th);
+    b.sp = std::sin(ph);
+    b.cp = std::cos(ph);
+    b.aspect = static_cast<double>(cam.screen_width) / static_cast<double>(cam.screen_height);
+    b.tan_half_fov = std::tan(cam.field_of_view_rad * 0.5);
+    for (int i = 0; i < 3; ++i) {
+        b.fwd[i] = cam.tetrad_e1[1 + i];
+        b.rgt[i] = cam.tetrad_e2[1 + i];
+        b.up[i] = cam.tetrad_e3[1 + i];
+    }
+
+    // metric at the observer (kerr_newman.hpp:141-169)
+    const double s = std::sin(th), c = std::cos(th);
+    const double s2 = s * s, a2 = a * a, r2 = r_obs * r_obs;
+    const double rho2 = r2 + a2 * c * c;
+    const double delta = r2 - 2.0 * m * r_obs + a2 + b.q2;
+    const double F = (2.0 * m * r_obs - b.q2) / rho2;
+    const double g_tt = F - 1.0, g_tp = -a * s2 * F, g_rr = rho2 / delta, g_thth = rho2;
+    const double g_pp = s2 * (r2 + a2 + a2 * s2 * F);
+    const double omega = -g_tp / g_pp;
+    const double alpha = std::sqrt(maxd(-(g_tt + omega * g_tp), 1e-30));
+    b.e0_t = 1.0 / alpha;
+    b.e0_phi = omega / alpha;
+    b.e_r = 1.0 / std::sqrt(maxd(g_rr, 1e-30));
+    b.e_th = 1.0 / std::sqrt(maxd(g_thth, 1e-30));
+    b.e_ph = 1.0 / std::sqrt(maxd(g_pp, 1e-30));
+
+    b.r_capture = cam.capture_scale * rh;
+    b.r_esc = cam.escape_radius;
+    const bool disk = cam.disk_outer_radius > 0.0;
+    b.r_in = (cam.disk_inner_radius > 0.0) ? cam.disk_inner_radius : kerr_isco_radius(m, a);
+    b.r_out = cam.disk_outer_radius;
+    b.r_early = disk ? b.r_in : 1e300;
+    b.rtol = cam.rtol;
+    b.atol = cam.atol;
+    b.cap_c = cam.step_cap_fraction;
+    b.h0 = cam.initial_step_fraction * r_obs;
+    b.proj_tol = cam.projection_tol;
+    b.flags = (disk ? BF_DISK : 0u) | (cam.early_capture ? BF_EARLY_CAPTURE : 0u);
+}
+
 // Source table of a multi-source scene (software_compute_engine.hpp:2738-2798):
 // the camera's hole at the origin, then each body with its spin axis
 // normalised and a local frame from a helper axis (z unless the spin axis is

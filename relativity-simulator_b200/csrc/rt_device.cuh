@@ -150,6 +150,50 @@ __device__ inline double disk_redshift(double M, double a, double r, double lz) 
     return (fabs(den) > 1e-9) ? clampd(1.0 / den, 0.05, 4.0) : 1.0;
 }
 
+// Signed distance of (xi, eta) from the critical curve of a Kerr (q2 = 0) or
+// Kerr-Newman hole, in impact parameter (units of M): the smallest local
+// minimum R_min of the radial quartic
+//   R(r) = (r^2 + a^2 - a xi)^2 - Delta (eta + (xi - a)^2)
+//        = r^4 + P r^2 + Qc r + R0,  Delta = r^2 - 2 M r + a^2 + q2
+// (carter_ray_classifier.hpp:132-135 for q2 = 0) outside r_+ is moved to zero
+// by d_eta = R_min / Delta.  > 0: no turning point.
+static __device__ __noinline__ double shadow_distance(double M, double a, double q2, double rh, double xi,
+                                                      double eta) {
+    const double a2 = a * a;
+    const double K = eta + (xi - a) * (xi - a);
+    const double P = a2 - xi * xi - eta;
+    const double Qc = 2.0 * M * K;
+    const double R0 = -a2 * eta - q2 * K;
+    const double pp = 0.5 * P, qq = 0.25 * Qc;
+    double best = INFINITY, best_r = 0.0;
+    auto consider = [&](double r) {
+        if (!(r > rh)) return;
+        if (12.0 * r * r + 2.0 * P <= 0.0) return;
+        const double R = ((r * r + P) * r + Qc) * r + R0;
+        if (R < best) {
+            best = R;
+            best_r = r;
+        }
+    };
+    const double disc = -(4.0 * pp * pp * pp + 27.0 * qq * qq);
+    if (disc > 0.0 && pp < 0.0) {
+        const double m2 = 2.0 * sqrt(-pp / 3.0);
+        const double arg = clampd(3.0 * qq / (pp * m2), -1.0, 1.0);
+        const double th = acos(arg) / 3.0;
+        constexpr double kThird = 2.0 * 3.14159265358979323846 / 3.0;
+        consider(m2 * cos(th));
+        consider(m2 * cos(th - kThird));
+        consider(m2 * cos(th - 2.0 * kThird));
+    } else {
+        const double sq = sqrt(fmax(qq * qq / 4.0 + pp * pp * pp / 27.0, 0.0));
+        consider(cbrt(-qq / 2.0 + sq) + cbrt(-qq / 2.0 - sq));
+    }
+    if (!isfinite(best)) return INFINITY;
+    const double delta = best_r * best_r - 2.0 * M * best_r + a2 + q2;
+    const double b = sqrt(fmax(eta + xi * xi, 1e-30));
+    return best / fmax(delta, 1e-30) / (2.0 * b);
+}
+
 // Cubic Hermite interpolant of a step from its end points and FSAL slopes.
 __device__ __forceinline__ void hermite(const double* y0, const double* f0, const double* y1, const double* f1,
                                         double h, double t, int n, double* out) {

@@ -138,7 +138,43 @@ struct MsArgs {
     OutPtrs out;
 };
 
+// Per-camera constants of the Boyer-Lindquist Kerr-Newman tracer, precomputed
+// on the host in FP64: the pinhole camera, the observer's position and ZAMO
+// tetrad (observer_tetrad.hpp:82-100; the tetrad is diagonal in (r, theta,
+// phi) apart from e0's phi component), metric and integration constants.
+struct alignas(16) BlDesc {
+    uint64_t ray_begin, out_offset;
+    uint32_t width, height, col0, ncols, row0, nrows;
+    uint32_t max_steps, flags, pad0, pad1;
+    double aspect, tan_half_fov;
+    double fwd[3], rgt[3], up[3];
+    double st, ct, sp, cp;          // sin/cos of the observer's theta and phi
+    double r_obs, th_obs, ph_obs;
+    double e0_t, e0_phi;            // ZAMO e0 = (1/alpha, 0, 0, omega/alpha)
+    double e_r, e_th, e_ph;         // 1/sqrt(g_rr), 1/sqrt(g_thth), 1/sqrt(g_phiphi)
+    double m, a, q2, rh;
+    double r_capture, r_esc, r_in, r_out, r_early;
+    double rtol, atol, cap_c, h0, proj_tol;
+};
+
+struct BlArgs {
+    const BlDesc* bundles;
+    uint32_t n_bundles;
+    uint32_t refill_threshold;
+    uint32_t claim;
+    uint32_t pad;
+    uint64_t total_rays;
+    unsigned long long* queue;
+    unsigned long long* stats;
+    OutPtrs out;
+};
+
 // Host-side helpers implemented in rt_bundle.cpp.
+// Boyer-Lindquist bundle of a camera window (metric_form RT_METRIC_BOYER_LINDQUIST).
+void build_bl_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
+                     uint64_t ray_begin, uint64_t out_offset, BlDesc& b);
+// Outer horizon r_+ = M + sqrt(M^2 - a^2 - Q^2) (M when the root is imaginary).
+double kn_horizon(double m, double a, double q);
 // Source table of a multi-source camera: the camera's hole and up to 15
 // sources; returns the count.
 uint32_t build_ms_sources(const rt_camera& cam, const rt_source* src, uint32_t n, MsSource* out);
@@ -184,5 +220,9 @@ rt_launch_config resolve_launch_config(rt_launch_config c, bool mixed);
 // Multi-source tracer (rt_multi.cu).
 void launch_ms_trace(const MsArgs& args, uint32_t grid, void* stream);
 uint32_t ms_trace_grid(int sm_count);
+
+// Boyer-Lindquist Kerr-Newman tracer (rt_bl.cu).
+void launch_bl_trace(const BlArgs& args, uint32_t grid, void* stream);
+uint32_t bl_trace_grid(int sm_count);
 
 }  // namespace relsim

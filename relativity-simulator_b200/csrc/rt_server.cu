@@ -107,8 +107,13 @@ struct Request {
     rt_status status = RT_OK;
     uint32_t n_sources = 0;       // multi-source scene: its source table (0: single hole)
     MsSource sources[kMaxSources];
-    // epochs trace one kind of request: FP64, mixed precision, or multi-source
-    int kind() const { return n_sources ? 2 : static_cast<int>(cam.precision_mode); }
+    // epochs trace one kind of request: Kerr-Schild FP64 (0) or mixed precision (1),
+    // multi-source (2), Boyer-Lindquist Kerr-Newman (3)
+    int kind() const {
+        if (n_sources) return 2;
+        if (cam.metric_form == RT_METRIC_BOYER_LINDQUIST) return 3;
+        return static_cast<int>(cam.precision_mode);
+    }
 };
 
 struct Chunk {
@@ -128,6 +133,8 @@ struct Slot {
     MsDesc* dev_ms = nullptr;
     MsSource* host_src = nullptr;
     MsSource* dev_src = nullptr;
+    BlDesc* host_bl = nullptr;               // Boyer-Lindquist epochs: camera table (pinned)
+    BlDesc* dev_bl = nullptr;
     std::vector<Chunk> chunks;
     bool busy = false;
 };
@@ -252,6 +259,7 @@ bool launch_epoch(rt_server* s, Slot& slot) {
     s->last_kind = kind;
     const bool mixed = kind == RT_PRECISION_MIXED;
     const bool multi = kind == 2;
+    const bool bl = kind == 3;
     uint32_t n_src = 0;               // sources copied into this epoch's table
     std::vector<std::pair<Request*, uint32_t>> src_at;  // request -> its first source in the table
     slot.chunks.clear();
@@ -282,6 +290,9 @@ bool launch_epoch(rt_server* s, Slot& slot) {
                 build_ms_bundle(r->cam, 0, r->width, r->row0 + r->rows_issued, rows, total,
                                 r->base + static_cast<uint64_t>(r->rows_issued) * r->width, begin, r->n_sources,
                                 slot.host_ms[nb]);
+            } else if (bl) {
+                build_bl_bundle(r->cam, 0, r->width, r->row0 + r->rows_issued, rows, total,
+                                r->base + static_cast<uint64_t>(r->rows_issued) * r->width, slot.host_bl[nb]);
             } else {
                 build_bundle(r->cam, 0, r->width, r->row0 + r->rows_issued, rows, total,
                              r->base + static_cast<uint64_t>(r->rows_issued) * r->width, slot.host_table[nb]);
@@ -306,6 +317,8 @@ bool launch_epoch(rt_server* s, Slot& slot) {
         e = cudaMemcpyAsync(slot.dev_ms, slot.host_ms, sizeof(MsDesc) * nb, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(slot.dev_src, slot.host_src, sizeof(MsSource) * n_src, cudaMemcpyHostToDevice, st);
+    } else if (bl) {
+        e = cudaMemcpyAsync(slot.dev_bl, slot.host_bl, sizeof(BlDesc) * nb, cudaMemcpyHostToDevice, st);
     } else {
         e = cudaMemcpyAsync(slot.dev_table, slot.host_table, sizeof(BundleDesc) * nb, cudaMemcpyHostToDevice, st);
     }
@@ -337,6 +350,18 @@ bool launch_epoch(rt_server* s, Slot& slot) {
         ma.stats = slot.counters + 8;
         ma.out = args.out;
         launch_ms_trace(ma, ms_trace_grid(s->sm_count), st);
+        e = cudaGetLastError();
+    } else if (bl) {
+        BlArgs ba{};
+        ba.bundles = slot.dev_bl;
+        ba.n_bundles = nb;
+        ba.refill_threshold = c.refill_threshold;
+        ba.claim = 32u * c.rays_per_thread;
+        ba.total_rays = total;
+        ba.queue = slot.counters;
+        ba.stats = slot.counters + 8;
+        ba.out = args.out;
+        launch_bl_trace(ba, bl_trace_grid(s->sm_count), st);
         e = cudaGetLastError();
     } else if (mixed && c.mixed_single_kernel == 0) {
         // parked state of the epoch's rays: SoA with `total` slots in the slot's buffer
@@ -517,6 +542,8 @@ rt_status rt_server_create(rt_server** out, int device_ordinal, const rt_server_
         ok = ok && cudaMallocHost(&slot.host_src, sizeof(MsSource) * kMaxSources * cfg->max_epoch_bundles) ==
                        cudaSuccess;
         ok = ok && cudaMalloc(&slot.dev_src, sizeof(MsSource) * kMaxSources * cfg->max_epoch_bundles) == cudaSuccess;
+        ok = ok && cudaMallocHost(&slot.host_bl, sizeof(BlDesc) * cfg->max_epoch_bundles) == cudaSuccess;
+        ok = ok && cudaMalloc(&slot.dev_bl, sizeof(BlDesc) * cfg->max_epoch_bundles) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();
@@ -549,6 +576,8 @@ void rt_server_destroy(rt_server* s) {
         if (slot.dev_ms) cudaFree(slot.dev_ms);
         if (slot.host_src) cudaFreeHost(slot.host_src);
         if (slot.dev_src) cudaFree(slot.dev_src);
+        if (slot.host_bl) cudaFreeHost(slot.host_bl);
+        if (slot.dev_bl) cudaFree(slot.dev_bl);
         if (slot.stream) cudaStreamDestroy(slot.stream);
     }
     if (s->copy_stream) {
@@ -574,6 +603,15 @@ rt_status submit_request(rt_server* s, const rt_camera* cam, const rt_source* sr
     if (cam->screen_width == 0 || cam->screen_height == 0 || cam->rtol <= 0.0 ||
         (cam->precision_mode != RT_PRECISION_FP64 && cam->precision_mode != RT_PRECISION_MIXED))
         return RT_ERR_INVALID_ARG;
+    if (cam->metric_form == RT_METRIC_BOYER_LINDQUIST) {
+        // a horizon (a^2 + Q^2 < M^2 after the spin clamp); the multi-source tracer is Kerr-Schild only
+        const double m = std::max(cam->metric_mass, 1e-4);
+        const double a = std::min(std::max(cam->metric_spin, -0.999 * m), 0.999 * m);
+        if (multi || !std::isfinite(cam->metric_charge) || !(m * m - a * a - cam->metric_charge * cam->metric_charge > 0.0))
+            return RT_ERR_INVALID_ARG;
+    } else if (cam->metric_form != RT_METRIC_KERR_SCHILD) {
+        return RT_ERR_INVALID_ARG;
+    }
     if (multi) {
         if (n_src > RT_MAX_SOURCES - 1 || (n_src > 0 && !src)) return RT_ERR_INVALID_ARG;
         for (uint32_t i = 0; i < n_src; ++i)

@@ -64,44 +64,6 @@ struct Cold {
 
 
 
-// Signed distance of (xi, eta) from the Kerr critical curve in impact
-// parameter (units of M): the smallest local minimum R_min of the radial
-// quartic R(r) = r^4 + P r^2 + Qc r - a^2 eta (carter_ray_classifier.hpp:132-135)
-// outside r_+ is moved to zero by d_eta = R_min / Delta.  > 0: no turning point.
-__device__ __noinline__ double shadow_distance(double M, double a, double rh, double xi, double eta) {
-    const double a2 = a * a;
-    const double P = a2 - xi * xi - eta;
-    const double Qc = 2.0 * M * (eta + (xi - a) * (xi - a));
-    const double R0 = -a2 * eta;
-    const double pp = 0.5 * P, qq = 0.25 * Qc;
-    double best = INFINITY, best_r = 0.0;
-    auto consider = [&](double r) {
-        if (!(r > rh)) return;
-        if (12.0 * r * r + 2.0 * P <= 0.0) return;
-        const double R = ((r * r + P) * r + Qc) * r + R0;
-        if (R < best) {
-            best = R;
-            best_r = r;
-        }
-    };
-    const double disc = -(4.0 * pp * pp * pp + 27.0 * qq * qq);
-    if (disc > 0.0 && pp < 0.0) {
-        const double m2 = 2.0 * sqrt(-pp / 3.0);
-        const double arg = clampd(3.0 * qq / (pp * m2), -1.0, 1.0);
-        const double th = acos(arg) / 3.0;
-        consider(m2 * cos(th));
-        consider(m2 * cos(th - 2.0 * kPi / 3.0));
-        consider(m2 * cos(th - 4.0 * kPi / 3.0));
-    } else {
-        const double sq = sqrt(fmax(qq * qq / 4.0 + pp * pp * pp / 27.0, 0.0));
-        consider(cbrt(-qq / 2.0 + sq) + cbrt(-qq / 2.0 - sq));
-    }
-    if (!isfinite(best)) return INFINITY;
-    const double delta = best_r * best_r - 2.0 * M * best_r + a2;
-    const double b = sqrt(fmax(eta + xi * xi, 1e-30));
-    return best / fmax(delta, 1e-30) / (2.0 * b);
-}
-
 // Carter constant with E = 1, mu = 0 (kerr_invariants.hpp:45-48); BL p_theta
 // from the Kerr-Schild covector through dx^i/dtheta of the map at
 // kerr_schild_null_integrator.hpp:47-53.
@@ -1051,7 +1013,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 target = Bp->r_esc;
             } else if (can_early != 0 && r5 < Bp->r_early) {
                 if (can_early < 0)  // Carter test, once per ray, when first inside r_early
-                    can_early = shadow_distance(M, a, Bp->rh, S.lz0[tid], S.q0[tid]) > kEarlyCaptureMargin;
+                    can_early = shadow_distance(M, a, 0.0, Bp->rh, S.lz0[tid], S.q0[tid]) > kEarlyCaptureMargin;
                 // dr_BL/dlambda (kerr_invariants.hpp:140); the trace runs towards
                 // decreasing lambda, so dr/dlambda > 0 means inwards
                 const double rr2 = r5 * r5, z = y5[2];

@@ -29,6 +29,7 @@ RAY_UNFINISHED, RAY_CAPTURED, RAY_ESCAPED, RAY_DISK = 0, 1, 2, 3
 RAYFLAG_NONFINITE, RAYFLAG_STEP_UNDERFLOW, RAYFLAG_MAX_STEPS, RAYFLAG_EARLY_CAPTURE = 1, 2, 4, 8
 PIXEL_HORIZON_ABSORBED, PIXEL_CELESTIAL_HIT, PIXEL_ACCRETION_DISK_HIT = 1, 2, 4
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+METRIC_KERR_SCHILD, METRIC_BOYER_LINDQUIST = 0, 1  # rt_metric_form
 MIXED_RTOL = 1e-8  # DP45 tolerance of the mixed-precision mode
 
 _d = ctypes.c_double
@@ -41,10 +42,11 @@ class Camera(ctypes.Structure):
         ("field_of_view_rad", _d), ("metric_mass", _d), ("metric_spin", _d), ("escape_radius", _d),
         ("capture_scale", _d), ("disk_inner_radius", _d), ("disk_outer_radius", _d), ("rtol", _d), ("atol", _d),
         ("step_cap_fraction", _d), ("initial_step_fraction", _d), ("projection_tol", _d), ("mixed_fp64_radius", _d),
+        ("metric_charge", _d),
         ("screen_width", _u32), ("screen_height", _u32), ("max_integration_steps", _u32), ("early_capture", _u32),
         ("precision_mode", _u32), ("dispatch_row_offset", _u32), ("dispatch_row_count", _u32),
         ("tile_origin_x", _u32), ("tile_origin_y", _u32), ("tile_extent_x", _u32), ("tile_extent_y", _u32),
-        ("reserved", _u32),
+        ("metric_form", _u32),
     ]
 
 
@@ -191,8 +193,11 @@ def make_camera(*, spin: float = 0.94, mass: float = 1.0, r_obs: float = 100.0, 
                 max_steps: int = 20000,
                 step_cap: float = 0.1, h0: float = 0.01, projection_tol: float = 1e-12, early_capture: bool = True,
                 precision: int = PRECISION_FP64, mixed_fp64_radius: float = 0.0, row_offset: int = 0,
-                row_count: int = 0) -> Camera:
+                row_count: int = 0, metric_form: int = METRIC_KERR_SCHILD, charge: float = 0.0) -> Camera:
     """A camera looking at the hole from (r_obs, incl, phi_obs) with a static-observer tetrad.
+
+    metric_form METRIC_BOYER_LINDQUIST traces the Kerr-Newman metric of the
+    given charge in Boyer-Lindquist coordinates (FP64, ZAMO observer).
 
     Tolerances default to rtol = atol = 1e-10 for FP64 and 1e-8 for the mixed
     precision mode (whose FP32 stages carry ~1e-7 relative increments)."""
@@ -213,6 +218,7 @@ def make_camera(*, spin: float = 0.94, mass: float = 1.0, r_obs: float = 100.0, 
     c.early_capture = 1 if early_capture else 0
     c.precision_mode = precision
     c.dispatch_row_offset, c.dispatch_row_count = row_offset, row_count
+    c.metric_form, c.metric_charge = metric_form, charge
     th, ph = math.radians(incl_deg), phi_obs
     st, ct, sp, cp = math.sin(th), math.cos(th), math.sin(ph), math.cos(ph)
     er, eth, eph = (st * cp, st * sp, ct), (ct * cp, ct * sp, -st), (-sp, cp, 0.0)

@@ -2,6 +2,7 @@
 
     python relativity-simulator_b200/trace_once.py [--side 512] [--spin 0.94] [--r-obs 100]
         [--incl 17] [--fov 12] [--precision fp64|mixed] [--repeat 1]
+        [--metric ks|bl] [--charge 0]
 """
 from __future__ import annotations
 
@@ -34,6 +35,9 @@ def main() -> None:
     ap.add_argument("--fp64-radius", type=float, default=0.0)
     ap.add_argument("--mixed-single", type=int, default=0,
                     help="mixed precision: 1 = the single-kernel form instead of far/near passes")
+    ap.add_argument("--metric", choices=["ks", "bl"], default="ks",
+                    help="ks: Kerr-Schild Hamiltonian tracer; bl: Boyer-Lindquist Kerr-Newman tracer (FP64)")
+    ap.add_argument("--charge", type=float, default=0.0, help="Kerr-Newman charge Q (--metric bl)")
     ap.add_argument("--record", choices=["minimal", "bench"], default="minimal",
                     help="outputs written: class and step counts, or the bench's record (class, r, theta, "
                          "phi, r_hit, g) plus the 32-byte pixels")
@@ -41,7 +45,9 @@ def main() -> None:
     cam = relsim.make_camera(spin=a.spin, r_obs=a.r_obs, incl_deg=a.incl, fov_deg=a.fov, width=a.side,
                              height=a.side,
                              precision=relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64,
-                             rtol=a.rtol, mixed_fp64_radius=a.fp64_radius)
+                             rtol=a.rtol, mixed_fp64_radius=a.fp64_radius,
+                             metric_form=relsim.METRIC_BOYER_LINDQUIST if a.metric == "bl" else relsim.METRIC_KERR_SCHILD,
+                             charge=a.charge)
     with relsim.Tracer(0) as tr:
         tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread, a.fp64_rolled, a.mixed_single)
         for _ in range(a.repeat):

@@ -1,6 +1,7 @@
 // Drives relsim::CudaComputeExecutor (include/relsim_executor.hpp) the way the
 // reference's pipeline drives VulkanComputeExecutor.  Used by tests/test_adapter.py.
 //   adapter_main map                 print the mapped camera of a push-constant struct
+//   adapter_main route               metric type routing: form, spin, charge for types 3, 5, 1
 //   adapter_main cpu                 platform/initialise answers without a device
 //   adapter_main gpu <out.bin>       dispatch_and_readback of a 96x64 image -> raw pixels; cancel check
 #include <atomic>
@@ -20,6 +21,8 @@ struct DiskProfile {
 struct Push {  // the fields of GpuCameraPushConstants the tracer reads (gpu_types.hpp:966-1109)
     std::array<double, 4> observer_position{}, tetrad_e1{}, tetrad_e2{}, tetrad_e3{};
     double field_of_view_rad = 1.0471975511965976, metric_mass = 1.0, metric_spin = 0.0, escape_radius = 100.0;
+    double metric_charge = 0.0;
+    uint32_t metric_type = 3;
     uint32_t screen_width = 3840, screen_height = 2160, max_integration_steps = 2048;
     uint32_t dispatch_row_offset = 0, dispatch_row_count = 0;
     uint32_t tile_origin_x = 0, tile_origin_y = 0, tile_extent_x = 0, tile_extent_y = 0;
@@ -41,6 +44,8 @@ static Push headline_push(uint32_t w, uint32_t h) {
     p.field_of_view_rad = d.field_of_view_rad;
     p.metric_mass = 1.0;
     p.metric_spin = 0.94;
+    p.metric_type = 3;
+    p.metric_charge = 0.0;
     p.escape_radius = 1000.0;
     p.screen_width = w;
     p.screen_height = h;
@@ -66,6 +71,18 @@ int main(int argc, char** argv) {
         std::printf("%.17g %.17g %.17g %.17g %u %u %u %.17g\n", c.metric_spin, c.disk_inner_radius,
                     c.disk_outer_radius, c.escape_radius, c.screen_width, c.screen_height, c.max_integration_steps,
                     rt_kerr_isco_radius(1.0, 0.999));
+        return 0;
+    }
+    if (!std::strcmp(mode, "route")) {
+        for (uint32_t type : {3u, 5u, 1u}) {
+            Push p = headline_push(32, 32);
+            p.metric_type = type;
+            p.metric_charge = 0.4;
+            const rt_camera c = relsim::camera_from_push_constants(p);
+            std::printf("%u %d %u %.17g %.17g\n", type, relsim::metric_type_supported(type) ? 1 : 0, c.metric_form,
+                        c.metric_spin, c.metric_charge);
+        }
+        std::printf("%d %d\n", relsim::metric_type_supported(4u) ? 1 : 0, relsim::metric_type_supported(0u) ? 1 : 0);
         return 0;
     }
     if (!std::strcmp(mode, "cpu")) {

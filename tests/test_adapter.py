@@ -40,6 +40,18 @@ def test_push_constant_mapping(tmp_path):
     assert isco == pytest.approx(relsim.lib().rt_kerr_isco_radius(1.0, 0.999), rel=0)
 
 
+def test_metric_type_routing(tmp_path):
+    """Types 2/3 trace the Kerr-Schild form; 5 the Boyer-Lindquist Kerr-Newman
+    form with the push constants' charge; 1 Boyer-Lindquist with spin and
+    charge 0 (trace_exact_photon_dispatch, software_compute_engine.hpp:3316-3392)."""
+    lines = subprocess.run([_build(tmp_path), "route"], capture_output=True, text=True, check=True).stdout.splitlines()
+    rows = [ln.split() for ln in lines]
+    assert rows[0] == ["3", "1", str(relsim.METRIC_KERR_SCHILD), "0.93999999999999995", "0"]
+    assert rows[1] == ["5", "1", str(relsim.METRIC_BOYER_LINDQUIST), "0.93999999999999995", "0.40000000000000002"]
+    assert rows[2] == ["1", "1", str(relsim.METRIC_BOYER_LINDQUIST), "0", "0"]
+    assert rows[3] == ["0", "0"]
+
+
 def test_no_device_answers(tmp_path):
     import torch
     if torch.cuda.is_available():
