@@ -47,6 +47,14 @@ FLOP_PER_ATTEMPT = 1578.0  # Kerr-Schild RHS as written (206 ops) x 6 + DP45 sta
 SIDE = 2048
 RECORD_FIELDS = ["status", "r", "theta", "phi", "r_hit", "g"]
 H2D_BYTES_PER_IMAGE = 464  # one bundle descriptor (per-camera constants) per image
+# Boyer-Lindquist Kerr-Newman path (metric type 5): the reference's RHS as written,
+# KerrNewmanMetric::christoffel_symbols (88 ops of metric derivatives, 37 of the
+# inverse metric, 240 of the lambda loop over its 6 non-zero entries) and the
+# RK45 contraction -Gamma u u (144 ops) = 509 ops, x 6 evaluations, + 488 ops of
+# stage sums and error norm for the reference's 8-component state
+BL_FLOP_PER_ATTEMPT = 3542.0
+BL_CAMERA = dict(spin=0.9, charge=0.3, r_obs=50.0, incl_deg=75.0, fov_deg=30.0)
+BL_H2D_BYTES_PER_IMAGE = 352  # the Boyer-Lindquist camera descriptor (sizeof BlDesc)
 
 
 def headline_camera(relsim, precision: int, side: int = SIDE):
@@ -288,6 +296,84 @@ def time_bundles(tr, relsim, steps: int, warmup: int, device: str) -> dict:
             "launch": vars_of(tr.launch_config())}
 
 
+def bl_camera(relsim, side: int):
+    return relsim.make_camera(width=side, height=side, metric_form=relsim.METRIC_BOYER_LINDQUIST, **BL_CAMERA)
+
+
+def time_boyer_lindquist(tr, relsim, side, ro, pix, flush, steps, warmup, fp64_peak, ws, device) -> dict:
+    """The Boyer-Lindquist Kerr-Newman tracer on its own workload: device time with
+    resident outputs (L2 flushed between steps) and end to end through rt_dispatch."""
+    cam = bl_camera(relsim, side)
+    n = side * side
+    tr.set_launch_config()
+    d = time_device(tr, relsim, cam, n, ro, pix, flush, steps, warmup)
+    own_ms = float(sum(d["ms"]))
+    total_ms = max_over_ranks(own_ms, ws, device)
+    _, lat = time_e2e(tr, relsim, cam, n, steps, warmup)
+    e2e_wall = max_over_ranks(sum(lat), ws, device)
+    achieved = d["attempts"] * BL_FLOP_PER_ATTEMPT / (own_ms * 1e-3) / 1e12
+    return {
+        "workload": f"Kerr-Newman a=0.9 Q=0.3 {side}^2 pinhole r=50 M i=75 deg FOV 30 deg, disk [r_isco, 20 M]; "
+                    f"Boyer-Lindquist geodesic equation (-Gamma u u), ZAMO observer, FP64 DP45 rtol=atol=1e-10",
+        "value": replica_value(n, ws, steps, total_ms), "unit": "Mrays/s", "ms_per_step": total_ms / steps,
+        "attempts_per_ray": d["attempts"] / (n * steps), "msteps_per_s": d["accepted"] / (own_ms * 1e-3) / 1e6,
+        "latency_ms": {"kernel_p50": float(np.percentile(d["ms"], 50)), "kernel_p99": float(np.percentile(d["ms"], 99)),
+                       "e2e_p50": 1e3 * float(np.percentile(lat, 50)), "e2e_p99": 1e3 * float(np.percentile(lat, 99))},
+        "e2e": {"value": replica_value(n, ws, steps, e2e_wall * 1e3), "unit": "Mrays/s",
+                "h2d_bytes_per_step": BL_H2D_BYTES_PER_IMAGE, "d2h_bytes_per_step": n * (32 + 4 + 8 * (len(RECORD_FIELDS) - 1))},
+        "roofline": {"bound": "fp64 pipe", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp64_peak, "flop_per_attempt": BL_FLOP_PER_ATTEMPT,
+                     "peak_source": "measured in this run: register FMA-chain kernel (rt_measure_fma_peak)",
+                     "traffic": committed_traffic("bl")},
+    }
+
+
+def bl_cpu_baselines(side: int, seconds: float) -> dict:
+    """The reference's own CPU path for the same Kerr-Newman camera (trace_exact_photon,
+    heuristic RK4, oracle/_ref) on whole images at a reduced side, and the FP64 DP45
+    oracle (oracle/bl_oracle.c) on a random sample of the full image's rays."""
+    from oracle import oracle as O
+    import relsim
+
+    cores = os.cpu_count() or 1
+    out = {}
+    d = relsim.camera_dict(bl_camera(relsim, side))
+    if O.ref_available():
+        R = O.ref()
+        obs, e1, e2, e3 = (np.ascontiguousarray(d[k], dtype=np.float64)
+                           for k in ("observer_position", "tetrad_e1", "tetrad_e2", "tetrad_e3"))
+
+        def image(w):
+            st = np.zeros(w * w, np.uint32)
+            it = np.zeros(w * w, np.uint32)
+            z = np.zeros(w * w, np.float32)
+            t = R.ref_dispatch_fp64_kn(O._p(obs), O._p(e1), O._p(e2), O._p(e3), d["field_of_view_rad"], 1.0,
+                                       BL_CAMERA["spin"], BL_CAMERA["charge"], 1000.0, 20.0, w, w, 20000, 0, 0, 1.0,
+                                       O._p(st), O._p(it), O._p(z))
+            return t, float(it.mean())
+        t, _ = image(64)
+        w = int(min(max(64 * math.sqrt(seconds / 2 / max(t, 1e-3)) // 32 * 32, 64), side))
+        t, iters = image(w)
+        out["reference"] = {"value": w * w / t / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "reference",
+                            "sample": f"SoftwareComputeEngine::dispatch_fp64 (metric type 5, trace_exact_photon, "
+                                      f"heuristic-step RK4, {iters:.1f} steps/ray) on the same camera at {w}^2, "
+                                      f"hardware_concurrency threads, {t:.1f} s"}
+    rng = np.random.default_rng(0)
+    probe = rng.choice(side * side, 500, replace=False).astype(np.uint64)
+    t0 = time.perf_counter()
+    O.bl_trace(d, BL_CAMERA["charge"], pixels=probe, threads=cores)
+    rate = probe.size / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(max(rate * seconds / 2, 2000), side * side))
+    sample = rng.choice(side * side, n, replace=False).astype(np.uint64)
+    t0 = time.perf_counter()
+    O.bl_trace(d, BL_CAMERA["charge"], pixels=sample, threads=cores)
+    dt = time.perf_counter() - t0
+    out["port"] = {"value": n / dt / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                   "sample": f"{n} uniformly random rays of the {side}^2 image, FP64 DP45 oracle (oracle/bl_oracle.c), "
+                             f"{dt:.1f} s"}
+    return out
+
+
 def max_over_ranks(x: float, ws: int, device: str) -> float:
     """The slowest rank's time (every rank gets it); one all-reduce, no data-path collective."""
     if ws == 1:
@@ -360,6 +446,13 @@ def ours(args) -> None:
     if not args.no_bundles:
         batched = time_bundles(tr, relsim, args.steps, args.warmup, f"cuda:{local}")
 
+    bl = None
+    if not args.no_bl:
+        bl = time_boyer_lindquist(tr, relsim, args.side, ro, pix, flush, args.steps, args.warmup, fp64_peak, ws,
+                                  f"cuda:{local}")
+        if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+            bl["cpu_baseline"] = bl_cpu_baselines(args.side, args.cpu_seconds)
+
     summary = {}
     for prec, d in res.items():
         own_ms = float(sum(d["ms"]))
@@ -424,6 +517,8 @@ def ours(args) -> None:
             line["mixed_vs_fp64"] = summary["mixed"]["value"] / summary["fp64"]["value"]
         if batched is not None:
             line["batched_c4"] = batched
+        if bl is not None:
+            line["boyer_lindquist"] = bl
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -436,13 +531,14 @@ def vars_of(c) -> dict:
     return {f: getattr(c, f) for f, _ in c._fields_}
 
 
-def committed_traffic(precision: int):
-    """DRAM bytes per launch of the tracer kernel from the committed ncu summary, if present."""
+def committed_traffic(precision):
+    """DRAM bytes per launch of the tracer kernel from the committed ncu summary, if present
+    (precision 0: FP64, "bl": the Boyer-Lindquist kernel, else mixed)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
-        return d.get("fp64" if precision == 0 else "mixed")
+        return d.get(precision if isinstance(precision, str) else ("fp64" if precision == 0 else "mixed"))
     except (OSError, ValueError):
         return None
 
@@ -476,6 +572,7 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-bundles", action="store_true", help="skip the 512-bundle batched measurement")
+    ap.add_argument("--no-bl", action="store_true", help="skip the Boyer-Lindquist Kerr-Newman measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

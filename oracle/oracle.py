@@ -170,6 +170,8 @@ def ref() -> ctypes.CDLL:
         L.ref_rk45_trace.argtypes = [v, d, d, d, d, d, d, d, d, d, ctypes.c_int, v]
         L.ref_dispatch_fp64.argtypes = [v, v, v, v, d, d, d, d, d, u, u, u, u, u, v, v, v]
         L.ref_dispatch_fp64.restype = d
+        L.ref_dispatch_fp64_kn.argtypes = [v, v, v, v, d, d, d, d, d, d, u, u, u, u, u, d, v, v, v]
+        L.ref_dispatch_fp64_kn.restype = d
         L.ref_ms_case.argtypes = [v, u, v, v, v, v, v, v, v, v]
         L.ref_ms_case.restype = u
         L.ref_kn_metric.argtypes = [d, d, d, v, v]

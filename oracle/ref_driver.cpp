@@ -204,13 +204,14 @@ void ref_rk45_trace(const double y0[6], double mass, double spin, double rtol, d
 	out[6] = static_cast<double>(integ.statistics().rejected_steps);
 }
 
-// Oracle A: the reference's own CPU image path for a Kerr-Schild camera
-// (metric_type 3), heuristic-step RK4, thin Novikov-Thorne disk.  Writes
-// status_flags, iterations and redshift per pixel; returns wall seconds.
-double ref_dispatch_fp64(const double observer[4], const double e1[4], const double e2[4], const double e3[4], double fov,
-                         double mass, double spin, double escape_radius, double disk_outer, uint32_t width,
-                         uint32_t height, uint32_t max_steps, uint32_t row_offset, uint32_t row_count,
-                         uint32_t* status, uint32_t* iterations, float* redshift) {
+// The reference's own CPU image path (SoftwareComputeEngine::dispatch_fp64)
+// for one camera of the given metric type and charge.  Writes status_flags,
+// iterations and redshift per pixel; returns wall seconds.
+static double dispatch_fp64_metric(const double observer[4], const double e1[4], const double e2[4],
+                                   const double e3[4], double fov, double mass, double spin, double charge,
+                                   uint32_t metric_type, double escape_radius, double disk_outer, uint32_t width,
+                                   uint32_t height, uint32_t max_steps, uint32_t row_offset, uint32_t row_count,
+                                   double step_scale, uint32_t* status, uint32_t* iterations, float* redshift) {
 	R::GpuCameraPushConstants p{};
 	for (int i = 0; i < 4; ++i) {
 		p.observer_position[i] = observer[i];
@@ -222,7 +223,8 @@ double ref_dispatch_fp64(const double observer[4], const double e1[4], const dou
 	p.field_of_view_rad = fov;
 	p.metric_mass = mass;
 	p.metric_spin = spin;
-	p.metric_type = 3;
+	p.metric_charge = charge;
+	p.metric_type = metric_type;
 	p.escape_radius = escape_radius;
 	p.max_integration_steps = max_steps;
 	p.screen_width = width;
@@ -235,6 +237,9 @@ double ref_dispatch_fp64(const double observer[4], const double e1[4], const dou
 	p.primary_disk.inner_radius_scale = 1.0f;
 	p.primary_disk.outer_radius_mass_units = static_cast<float>(disk_outer);
 	p.hydro_disk.model = 1;  // Novikov-Thorne
+	// heuristic step (software_compute_engine.hpp:1424-1427) scaled for convergence studies
+	p.step_size_factor *= step_scale;
+	p.min_step_size *= step_scale;
 	const size_t rows = (row_count == 0) ? height : row_count;
 	std::vector<R::GpuPixelOutput> out(static_cast<size_t>(width) * rows);
 	const auto t0 = std::chrono::steady_clock::now();
@@ -246,6 +251,28 @@ double ref_dispatch_fp64(const double observer[4], const double e1[4], const dou
 		if (redshift) redshift[i] = out[i].redshift;
 	}
 	return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// Oracle A: the reference's own CPU image path for a Kerr-Schild camera
+// (metric_type 3), heuristic-step RK4, thin Novikov-Thorne disk.
+double ref_dispatch_fp64(const double observer[4], const double e1[4], const double e2[4], const double e3[4], double fov,
+                         double mass, double spin, double escape_radius, double disk_outer, uint32_t width,
+                         uint32_t height, uint32_t max_steps, uint32_t row_offset, uint32_t row_count,
+                         uint32_t* status, uint32_t* iterations, float* redshift) {
+	return dispatch_fp64_metric(observer, e1, e2, e3, fov, mass, spin, 0.0, 3u, escape_radius, disk_outer, width,
+	                            height, max_steps, row_offset, row_count, 1.0, status, iterations, redshift);
+}
+
+// The same for a Kerr-Newman camera (metric_type 5): trace_exact_photon with
+// KerrNewmanMetric, the ZAMO ray and heuristic-step RK4 on -Gamma u u, its
+// step_size_factor and min_step_size multiplied by step_scale (1: as shipped).
+double ref_dispatch_fp64_kn(const double observer[4], const double e1[4], const double e2[4], const double e3[4],
+                            double fov, double mass, double spin, double charge, double escape_radius,
+                            double disk_outer, uint32_t width, uint32_t height, uint32_t max_steps,
+                            uint32_t row_offset, uint32_t row_count, double step_scale, uint32_t* status,
+                            uint32_t* iterations, float* redshift) {
+	return dispatch_fp64_metric(observer, e1, e2, e3, fov, mass, spin, charge, 5u, escape_radius, disk_outer, width,
+	                            height, max_steps, row_offset, row_count, step_scale, status, iterations, redshift);
 }
 
 }  // extern "C"

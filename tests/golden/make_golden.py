@@ -17,6 +17,10 @@ committed so that the pins run without the reference tree:
                       (build_multi_source_data), superposed RHS (ms_rhs),
                       initial momentum (ms_initial_momentum) and inside-horizon
                       answer (ms_inside_horizon) at random points
+  ref_bl_image_path.npz  per-pixel status/iterations/redshift of the reference's
+                      CPU image path for a Kerr-Newman camera (metric type 5,
+                      trace_exact_photon, heuristic RK4) at its shipped step and
+                      at 1/4 and 1/20 of it, 64x64
   ref_boyer_lindquist.npz  Boyer-Lindquist Kerr-Newman form: the reference's
                       metric tensor, analytic Christoffel symbols and their
                       contraction -Gamma u u (KerrNewmanMetric and KerrMetric),
@@ -301,6 +305,33 @@ def boyer_lindquist(rng: np.random.Generator) -> dict:
     return out
 
 
+BL_IMAGE_CAMERA = dict(spin=0.9, charge=0.3, r_obs=50.0, incl_deg=75.0, fov_deg=30.0, side=64)
+
+
+def bl_image_path() -> dict:
+    import relsim
+
+    R = O.ref()
+    c = BL_IMAGE_CAMERA
+    W = c["side"]
+    cam = relsim.camera_dict(relsim.make_camera(spin=c["spin"], r_obs=c["r_obs"], incl_deg=c["incl_deg"],
+                                                fov_deg=c["fov_deg"], width=W, height=W,
+                                                metric_form=relsim.METRIC_BOYER_LINDQUIST, charge=c["charge"]))
+    obs, e1, e2, e3 = (np.ascontiguousarray(cam[k], dtype=np.float64)
+                       for k in ("observer_position", "tetrad_e1", "tetrad_e2", "tetrad_e3"))
+    out = {"step_scale": np.array([1.0, 0.25, 0.05])}
+    for i, sc in enumerate(out["step_scale"]):
+        st = np.zeros(W * W, np.uint32)
+        it = np.zeros(W * W, np.uint32)
+        z = np.zeros(W * W, np.float32)
+        R.ref_dispatch_fp64_kn(_p(obs), _p(e1), _p(e2), _p(e3), cam["field_of_view_rad"], 1.0, c["spin"], c["charge"],
+                               1000.0, 20.0, W, W, 200000, 0, 0, float(sc), _p(st), _p(it), _p(z))
+        out[f"status_flags_{i}"] = st
+        out[f"iterations_{i}"] = it
+        out[f"redshift_{i}"] = z
+    return out
+
+
 def main() -> None:
     O.build(ref=True)
     rng = np.random.default_rng(20261203)
@@ -310,6 +341,7 @@ def main() -> None:
         "ref_image_path": image_path,
         "ref_multi_source": lambda: multi_source(np.random.default_rng(12)),
         "ref_boyer_lindquist": lambda: boyer_lindquist(np.random.default_rng(5)),
+        "ref_bl_image_path": bl_image_path,
     }
     wanted = sys.argv[1:] or list(makers)
     for name in makers:  # in this order: the first two share one generator
