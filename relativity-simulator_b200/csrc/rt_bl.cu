@@ -145,7 +145,7 @@ template <int BLOCK>
 __device__ __forceinline__ double bl_stages(const BlDesc& B, const double* __restrict__ y,
                                             const double* __restrict__ k1, double hh, BlCold<BLOCK>& S, int tid,
                                             double* __restrict__ y5) {
-#pragma unroll 1
+#pragma unroll
     for (int st = 0; st < 6; ++st) {
         double in[NB];
         // the stage sum unrolled over j (predicated on j <= st): every shared-memory

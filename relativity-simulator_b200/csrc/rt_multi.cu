@@ -104,14 +104,11 @@ __device__ __forceinline__ void ms_stages(const MsSource* __restrict__ src, uint
 #pragma unroll 1
     for (int st = 0; st < 6; ++st) {
         double in[6];
-        // the stage sum unrolled over j (predicated on j <= st): the shared-memory loads
-        // of a stage are independent and issue up front instead of one per FMA
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
             double acc = kMsA[st][0] * k1[i];
-#pragma unroll
-            for (int j = 1; j < 6; ++j)
-                if (j <= st) acc += kMsA[st][j] * S.k[j - 1][i][tid];
+#pragma unroll 1
+            for (int j = 1; j <= st; ++j) acc += kMsA[st][j] * S.k[j - 1][i][tid];
             in[i] = y[i] + hh * acc;
         }
         if (st == 5) {
@@ -133,7 +130,7 @@ __device__ __forceinline__ void ms_stages(const MsSource* __restrict__ src, uint
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         double acc = kMsE[0] * k1[i];
-#pragma unroll
+#pragma unroll 1
         for (int j = 2; j < 7; ++j) acc += kMsE[j] * S.k[j - 1][i][tid];
         est[i] = fabs(hh) * fabs(acc);
     }
