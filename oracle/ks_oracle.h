@@ -183,6 +183,22 @@ void orc_bl_initial_state(const orc_camera* cam, double charge, uint32_t px, uin
 void orc_bl_trace(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first, uint64_t count,
                   orc_ray* out, int threads);
 
+/* --- pixel shading tail (shade_oracle.c) ---
+ * Disk profiles are GpuDiskProfile's 32 floats in declaration order.  A
+ * surface point is (mass, spin, inner, outer, radius, azimuth, redshift, time,
+ * detail); shading output is (r, g, b, opacity). */
+void orc_planck_xyz(double temperature_k, double xyz[3]);
+void orc_blackbody_rgb(double temperature_k, double reference_luminance, double rgb[3]);
+void orc_resolve_profile(const float in[32], const double overrides[4], float out[32]);
+void orc_nt_context(double mass, double spin, double inner, double outer, float accretion_rate_scale, double out[2]);
+void orc_disk_shade(const float profile[32], const double point[9], uint32_t hydro_model, float accretion_rate_scale,
+                    double out[4]);
+void orc_tonemap(const double rgb[3], uint32_t mode, double exposure_ev, float out[3]);
+void orc_shade_pixel(const float resolved_profile[32], uint32_t hydro_model, float accretion_rate_scale,
+                     uint32_t tonemap_mode, double exposure_ev, double mass, double disk_spin, double inner,
+                     double outer, double time, double detail, uint32_t status, double r_hit, double phi, double g,
+                     float out[3]);
+
 #ifdef __cplusplus
 }
 #endif

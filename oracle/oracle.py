@@ -137,6 +137,15 @@ def lib() -> ctypes.CDLL:
         L.orc_bl_initial_state.argtypes = [v, d, ctypes.c_uint32, ctypes.c_uint32, v]
         L.orc_bl_trace.argtypes = [v, d, v, ctypes.c_uint64, ctypes.c_uint64, v, ctypes.c_int]
         L.orc_bl_trace.restype = None
+        f = ctypes.c_float
+        L.orc_planck_xyz.argtypes = [d, v]
+        L.orc_blackbody_rgb.argtypes = [d, d, v]
+        L.orc_resolve_profile.argtypes = [v, v, v]
+        L.orc_nt_context.argtypes = [d, d, d, d, f, v]
+        L.orc_disk_shade.argtypes = [v, v, ctypes.c_uint32, f, v]
+        L.orc_tonemap.argtypes = [v, ctypes.c_uint32, d, v]
+        L.orc_shade_pixel.argtypes = [v, ctypes.c_uint32, f, ctypes.c_uint32, d, d, d, d, d, d, d, ctypes.c_uint32,
+                                      d, d, d, v]
         _lib = L
     return _lib
 

@@ -21,6 +21,11 @@ committed so that the pins run without the reference tree:
                       CPU image path for a Kerr-Newman camera (metric type 5,
                       trace_exact_photon, heuristic RK4) at its shipped step and
                       at 1/4 and 1/20 of it, 64x64
+  ref_shading.npz     pixel shading tail: the reference's resolved disk profile
+                      (resolve_primary_profile), thin-disk shading for both
+                      temperature models (AccretionDiskModel::shade,
+                      HydroDiskShader Novikov-Thorne context), blackbody colour
+                      and apply_tonemapping on random inputs
   ref_boyer_lindquist.npz  Boyer-Lindquist Kerr-Newman form: the reference's
                       metric tensor, analytic Christoffel symbols and their
                       contraction -Gamma u u (KerrNewmanMetric and KerrMetric),
@@ -332,6 +337,57 @@ def bl_image_path() -> dict:
     return out
 
 
+DISK_PROFILE_DEFAULT = [1.0, 1.0, 24.0, 9500.0, 1200.0, 0.75, 1.0, 2.0, 0.45, 1.0, 0.0, 1.0, 1.0, 1.0, 1.0, 4.0,
+                        0.35, 9.0, 3.0, 2.0, 1.2, 0.25, 0.45, 5.0, 4.0, 3.0, 0.2, 40.0, 1.0, 1.0, 1.0, 1.0]
+
+
+def shading(rng: np.random.Generator, n: int = 400) -> dict:
+    R = O.ref()
+    f32, f64, u32 = ctypes.c_float, ctypes.c_double, ctypes.c_uint32
+    v = ctypes.c_void_p
+    R.ref_resolve_profile.argtypes = [v, v, v]
+    R.ref_disk_shade.argtypes = [v, v, u32, f32, v]
+    R.ref_nt_context.argtypes = [f64, f64, f64, f64, f32, v]
+    R.ref_blackbody_rgb.argtypes = [f64, f64, v]
+    R.ref_tonemap.argtypes = [v, u32, f64, v]
+    base = np.array(DISK_PROFILE_DEFAULT, np.float32)
+    prof = np.tile(base, (n, 1))
+    prof[1::2] *= rng.uniform(0.5, 1.5, (n // 2, 32)).astype(np.float32)
+    prof[1::2, 24] = rng.integers(1, 7, n // 2)
+    over = np.stack([rng.uniform(3000, 50000, n), rng.uniform(0, 3000, n), rng.uniform(0.5, 1.5, n),
+                     rng.uniform(0, 6, n)], 1)
+    over[0] = [23796.0, 1200.0, 1.0, 5.32]  # the push constants' defaults
+    resolved = np.zeros((n, 32), np.float32)
+    points = np.zeros((n, 9))
+    model = (np.arange(n) % 2).astype(np.uint32)
+    rate = (1.0 + np.arange(n) % 3).astype(np.float32)
+    shade = np.zeros((n, 4))
+    ntc = np.zeros((n, 2))
+    for i in range(n):
+        R.ref_resolve_profile(_p(prof[i]), _p(over[i]), _p(resolved[i]))
+        spin = rng.uniform(-0.99, 0.99)
+        inner = rng.uniform(1.5, 7.0)
+        outer = rng.uniform(inner * 1.1, 40.0)
+        points[i] = [1.0, spin, inner, outer, rng.uniform(inner * 0.9, outer * 1.1), rng.uniform(-20, 20),
+                     rng.uniform(0.2, 2.5), rng.uniform(0, 50), rng.uniform(0, 1)]
+        R.ref_disk_shade(_p(resolved[i]), _p(points[i]), int(model[i]), float(rate[i]), _p(shade[i]))
+        R.ref_nt_context(1.0, spin, inner, outer, float(rate[i]), _p(ntc[i]))
+    temps = np.exp(rng.uniform(np.log(200.0), np.log(5e5), n))
+    bb = np.zeros((n, 3))
+    for i in range(n):
+        R.ref_blackbody_rgb(temps[i], 0.7, _p(bb[i]))
+    rgb = rng.exponential(0.5, (n, 3))
+    rgb[:4] = 0.0
+    ev = rng.uniform(-2, 2, n)
+    tone = np.zeros((n, 4, 3), np.float32)
+    for i in range(n):
+        for mode in range(4):
+            R.ref_tonemap(_p(rgb[i]), mode, ev[i], _p(tone[i, mode]))
+    return {"profile_in": prof, "overrides": over, "profile": resolved, "points": points, "model": model,
+            "rate": rate, "shade": shade, "nt_context": ntc, "temperature": temps, "blackbody": bb, "rgb": rgb,
+            "exposure": ev, "tonemap": tone}
+
+
 def main() -> None:
     O.build(ref=True)
     rng = np.random.default_rng(20261203)
@@ -342,6 +398,7 @@ def main() -> None:
         "ref_multi_source": lambda: multi_source(np.random.default_rng(12)),
         "ref_boyer_lindquist": lambda: boyer_lindquist(np.random.default_rng(5)),
         "ref_bl_image_path": bl_image_path,
+        "ref_shading": lambda: shading(np.random.default_rng(9)),
     }
     wanted = sys.argv[1:] or list(makers)
     for name in makers:  # in this order: the first two share one generator
