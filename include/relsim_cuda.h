@@ -133,6 +133,41 @@ typedef struct rt_pixel_out {
     uint32_t iterations_used;
 } rt_pixel_out;
 
+/* GpuDiskProfile (gpu_types.hpp:42-78): the disk's appearance, 32 floats in
+ * the reference's order (a GpuDiskProfile can be copied in directly). */
+typedef struct rt_disk_profile {
+    float enabled, inner_radius_scale, outer_radius_mass_units, peak_temperature_k;
+    float floor_temperature_k, temperature_exponent, zero_torque_strength, extra_beaming_exponent;
+    float brightness, color_saturation, tint_strength, opacity_scale;
+    float tint_r, tint_g, tint_b, rotation_speed_scale;
+    float ring_amplitude, ring_frequency, ring_sharpness, spiral_arm_count;
+    float spiral_pitch, spiral_amplitude, turbulence_amplitude, turbulence_scale;
+    float turbulence_octaves, radial_stretch, grain_amplitude, grain_scale;
+    float reference_luminance, noise_seed, temperature_normalization, edge_softness;
+} rt_disk_profile;
+
+/* Pixel shading of GpuPixelOutput's colour (the reference's shading tail,
+ * software_compute_engine.hpp:1538-1611): a disk hit is shaded as the thin
+ * disk at (r_hit, phi, g) -- temperature profile, rings, spiral arms,
+ * turbulence, blackbody colour, Doppler beaming, grading -- then tonemapped
+ * to sRGB; escaped and captured rays are black (the procedural sky is not
+ * part of this library: sky_enabled must be 0).  Fields as in
+ * GpuCameraPushConstants (gpu_types.hpp:990-1106); the profile is resolved as
+ * AccretionDiskModel::resolve_primary_profile does. */
+typedef struct rt_shading {
+    rt_disk_profile disk;                 /* primary_disk */
+    double disk_temperature_scale_k;      /* overrides disk.peak_temperature_k */
+    double disk_temperature_floor_k;      /* overrides disk.floor_temperature_k */
+    double disk_color_saturation;         /* overrides disk.color_saturation */
+    double disk_doppler_beaming_exponent; /* overrides disk.extra_beaming_exponent */
+    double time;                          /* animation time of the disk pattern */
+    double camera_exposure;               /* EV */
+    uint32_t tonemapping_mode;            /* 0 clamp, 1 ACES fit, 2 log luminance, 3 extended Reinhard */
+    uint32_t hydro_model;                 /* hydro_disk.model: 0 procedural profile, 1 Novikov-Thorne flux */
+    float accretion_rate_scale;           /* hydro_disk.accretion_rate_scale (Novikov-Thorne) */
+    uint32_t sky_enabled;                 /* must be 0 */
+} rt_shading;
+
 /* Per-ray record, structure of arrays.  Any pointer may be NULL (not written).
  * Pointers are host pointers for rt_dispatch* and device pointers for the
  * *_device entry points. */
@@ -265,6 +300,14 @@ uint64_t rt_bundle_rays(const rt_camera* cams, uint32_t n_bundles);
 
 /* Launch configuration (the autotuner writes it; zeros select defaults). */
 rt_status rt_set_launch_config(rt_handle* h, const rt_launch_config* cfg);
+
+/* Shade the pixels of later rt_dispatch, rt_dispatch_tile and
+ * rt_dispatch_device calls on this handle (single-hole cameras, both metric
+ * forms); NULL turns shading off (r = g = b = 0, a = 1, the default).
+ * RT_ERR_INVALID_ARG for hydro_model 2 (the Fishbone-Moncrief torus) or
+ * sky_enabled != 0. */
+void rt_shading_defaults(rt_shading* s);
+rt_status rt_set_shading(rt_handle* h, const rt_shading* s);
 rt_status rt_get_launch_config(const rt_handle* h, rt_launch_config* cfg);
 
 /* Counters of the last dispatch; waits for it to finish. */

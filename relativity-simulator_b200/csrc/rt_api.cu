@@ -45,6 +45,9 @@ struct rt_handle {
     DevBuf park_d, park_u, pass_queues;  // two-pass mixed tracer: parked state, far/near queues
     DevBuf ms_desc, ms_sources;          // multi-source camera and source table
     DevBuf bl_desc;                      // Boyer-Lindquist camera
+    DevBuf shade_desc;                   // pixel shading constants of the last shaded camera
+    bool shade_on = false;               // rt_set_shading
+    rt_shading shading{};
     DevBuf ray_fields[14];
     DevBuf pixels;
     // pinned staging of the bundle table
@@ -268,6 +271,36 @@ rt_status wait_stream(rt_handle* h, cudaStream_t s, double timeout_ms) {
 rt_status bl_launch(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
                     uint64_t out_offset, const OutPtrs& out, cudaStream_t s);
 
+// The record fields the shading pass reads (status, phi, r_hit, g), taken from
+// the handle's scratch where the caller did not ask for them.
+rt_status add_shade_fields(rt_handle* h, rt_ray_out& dev, size_t n) {
+    void** dp = reinterpret_cast<void**>(&dev);
+    const int fields[4] = {0, 6, 7, 8};
+    const size_t elem[4] = {4, 8, 8, 8};
+    for (int k = 0; k < 4; ++k) {
+        const int f = fields[k];
+        if (dp[f]) continue;
+        const rt_status st = ensure(h, h->ray_fields[f], n * elem[k]);
+        if (st != RT_OK) return st;
+        dp[f] = h->ray_fields[f].ptr;
+    }
+    return RT_OK;
+}
+
+// Enqueue the shading pass over n traced rays (after the trace, same stream).
+rt_status shade_launch(rt_handle* h, const rt_camera* cam, const rt_ray_out& dev, rt_pixel_out* pixels, size_t n,
+                       cudaStream_t s) {
+    ShadeDesc d;
+    if (!build_shade_desc(*cam, h->shading, d)) return fail(h, RT_ERR_INVALID_ARG, "unsupported shading settings");
+    rt_status st;
+    if ((st = ensure(h, h->shade_desc, sizeof(ShadeDesc))) != RT_OK) return st;
+    // pageable descriptor: the copy is staged before the call returns
+    RT_CUDA(h, cudaMemcpyAsync(h->shade_desc.ptr, &d, sizeof d, cudaMemcpyHostToDevice, s));
+    launch_shade(static_cast<const ShadeDesc*>(h->shade_desc.ptr), dev.status, dev.r_hit, dev.phi, dev.g, pixels, n, s);
+    RT_CUDA(h, cudaGetLastError());
+    return RT_OK;
+}
+
 // One host-buffer dispatch over a window (dispatch_and_readback semantics).
 rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0,
                           uint32_t nrows, rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity,
@@ -285,6 +318,8 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
         if ((st = ensure(h, h->pixels, n * sizeof(rt_pixel_out))) != RT_OK) return st;
         dpix = static_cast<rt_pixel_out*>(h->pixels.ptr);
     }
+    const bool shade = h->shade_on && pixels;
+    if (shade && (st = add_shade_fields(h, dev, n)) != RT_OK) return st;
     // bands of at most 2^24 rays; the cancel flag is polled between bands
     const uint64_t band_rows = std::max<uint64_t>(1, (uint64_t{1} << 24) / ncols);
     for (uint32_t r = 0; r < nrows; r += static_cast<uint32_t>(band_rows)) {
@@ -306,6 +341,7 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
             return st;
         if ((st = wait_stream(h, h->stream, 0.0)) != RT_OK) return st;
     }
+    if (shade && (st = shade_launch(h, cam, dev, dpix, n, h->stream)) != RT_OK) return st;
     if ((st = copy_back(h, rays, dev, pixels, dpix, n, h->stream)) != RT_OK) return st;
     return wait_stream(h, h->stream, 0.0);
 }
@@ -488,6 +524,7 @@ void rt_destroy(rt_handle* h) {
     release(h->ms_desc);
     release(h->ms_sources);
     release(h->bl_desc);
+    release(h->shade_desc);
     release(h->park_d);
     release(h->park_u);
     release(h->pass_queues);
@@ -548,6 +585,43 @@ void rt_camera_look_at_hole(rt_camera* c, double r, double theta, double phi) {
     }
 }
 
+void rt_shading_defaults(rt_shading* s) {
+    if (!s) return;
+    std::memset(s, 0, sizeof *s);
+    // GpuDiskProfile's defaults (gpu_types.hpp:42-75), in its field order
+    const float disk[32] = {1.0f, 1.0f, 24.0f, 9500.0f, 1200.0f, 0.75f, 1.0f, 2.0f, 0.45f, 1.0f, 0.0f,
+                            1.0f, 1.0f, 1.0f, 1.0f, 4.0f, 0.35f, 9.0f, 3.0f, 2.0f, 1.2f, 0.25f,
+                            0.45f, 5.0f, 4.0f, 3.0f, 0.2f, 40.0f, 1.0f, 1.0f, 1.0f, 1.0f};
+    std::memcpy(&s->disk, disk, sizeof disk);
+    // GpuCameraPushConstants' defaults (gpu_types.hpp:990-1041)
+    s->disk_temperature_scale_k = 23796.0;
+    s->disk_temperature_floor_k = 1200.0;
+    s->disk_color_saturation = 1.0;
+    s->disk_doppler_beaming_exponent = 5.32;
+    s->time = 0.0;
+    s->camera_exposure = 0.0;
+    s->tonemapping_mode = 0;
+    s->hydro_model = 0;
+    s->accretion_rate_scale = 1.0f;
+    s->sky_enabled = 0;
+}
+
+rt_status rt_set_shading(rt_handle* h, const rt_shading* s) {
+    if (!h) return RT_ERR_INVALID_ARG;
+    if (!s) {
+        h->shade_on = false;
+        return RT_OK;
+    }
+    rt_camera probe;
+    rt_camera_defaults(&probe);
+    ShadeDesc d;
+    if (!build_shade_desc(probe, *s, d))
+        return fail(h, RT_ERR_INVALID_ARG, "shading: hydro_model 0 or 1, tonemapping_mode 0..3, sky_enabled 0");
+    h->shading = *s;
+    h->shade_on = true;
+    return RT_OK;
+}
+
 rt_status rt_dispatch(rt_handle* h, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
                       size_t capacity, const volatile int* cancel) {
     if (!h) return RT_ERR_INVALID_ARG;
@@ -588,17 +662,22 @@ rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* p
     if (capacity < n) return fail(h, RT_ERR_INVALID_ARG, "capacity smaller than the window");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
     RT_CUDA(h, cudaSetDevice(h->device));
-    if (is_bl(cam))
-        return bl_launch(h, cam, 0, cam->screen_width, row0, nrows, 0, OutPtrs{pixels, rays ? *rays : rt_ray_out{}}, s);
-    rt_status st = ensure_host_bundles(h, 1);
-    if (st != RT_OK) return st;
+    rt_ray_out dev = rays ? *rays : rt_ray_out{};
+    const bool shade = h->shade_on && pixels;
+    rt_status st;
+    if (shade && (st = add_shade_fields(h, dev, n)) != RT_OK) return st;
+    if (is_bl(cam)) {
+        if ((st = bl_launch(h, cam, 0, cam->screen_width, row0, nrows, 0, OutPtrs{pixels, dev}, s)) != RT_OK) return st;
+        return shade ? shade_launch(h, cam, dev, pixels, n, s) : RT_OK;
+    }
+    if ((st = ensure_host_bundles(h, 1)) != RT_OK) return st;
     if ((st = ensure(h, h->bundles, sizeof(BundleDesc))) != RT_OK) return st;
     // the staging buffer is reused by the next call: wait for the previous upload
     RT_CUDA(h, cudaStreamSynchronize(s));
     build_bundle(*cam, 0, cam->screen_width, row0, nrows, 0, 0, h->host_bundles[0]);
     RT_CUDA(h, cudaMemcpyAsync(h->bundles.ptr, h->host_bundles, sizeof(BundleDesc), cudaMemcpyHostToDevice, s));
-    OutPtrs out{pixels, rays ? *rays : rt_ray_out{}};
-    return launch(h, 1, n, out, cam->precision_mode == RT_PRECISION_MIXED, s);
+    if ((st = launch(h, 1, n, OutPtrs{pixels, dev}, cam->precision_mode == RT_PRECISION_MIXED, s)) != RT_OK) return st;
+    return shade ? shade_launch(h, cam, dev, pixels, n, s) : RT_OK;
 }
 
 uint64_t rt_bundle_rays(const rt_camera* cams, uint32_t n) {

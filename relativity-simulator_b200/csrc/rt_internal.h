@@ -169,6 +169,28 @@ struct BlArgs {
     OutPtrs out;
 };
 
+// Per-camera constants of the pixel shading pass (rt_shade.cu): the resolved
+// disk profile, the disk's geometry, the Novikov-Thorne flux normalisation and
+// its Page-Thorne roots, and the spectral table of the blackbody colour
+// (33 trapezoid nodes over 380-780 nm, weights = node weight x CIE 1931 fit).
+struct alignas(16) ShadeDesc {
+    float profile[32];
+    double mass, disk_spin, inner, outer, time, detail, exposure;
+    double pattern_omega;                 // orbital angular velocity at sqrt(inner outer)
+    double nt_flux_peak, nt_rate_factor;  // Novikov-Thorne: peak flux over the disk, rate^(1/4)
+    double nt_m, nt_a_star, nt_x0, nt_x1, nt_x2, nt_x3, nt_r_isco;
+    uint32_t hydro_model, tonemap, pad0, pad1;
+    double lambda_um[33];
+    double weight[33][3];
+};
+
+// Build the shading constants of a camera; false if the settings are not
+// supported (hydro model 2, sky enabled).
+bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d);
+// Shade n rays: pixels[i].rgba from the record's status, r_hit, phi and g.
+void launch_shade(const ShadeDesc* desc, const uint32_t* status, const double* r_hit, const double* phi,
+                  const double* g, rt_pixel_out* pixels, uint64_t n, void* stream);
+
 // Host-side helpers implemented in rt_bundle.cpp.
 // Boyer-Lindquist bundle of a camera window (metric_form RT_METRIC_BOYER_LINDQUIST).
 void build_bl_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,

@@ -50,6 +50,25 @@ class Camera(ctypes.Structure):
     ]
 
 
+class DiskProfile(ctypes.Structure):
+    """rt_disk_profile: GpuDiskProfile's 32 floats in the reference's order."""
+    _fields_ = [(n, ctypes.c_float) for n in (
+        "enabled", "inner_radius_scale", "outer_radius_mass_units", "peak_temperature_k", "floor_temperature_k",
+        "temperature_exponent", "zero_torque_strength", "extra_beaming_exponent", "brightness", "color_saturation",
+        "tint_strength", "opacity_scale", "tint_r", "tint_g", "tint_b", "rotation_speed_scale", "ring_amplitude",
+        "ring_frequency", "ring_sharpness", "spiral_arm_count", "spiral_pitch", "spiral_amplitude",
+        "turbulence_amplitude", "turbulence_scale", "turbulence_octaves", "radial_stretch", "grain_amplitude",
+        "grain_scale", "reference_luminance", "noise_seed", "temperature_normalization", "edge_softness")]
+
+
+class Shading(ctypes.Structure):
+    """rt_shading: the pixel shading tail (disk colour, tonemapping)."""
+    _fields_ = [("disk", DiskProfile), ("disk_temperature_scale_k", _d), ("disk_temperature_floor_k", _d),
+                ("disk_color_saturation", _d), ("disk_doppler_beaming_exponent", _d), ("time", _d),
+                ("camera_exposure", _d), ("tonemapping_mode", _u32), ("hydro_model", _u32),
+                ("accretion_rate_scale", ctypes.c_float), ("sky_enabled", _u32)]
+
+
 class PixelOut(ctypes.Structure):
     _fields_ = [("r", ctypes.c_float), ("g", ctypes.c_float), ("b", ctypes.c_float), ("a", ctypes.c_float),
                 ("redshift", ctypes.c_float), ("affine_parameter", ctypes.c_float), ("status_flags", _u32),
@@ -125,7 +144,8 @@ EXPORTS = ["rt_create", "rt_destroy", "rt_is_ready", "rt_is_platform_supported",
            "rt_trace_bundles_device", "rt_bundle_rays", "rt_set_launch_config", "rt_get_launch_config",
            "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc", "rt_kerr_isco_radius", "rt_dispatch_multi", "rt_dispatch_multi_device",
            "rt_server_config_defaults", "rt_server_create", "rt_server_destroy", "rt_server_submit",
-           "rt_server_poll", "rt_server_get_stats", "rt_server_last_error", "rt_server_submit_multi"]
+           "rt_server_poll", "rt_server_get_stats", "rt_server_last_error", "rt_server_submit_multi",
+           "rt_shading_defaults", "rt_set_shading"]
 NOALLOC_MAX_BUNDLES = 32  # RT_NOALLOC_MAX_BUNDLES
 
 
@@ -154,6 +174,9 @@ def lib() -> ctypes.CDLL:
         L.rt_bundle_rays.argtypes = [p(Camera), _u32]
         L.rt_bundle_rays.restype = ctypes.c_uint64
         L.rt_set_launch_config.argtypes = [v, p(LaunchConfig)]
+        L.rt_shading_defaults.argtypes = [p(Shading)]
+        L.rt_shading_defaults.restype = None
+        L.rt_set_shading.argtypes = [v, p(Shading)]
         L.rt_get_launch_config.argtypes = [v, p(LaunchConfig)]
         L.rt_get_stats.argtypes = [v, p(Stats)]
         L.rt_synchronize.argtypes = [v, _d]
@@ -359,6 +382,10 @@ class Tracer:
     def synchronize(self, timeout_ms: float = 0.0) -> None:
         self._check(self.lib.rt_synchronize(self._h, timeout_ms))
 
+    def set_shading(self, shading: "Shading | None") -> None:
+        """Shade the pixels of later dispatches (None: colour off)."""
+        self._check(self.lib.rt_set_shading(self._h, ctypes.byref(shading) if shading is not None else None))
+
     def set_launch_config(self, block_size: int = 0, ctas_per_sm: int = 0, refill_threshold: int = 0,
                           rays_per_thread: int = 0, fp64_rolled: int = 0, mixed_single_kernel: int = 0) -> None:
         c = LaunchConfig(block_size, ctas_per_sm, refill_threshold, rays_per_thread, fp64_rolled, mixed_single_kernel)
@@ -390,6 +417,15 @@ def trace_bundles_noalloc(cams: list[Camera], rays: RayOut, pixels_ptr: int | No
                                         ctypes.byref(launch) if launch is not None else None, stream, err, len(err))
     if st != RT_OK:
         raise RelsimError(st, err.value.decode())
+
+
+def shading(**kw) -> Shading:
+    """rt_shading with the reference's defaults, overridden by keyword (field names)."""
+    s = Shading()
+    lib().rt_shading_defaults(ctypes.byref(s))
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
 
 
 def server_config(budget_bytes: int | None = None, record: Iterable[str] | None = None, **kw) -> ServerConfig:

@@ -50,6 +50,25 @@ def test_layouts_match_header(tmp_path):
     assert relsim.PIXEL_DTYPE.itemsize == 32
 
 
+def test_shading_layout_matches_header(tmp_path):
+    prog = tmp_path / "sh.c"
+    prog.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "relsim_cuda.h"\nint main(void){'
+                    'printf("%zu %zu %zu %zu %zu\\n", sizeof(rt_shading), sizeof(rt_disk_profile),'
+                    ' offsetof(rt_shading, disk_temperature_scale_k), offsetof(rt_shading, tonemapping_mode),'
+                    ' offsetof(rt_disk_profile, edge_softness)); return 0;}\n')
+    exe = tmp_path / "sh"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    exp = [ctypes.sizeof(relsim.Shading), ctypes.sizeof(relsim.DiskProfile),
+           relsim.Shading.disk_temperature_scale_k.offset, relsim.Shading.tonemapping_mode.offset,
+           relsim.DiskProfile.edge_softness.offset]
+    assert got == exp
+    assert got[1] == 128  # GpuDiskProfile (gpu_types.hpp:80 static_assert)
+    s = relsim.shading()
+    assert s.disk.peak_temperature_k == 9500.0 and s.disk_temperature_scale_k == 23796.0
+    assert s.disk_doppler_beaming_exponent == 5.32 and s.sky_enabled == 0
+
+
 def test_server_layouts_match_header(tmp_path):
     prog = tmp_path / "srv.c"
     prog.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "relsim_cuda.h"\nint main(void){'
