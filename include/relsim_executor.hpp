@@ -28,6 +28,7 @@
 #include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -100,6 +101,30 @@ rt_camera camera_from_push_constants(const PushConstants& p, const TraceSettings
     return c;
 }
 
+// rt_shading from the reference's push constants: primary_disk (a
+// GpuDiskProfile, copied as it lies), the disk temperature, saturation and
+// beaming overrides, time, exposure, tonemapping mode, and the hydro disk
+// model and accretion rate.  The procedural sky (params.sky) is not part of
+// the library and is left out: rays that escape stay black.
+template <class PushConstants>
+rt_shading shading_from_push_constants(const PushConstants& p) {
+    rt_shading s;
+    rt_shading_defaults(&s);
+    static_assert(sizeof(p.primary_disk) == sizeof(rt_disk_profile), "GpuDiskProfile layout");
+    std::memcpy(&s.disk, &p.primary_disk, sizeof s.disk);
+    s.disk_temperature_scale_k = p.disk_temperature_scale_k;
+    s.disk_temperature_floor_k = p.disk_temperature_floor_k;
+    s.disk_color_saturation = p.disk_color_saturation;
+    s.disk_doppler_beaming_exponent = p.disk_doppler_beaming_exponent;
+    s.time = p.time;
+    s.camera_exposure = p.camera_exposure;
+    s.tonemapping_mode = p.tonemapping_mode;
+    s.hydro_model = p.hydro_disk.model;
+    s.accretion_rate_scale = p.hydro_disk.accretion_rate_scale;
+    s.sky_enabled = 0;
+    return s;
+}
+
 class CudaComputeExecutor {
 public:
     CudaComputeExecutor() = default;
@@ -121,6 +146,9 @@ public:
     }
 
     [[nodiscard]] bool is_ready() const noexcept { return h_ != nullptr && rt_is_ready(h_) != 0; }
+
+    // Shade the pixels of later dispatches (nullptr: colour off, the default).
+    [[nodiscard]] bool set_shading(const rt_shading* s) { return h_ != nullptr && check(rt_set_shading(h_, s)); }
 
     void shutdown() noexcept {
         if (h_) rt_destroy(h_);

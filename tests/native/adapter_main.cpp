@@ -2,6 +2,7 @@
 // reference's pipeline drives VulkanComputeExecutor.  Used by tests/test_adapter.py.
 //   adapter_main map                 print the mapped camera of a push-constant struct
 //   adapter_main route               metric type routing: form, spin, charge for types 3, 5, 1
+//   adapter_main shade               the push constants' shading settings as rt_shading
 //   adapter_main cpu                 platform/initialise answers without a device
 //   adapter_main gpu <out.bin>       dispatch_and_readback of a 96x64 image -> raw pixels; cancel check
 #include <atomic>
@@ -14,15 +15,30 @@
 using Push = Relativistic::Render::GpuCameraPushConstants;
 #else
 #include <array>
-struct DiskProfile {
-    float inner_radius_scale = 1.0f;
-    float outer_radius_mass_units = 24.0f;
+struct DiskProfile {  // GpuDiskProfile's 32 floats (gpu_types.hpp:42-75)
+    float enabled = 1.0f, inner_radius_scale = 1.0f, outer_radius_mass_units = 24.0f, peak_temperature_k = 9500.0f;
+    float floor_temperature_k = 1200.0f, temperature_exponent = 0.75f, zero_torque_strength = 1.0f;
+    float extra_beaming_exponent = 2.0f, brightness = 0.45f, color_saturation = 1.0f, tint_strength = 0.0f;
+    float opacity_scale = 1.0f, tint_r = 1.0f, tint_g = 1.0f, tint_b = 1.0f, rotation_speed_scale = 4.0f;
+    float ring_amplitude = 0.35f, ring_frequency = 9.0f, ring_sharpness = 3.0f, spiral_arm_count = 2.0f;
+    float spiral_pitch = 1.2f, spiral_amplitude = 0.25f, turbulence_amplitude = 0.45f, turbulence_scale = 5.0f;
+    float turbulence_octaves = 4.0f, radial_stretch = 3.0f, grain_amplitude = 0.2f, grain_scale = 40.0f;
+    float reference_luminance = 1.0f, noise_seed = 1.0f, temperature_normalization = 1.0f, edge_softness = 1.0f;
+};
+struct HydroDisk {
+    uint32_t model = 0;
+    float accretion_rate_scale = 1.0f;
 };
 struct Push {  // the fields of GpuCameraPushConstants the tracer reads (gpu_types.hpp:966-1109)
     std::array<double, 4> observer_position{}, tetrad_e1{}, tetrad_e2{}, tetrad_e3{};
     double field_of_view_rad = 1.0471975511965976, metric_mass = 1.0, metric_spin = 0.0, escape_radius = 100.0;
     double metric_charge = 0.0;
     uint32_t metric_type = 3;
+    double time = 0.0, camera_exposure = 0.0;
+    double disk_temperature_scale_k = 23796.0, disk_temperature_floor_k = 1200.0;
+    double disk_doppler_beaming_exponent = 5.32, disk_color_saturation = 1.0;
+    uint32_t tonemapping_mode = 0;
+    HydroDisk hydro_disk{};
     uint32_t screen_width = 3840, screen_height = 2160, max_integration_steps = 2048;
     uint32_t dispatch_row_offset = 0, dispatch_row_count = 0;
     uint32_t tile_origin_x = 0, tile_origin_y = 0, tile_extent_x = 0, tile_extent_y = 0;
@@ -83,6 +99,22 @@ int main(int argc, char** argv) {
                         c.metric_spin, c.metric_charge);
         }
         std::printf("%d %d\n", relsim::metric_type_supported(4u) ? 1 : 0, relsim::metric_type_supported(0u) ? 1 : 0);
+        return 0;
+    }
+    if (!std::strcmp(mode, "shade")) {
+        Push p = headline_push(32, 32);
+        p.primary_disk.ring_frequency = 7.0f;
+        p.disk_temperature_scale_k = 15000.0;
+        p.disk_doppler_beaming_exponent = 3.0;
+        p.time = 2.5;
+        p.camera_exposure = -1.0;
+        p.tonemapping_mode = 1;
+        p.hydro_disk.model = 1;
+        p.hydro_disk.accretion_rate_scale = 2.0f;
+        const rt_shading s = relsim::shading_from_push_constants(p);
+        std::printf("%g %g %g %g %g %u %u %g %u %g\n", s.disk.ring_frequency, s.disk_temperature_scale_k,
+                    s.disk_doppler_beaming_exponent, s.time, s.camera_exposure, s.tonemapping_mode, s.hydro_model,
+                    s.accretion_rate_scale, s.sky_enabled, s.disk.edge_softness);
         return 0;
     }
     if (!std::strcmp(mode, "cpu")) {
