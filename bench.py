@@ -17,7 +17,8 @@ value: Mrays/s of the mixed tracer (the fp64 one with --precision fp64) with
        stream, L2 flushed between steps (a 256 MiB write); "precisions" holds
        both tracers' numbers and "mixed_vs_fp64" their ratio.
 e2e:   Mrays/s through rt_dispatch (the dispatch_and_readback-shaped C call)
-       with pinned host buffers, host<->device copies inside the timed region;
+       with pinned host buffers, host<->device copies inside the timed region,
+       pixels shaded (disk colour and tonemapping, rt_set_shading defaults);
        its per-image p50/p99 wall latency.
 N > 1: one independent image per GPU (replicas, no collective); value is the
        total over ranks divided by the slowest rank's time.
@@ -55,6 +56,7 @@ H2D_BYTES_PER_IMAGE = 464  # one bundle descriptor (per-camera constants) per im
 BL_FLOP_PER_ATTEMPT = 3542.0
 BL_CAMERA = dict(spin=0.9, charge=0.3, r_obs=50.0, incl_deg=75.0, fov_deg=30.0)
 BL_H2D_BYTES_PER_IMAGE = 352  # the Boyer-Lindquist camera descriptor (sizeof BlDesc)
+SHADE_H2D_BYTES = 1344  # the shading pass's per-camera constants (sizeof ShadeDesc)
 
 
 def headline_camera(relsim, precision: int, side: int = SIDE):
@@ -243,7 +245,8 @@ def time_device(tr, relsim, cam, n, ro, pix, flush, steps: int, warmup: int) -> 
 
 
 def time_e2e(tr, relsim, cam, n, steps: int, warmup: int):
-    """Trace through rt_dispatch (host buffers, copies inside); per-image wall latency."""
+    """Trace and shade through rt_dispatch (host buffers, copies inside), as the
+    reference's dispatch_and_readback returns coloured pixels; per-image wall latency."""
     import torch
 
     host = {f: torch.empty(n, dtype=(torch.int32 if f == "status" else torch.float64), pin_memory=True)
@@ -254,14 +257,18 @@ def time_e2e(tr, relsim, cam, n, steps: int, warmup: int):
         setattr(hro, f, t.data_ptr())
     L = relsim.lib()
     lat = []
-    for i in range(warmup + steps):
-        t0 = time.perf_counter()
-        st = L.rt_dispatch(tr.handle, ctypes.byref(cam), hpix.data_ptr(), ctypes.byref(hro), n, None)
-        dt = time.perf_counter() - t0
-        if st != 0:
-            raise RuntimeError(L.rt_last_error(tr.handle).decode())
-        if i >= warmup:
-            lat.append(dt)
+    tr.set_shading(relsim.shading())
+    try:
+        for i in range(warmup + steps):
+            t0 = time.perf_counter()
+            st = L.rt_dispatch(tr.handle, ctypes.byref(cam), hpix.data_ptr(), ctypes.byref(hro), n, None)
+            dt = time.perf_counter() - t0
+            if st != 0:
+                raise RuntimeError(L.rt_last_error(tr.handle).decode())
+            if i >= warmup:
+                lat.append(dt)
+    finally:
+        tr.set_shading(None)
     return host, lat
 
 
@@ -320,7 +327,9 @@ def time_boyer_lindquist(tr, relsim, side, ro, pix, flush, steps, warmup, fp64_p
         "latency_ms": {"kernel_p50": float(np.percentile(d["ms"], 50)), "kernel_p99": float(np.percentile(d["ms"], 99)),
                        "e2e_p50": 1e3 * float(np.percentile(lat, 50)), "e2e_p99": 1e3 * float(np.percentile(lat, 99))},
         "e2e": {"value": replica_value(n, ws, steps, e2e_wall * 1e3), "unit": "Mrays/s",
-                "h2d_bytes_per_step": BL_H2D_BYTES_PER_IMAGE, "d2h_bytes_per_step": n * (32 + 4 + 8 * (len(RECORD_FIELDS) - 1))},
+                "h2d_bytes_per_step": BL_H2D_BYTES_PER_IMAGE + SHADE_H2D_BYTES,
+                "d2h_bytes_per_step": n * (32 + 4 + 8 * (len(RECORD_FIELDS) - 1)),
+                "pixels": "shaded (disk colour + tonemapping, sky off)"},
         "roofline": {"bound": "fp64 pipe", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak, "flop_per_attempt": BL_FLOP_PER_ATTEMPT,
                      "peak_source": "measured in this run: register FMA-chain kernel (rt_measure_fma_peak)",
@@ -504,8 +513,8 @@ def ours(args) -> None:
                            "e2e_p50": 1e3 * float(np.percentile(lat, 50)),
                            "e2e_p99": 1e3 * float(np.percentile(lat, 99))},
             "roofline": h["roofline"],
-            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": H2D_BYTES_PER_IMAGE,
-                    "d2h_bytes_per_step": d2h,
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": H2D_BYTES_PER_IMAGE + SHADE_H2D_BYTES,
+                    "d2h_bytes_per_step": d2h, "pixels": "shaded (disk colour + tonemapping, sky off)",
                     "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
                     "latency_ms_p99": 1e3 * float(np.percentile(lat, 99))},
             "gpu_launches": args.steps,
