@@ -361,12 +361,13 @@ rt_status ms_launch(rt_handle* h, const rt_camera* cam, const rt_source* src, ui
     RT_CUDA(h, cudaMemcpyAsync(h->ms_sources.ptr, table, sizeof(MsSource) * count, cudaMemcpyHostToDevice, s));
     RT_CUDA(h, cudaMemsetAsync(h->queue.ptr, 0, sizeof(unsigned long long), s));
     RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
+    const rt_launch_config c = effective_cfg(h, false);
     MsArgs args{};
     args.bundles = static_cast<const MsDesc*>(h->ms_desc.ptr);
     args.sources = static_cast<const MsSource*>(h->ms_sources.ptr);
     args.n_bundles = 1;
-    args.refill_threshold = 32;
-    args.claim = 32;
+    args.refill_threshold = c.refill_threshold;
+    args.claim = 32u * c.rays_per_thread;
     args.total_rays = static_cast<uint64_t>(cam->screen_width) * nrows;
     args.queue = static_cast<unsigned long long*>(h->queue.ptr);
     args.stats = static_cast<unsigned long long*>(h->stats.ptr);

@@ -207,3 +207,31 @@ def test_server_rejects_invalid_boyer_lindquist(tracer):
         assert e.value.status == 1
         with pytest.raises(relsim.RelsimError):
             srv.submit(bl_cam("kn", side=8), sources=[relsim.make_source((10.0, 0.0, 0.0), 0.5, 0.3, (0, 0, 1))])
+
+
+EDGE_CASES = {
+    # observer 0.6 deg off the axis: rays pass the pole and are reflected
+    "near_axis": (0.9, 0.3, dict(r_obs=30.0, incl_deg=0.6, fov_deg=40.0)),
+    # close observer inside the disk's outer radius
+    "close": (0.7, 0.5, dict(r_obs=5.0, incl_deg=60.0, fov_deg=90.0)),
+    # near-extremal: a^2 + Q^2 = 0.9925 M^2, r_+ = 1.087 M
+    "near_extremal": (0.95, 0.3, dict(r_obs=40.0, incl_deg=80.0, fov_deg=25.0)),
+}
+
+
+@pytest.mark.parametrize("tag", list(EDGE_CASES))
+def test_edge_cases_match_oracle(tracer, tag):
+    spin, charge, kw = EDGE_CASES[tag]
+    cam = relsim.make_camera(spin=spin, width=48, height=48, metric_form=relsim.METRIC_BOYER_LINDQUIST, charge=charge,
+                             **kw)
+    _compare(tracer, cam)
+
+
+def test_charge_sign_does_not_matter(tracer):
+    """The Kerr-Newman metric depends on Q^2 only."""
+    a = tracer.dispatch(bl_cam("kn_hi_q", side=32), fields=FIELDS, pixels=True)
+    neg = bl_cam("kn_hi_q", side=32)
+    neg.metric_charge = -neg.metric_charge
+    b = tracer.dispatch(neg, fields=FIELDS, pixels=True)
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k])

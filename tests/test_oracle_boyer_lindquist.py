@@ -217,3 +217,22 @@ def test_reference_image_path_converges_to_oracle():
     assert agree[0] > 0.85
     assert agree[0] < agree[1] < agree[2] + 1e-3
     assert agree[2] >= 0.98, agree
+
+
+def test_pole_reflection_keeps_theta_in_range():
+    """An observer 0.6 deg off the axis: rays pass the pole, are reflected
+    (theta -> -theta, phi + pi) and end with theta in [0, pi]; the image of
+    a = Q = 0 is rotationally symmetric about the axis, so opposite pixels
+    through the image centre agree in class."""
+    W = 33
+    cam = relsim.camera_dict(relsim.make_camera(spin=0.0, r_obs=30.0, incl_deg=0.6, fov_deg=40.0, width=W, height=W,
+                                                disk_outer=0.0))
+    rays = O.bl_trace(cam, 0.0)
+    assert np.all((rays["theta"] >= 0.0) & (rays["theta"] <= np.pi))
+    st = rays["status"].reshape(W, W)
+    np.testing.assert_array_equal(st, st[::-1, ::-1])
+    cam_kn = relsim.camera_dict(relsim.make_camera(spin=0.9, r_obs=30.0, incl_deg=0.6, fov_deg=40.0, width=24,
+                                                   height=24))
+    kn = O.bl_trace(cam_kn, 0.3)
+    assert np.all(kn["status"] != O.UNFINISHED)
+    assert np.all((kn["theta"] >= 0.0) & (kn["theta"] <= np.pi))
