@@ -484,11 +484,14 @@ __device__ __forceinline__ void fp64_stages_rolled(const double* __restrict__ y,
 #pragma unroll 1
     for (int st = 0; st < 6; ++st) {
         double in[6];
+        // the stage sum unrolled over j (predicated on j <= st): the shared-memory loads
+        // of a stage are independent and issue up front instead of one per FMA
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
             double acc = kDpA[st][0] * k1[i];
-#pragma unroll 1
-            for (int j = 1; j <= st; ++j) acc += kDpA[st][j] * K.k[j - 1][i][tid];
+#pragma unroll
+            for (int j = 1; j < 6; ++j)
+                if (j <= st) acc += kDpA[st][j] * K.k[j - 1][i][tid];
             in[i] = y[i] + hh * acc;
         }
         if (st == 5) {
@@ -511,7 +514,7 @@ __device__ __forceinline__ void fp64_stages_rolled(const double* __restrict__ y,
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         double acc = kDpE[0] * k1[i];
-#pragma unroll 1
+#pragma unroll
         for (int j = 2; j < 7; ++j) acc += kDpE[j] * K.k[j - 1][i][tid];
         est[i] = fabs(hh) * fabs(acc);
     }
