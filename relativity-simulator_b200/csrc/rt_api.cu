@@ -37,7 +37,11 @@ struct rt_handle {
     int sm_count = 0;
     bool ready = false;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;          // second stream of banded host dispatches
+    cudaStream_t copy_stream = nullptr;      // their device-to-host copies
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t band_ev[8] = {};             // band traced (and shaded): its copies may start
     std::string error;
     rt_launch_config cfg{};
     // device scratch
@@ -64,6 +68,12 @@ struct rt_handle {
 };
 
 namespace {
+
+bool create_band_events(rt_handle* h) {
+    for (cudaEvent_t& e : h->band_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+    return true;
+}
 
 rt_status fail(rt_handle* h, rt_status st, const std::string& msg) {
     if (h) h->error = msg;
@@ -164,7 +174,8 @@ bool uses_two_pass(const rt_launch_config& c, bool mixed, uint64_t total) {
 }
 
 rt_status launch_two_pass(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs& out,
-                          const rt_launch_config& c, cudaStream_t s, bool capturing) {
+                          const rt_launch_config& c, cudaStream_t s, bool capturing, uint32_t bands = 1,
+                          BandHook hook = nullptr, void* hook_ctx = nullptr) {
     if (!capturing) {
         const rt_status st = ensure_two_pass(h, total);
         if (st != RT_OK) return st;
@@ -187,8 +198,10 @@ rt_status launch_two_pass(rt_handle* h, uint32_t n_bundles, uint64_t total, cons
     buf.counters = static_cast<char*>(h->queue.ptr);
     RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
     if (!capturing) RT_CUDA(h, cudaEventRecord(h->ev0, s));
-    RT_CUDA(h, static_cast<cudaError_t>(
-                   enqueue_two_pass(args, buf, h->sm_count, c.block_size, s, nullptr, nullptr, nullptr, 1)));
+    const bool banded = bands > 1 && !capturing;
+    RT_CUDA(h, static_cast<cudaError_t>(enqueue_two_pass(
+                   args, buf, h->sm_count, c.block_size, s, banded ? h->stream2 : nullptr,
+                   banded ? h->ev_fork : nullptr, banded ? h->ev_join : nullptr, banded ? bands : 1, hook, hook_ctx)));
     if (!capturing) {
         RT_CUDA(h, cudaEventRecord(h->ev1, s));
         h->timed = true;
@@ -287,19 +300,81 @@ rt_status add_shade_fields(rt_handle* h, rt_ray_out& dev, size_t n) {
     return RT_OK;
 }
 
-// Enqueue the shading pass over n traced rays (after the trace, same stream).
-rt_status shade_launch(rt_handle* h, const rt_camera* cam, const rt_ray_out& dev, rt_pixel_out* pixels, size_t n,
-                       cudaStream_t s) {
+// Upload the shading constants of a camera (before the trace, on its stream).
+rt_status shade_prepare(rt_handle* h, const rt_camera* cam, cudaStream_t s) {
     ShadeDesc d;
     if (!build_shade_desc(*cam, h->shading, d)) return fail(h, RT_ERR_INVALID_ARG, "unsupported shading settings");
     rt_status st;
     if ((st = ensure(h, h->shade_desc, sizeof(ShadeDesc))) != RT_OK) return st;
     // pageable descriptor: the copy is staged before the call returns
     RT_CUDA(h, cudaMemcpyAsync(h->shade_desc.ptr, &d, sizeof d, cudaMemcpyHostToDevice, s));
+    return RT_OK;
+}
+
+// Enqueue the shading pass over n traced rays (after the trace, same stream).
+rt_status shade_launch(rt_handle* h, const rt_camera* cam, const rt_ray_out& dev, rt_pixel_out* pixels, size_t n,
+                       cudaStream_t s) {
+    rt_status st;
+    if ((st = shade_prepare(h, cam, s)) != RT_OK) return st;
     launch_shade(static_cast<const ShadeDesc*>(h->shade_desc.ptr), dev.status, dev.r_hit, dev.phi, dev.g, pixels, n, s);
     RT_CUDA(h, cudaGetLastError());
     return RT_OK;
 }
+
+// Per-band work of a banded host dispatch: shade the band's rays on the band's
+// stream, then copy its slice of the pixels and of every record field the
+// caller asked for on the copy stream (once the band is done), so that no
+// trace waits behind a copy.
+struct BandCopyCtx {
+    rt_handle* h;
+    const rt_ray_out* host;
+    rt_ray_out dev;
+    rt_pixel_out* hpix;
+    rt_pixel_out* dpix;
+    uint64_t offset;  // output element of the launch's first ray
+    bool shade;
+    uint32_t band;    // next band event
+};
+
+int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
+    BandCopyCtx& c = *static_cast<BandCopyCtx*>(vctx);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint64_t o = c.offset + begin;
+    if (c.shade && c.dpix) {
+        launch_shade(static_cast<const ShadeDesc*>(c.h->shade_desc.ptr), c.dev.status + o, c.dev.r_hit + o,
+                     c.dev.phi + o, c.dev.g + o, c.dpix + o, count, s);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return static_cast<int>(e);
+    }
+    cudaEvent_t ev = c.h->band_ev[c.band++ % 8];
+    cudaError_t e0 = cudaEventRecord(ev, s);
+    if (e0 == cudaSuccess) e0 = cudaStreamWaitEvent(c.h->copy_stream, ev, 0);
+    if (e0 != cudaSuccess) return static_cast<int>(e0);
+    s = c.h->copy_stream;
+    if (c.host) {
+        void* const* hp = reinterpret_cast<void* const*>(c.host);
+        void* const* dp = reinterpret_cast<void* const*>(&c.dev);
+        const size_t elem[14] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
+        for (int f = 0; f < 14; ++f) {
+            if (!hp[f]) continue;
+            const cudaError_t e = cudaMemcpyAsync(static_cast<char*>(hp[f]) + o * elem[f],
+                                                  static_cast<const char*>(dp[f]) + o * elem[f], count * elem[f],
+                                                  cudaMemcpyDeviceToHost, s);
+            if (e != cudaSuccess) return static_cast<int>(e);
+        }
+    }
+    if (c.hpix) {
+        const cudaError_t e = cudaMemcpyAsync(c.hpix + o, c.dpix + o, count * sizeof(rt_pixel_out),
+                                              cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) return static_cast<int>(e);
+    }
+    return static_cast<int>(cudaSuccess);
+}
+
+// Bands of a host dispatch on the two-pass tracer: each band's copies overlap
+// the next band's trace (1 M rays and up).
+constexpr uint32_t kCopyBands = 4;
+constexpr uint64_t kBandedMinRays = uint64_t{1} << 20;
 
 // One host-buffer dispatch over a window (dispatch_and_readback semantics).
 rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0,
@@ -320,30 +395,41 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
     }
     const bool shade = h->shade_on && pixels;
     if (shade && (st = add_shade_fields(h, dev, n)) != RT_OK) return st;
-    // bands of at most 2^24 rays; the cancel flag is polled between bands
+    if (shade && (st = shade_prepare(h, cam, h->stream)) != RT_OK) return st;
+    // bands of at most 2^24 rays; the cancel flag is polled between bands.  Each
+    // band's shading and copies follow its trace; on the two-pass tracer a band
+    // is traced in sub-bands whose copies overlap the next sub-band's trace.
     const uint64_t band_rows = std::max<uint64_t>(1, (uint64_t{1} << 24) / ncols);
     for (uint32_t r = 0; r < nrows; r += static_cast<uint32_t>(band_rows)) {
         if (cancel && *cancel) return fail(h, RT_ERR_CANCELLED, "cancelled");
         const uint32_t rows = static_cast<uint32_t>(std::min<uint64_t>(band_rows, nrows - r));
         const uint64_t offset = static_cast<uint64_t>(r) * ncols;
+        const uint64_t launch_rays = static_cast<uint64_t>(rows) * ncols;
+        BandCopyCtx ctx{h, rays, dev, pixels, dpix, offset, shade, 0};
         if (is_bl(cam)) {
             if ((st = bl_launch(h, cam, col0, ncols, row0 + r, rows, offset, OutPtrs{dpix, dev}, h->stream)) != RT_OK)
                 return st;
-            if ((st = wait_stream(h, h->stream, 0.0)) != RT_OK) return st;
-            continue;
+        } else {
+            build_bundle(*cam, col0, ncols, row0 + r, rows, 0, offset, h->host_bundles[0]);
+            RT_CUDA(h, cudaMemcpyAsync(h->bundles.ptr, h->host_bundles, sizeof(BundleDesc), cudaMemcpyHostToDevice,
+                                       h->stream));
+            const bool mixed = cam->precision_mode == RT_PRECISION_MIXED;
+            const rt_launch_config c = effective_cfg(h, mixed);
+            if (uses_two_pass(c, mixed, launch_rays) && launch_rays >= kBandedMinRays) {
+                if ((st = launch_two_pass(h, 1, launch_rays, OutPtrs{dpix, dev}, c, h->stream, false, kCopyBands,
+                                          band_copy_hook, &ctx)) != RT_OK)
+                    return st;
+                if ((st = wait_stream(h, h->stream, 0.0)) != RT_OK) return st;
+                if ((st = wait_stream(h, h->copy_stream, 0.0)) != RT_OK) return st;
+                continue;
+            }
+            if ((st = launch(h, 1, launch_rays, OutPtrs{dpix, dev}, mixed, h->stream)) != RT_OK) return st;
         }
-        build_bundle(*cam, col0, ncols, row0 + r, rows, 0, offset, h->host_bundles[0]);
-        RT_CUDA(h, cudaMemcpyAsync(h->bundles.ptr, h->host_bundles, sizeof(BundleDesc), cudaMemcpyHostToDevice,
-                                   h->stream));
-        OutPtrs out{dpix, dev};
-        if ((st = launch(h, 1, static_cast<uint64_t>(rows) * ncols, out, cam->precision_mode == RT_PRECISION_MIXED,
-                         h->stream)) != RT_OK)
-            return st;
+        RT_CUDA(h, static_cast<cudaError_t>(band_copy_hook(&ctx, 0, launch_rays, h->stream)));
         if ((st = wait_stream(h, h->stream, 0.0)) != RT_OK) return st;
+        if ((st = wait_stream(h, h->copy_stream, 0.0)) != RT_OK) return st;
     }
-    if (shade && (st = shade_launch(h, cam, dev, dpix, n, h->stream)) != RT_OK) return st;
-    if ((st = copy_back(h, rays, dev, pixels, dpix, n, h->stream)) != RT_OK) return st;
-    return wait_stream(h, h->stream, 0.0);
+    return RT_OK;
 }
 
 // Enqueue a multi-source trace of the camera's row window (outputs: device).
@@ -502,7 +588,11 @@ rt_status rt_create(rt_handle** out, int device_ordinal) {
     h->device = device_ordinal;
     h->sm_count = p.multiProcessorCount;
     if (cudaSetDevice(device_ordinal) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess || !create_band_events(h)) {
         cudaGetLastError();
         rt_destroy(h);
         return RT_ERR_DEVICE;
@@ -536,6 +626,12 @@ void rt_destroy(rt_handle* h) {
     if (h->host_bundles) cudaFreeHost(h->host_bundles);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    for (cudaEvent_t& e : h->band_ev)
+        if (e) cudaEventDestroy(e);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+    if (h->stream2) cudaStreamDestroy(h->stream2);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }

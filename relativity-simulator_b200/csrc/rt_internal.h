@@ -224,6 +224,10 @@ struct TwoPassBuffers {
 constexpr uint32_t kMaxBands = 8;
 // Bytes of park.d, park.u and queues for n rays.
 uint64_t two_pass_state_bytes(uint64_t n);
+// Work enqueued on a band's stream once the band is traced (rays [begin,
+// begin + count) of the launch); returns a cudaError_t value.
+typedef int (*BandHook)(void* ctx, uint64_t begin, uint64_t count, void* stream);
+
 // Enqueue the rounds of the two-pass mixed tracer (memsets, launches and event
 // records only, so it can be captured into a graph).  `base` carries the
 // bundles, outputs, zeroed stats, the far pass's refill threshold and claim,
@@ -232,8 +236,11 @@ uint64_t two_pass_state_bytes(uint64_t n);
 // overlaps the next band's far pass; fork and join (events created by the
 // caller) bring stream2 into and out of the sequence.  bands = 1 uses
 // `stream` alone.  Returns a cudaError_t value.
+// after_band (optional) runs for each band after the next band's trace has been
+// enqueued, so a band's copies can overlap the next band's trace.
 int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_count, uint32_t far_block,
-                     void* stream, void* stream2, void* fork, void* join, uint32_t bands);
+                     void* stream, void* stream2, void* fork, void* join, uint32_t bands,
+                     BandHook after_band = nullptr, void* hook_ctx = nullptr);
 int trace_occupancy(uint32_t block, bool mixed, bool rolled);
 uint32_t kernel_block(uint32_t block, bool mixed, bool rolled);
 // Launch shape with defaults filled in and limits applied for one precision.

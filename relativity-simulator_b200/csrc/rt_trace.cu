@@ -1280,7 +1280,8 @@ cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t beg
 }  // namespace
 
 int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_count, uint32_t far_block,
-                     void* stream, void* stream2, void* fork, void* join, uint32_t bands) {
+                     void* stream, void* stream2, void* fork, void* join, uint32_t bands, BandHook after_band,
+                     void* hook_ctx) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaStream_t s2 = static_cast<cudaStream_t>(stream2);
     const uint64_t n = base.total_rays;
@@ -1298,15 +1299,25 @@ int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_co
         if ((e = cudaEventRecord(static_cast<cudaEvent_t>(fork), s)) != cudaSuccess) return static_cast<int>(e);
         if ((e = cudaStreamWaitEvent(s2, static_cast<cudaEvent_t>(fork), 0)) != cudaSuccess) return static_cast<int>(e);
     }
-    // bands of whole warps' worth of rays (multiples of 32)
+    // bands of whole warps' worth of rays (multiples of 32); a band's hook is
+    // enqueued after the next band's trace, so its work overlaps that trace
     const uint64_t per = ((n + bands - 1) / bands + 31) / 32 * 32;
-    uint64_t begin = 0;
+    uint64_t begin = 0, prev_begin = 0, prev_count = 0;
+    cudaStream_t prev_stream = nullptr;
     for (uint32_t b = 0; b < bands && begin < n && e == cudaSuccess; ++b) {
         const uint64_t count = (n - begin < per) ? n - begin : per;
+        cudaStream_t sb = (b & 1u) ? s2 : s;
         e = enqueue_band(base, buf, begin, count, buf.counters + 32 * b, far_grid, far_block, near_grid, finish_grid,
-                         (b & 1u) ? s2 : s);
+                         sb);
+        if (e == cudaSuccess && after_band && prev_stream)
+            e = static_cast<cudaError_t>(after_band(hook_ctx, prev_begin, prev_count, prev_stream));
+        prev_begin = begin;
+        prev_count = count;
+        prev_stream = sb;
         begin += count;
     }
+    if (e == cudaSuccess && after_band && prev_stream)
+        e = static_cast<cudaError_t>(after_band(hook_ctx, prev_begin, prev_count, prev_stream));
     if (e != cudaSuccess) return static_cast<int>(e);
     if (bands > 1) {
         if ((e = cudaEventRecord(static_cast<cudaEvent_t>(join), s2)) != cudaSuccess) return static_cast<int>(e);
