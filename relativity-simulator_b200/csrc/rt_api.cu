@@ -373,7 +373,7 @@ int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
 
 // Bands of a host dispatch on the two-pass tracer: each band's copies overlap
 // the next band's trace (1 M rays and up).
-constexpr uint32_t kCopyBands = 4;
+constexpr uint32_t kCopyBands = 8;
 constexpr uint64_t kBandedMinRays = uint64_t{1} << 20;
 
 // One host-buffer dispatch over a window (dispatch_and_readback semantics).
