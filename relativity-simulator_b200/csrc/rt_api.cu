@@ -49,6 +49,7 @@ struct rt_handle {
     DevBuf park_d, park_u, pass_queues;  // two-pass mixed tracer: parked state, far/near queues
     DevBuf ms_desc, ms_sources;          // multi-source camera and source table
     DevBuf bl_desc;                      // Boyer-Lindquist camera
+    DevBuf band_desc, band_queue;        // banded single-kernel host dispatches: per-band camera and counter
     DevBuf shade_desc;                   // pixel shading constants of the last shaded camera
     bool shade_on = false;               // rt_set_shading
     rt_shading shading{};
@@ -283,6 +284,9 @@ rt_status wait_stream(rt_handle* h, cudaStream_t s, double timeout_ms) {
 
 rt_status bl_launch(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0, uint32_t nrows,
                     uint64_t out_offset, const OutPtrs& out, cudaStream_t s);
+struct BandCopyCtx;
+rt_status launch_banded_single(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0,
+                               uint32_t nrows, uint64_t out_offset, const OutPtrs& out, BandCopyCtx& ctx);
 
 // The record fields the shading pass reads (status, phi, r_hit, g), taken from
 // the handle's scratch where the caller did not ask for them.
@@ -406,6 +410,16 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
         const uint64_t offset = static_cast<uint64_t>(r) * ncols;
         const uint64_t launch_rays = static_cast<uint64_t>(rows) * ncols;
         BandCopyCtx ctx{h, rays, dev, pixels, dpix, offset, shade, 0};
+        const bool two_pass = !is_bl(cam) && uses_two_pass(effective_cfg(h, cam->precision_mode == RT_PRECISION_MIXED),
+                                                          cam->precision_mode == RT_PRECISION_MIXED, launch_rays);
+        if (!two_pass && launch_rays >= kBandedMinRays && rows >= kCopyBands) {
+            if ((st = launch_banded_single(h, cam, col0, ncols, row0 + r, rows, offset, OutPtrs{dpix, dev}, ctx)) !=
+                RT_OK)
+                return st;
+            if ((st = wait_stream(h, h->stream, 0.0)) != RT_OK) return st;
+            if ((st = wait_stream(h, h->copy_stream, 0.0)) != RT_OK) return st;
+            continue;
+        }
         if (is_bl(cam)) {
             if ((st = bl_launch(h, cam, col0, ncols, row0 + r, rows, offset, OutPtrs{dpix, dev}, h->stream)) != RT_OK)
                 return st;
@@ -503,6 +517,82 @@ rt_status bl_launch(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t 
     RT_CUDA(h, cudaEventRecord(h->ev0, s));
     launch_bl_trace(args, bl_trace_grid(h->sm_count), s);
     RT_CUDA(h, cudaGetLastError());
+    RT_CUDA(h, cudaEventRecord(h->ev1, s));
+    h->timed = true;
+    return RT_OK;
+}
+
+// A single-kernel host dispatch (the plain FP64 or single mixed Kerr-Schild
+// tracer, or the Boyer-Lindquist tracer) in kCopyBands row bands: each band is
+// one persistent launch with its own camera descriptor and work counter, the
+// bands alternate between the handle's two streams, and each band's shading and
+// copies (band_copy_hook) are enqueued after the next band's launch.
+rt_status launch_banded_single(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t ncols, uint32_t row0,
+                               uint32_t nrows, uint64_t out_offset, const OutPtrs& out, BandCopyCtx& ctx) {
+    const bool bl = is_bl(cam);
+    const bool mixed = !bl && cam->precision_mode == RT_PRECISION_MIXED;
+    const size_t desc_bytes = bl ? sizeof(BlDesc) : sizeof(BundleDesc);
+    rt_status st;
+    if ((st = ensure(h, h->band_desc, desc_bytes * kCopyBands)) != RT_OK) return st;
+    if ((st = ensure(h, h->band_queue, sizeof(unsigned long long) * kCopyBands)) != RT_OK) return st;
+    const rt_launch_config c = effective_cfg(h, mixed);
+    cudaStream_t s = h->stream, s2 = h->stream2;
+    RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
+    RT_CUDA(h, cudaMemsetAsync(h->band_queue.ptr, 0, sizeof(unsigned long long) * kCopyBands, s));
+    RT_CUDA(h, cudaEventRecord(h->ev0, s));
+    RT_CUDA(h, cudaEventRecord(h->ev_fork, s));
+    RT_CUDA(h, cudaStreamWaitEvent(s2, h->ev_fork, 0));
+    const uint32_t per = (nrows + kCopyBands - 1) / kCopyBands;
+    uint64_t prev_begin = 0, prev_count = 0;
+    cudaStream_t prev_stream = nullptr;
+    uint32_t b = 0;
+    for (uint32_t r = 0; r < nrows; r += per, ++b) {
+        const uint32_t rows = std::min(per, nrows - r);
+        const uint64_t begin = static_cast<uint64_t>(r) * ncols;
+        const uint64_t count = static_cast<uint64_t>(rows) * ncols;
+        cudaStream_t sb = (b & 1u) ? s2 : s;
+        char* dd = static_cast<char*>(h->band_desc.ptr) + desc_bytes * b;
+        unsigned long long* q = static_cast<unsigned long long*>(h->band_queue.ptr) + b;
+        // pageable descriptors: each copy is staged before the call returns
+        if (bl) {
+            BlDesc d;
+            build_bl_bundle(*cam, col0, ncols, row0 + r, rows, 0, out_offset + begin, d);
+            RT_CUDA(h, cudaMemcpyAsync(dd, &d, sizeof d, cudaMemcpyHostToDevice, sb));
+            BlArgs args{};
+            args.bundles = reinterpret_cast<const BlDesc*>(dd);
+            args.n_bundles = 1;
+            args.refill_threshold = c.refill_threshold;
+            args.claim = 32u * c.rays_per_thread;
+            args.total_rays = count;
+            args.queue = q;
+            args.stats = static_cast<unsigned long long*>(h->stats.ptr);
+            args.out = out;
+            launch_bl_trace(args, bl_trace_grid(h->sm_count), sb);
+        } else {
+            BundleDesc d;
+            build_bundle(*cam, col0, ncols, row0 + r, rows, 0, out_offset + begin, d);
+            RT_CUDA(h, cudaMemcpyAsync(dd, &d, sizeof d, cudaMemcpyHostToDevice, sb));
+            TraceArgs args{};
+            args.bundles = reinterpret_cast<const BundleDesc*>(dd);
+            args.n_bundles = 1;
+            args.refill_threshold = c.refill_threshold;
+            args.claim = 32u * c.rays_per_thread;
+            args.total_rays = count;
+            args.queue = q;
+            args.stats = static_cast<unsigned long long*>(h->stats.ptr);
+            args.out = out;
+            launch_trace(args, static_cast<uint32_t>(h->sm_count) * c.ctas_per_sm, c.block_size, mixed,
+                         c.fp64_rolled != 0, sb);
+        }
+        RT_CUDA(h, cudaGetLastError());
+        if (prev_stream) RT_CUDA(h, static_cast<cudaError_t>(band_copy_hook(&ctx, prev_begin, prev_count, prev_stream)));
+        prev_begin = begin;
+        prev_count = count;
+        prev_stream = sb;
+    }
+    if (prev_stream) RT_CUDA(h, static_cast<cudaError_t>(band_copy_hook(&ctx, prev_begin, prev_count, prev_stream)));
+    RT_CUDA(h, cudaEventRecord(h->ev_join, s2));
+    RT_CUDA(h, cudaStreamWaitEvent(s, h->ev_join, 0));
     RT_CUDA(h, cudaEventRecord(h->ev1, s));
     h->timed = true;
     return RT_OK;
@@ -615,6 +705,8 @@ void rt_destroy(rt_handle* h) {
     release(h->ms_desc);
     release(h->ms_sources);
     release(h->bl_desc);
+    release(h->band_desc);
+    release(h->band_queue);
     release(h->shade_desc);
     release(h->park_d);
     release(h->park_u);

@@ -137,3 +137,36 @@ def test_repeat_dispatch_is_deterministic(tracer):
     b = tracer.dispatch(cam)
     for f in ("status", "r", "theta", "phi", "r_hit", "g", "lambda", "steps_accepted"):
         np.testing.assert_array_equal(a[f], b[f])
+
+
+@pytest.mark.parametrize("form", ["kerr_schild_fp64", "boyer_lindquist"])
+def test_banded_single_kernel_host_dispatch(tracer, form):
+    """A host dispatch of 2^20 rays and more on a single-kernel tracer (plain
+    FP64 Kerr-Schild, Boyer-Lindquist) runs as eight row bands on two streams,
+    each band's shading and copies overlapping the next band's launch; records
+    and shaded pixels equal a one-launch device dispatch bit for bit."""
+    import torch
+
+    kw = dict(spin=0.9, r_obs=50.0, incl_deg=75.0, fov_deg=30.0, width=1024, height=1024)
+    if form == "boyer_lindquist":
+        kw.update(metric_form=relsim.METRIC_BOYER_LINDQUIST, charge=0.3)
+    cam = relsim.make_camera(**kw)
+    fields = ["status", "steps_accepted", "r", "theta", "phi", "r_hit", "g"]
+    tracer.set_launch_config()
+    tracer.set_shading(relsim.shading(tonemapping_mode=1))
+    try:
+        host = tracer.dispatch(cam, fields=fields, pixels=True)
+        n = 1024 * 1024
+        ro, dev = relsim.device_ray_out(n, fields)
+        pix = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+        tracer.dispatch_device(cam, ro, pix.data_ptr(), n)
+        tracer.synchronize()
+    finally:
+        tracer.set_shading(None)
+    for f in fields:
+        d = dev[f].cpu().numpy()
+        if f in ("status", "steps_accepted"):
+            d = d.view(np.uint32)
+        np.testing.assert_array_equal(host[f], d)
+    np.testing.assert_array_equal(host["pixels"], pix.cpu().numpy().view(relsim.PIXEL_DTYPE))
+    assert np.bincount(host["status"], minlength=4)[3] > 100000
