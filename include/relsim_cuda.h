@@ -386,6 +386,12 @@ rt_status rt_server_poll(rt_server* s, rt_request_done* done, uint32_t max_done,
                          double timeout_ms);
 rt_status rt_server_get_stats(rt_server* s, rt_server_stats* stats);
 const char* rt_server_last_error(const rt_server* s);
+/* Shade the pixels of requests that finish from now on (single-hole cameras of
+ * both metric forms; multi-source requests keep r = g = b = 0), as
+ * rt_set_shading does for a handle; NULL turns it off.  The server's
+ * record_mask must hold status, phi, r_hit, g and the pixels, else
+ * RT_ERR_INVALID_ARG. */
+rt_status rt_server_set_shading(rt_server* s, const rt_shading* shading);
 
 /* Allocation-free bundle trace.  No counterpart in the reference: its compute
  * executor always owns its device buffers and grows them on demand.

@@ -41,6 +41,9 @@ using Clock = std::chrono::steady_clock;
 constexpr int kFields = 14;                                          // rt_ray_out fields
 constexpr size_t kFieldBytes[kFields] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
 constexpr uint32_t kPixelBit = 1u << 14;                             // record_mask bit of the pixels
+constexpr uint32_t kShadeSlots = 64;                                  // ring of per-request shading constants
+// record_mask bits the shading pass needs: status, phi, r_hit, g and the pixels
+constexpr uint32_t kShadeMask = (1u << 0) | (1u << 6) | (1u << 7) | (1u << 8) | kPixelBit;
 constexpr int kSlots = 2;                                            // epochs in flight
 
 // First-fit allocator over ray slots [0, capacity) of the output arena.
@@ -167,6 +170,11 @@ struct rt_server {
     std::thread worker;
     size_t rr = 0;       // round-robin start in `active`
     int last_kind = -1;  // kind of the last epoch launched
+    // pixel shading of finished single-hole requests (rt_server_set_shading)
+    bool shade_on = false;
+    rt_shading shading{};
+    ShadeDesc* dev_shade = nullptr;  // ring of per-request shading constants, used in copy-stream order
+    uint32_t shade_next = 0;
 };
 
 namespace {
@@ -220,9 +228,27 @@ void admit(rt_server* s) {
     }
 }
 
-// Copy a finished request's records to the caller's host buffers (lock held).
+// Copy a finished request's records to the caller's host buffers (lock held);
+// with shading on, a single-hole request's pixels are shaded first, on the
+// copy stream.
 bool start_copy(rt_server* s, Request* r) {
     cudaStream_t cs = s->copy_stream;
+    if (s->shade_on && r->n_sources == 0 && r->host_pixels) {
+        ShadeDesc d;
+        if (build_shade_desc(r->cam, s->shading, d)) {
+            ShadeDesc* slot = s->dev_shade + (s->shade_next++ % kShadeSlots);
+            // pageable descriptor: the copy is staged before the call returns; the ring slot
+            // is next written kShadeSlots requests later, after this kernel in stream order
+            cudaError_t e = cudaMemcpyAsync(slot, &d, sizeof d, cudaMemcpyHostToDevice, cs);
+            if (e != cudaSuccess) return fail_server(s, "cudaMemcpyAsync", e), false;
+            const uint64_t b = r->base;
+            launch_shade(slot, static_cast<const uint32_t*>(s->field_base[0]) + b,
+                         static_cast<const double*>(s->field_base[7]) + b, static_cast<const double*>(s->field_base[6]) + b,
+                         static_cast<const double*>(s->field_base[8]) + b, s->pixel_base + b, r->rays, cs);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return fail_server(s, "shade launch", e), false;
+        }
+    }
     void* const* hp = reinterpret_cast<void* const*>(&r->host_rays);
     for (int f = 0; f < kFields; ++f) {
         if (!hp[f]) continue;
@@ -590,6 +616,7 @@ void rt_server_destroy(rt_server* s) {
         delete r;
     }
     if (s->arena) cudaFree(s->arena);
+    if (s->dev_shade) cudaFree(s->dev_shade);
     delete s;
 }
 
@@ -697,5 +724,29 @@ rt_status rt_server_get_stats(rt_server* s, rt_server_stats* out) {
 }
 
 const char* rt_server_last_error(const rt_server* s) { return s ? s->error.c_str() : "null server"; }
+
+rt_status rt_server_set_shading(rt_server* s, const rt_shading* sh) {
+    if (!s) return RT_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!sh) {
+        s->shade_on = false;
+        return RT_OK;
+    }
+    rt_camera probe;
+    rt_camera_defaults(&probe);
+    ShadeDesc d;
+    if (!build_shade_desc(probe, *sh, d) || (s->cfg.record_mask & kShadeMask) != kShadeMask) return RT_ERR_INVALID_ARG;
+    if (!s->dev_shade) {
+        cudaSetDevice(s->device);
+        if (cudaMalloc(&s->dev_shade, sizeof(ShadeDesc) * kShadeSlots) != cudaSuccess) {
+            cudaGetLastError();
+            s->dev_shade = nullptr;
+            return RT_ERR_OOM;
+        }
+    }
+    s->shading = *sh;
+    s->shade_on = true;
+    return RT_OK;
+}
 
 }  // extern "C"

@@ -145,7 +145,7 @@ EXPORTS = ["rt_create", "rt_destroy", "rt_is_ready", "rt_is_platform_supported",
            "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc", "rt_kerr_isco_radius", "rt_dispatch_multi", "rt_dispatch_multi_device",
            "rt_server_config_defaults", "rt_server_create", "rt_server_destroy", "rt_server_submit",
            "rt_server_poll", "rt_server_get_stats", "rt_server_last_error", "rt_server_submit_multi",
-           "rt_shading_defaults", "rt_set_shading"]
+           "rt_shading_defaults", "rt_set_shading", "rt_server_set_shading"]
 NOALLOC_MAX_BUNDLES = 32  # RT_NOALLOC_MAX_BUNDLES
 
 
@@ -177,6 +177,7 @@ def lib() -> ctypes.CDLL:
         L.rt_shading_defaults.argtypes = [p(Shading)]
         L.rt_shading_defaults.restype = None
         L.rt_set_shading.argtypes = [v, p(Shading)]
+        L.rt_server_set_shading.argtypes = [v, p(Shading)]
         L.rt_get_launch_config.argtypes = [v, p(LaunchConfig)]
         L.rt_get_stats.argtypes = [v, p(Stats)]
         L.rt_synchronize.argtypes = [v, _d]
@@ -509,6 +510,12 @@ class Server:
         for d in done:
             self._keep.pop(d.id, None)
         return done
+
+    def set_shading(self, shading: "Shading | None") -> None:
+        """Shade the pixels of requests that finish from now on (None: colour off)."""
+        st = self.lib.rt_server_set_shading(self._h, ctypes.byref(shading) if shading is not None else None)
+        if st != RT_OK:
+            raise RelsimError(st, "rt_server_set_shading")
 
     def stats(self) -> ServerStats:
         s = ServerStats()

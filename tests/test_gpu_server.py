@@ -145,3 +145,37 @@ def test_multi_source_request_matches_direct_trace(tracer):
     ref = tracer.dispatch_multi(cam, srcs, fields=list(FIELDS), pixels=False)
     for k in FIELDS:
         assert same(out_a[k], ref[k]), k
+
+
+def test_shaded_requests_match_shaded_dispatch(tracer):
+    """With rt_server_set_shading, a finished single-hole request's pixels are
+    shaded (disk colour, tonemapping) exactly as a shaded rt_dispatch of the same
+    camera; a multi-source request keeps black pixels; a server that does not
+    record the fields the shading reads refuses it."""
+    sh = relsim.shading(tonemapping_mode=1, hydro_model=1)
+    cams = [config_cam("c2", width=128, height=96, precision=relsim.PRECISION_MIXED),
+            relsim.make_camera(spin=0.9, r_obs=50.0, incl_deg=75.0, fov_deg=30.0, width=96, height=64,
+                               metric_form=relsim.METRIC_BOYER_LINDQUIST, charge=0.3)]
+    tracer.set_launch_config()
+    tracer.set_shading(sh)
+    try:
+        ref = [tracer.dispatch(c, fields=list(FIELDS), pixels=True) for c in cams]
+    finally:
+        tracer.set_shading(None)
+    req = [r for r in scenes.request_stream() if r.multi_source][0]
+    mcam = req.bundle.camera(relsim.PRECISION_FP64)
+    mcam.screen_width = mcam.screen_height = 32
+    with _server() as srv:
+        srv.set_shading(sh)
+        subs = [srv.submit(c, FIELDS, pixels=True) for c in cams]
+        mid, mout = srv.submit(mcam, FIELDS, pixels=True, sources=scenes.rt_sources(req.sources))
+        done = srv.wait([i for i, _ in subs] + [mid])
+    for (rid, out), r in zip(subs, ref):
+        assert done[rid].status == relsim.RT_OK
+        assert np.array_equal(out["pixels"], r["pixels"])
+        assert out["pixels"]["r"].max() > 0.0
+    assert done[mid].status == relsim.RT_OK
+    assert np.all(mout["pixels"]["r"] == 0.0) and np.all(mout["pixels"]["a"] == 1.0)
+    with relsim.Server(0, relsim.server_config(1 << 26, record=("status", "pixels"))) as bare:
+        with pytest.raises(relsim.RelsimError):
+            bare.set_shading(sh)
