@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define RT_ABI_VERSION 2
+#define RT_ABI_VERSION 3
 
 typedef enum rt_status {
     RT_OK = 0,
@@ -339,12 +339,17 @@ typedef struct rt_server rt_server;
 typedef struct rt_server_config {
     uint64_t memory_budget_bytes;  /* device bytes for in-flight output records (admission budget) */
     uint32_t max_requests;         /* waiting + admitted requests; more: RT_ERR_AGAIN */
-    uint32_t chunk_rays;           /* rays a request contributes to one epoch (whole rows, >= 1 row) */
-    uint32_t epoch_rays;           /* rays per epoch launch */
+    uint32_t chunk_rays;           /* cost units a request contributes to one epoch (whole rows) */
+    uint32_t epoch_rays;           /* cost units per epoch launch; also its ray capacity.  A ray costs
+                                      1 unit (mixed Kerr-Schild), 2 (FP64), 4 (Boyer-Lindquist) or
+                                      5 per hole (multi-source); an epoch's first chunk takes at least
+                                      one row */
     uint32_t max_epoch_bundles;    /* row chunks per epoch launch */
     uint32_t record_mask;          /* bit f: rt_ray_out field f (declaration order) is recorded;
                                       bit 14: the 32-byte pixels */
-    uint32_t reserved;
+    uint32_t min_epoch_rays;       /* an epoch keeps taking rows up to this many rays even past its
+                                      cost units (keeps a launch of slow rays long enough to fill
+                                      the GPU); capped at epoch_rays */
     rt_launch_config launch_fp64;  /* launch shapes; zeros select the defaults */
     rt_launch_config launch_mixed;
 } rt_server_config;
@@ -365,17 +370,19 @@ typedef struct rt_server_stats {
     uint64_t budget_bytes;                     /* usable budget (whole rays) */
     uint32_t pending;                          /* waiting + admitted, not yet polled as done */
     uint32_t peak_active;                      /* most requests admitted at once */
+    uint64_t peak_epoch_rays;                  /* most rays in one epoch launch (<= epoch_rays) */
 } rt_server_stats;
 
-/* Defaults: 1 GiB budget, 4096 requests, 2^18-ray chunks, 2^22-ray epochs,
- * records status, r, theta, phi, r_hit, g and the pixels. */
+/* Defaults: 1 GiB budget, 4096 requests, 2^18-unit chunks, 2^22-unit epochs of at
+ * least 2^18 rays, records status, r, theta, phi, r_hit, g and the pixels. */
 void rt_server_config_defaults(rt_server_config* cfg);
 rt_status rt_server_create(rt_server** out, int device_ordinal, const rt_server_config* cfg);
 /* Stops the scheduler; requests not yet done are dropped. */
 void rt_server_destroy(rt_server* s);
 /* Queue one request.  Host buffers (pinned memory overlaps best) must stay valid
  * until the request is polled as done and may only name recorded fields.
- * RT_ERR_AGAIN: max_requests reached; RT_ERR_BUDGET: larger than the whole budget. */
+ * RT_ERR_AGAIN: max_requests reached; RT_ERR_BUDGET: larger than the whole budget;
+ * RT_ERR_INVALID_ARG also for a row wider than epoch_rays. */
 rt_status rt_server_submit(rt_server* s, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
                            size_t capacity, uint64_t* id);
 /* Queue a multi-source scene (see rt_dispatch_multi; traced in FP64). */

@@ -117,6 +117,18 @@ struct Request {
         if (cam.metric_form == RT_METRIC_BOYER_LINDQUIST) return 3;
         return static_cast<int>(cam.precision_mode);
     }
+    // GPU time of one ray in units of a mixed-precision Kerr-Schild ray (measured
+    // on B200: mixed 194 Mrays/s, FP64 105, Boyer-Lindquist 47, multi-source about
+    // 39 / holes); epochs are budgeted in these units so that an epoch of slow
+    // rays does not hold the GPU much longer than one of fast rays
+    uint64_t cost() const {
+        switch (kind()) {
+            case 2: return 5ull * n_sources;
+            case 3: return 4;
+            case RT_PRECISION_MIXED: return 1;
+            default: return 2;
+        }
+    }
 };
 
 struct Chunk {
@@ -289,20 +301,34 @@ bool launch_epoch(rt_server* s, Slot& slot) {
     uint32_t n_src = 0;               // sources copied into this epoch's table
     std::vector<std::pair<Request*, uint32_t>> src_at;  // request -> its first source in the table
     slot.chunks.clear();
-    uint64_t total = 0;
+    // An epoch holds at most epoch_rays rays (the slot's buffers) and takes rows
+    // while its cost stays within epoch_rays units or it holds fewer than
+    // min_epoch_rays rays; round robin over active requests, each taking about
+    // chunk_rays units (at least one row) per turn.
+    uint64_t total = 0;  // rays of the epoch
+    uint64_t units = 0;  // their cost in mixed-ray units
     uint32_t nb = 0;
+    const uint64_t epoch = s->cfg.epoch_rays;
+    const uint64_t min_rays = std::min<uint64_t>(s->cfg.min_epoch_rays, epoch);
     const size_t n_active = s->active.size();
-    // round robin over active requests: each gets up to chunk_rays per epoch
+    auto open = [&] { return total < epoch && (units < epoch || total < min_rays) && nb < s->cfg.max_epoch_bundles; };
     bool progress = true;
-    while (progress && total < s->cfg.epoch_rays && nb < s->cfg.max_epoch_bundles) {
+    while (progress && open()) {
         progress = false;
-        for (size_t k = 0; k < n_active && total < s->cfg.epoch_rays && nb < s->cfg.max_epoch_bundles; ++k) {
+        for (size_t k = 0; k < n_active && open(); ++k) {
             Request* r = s->active[(s->rr + k) % n_active];
             if (r->state != ReqState::Active || r->rows_issued >= r->nrows) continue;
             if (r->kind() != kind) continue;
-            const uint64_t budget = std::min<uint64_t>(s->cfg.chunk_rays, s->cfg.epoch_rays - total);
-            uint32_t rows = static_cast<uint32_t>(std::max<uint64_t>(1, budget / r->width));
-            rows = std::min(rows, r->nrows - r->rows_issued);
+            const uint64_t w = r->cost();
+            const uint64_t by_units = (units < epoch) ? (epoch - units) / w : 0;
+            const uint64_t by_floor = (total < min_rays) ? min_rays - total : 0;
+            const uint64_t room = std::min<uint64_t>(std::max(by_units, by_floor), epoch - total);
+            uint64_t fit = std::min<uint64_t>(std::max<uint64_t>(1, s->cfg.chunk_rays / w / r->width), room / r->width);
+            // a row that does not fit: only as the epoch's first chunk (submit
+            // guarantees width <= epoch_rays, so its rays fit the buffers)
+            if (fit == 0 && nb == 0) fit = 1;
+            if (fit == 0) continue;
+            const uint32_t rows = static_cast<uint32_t>(std::min<uint64_t>(fit, r->nrows - r->rows_issued));
             const uint64_t n = static_cast<uint64_t>(rows) * r->width;
             if (multi) {
                 uint32_t begin = UINT32_MAX;
@@ -330,6 +356,7 @@ bool launch_epoch(rt_server* s, Slot& slot) {
             r->rows_issued += rows;
             slot.chunks.push_back({r, n});
             total += n;
+            units += n * w;
             ++nb;
             progress = true;
         }
@@ -410,6 +437,7 @@ bool launch_epoch(rt_server* s, Slot& slot) {
     slot.busy = true;
     ++s->stats.epochs;
     s->stats.bundles += nb;
+    s->stats.peak_epoch_rays = std::max<uint64_t>(s->stats.peak_epoch_rays, total);
     return true;
 }
 
@@ -501,6 +529,7 @@ void rt_server_config_defaults(rt_server_config* c) {
     c->max_requests = 4096;
     c->chunk_rays = 1u << 18;
     c->epoch_rays = 1u << 22;
+    c->min_epoch_rays = 1u << 18;
     c->max_epoch_bundles = 4096;
     // class, final position, disk radius and g, plus the 32-byte pixels
     c->record_mask = (1u << 0) | (1u << 4) | (1u << 5) | (1u << 6) | (1u << 7) | (1u << 8) | kPixelBit;
@@ -652,6 +681,7 @@ rt_status submit_request(rt_server* s, const rt_camera* cam, const rt_source* sr
     const uint64_t n = static_cast<uint64_t>(cam->screen_width) * nrows;
     if (n == 0 || capacity < n) return RT_ERR_INVALID_ARG;
     if (n > s->arena_rays) return RT_ERR_BUDGET;  // could never be admitted
+    if (cam->screen_width > s->cfg.epoch_rays) return RT_ERR_INVALID_ARG;  // a row must fit one epoch
     Request* r = new (std::nothrow) Request();
     if (!r) return RT_ERR_OOM;
     r->cam = *cam;

@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     // warp-uniform claim state: rays [chunk_next, chunk_end) belong to this warp
     bool queue_open = true;
     uint64_t chunk_next = 0, chunk_end = 0;
-    unsigned long long n_att = 0, n_acc = 0, n_rays = 0, n_rhs = 0, n_far = 0;
+    uint32_t n_att = 0, n_acc = 0, n_rays = 0, n_rhs = 0, n_far = 0;
 
     for (;;) {
         if constexpr (PASS != PASS_SINGLE) {
@@ -1088,20 +1088,21 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
         h = -clampd(ah, 1e-8, 1e13);
     }
 
-    // warp-reduced counters
+    // warp-reduced counters (per-lane counts fit 32 bits; the sums are 64-bit)
+    unsigned long long w_att = n_att, w_acc = n_acc, w_rays = n_rays, w_rhs = n_rhs, w_far = n_far;
     for (int off = 16; off > 0; off >>= 1) {
-        n_att += __shfl_down_sync(FULL, n_att, off);
-        n_acc += __shfl_down_sync(FULL, n_acc, off);
-        n_rays += __shfl_down_sync(FULL, n_rays, off);
-        n_rhs += __shfl_down_sync(FULL, n_rhs, off);
-        n_far += __shfl_down_sync(FULL, n_far, off);
+        w_att += __shfl_down_sync(FULL, w_att, off);
+        w_acc += __shfl_down_sync(FULL, w_acc, off);
+        w_rays += __shfl_down_sync(FULL, w_rays, off);
+        w_rhs += __shfl_down_sync(FULL, w_rhs, off);
+        w_far += __shfl_down_sync(FULL, w_far, off);
     }
     if (lane == 0) {
-        atomicAdd(args.stats + ST_RAYS, n_rays);
-        atomicAdd(args.stats + ST_ATTEMPTS, n_att);
-        atomicAdd(args.stats + ST_ACCEPTED, n_acc);
-        atomicAdd(args.stats + ST_RHS, n_rhs);
-        atomicAdd(args.stats + ST_FP64_ATTEMPTS, n_att - n_far);
+        atomicAdd(args.stats + ST_RAYS, w_rays);
+        atomicAdd(args.stats + ST_ATTEMPTS, w_att);
+        atomicAdd(args.stats + ST_ACCEPTED, w_acc);
+        atomicAdd(args.stats + ST_RHS, w_rhs);
+        atomicAdd(args.stats + ST_FP64_ATTEMPTS, w_att - w_far);
     }
 }
 

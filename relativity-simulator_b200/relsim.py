@@ -115,7 +115,7 @@ def make_source(position, mass: float = 1.0, spin_parameter: float = 0.0, axis=(
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("memory_budget_bytes", ctypes.c_uint64), ("max_requests", _u32), ("chunk_rays", _u32),
-                ("epoch_rays", _u32), ("max_epoch_bundles", _u32), ("record_mask", _u32), ("reserved", _u32),
+                ("epoch_rays", _u32), ("max_epoch_bundles", _u32), ("record_mask", _u32), ("min_epoch_rays", _u32),
                 ("launch_fp64", LaunchConfig), ("launch_mixed", LaunchConfig)]
 
 
@@ -128,7 +128,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("requests_submitted", ctypes.c_uint64), ("requests_done", ctypes.c_uint64),
                 ("rays_done", ctypes.c_uint64), ("epochs", ctypes.c_uint64), ("bundles", ctypes.c_uint64),
                 ("bytes_in_use", ctypes.c_uint64), ("peak_bytes_in_use", ctypes.c_uint64),
-                ("budget_bytes", ctypes.c_uint64), ("pending", _u32), ("peak_active", _u32)]
+                ("budget_bytes", ctypes.c_uint64), ("pending", _u32), ("peak_active", _u32),
+                ("peak_epoch_rays", ctypes.c_uint64)]
 
 
 # record_mask bits: rt_ray_out fields in declaration order, then the pixels

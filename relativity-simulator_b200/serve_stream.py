@@ -73,9 +73,11 @@ def replay(server: relsim.Server, reqs: list[scenes.Request], precision: int, sp
     rays = sum(d.rays for _, d in done)
     bad = [d.status for _, d in done if d.status != 0]
     lat_m = np.array([d.latency_ms for r, d in done if r.multi_source])
+    lat_s = np.array([d.latency_ms for r, d in done if not r.multi_source])
+    q = (lambda x, p: float(np.percentile(x, p)) if x.size else None)
     return {"served": len(done), "multi_source": multi, "failed": len(bad), "rays": int(rays),
-            "multi_source_latency_ms_p50": float(np.percentile(lat_m, 50)) if lat_m.size else None,
-            "multi_source_latency_ms_p99": float(np.percentile(lat_m, 99)) if lat_m.size else None,
+            "single_source_latency_ms_p50": q(lat_s, 50), "single_source_latency_ms_p99": q(lat_s, 99),
+            "multi_source_latency_ms_p50": q(lat_m, 50), "multi_source_latency_ms_p99": q(lat_m, 99),
             "wall_s": wall, "mrays_per_s": rays / wall / 1e6,
             "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
             "latency_ms_max": float(lat.max()), "queue_ms_p50": float(np.percentile(queue, 50)),
@@ -122,6 +124,8 @@ def main() -> None:
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--check-requests", type=int, default=16)
     ap.add_argument("--speed", type=float, default=1.0, help="arrival-rate multiplier")
+    ap.add_argument("--epoch-units", type=int, default=0, help="rt_server_config.epoch_rays (0: default)")
+    ap.add_argument("--min-epoch-rays", type=int, default=-1, help="rt_server_config.min_epoch_rays (-1: default)")
     a = ap.parse_args()
     reqs = scenes.request_stream(a.requests)
     prec = relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64
@@ -130,6 +134,10 @@ def main() -> None:
     from autotune import load_tuned
 
     cfg = relsim.server_config(int(a.budget_gb * (1 << 30)), record=FIELDS)
+    if a.epoch_units > 0:
+        cfg.epoch_rays = a.epoch_units
+    if a.min_epoch_rays >= 0:
+        cfg.min_epoch_rays = a.min_epoch_rays
     tuned = load_tuned()
     for prec_name, field in (("fp64", "launch_fp64"), ("mixed", "launch_mixed")):
         t = tuned.get(prec_name)
@@ -144,7 +152,9 @@ def main() -> None:
     res.update({"workload": f"{a.requests} requests, Poisson {200 * a.speed:g}/s, seed 1, cameras as the "
                             f"512-bundle table draws; {a.precision} precision",
                 "budget_bytes": int(st.budget_bytes), "peak_bytes_in_use": int(st.peak_bytes_in_use),
-                "peak_active": int(st.peak_active), "epochs": int(st.epochs), "chunks": int(st.bundles)})
+                "peak_active": int(st.peak_active), "epochs": int(st.epochs), "chunks": int(st.bundles),
+                "epoch_units": int(cfg.epoch_rays), "min_epoch_rays": int(cfg.min_epoch_rays),
+                "peak_epoch_rays": int(st.peak_epoch_rays)})
     print(json.dumps(res))
 
 

@@ -179,3 +179,43 @@ def test_shaded_requests_match_shaded_dispatch(tracer):
     with relsim.Server(0, relsim.server_config(1 << 26, record=("status", "pixels"))) as bare:
         with pytest.raises(relsim.RelsimError):
             bare.set_shading(sh)
+
+
+def test_epochs_budgeted_by_cost(tracer):
+    """Epochs are budgeted in cost units (a mixed ray 1, FP64 2, Boyer-Lindquist
+    4, multi-source 5 per hole), fill up to min_epoch_rays rays past that
+    budget, and never hold more rays than epoch_rays, even when a row does not
+    fit the room left (it waits for the next epoch); a row wider than an epoch
+    is refused."""
+    tracer.set_launch_config()
+    cams = [config_cam("c2", width=96, height=40, precision=relsim.PRECISION_MIXED),
+            config_cam("c2", width=100, height=30, precision=relsim.PRECISION_MIXED),
+            config_cam("c3", width=70, height=20)]
+    with _server(epoch_rays=1000, chunk_rays=1000) as srv:
+        subs = [srv.submit(c, FIELDS) for c in cams]
+        got = srv.wait([rid for rid, _ in subs])
+        st = srv.stats()
+        with pytest.raises(relsim.RelsimError) as e:
+            srv.submit(config_cam("c2", width=1001, height=2), FIELDS)
+        assert e.value.status == 1  # INVALID_ARG
+    assert all(d.status == relsim.RT_OK for d in got.values())
+    assert 0 < st.peak_epoch_rays <= 1000
+    for cam, (rid, out) in zip(cams, subs):
+        ref = tracer.dispatch(cam, fields=list(FIELDS), pixels=False)
+        for k in FIELDS:
+            assert same(out[k], ref[k]), k
+    # a 4-hole scene costs 20 units a ray: 4096-unit epochs take 3 rows of 64
+    req = [r for r in scenes.request_stream() if r.multi_source and len(r.sources) == 3][0]
+    cam = req.bundle.camera(relsim.PRECISION_FP64)
+    cam.screen_width = cam.screen_height = 64
+    srcs = scenes.rt_sources(req.sources)
+    ref = tracer.dispatch_multi(cam, srcs, fields=list(FIELDS), pixels=False)
+    for floor, peak, epochs in ((1, 3 * 64, 22), (4096, 4096, 1)):
+        with _server(epoch_rays=4096, chunk_rays=4096, min_epoch_rays=floor) as srv:
+            rid, out = srv.submit(cam, FIELDS, sources=srcs)
+            got = srv.wait([rid])
+            st = srv.stats()
+        assert got[rid].status == relsim.RT_OK
+        assert (st.peak_epoch_rays, st.epochs) == (peak, epochs), floor
+        for k in FIELDS:
+            assert same(out[k], ref[k]), k
