@@ -905,23 +905,10 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
             continue;
         }
 
-        // error norm (rk45_adaptive.hpp:254-261); kA holds k7.  FP64 in the FP64
-        // mode; FP32 in the mixed mode, whose estimate carries FP32 stages
+        // error norm (rk45_adaptive.hpp:254-261) in FP64 in every mode (in the
+        // far pass on the FP32 stages' estimate); kA holds k7
         double err;
-        if constexpr (MIXED) {
-            float num = 0.0f, den = 1.0f;
-            const float rtol = static_cast<float>(Bp->rtol), atol = static_cast<float>(Bp->atol);
-#pragma unroll
-            for (int i = 0; i < 6; ++i) {
-                const float sc = rtol * static_cast<float>(fmax(fabs(y[i]), fabs(y5[i]))) + atol;
-                const float e = static_cast<float>(est[i]);
-                if (e * den > num * sc) {
-                    num = e;
-                    den = sc;
-                }
-            }
-            err = static_cast<double>(num / den);
-        } else {
+        {
             double num = 0.0, den = 1.0;
             const double rtol = Bp->rtol, atol = Bp->atol;
 #pragma unroll
