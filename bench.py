@@ -17,9 +17,11 @@ value: Mrays/s of the mixed tracer (the fp64 one with --precision fp64) with
        stream, L2 flushed between steps (a 256 MiB write); "precisions" holds
        both tracers' numbers and "mixed_vs_fp64" their ratio.
 e2e:   Mrays/s through rt_dispatch (the dispatch_and_readback-shaped C call)
-       with pinned host buffers, host<->device copies inside the timed region,
-       pixels shaded (disk colour and tonemapping, rt_set_shading defaults);
-       its per-image p50/p99 wall latency.
+       into pinned host pixels (32-byte GpuPixelOutput, what the reference's
+       call returns), host<->device copies inside the timed region, pixels
+       shaded (disk colour and tonemapping, rt_set_shading defaults); its
+       per-image p50/p99 wall latency.  e2e.with_records: the same call that
+       also copies back the per-ray records (class, r, theta, phi, r_hit, g).
 N > 1: one independent image per GPU (replicas, no collective); value is the
        total over ranks divided by the slowest rank's time.
 """
@@ -65,30 +67,75 @@ def headline_camera(relsim, precision: int, side: int = SIDE):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock, power and clock-event reasons sampled through NVML every 10 ms
+    during the timed region (read-only queries; nvidia-smi at 200 ms when the
+    NVML bindings are missing)."""
 
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu: int):
         self.gpu = gpu
+        self.rows = []  # (sm_mhz, max_mhz, power_w, util_pct, reason_bits)
+        self.stop = None
+        self.thread = None
         self.proc = None
         self.path = None
 
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.gpu)
+        for get in (lambda: pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(p.uuid)),
+                    lambda: pynvml.nvmlDeviceGetHandleByPciBusId(
+                        f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"),
+                    lambda: pynvml.nvmlDeviceGetHandleByIndex(self.gpu)):
+            try:
+                return pynvml, get()
+            except Exception:
+                continue
+        raise RuntimeError("no NVML handle")
+
+    def _poll(self, nv, h):
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx,
+                                  nv.nvmlDeviceGetPowerUsage(h) / 1e3, nv.nvmlDeviceGetUtilizationRates(h).gpu,
+                                  nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception:
+                break
+            self.stop.wait(0.01)
+
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
+
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
-        time.sleep(0.3)
+            nv, h = self._nvml_handle()
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.thread.start()
+        except Exception:
+            self.thread = None
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                     "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            except OSError:
+                self.proc = None
+            time.sleep(0.3)
         return self
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -96,31 +143,34 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self) -> dict:
+    def _smi_rows(self):
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return float("nan")
+
         rows = []
         try:
             with open(self.path) as f:
                 for line in f:
                     parts = [p.strip() for p in line.split(",")]
                     if len(parts) >= 10:
-                        rows.append(parts)
-        except OSError:
+                        bits = sum(b for i, b in enumerate(self.REASONS.values()) if parts[6 + i].lower() == "active")
+                        rows.append((num(parts[1]), num(parts[2]), num(parts[3]), num(parts[4]), bits))
+        except (OSError, TypeError):
             pass
+        return rows
+
+    def summary(self) -> dict:
+        rows = self.rows if self.thread is not None else self._smi_rows()
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
-
-        def num(s):
-            try:
-                return float(s)
-            except ValueError:
-                return float("nan")
-
-        load = [r for r in rows if num(r[4]) > 50] or rows
-        sm = [num(r[1]) for r in load]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in load for i in range(4) if r[6 + i].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": num(load[0][2]), "reasons": reasons,
-                "samples": len(load), "power_w_max": max(num(r[3]) for r in load)}
+        load = [r for r in rows if r[3] > 50] or rows
+        reasons = sorted({name for r in load for name, bit in self.REASONS.items() if int(r[4]) & bit})
+        return {"sm_mhz": float(np.median([r[0] for r in load])), "sm_max_mhz": float(load[0][1]),
+                "reasons": reasons, "samples": len(load), "power_w_max": float(max(r[2] for r in load)),
+                "source": "NVML, 10 ms" if self.thread is not None else "nvidia-smi, 200 ms"}
 
 
 def dist_env():
@@ -244,13 +294,14 @@ def time_device(tr, relsim, cam, n, ro, pix, flush, steps: int, warmup: int) -> 
     return {"ms": ms, "attempts": attempts, "accepted": accepted, "rhs": rhs, "fp64_attempts": fp64_att}
 
 
-def time_e2e(tr, relsim, cam, n, steps: int, warmup: int):
+def time_e2e(tr, relsim, cam, n, steps: int, warmup: int, fields=()):
     """Trace and shade through rt_dispatch (host buffers, copies inside), as the
-    reference's dispatch_and_readback returns coloured pixels; per-image wall latency."""
+    reference's dispatch_and_readback returns coloured pixels (32-byte
+    GpuPixelOutput), plus the per-ray record fields asked for; per-image wall latency."""
     import torch
 
     host = {f: torch.empty(n, dtype=(torch.int32 if f == "status" else torch.float64), pin_memory=True)
-            for f in RECORD_FIELDS}
+            for f in fields}
     hpix = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
     hro = relsim.RayOut()
     for f, t in host.items():
@@ -261,7 +312,8 @@ def time_e2e(tr, relsim, cam, n, steps: int, warmup: int):
     try:
         for i in range(warmup + steps):
             t0 = time.perf_counter()
-            st = L.rt_dispatch(tr.handle, ctypes.byref(cam), hpix.data_ptr(), ctypes.byref(hro), n, None)
+            st = L.rt_dispatch(tr.handle, ctypes.byref(cam), hpix.data_ptr(), ctypes.byref(hro) if fields else None,
+                               n, None)
             dt = time.perf_counter() - t0
             if st != 0:
                 raise RuntimeError(L.rt_last_error(tr.handle).decode())
@@ -270,6 +322,10 @@ def time_e2e(tr, relsim, cam, n, steps: int, warmup: int):
     finally:
         tr.set_shading(None)
     return host, lat
+
+
+def record_bytes(fields) -> int:
+    return sum(4 if f == "status" else 8 for f in fields)
 
 
 def time_bundles(tr, relsim, steps: int, warmup: int, device: str) -> dict:
@@ -318,6 +374,8 @@ def time_boyer_lindquist(tr, relsim, side, ro, pix, flush, steps, warmup, fp64_p
     total_ms = max_over_ranks(own_ms, ws, device)
     _, lat = time_e2e(tr, relsim, cam, n, steps, warmup)
     e2e_wall = max_over_ranks(sum(lat), ws, device)
+    _, lat_rec = time_e2e(tr, relsim, cam, n, steps, warmup, RECORD_FIELDS)
+    rec_wall = max_over_ranks(sum(lat_rec), ws, device)
     achieved = d["attempts"] * BL_FLOP_PER_ATTEMPT / (own_ms * 1e-3) / 1e12
     return {
         "workload": f"Kerr-Newman a=0.9 Q=0.3 {side}^2 pinhole r=50 M i=75 deg FOV 30 deg, disk [r_isco, 20 M]; "
@@ -327,9 +385,10 @@ def time_boyer_lindquist(tr, relsim, side, ro, pix, flush, steps, warmup, fp64_p
         "latency_ms": {"kernel_p50": float(np.percentile(d["ms"], 50)), "kernel_p99": float(np.percentile(d["ms"], 99)),
                        "e2e_p50": 1e3 * float(np.percentile(lat, 50)), "e2e_p99": 1e3 * float(np.percentile(lat, 99))},
         "e2e": {"value": replica_value(n, ws, steps, e2e_wall * 1e3), "unit": "Mrays/s",
-                "h2d_bytes_per_step": BL_H2D_BYTES_PER_IMAGE + SHADE_H2D_BYTES,
-                "d2h_bytes_per_step": n * (32 + 4 + 8 * (len(RECORD_FIELDS) - 1)),
-                "pixels": "shaded (disk colour + tonemapping, sky off)"},
+                "h2d_bytes_per_step": BL_H2D_BYTES_PER_IMAGE + SHADE_H2D_BYTES, "d2h_bytes_per_step": n * 32,
+                "pixels": "shaded (disk colour + tonemapping, sky off)",
+                "with_records": {"value": replica_value(n, ws, steps, rec_wall * 1e3), "fields": RECORD_FIELDS,
+                                 "d2h_bytes_per_step": n * (32 + record_bytes(RECORD_FIELDS))}},
         "roofline": {"bound": "fp64 pipe", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak, "flop_per_attempt": BL_FLOP_PER_ATTEMPT,
                      "peak_source": "measured in this run: register FMA-chain kernel (rt_measure_fma_peak)",
@@ -446,10 +505,16 @@ def ours(args) -> None:
     # end to end through rt_dispatch (host buffers) for the headline precision
     hcam = res[headline]["cam"]
     apply_tuned(tr, headline)
-    host, lat = time_e2e(tr, relsim, hcam, n, args.steps, args.warmup)
+    _, lat = time_e2e(tr, relsim, hcam, n, args.steps, args.warmup)
     e2e_wall = max_over_ranks(sum(lat), ws, f"cuda:{local}")
     e2e_value = replica_value(n, ws, args.steps, e2e_wall * 1e3)
-    d2h = n * (32 + 4 + 8 * (len(RECORD_FIELDS) - 1))
+    d2h = n * 32
+    _, lat_rec = time_e2e(tr, relsim, hcam, n, args.steps, args.warmup, RECORD_FIELDS)
+    rec_wall = max_over_ranks(sum(lat_rec), ws, f"cuda:{local}")
+    e2e_records = {"value": replica_value(n, ws, args.steps, rec_wall * 1e3), "fields": RECORD_FIELDS,
+                   "d2h_bytes_per_step": n * (32 + record_bytes(RECORD_FIELDS)),
+                   "latency_ms_p50": 1e3 * float(np.percentile(lat_rec, 50)),
+                   "latency_ms_p99": 1e3 * float(np.percentile(lat_rec, 99))}
 
     batched = None
     if not args.no_bundles:
@@ -515,8 +580,10 @@ def ours(args) -> None:
             "roofline": h["roofline"],
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": H2D_BYTES_PER_IMAGE + SHADE_H2D_BYTES,
                     "d2h_bytes_per_step": d2h, "pixels": "shaded (disk colour + tonemapping, sky off)",
+                    "call": "rt_dispatch into the 32-byte pixels, as dispatch_and_readback returns them",
                     "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
-                    "latency_ms_p99": 1e3 * float(np.percentile(lat, 99))},
+                    "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)),
+                    "with_records": e2e_records},
             "gpu_launches": args.steps,
             "clocks": clocks,
             "fma_peak_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
