@@ -69,6 +69,36 @@ def test_mixed_c3_fullsize_sample(tracer):
     _check(tracer, "c3", 4096, pixels=pix)
 
 
+def test_mixed_c3_full_image_vs_fp64(tracer):
+    """Every ray of the 4096^2 a = 0.998 image, mixed tracer against the FP64
+    tracer (which the parity tests hold to the FP64 oracle): rays whose class
+    differs lie in the 1e-6 M boundary band (checked by the oracle on those
+    rays); disk-hit radius and g within 1e-6 at the 99th percentile, at most
+    0.1 % of disk rays above 1e-6 in radius (near-critical rays, which amplify
+    any step difference), none above 1e-3."""
+    fields = ["status", "r_hit", "g"]
+    tracer.set_launch_config()
+    ref = tracer.dispatch(config_cam("c3", width=4096, height=4096), fields=fields, pixels=False)
+    out = tracer.dispatch(config_cam("c3", width=4096, height=4096, precision=relsim.PRECISION_MIXED), fields=fields,
+                          pixels=False)
+    diff = np.flatnonzero(out["status"] != ref["status"])
+    if diff.size:
+        cam = config_cam("c3", width=4096, height=4096)
+        orc = O.trace(relsim.camera_dict(cam), pixels=diff.astype(np.uint64))
+        r_in = O.lib().orc_isco_radius(1.0, cam.metric_spin)
+        band = O.boundary_band(orc, r_in, cam.disk_outer_radius, 1e-6)
+        assert band.all(), f"{(~band).sum()} of {diff.size} class differences outside the band"
+    both = (out["status"] == O.DISK) & (ref["status"] == O.DISK)
+    rel = np.abs(out["r_hit"][both] - ref["r_hit"][both]) / ref["r_hit"][both]
+    relg = np.abs(out["g"][both] - ref["g"][both]) / ref["g"][both]
+    over = int((rel > 1e-6).sum())
+    print(f"c3 4096^2: {diff.size} class differences (all in the band), {both.sum()} disk rays, r_hit rel max "
+          f"{rel.max():.2e} p99 {np.percentile(rel, 99):.2e} p99.9 {np.percentile(rel, 99.9):.2e} ({over} over 1e-6), "
+          f"g rel max {relg.max():.2e} p99 {np.percentile(relg, 99):.2e}")
+    assert np.percentile(rel, 99) < 1e-6 and np.percentile(relg, 99) < 1e-6
+    assert over <= 1e-3 * both.sum() and rel.max() < 1e-3 and relg.max() < 1e-3
+
+
 def test_mixed_is_deterministic(tracer):
     """With whole-warp refills each warp traces an aligned batch of 32 rays, so
     the warp-uniform precision choice (and every result) repeats bitwise."""
