@@ -5,7 +5,7 @@
  * cites the reference file:line it restates; paths are relative to the
  * Wartets/Relativity-Simulator source tree.
  *
- * Integration scheme ("north-star FP64 DP45", composed from reference parts):
+ * Integration scheme (FP64 DP45, composed from reference parts):
  *   state y = (x, y, z, p_x, p_y, p_z) in Kerr-Schild Cartesian coordinates with
  *   p_t = -1, integrated backwards (h < 0) with Dormand-Prince 5(4),
  *   PI30 control, FSAL reuse of the last stage, a constraint projection onto
