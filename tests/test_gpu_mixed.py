@@ -13,6 +13,8 @@ FP32 stages contribute ~ eps_32 x (deflection after the stage) x (path length)
 to the final position, so the rays that reach the innermost disk carry the
 largest errors, and rays near the photon ring amplify any step difference.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -112,11 +114,12 @@ def test_mixed_is_deterministic(tracer):
 
 
 def test_banded_host_dispatch_equals_device_dispatch(tracer):
-    """A host dispatch of 2^20 rays and more on the two-pass tracer runs in four
+    """A host dispatch of 2^20 rays and more on the two-pass tracer runs in eight
     sub-bands on two streams, each band's shading and copies overlapping the
     next band's trace; its records and (shaded) pixels equal a device dispatch
     of the whole window in one band, bit for bit, and a windowed host dispatch
-    below the banding size."""
+    below the banding size.  A host dispatch into the pixels alone (the shading
+    reads the record fields from the handle's scratch) gives the same pixels."""
     import torch
 
     cam = config_cam("c2", width=1024, height=1024, precision=relsim.PRECISION_MIXED)
@@ -133,6 +136,9 @@ def test_banded_host_dispatch_equals_device_dispatch(tracer):
         small = config_cam("c2", width=1024, height=1024, precision=relsim.PRECISION_MIXED, row_offset=300,
                            row_count=100)
         part = tracer.dispatch(small, fields=fields, pixels=True)
+        only = tracer.dispatch(cam, fields=[], pixels=True)["pixels"]
+        bare = np.empty(n, dtype=relsim.PIXEL_DTYPE)  # no record struct at all
+        assert tracer.lib.rt_dispatch(tracer._h, ctypes.byref(cam), bare.ctypes.data, None, n, None) == relsim.RT_OK
     finally:
         tracer.set_shading(None)
     for f in fields:
@@ -143,5 +149,7 @@ def test_banded_host_dispatch_equals_device_dispatch(tracer):
         np.testing.assert_array_equal(part[f], host[f][300 * 1024:400 * 1024])
     dp = pix.cpu().numpy().view(relsim.PIXEL_DTYPE)
     np.testing.assert_array_equal(host["pixels"], dp)
+    np.testing.assert_array_equal(only, dp)
+    np.testing.assert_array_equal(bare, dp)
     np.testing.assert_array_equal(part["pixels"], host["pixels"][300 * 1024:400 * 1024])
     assert host["pixels"]["r"].max() > 0.0
