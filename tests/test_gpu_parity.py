@@ -8,6 +8,8 @@ Ulp-level differences (FMA contraction, device vs host libm) grow only along
 near-critical rays; rays that orbit the photon region are excluded from the
 1e-9 position check by |d_b| > 1e-3 M (they stay in the class check).
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -144,7 +146,8 @@ def test_banded_single_kernel_host_dispatch(tracer, form):
     """A host dispatch of 2^20 rays and more on a single-kernel tracer (plain
     FP64 Kerr-Schild, Boyer-Lindquist) runs as eight row bands on two streams,
     each band's shading and copies overlapping the next band's launch; records
-    and shaded pixels equal a one-launch device dispatch bit for bit."""
+    and shaded pixels equal a one-launch device dispatch bit for bit, also when
+    the host asks for the pixels alone (no record struct)."""
     import torch
 
     kw = dict(spin=0.9, r_obs=50.0, incl_deg=75.0, fov_deg=30.0, width=1024, height=1024)
@@ -161,6 +164,8 @@ def test_banded_single_kernel_host_dispatch(tracer, form):
         pix = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
         tracer.dispatch_device(cam, ro, pix.data_ptr(), n)
         tracer.synchronize()
+        bare = np.empty(n, dtype=relsim.PIXEL_DTYPE)
+        assert tracer.lib.rt_dispatch(tracer._h, ctypes.byref(cam), bare.ctypes.data, None, n, None) == relsim.RT_OK
     finally:
         tracer.set_shading(None)
     for f in fields:
@@ -169,4 +174,5 @@ def test_banded_single_kernel_host_dispatch(tracer, form):
             d = d.view(np.uint32)
         np.testing.assert_array_equal(host[f], d)
     np.testing.assert_array_equal(host["pixels"], pix.cpu().numpy().view(relsim.PIXEL_DTYPE))
+    np.testing.assert_array_equal(bare, host["pixels"])
     assert np.bincount(host["status"], minlength=4)[3] > 100000
