@@ -11,7 +11,8 @@
   - parameters at their clamps (spin beyond 0.999 M, an observer inside
     1.02 r_+, a negative spin), which both sides clamp the same way;
   - the largest image of this suite, 8192^2 = 67 M rays in one mixed-precision
-    device dispatch: every ray classified, a sample within the mixed bars.
+    device dispatch: every ray classified, a sample within the mixed bars;
+  - empty images are refused (INVALID_ARG) by the handle and by the server.
 """
 import numpy as np
 import pytest
@@ -86,3 +87,16 @@ def test_largest_image_mixed(tracer):
     both = (s == O.DISK) & (ref["status"] == O.DISK)
     assert np.max(np.abs(r_hit[both] - ref["r_hit"][both]) / ref["r_hit"][both]) < 1e-6
     assert np.max(np.abs(g[both] - ref["g"][both]) / ref["g"][both]) < 1e-6
+
+
+def test_empty_images_are_refused(tracer):
+    for w, h in ((0, 16), (16, 0)):
+        cam = config_cam("c2", width=w, height=h)
+        with pytest.raises(relsim.RelsimError) as e:
+            tracer.dispatch(cam, fields=["status"], pixels=True)
+        assert e.value.status == 1  # INVALID_ARG
+        with relsim.Server(0, relsim.server_config(1 << 24, record=("status",))) as srv:
+            with pytest.raises(relsim.RelsimError) as e:
+                srv.submit(cam, ("status",))
+            assert e.value.status == 1
+    assert tracer.is_ready()
