@@ -5,7 +5,10 @@
 // persistent tracer launch over a bundle table of row chunks taken round-robin
 // from every admitted request with rows left, so a request that arrives while
 // others are on the GPU joins the next epoch instead of waiting for them to
-// finish.  Two epoch slots on separate streams keep the GPU busy while the
+// finish.  An epoch traces one kind of request (Kerr-Schild FP64 or mixed,
+// multi-source, Boyer-Lindquist) and is sized by the rays' cost, so that a
+// launch of slow rays does not hold back requests of other kinds for long.
+// Two epoch slots on separate streams keep the GPU busy while the
 // scheduler retires one epoch and builds the next (the tail of one launch
 // overlaps the start of the other).  Output records stay on the device, in a
 // budget-sized arena, until a request's last chunk is done; then they are copied
