@@ -16,6 +16,9 @@ value: Mrays/s of the mixed tracer (the fp64 one with --precision fp64) with
        outputs resident in HBM, tracer kernel timed with CUDA events on its
        stream, L2 flushed between steps (a 256 MiB write); "precisions" holds
        both tracers' numbers and "mixed_vs_fp64" their ratio.
+serving: the seeded request stream (2000 requests, Poisson 200/s) replayed in
+       real time through the continuous-batching server (N = 1): p50/p99
+       request latency, throughput and the error of sampled requests.
 e2e:   Mrays/s through rt_dispatch (the dispatch_and_readback-shaped C call)
        into pinned host pixels (32-byte GpuPixelOutput, what the reference's
        call returns), host<->device copies inside the timed region, pixels
@@ -560,6 +563,24 @@ def ours(args) -> None:
         out = tr.dispatch(res["mixed"]["cam"], fields=["status", "r_hit", "g"], pixels=False)
         summary["mixed"]["error_vs_fp64"] = error_vs_fp64(out, ref)
 
+    serving = None
+    if ws == 1 and not args.no_serving:
+        import serve_stream
+
+        torch.cuda.empty_cache()  # the server allocates its 120 GB budget arena up front
+        s = serve_stream.run(check_requests=args.serving_check, device=local)
+        err = s.get("error_vs_fp64") or {}
+        serving = {"workload": s["workload"] + "; 10 % multi-source scenes of 2-16 holes (FP64)",
+                   "served": s["served"], "failed": s["failed"], "multi_source": s["multi_source"],
+                   "mrays_per_s": s["mrays_per_s"], "latency_ms_p50": s["latency_ms_p50"],
+                   "latency_ms_p99": s["latency_ms_p99"], "latency_ms_max": s["latency_ms_max"],
+                   "single_source_latency_ms_p50": s["single_source_latency_ms_p50"],
+                   "single_source_latency_ms_p99": s["single_source_latency_ms_p99"],
+                   "multi_source_latency_ms_p50": s["multi_source_latency_ms_p50"],
+                   "multi_source_latency_ms_p99": s["multi_source_latency_ms_p99"],
+                   "budget_bytes": s["budget_bytes"], "epochs": s["epochs"],
+                   "error_vs_fp64": {k: v for k, v in err.items() if k != "per_request"} or None}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_port_baseline(relsim.camera_dict(res[headline]["cam"]), seconds=args.cpu_seconds)
@@ -602,6 +623,8 @@ def ours(args) -> None:
             line["batched_c4"] = batched
         if bl is not None:
             line["boyer_lindquist"] = bl
+        if serving is not None:
+            line["serving"] = serving
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -656,6 +679,9 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-bundles", action="store_true", help="skip the 512-bundle batched measurement")
     ap.add_argument("--no-bl", action="store_true", help="skip the Boyer-Lindquist Kerr-Newman measurement")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream replay (one GPU only)")
+    ap.add_argument("--serving-check", type=int, default=8,
+                    help="single-source stream requests compared ray by ray with the FP64 tracer")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

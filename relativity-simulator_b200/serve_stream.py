@@ -117,6 +117,43 @@ def request_error(kept: dict, device: int = 0) -> dict:
             "reference": "FP64 CUDA tracer, rtol 1e-10", "per_request": per}
 
 
+def run(requests: int = 2000, budget_gb: float = 120.0, precision: str = "mixed", check_requests: int = 16,
+        speed: float = 1.0, epoch_units: int = 0, min_epoch_rays: int = -1, device: int = 0) -> dict:
+    """Replay the seeded stream through a server on `device` (library defaults
+    for the epoch sizes unless given, autotuned launch shapes) and return the
+    measurements; `check_requests` single-source requests are compared with
+    the FP64 tracer afterwards."""
+    reqs = scenes.request_stream(requests)
+    prec = relsim.PRECISION_MIXED if precision == "mixed" else relsim.PRECISION_FP64
+    single = [r.index for r in reqs if not r.multi_source]
+    keep = set(np.random.default_rng(2).choice(single, min(check_requests, len(single)), replace=False).tolist())
+    from autotune import load_tuned
+
+    cfg = relsim.server_config(int(budget_gb * (1 << 30)), record=FIELDS)
+    if epoch_units > 0:
+        cfg.epoch_rays = epoch_units
+    if min_epoch_rays >= 0:
+        cfg.min_epoch_rays = min_epoch_rays
+    tuned = load_tuned()
+    for prec_name, field in (("fp64", "launch_fp64"), ("mixed", "launch_mixed")):
+        t = tuned.get(prec_name)
+        if t:
+            setattr(cfg, field, relsim.LaunchConfig(t["block_size"], t["ctas_per_sm"], t["refill_threshold"],
+                                                    t.get("rays_per_thread", 0), t.get("fp64_rolled", 0)))
+    with relsim.Server(device, cfg) as srv:
+        res = replay(srv, reqs, prec, speed, keep)
+        st = srv.stats()
+    kept = res.pop("kept")
+    res["error_vs_fp64"] = request_error(kept, device) if kept else None
+    res.update({"workload": f"{requests} requests, Poisson {200 * speed:g}/s, seed 1, cameras as the "
+                            f"512-bundle table draws; {precision} precision",
+                "budget_bytes": int(st.budget_bytes), "peak_bytes_in_use": int(st.peak_bytes_in_use),
+                "peak_active": int(st.peak_active), "epochs": int(st.epochs), "chunks": int(st.bundles),
+                "epoch_units": int(cfg.epoch_rays), "min_epoch_rays": int(cfg.min_epoch_rays),
+                "peak_epoch_rays": int(st.peak_epoch_rays)})
+    return res
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=2000)
@@ -127,35 +164,8 @@ def main() -> None:
     ap.add_argument("--epoch-units", type=int, default=0, help="rt_server_config.epoch_rays (0: default)")
     ap.add_argument("--min-epoch-rays", type=int, default=-1, help="rt_server_config.min_epoch_rays (-1: default)")
     a = ap.parse_args()
-    reqs = scenes.request_stream(a.requests)
-    prec = relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64
-    single = [r.index for r in reqs if not r.multi_source]
-    keep = set(np.random.default_rng(2).choice(single, min(a.check_requests, len(single)), replace=False).tolist())
-    from autotune import load_tuned
-
-    cfg = relsim.server_config(int(a.budget_gb * (1 << 30)), record=FIELDS)
-    if a.epoch_units > 0:
-        cfg.epoch_rays = a.epoch_units
-    if a.min_epoch_rays >= 0:
-        cfg.min_epoch_rays = a.min_epoch_rays
-    tuned = load_tuned()
-    for prec_name, field in (("fp64", "launch_fp64"), ("mixed", "launch_mixed")):
-        t = tuned.get(prec_name)
-        if t:
-            setattr(cfg, field, relsim.LaunchConfig(t["block_size"], t["ctas_per_sm"], t["refill_threshold"],
-                                                    t.get("rays_per_thread", 0), t.get("fp64_rolled", 0)))
-    with relsim.Server(0, cfg) as srv:
-        res = replay(srv, reqs, prec, a.speed, keep)
-        st = srv.stats()
-    kept = res.pop("kept")
-    res["error_vs_fp64"] = request_error(kept) if kept else None
-    res.update({"workload": f"{a.requests} requests, Poisson {200 * a.speed:g}/s, seed 1, cameras as the "
-                            f"512-bundle table draws; {a.precision} precision",
-                "budget_bytes": int(st.budget_bytes), "peak_bytes_in_use": int(st.peak_bytes_in_use),
-                "peak_active": int(st.peak_active), "epochs": int(st.epochs), "chunks": int(st.bundles),
-                "epoch_units": int(cfg.epoch_rays), "min_epoch_rays": int(cfg.min_epoch_rays),
-                "peak_epoch_rays": int(st.peak_epoch_rays)})
-    print(json.dumps(res))
+    print(json.dumps(run(a.requests, a.budget_gb, a.precision, a.check_requests, a.speed, a.epoch_units,
+                         a.min_epoch_rays)))
 
 
 if __name__ == "__main__":
