@@ -12,7 +12,9 @@
     1.02 r_+, a negative spin), which both sides clamp the same way;
   - the largest image of this suite, 8192^2 = 67 M rays in one mixed-precision
     device dispatch: every ray classified, a sample within the mixed bars;
-  - empty images are refused (INVALID_ARG) by the handle and by the server.
+  - empty images are refused (INVALID_ARG) by the handle and by the server;
+  - a host wait with a wall-clock limit returns TIMEOUT while work runs and the
+    handle stays usable (failure detection without a GPU fault).
 """
 import numpy as np
 import pytest
@@ -100,3 +102,25 @@ def test_empty_images_are_refused(tracer):
                 srv.submit(cam, ("status",))
             assert e.value.status == 1
     assert tracer.is_ready()
+
+
+def test_host_wait_times_out_and_recovers(tracer):
+    """rt_synchronize with a wall-clock limit returns RT_ERR_TIMEOUT while a long
+    trace is still running (the work is not cancelled and the handle stays
+    usable); a wait without a limit then completes, and the records equal a
+    host dispatch of the same camera."""
+    side = 4096
+    n = side * side
+    cam = config_cam("c3", width=side, height=side)
+    tracer.set_launch_config()
+    ro, dev = relsim.device_ray_out(n, ["status", "r_hit"])
+    tracer.dispatch_device(cam, ro, None, n)
+    assert tracer.lib.rt_synchronize(tracer._h, 1.0) == 3  # TIMEOUT: about 0.2 s of work was enqueued
+    assert tracer.is_ready()
+    tracer.synchronize()
+    st = dev["status"].cpu().numpy().view(np.uint32)
+    assert np.all(st != relsim.RAY_UNFINISHED)
+    small = config_cam("c3", width=side, height=side, row_offset=2000, row_count=8)
+    part = tracer.dispatch(small, fields=["status", "r_hit"], pixels=False)
+    np.testing.assert_array_equal(part["status"], st[2000 * side:2008 * side])
+    np.testing.assert_array_equal(part["r_hit"], dev["r_hit"].cpu().numpy()[2000 * side:2008 * side])
