@@ -2,7 +2,7 @@
 
     python relativity-simulator_b200/trace_once.py [--side 512] [--spin 0.94] [--r-obs 100]
         [--incl 17] [--fov 12] [--precision fp64|mixed] [--repeat 1]
-        [--metric ks|bl] [--charge 0]
+        [--metric ks|bl] [--charge 0] [--sources N]
 """
 from __future__ import annotations
 
@@ -38,6 +38,9 @@ def main() -> None:
     ap.add_argument("--metric", choices=["ks", "bl"], default="ks",
                     help="ks: Kerr-Schild Hamiltonian tracer; bl: Boyer-Lindquist Kerr-Newman tracer (FP64)")
     ap.add_argument("--charge", type=float, default=0.0, help="Kerr-Newman charge Q (--metric bl)")
+    ap.add_argument("--sources", type=int, default=0,
+                    help="multi-source scene: the first request of the seeded stream with this many bodies beside "
+                         "the camera's hole (its camera, at --side), traced by the multi-source tracer")
     ap.add_argument("--record", choices=["minimal", "bench"], default="minimal",
                     help="outputs written: class and step counts, or the bench's record (class, r, theta, "
                          "phi, r_hit, g) plus the 32-byte pixels")
@@ -48,17 +51,28 @@ def main() -> None:
                              rtol=a.rtol, mixed_fp64_radius=a.fp64_radius,
                              metric_form=relsim.METRIC_BOYER_LINDQUIST if a.metric == "bl" else relsim.METRIC_KERR_SCHILD,
                              charge=a.charge)
+    srcs = None
+    if a.sources > 0:
+        import scenes
+
+        req = [r for r in scenes.request_stream() if r.multi_source and len(r.sources) == a.sources][0]
+        cam = req.bundle.camera(relsim.PRECISION_FP64)
+        cam.screen_width = cam.screen_height = a.side
+        srcs = scenes.rt_sources(req.sources)
     with relsim.Tracer(0) as tr:
         tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread, a.fp64_rolled, a.mixed_single)
         for _ in range(a.repeat):
-            if a.record == "bench":
+            if srcs is not None:
+                out = tr.dispatch_multi(cam, srcs, fields=["status", "steps_accepted", "steps_rejected"],
+                                        pixels=False)
+            elif a.record == "bench":
                 out = tr.dispatch(cam, fields=["status", "r", "theta", "phi", "r_hit", "g"], pixels=True)
             else:
                 out = tr.dispatch(cam, fields=["status", "steps_accepted", "steps_rejected"], pixels=False)
             s = tr.stats()
     print(json.dumps({"rays": int(s.rays), "attempts": int(s.attempts), "accepted": int(s.accepted),
                       "fp64_attempts": int(s.fp64_attempts), "rhs_evals": int(s.rhs_evals),
-                      "kernel_ms": s.kernel_ms, "mrays_per_s": s.rays / s.kernel_ms / 1e3,
+                      "kernel_ms": s.kernel_ms, "mrays_per_s": s.rays / s.kernel_ms / 1e3 if s.kernel_ms > 0 else None,
                       "classes": np.bincount(out["status"], minlength=4).tolist()}))
 
 
