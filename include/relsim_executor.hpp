@@ -215,6 +215,7 @@ private:
         adv(o.status), adv(o.flags), adv(o.steps_accepted), adv(o.steps_rejected);
         adv(o.r), adv(o.theta), adv(o.phi), adv(o.r_hit), adv(o.g), adv(o.lambda);
         adv(o.dH), adv(o.dE), adv(o.dLz), adv(o.dQ);
+        adv(o.exit_x), adv(o.exit_y), adv(o.exit_z);
         return o;
     }
 

@@ -636,6 +636,7 @@ static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, ui
     out->dLz = (iv[1] - inv0[1]) / E0;
     out->dQ = (iv[2] - inv0[2]) / (E0 * E0);
     out->db_shadow = db0;
+    out->exit_dir[0] = out->exit_dir[1] = out->exit_dir[2] = NAN;
 }
 
 typedef struct {

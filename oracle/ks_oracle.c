@@ -708,6 +708,16 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
     out->dLz = (y[0] * y[4] - y[1] * y[3]) - lz0;
     out->dQ = orc_carter_q(y, m, a) - q0;
     out->db_shadow = db0;
+    /* sky-lookup direction of an escaped ray: minus the normalised dx/dlambda of
+     * the terminal state (software_compute_engine.hpp:1771-1775) */
+    out->exit_dir[0] = out->exit_dir[1] = out->exit_dir[2] = NAN;
+    if (status == ORC_RAY_ESCAPED) {
+        double dy[6];
+        ks_rhs(y, m, a, dy);
+        const double len = sqrt(dy[0] * dy[0] + dy[1] * dy[1] + dy[2] * dy[2]);
+        const double inv = 1.0 / max_d(len, 1e-12);
+        for (int i = 0; i < 3; ++i) out->exit_dir[i] = -dy[i] * inv;
+    }
 }
 
 typedef struct {

@@ -92,6 +92,9 @@ typedef struct orc_ray {
     double dLz;                  /* L_z(end) - L_z(start) */
     double dQ;                   /* Q(end) - Q(start) */
     double db_shadow;            /* signed distance to the critical curve (M) */
+    double exit_dir[3];          /* escaped Kerr-Schild rays: -dx/dlambda / |dx/dlambda| at the
+                                    terminal state (software_compute_engine.hpp:1771-1775); NaN
+                                    otherwise and in the other tracer forms */
 } orc_ray;
 
 /* --- single-function checks (pinned against the reference) --- */

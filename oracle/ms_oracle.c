@@ -588,6 +588,7 @@ static void trace_one(const orc_camera* cam, const orc_ms_table* t, uint32_t px,
     out->dLz = NAN;
     out->dQ = NAN;
     out->db_shadow = NAN;
+    out->exit_dir[0] = out->exit_dir[1] = out->exit_dir[2] = NAN;
 }
 
 typedef struct {

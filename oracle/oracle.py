@@ -49,7 +49,7 @@ CAMERA_DTYPE = np.dtype([
 RAY_DTYPE = np.dtype([
     ("status", "u4"), ("flags", "u4"), ("steps_accepted", "u4"), ("steps_rejected", "u4"),
     ("r", "f8"), ("theta", "f8"), ("phi", "f8"), ("r_hit", "f8"), ("g", "f8"), ("lambda", "f8"),
-    ("dH", "f8"), ("dE", "f8"), ("dLz", "f8"), ("dQ", "f8"), ("db_shadow", "f8"),
+    ("dH", "f8"), ("dE", "f8"), ("dLz", "f8"), ("dQ", "f8"), ("db_shadow", "f8"), ("exit_dir", "f8", (3,)),
 ])
 
 CAPTURED, ESCAPED, DISK, UNFINISHED = 1, 2, 3, 0

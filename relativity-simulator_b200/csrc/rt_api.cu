@@ -53,7 +53,7 @@ struct rt_handle {
     DevBuf shade_desc;                   // pixel shading constants of the last shaded camera
     bool shade_on = false;               // rt_set_shading
     rt_shading shading{};
-    DevBuf ray_fields[14];
+    DevBuf ray_fields[kRayFields];
     DevBuf pixels;
     // pinned staging of the bundle table
     BundleDesc* host_bundles = nullptr;
@@ -247,10 +247,9 @@ rt_status scratch_rays(rt_handle* h, const rt_ray_out* host, size_t n, rt_ray_ou
     if (!host) return RT_OK;
     void* const* hp = reinterpret_cast<void* const*>(host);
     void** dp = reinterpret_cast<void**>(&dev);
-    const size_t elem[14] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
-    for (int f = 0; f < 14; ++f) {
+    for (int f = 0; f < kRayFields; ++f) {
         if (!hp[f]) continue;
-        rt_status st = ensure(h, h->ray_fields[f], n * elem[f]);
+        rt_status st = ensure(h, h->ray_fields[f], n * kRayFieldBytes[f]);
         if (st != RT_OK) return st;
         dp[f] = h->ray_fields[f].ptr;
     }
@@ -262,9 +261,8 @@ rt_status copy_back(rt_handle* h, const rt_ray_out* host, const rt_ray_out& dev,
     if (host) {
         void* const* hp = reinterpret_cast<void* const*>(host);
         void* const* dp = reinterpret_cast<void* const*>(&dev);
-        const size_t elem[14] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
-        for (int f = 0; f < 14; ++f)
-            if (hp[f]) RT_CUDA(h, cudaMemcpyAsync(hp[f], dp[f], n * elem[f], cudaMemcpyDeviceToHost, s));
+        for (int f = 0; f < kRayFields; ++f)
+            if (hp[f]) RT_CUDA(h, cudaMemcpyAsync(hp[f], dp[f], n * kRayFieldBytes[f], cudaMemcpyDeviceToHost, s));
     }
     if (hpix) RT_CUDA(h, cudaMemcpyAsync(hpix, dpix, n * sizeof(rt_pixel_out), cudaMemcpyDeviceToHost, s));
     return RT_OK;
@@ -358,11 +356,11 @@ int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
     if (c.host) {
         void* const* hp = reinterpret_cast<void* const*>(c.host);
         void* const* dp = reinterpret_cast<void* const*>(&c.dev);
-        const size_t elem[14] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
-        for (int f = 0; f < 14; ++f) {
+        for (int f = 0; f < kRayFields; ++f) {
             if (!hp[f]) continue;
-            const cudaError_t e = cudaMemcpyAsync(static_cast<char*>(hp[f]) + o * elem[f],
-                                                  static_cast<const char*>(dp[f]) + o * elem[f], count * elem[f],
+            const size_t b = kRayFieldBytes[f];
+            const cudaError_t e = cudaMemcpyAsync(static_cast<char*>(hp[f]) + o * b,
+                                                  static_cast<const char*>(dp[f]) + o * b, count * b,
                                                   cudaMemcpyDeviceToHost, s);
             if (e != cudaSuccess) return static_cast<int>(e);
         }

@@ -362,6 +362,9 @@ __device__ __noinline__ void bl_finish(const BlDesc* __restrict__ Bp, BlCold<BLO
     if (R.dE) R.dE[o] = E / e0 - 1.0;
     if (R.dLz) R.dLz[o] = (L - S.l0[tid]) / e0;
     if (R.dQ) R.dQ[o] = (Q - S.q0[tid]) / (e0 * e0);
+    if (R.exit_x) R.exit_x[o] = NAN;  // exit directions: Kerr-Schild tracers only
+    if (R.exit_y) R.exit_y[o] = NAN;
+    if (R.exit_z) R.exit_z[o] = NAN;
     if (out.pixels) {
         const uint32_t pflags = (status == RT_RAY_CAPTURED)  ? RT_PIXEL_HORIZON_ABSORBED
                                 : (status == RT_RAY_ESCAPED) ? RT_PIXEL_CELESTIAL_HIT

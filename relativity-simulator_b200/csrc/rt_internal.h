@@ -1,11 +1,18 @@
 // rt_internal.h -- structures shared by the host code and the tracer kernels.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 #include "relsim_cuda.h"
 
 namespace relsim {
+
+// rt_ray_out as an array of pointers: its fields in declaration order and their
+// element sizes
+constexpr int kRayFields = 17;
+constexpr size_t kRayFieldBytes[kRayFields] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
+static_assert(sizeof(rt_ray_out) == kRayFields * sizeof(void*), "rt_ray_out is an array of pointers");
 
 // Bundle flags.
 enum : uint32_t {

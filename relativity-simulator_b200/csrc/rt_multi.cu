@@ -377,6 +377,9 @@ __device__ __noinline__ void ms_finish(const MsDesc* __restrict__ Bp, MsCold<BLO
     if (R.dE) R.dE[o] = NAN;
     if (R.dLz) R.dLz[o] = NAN;
     if (R.dQ) R.dQ[o] = NAN;
+    if (R.exit_x) R.exit_x[o] = NAN;  // exit directions: single-hole Kerr-Schild tracers only
+    if (R.exit_y) R.exit_y[o] = NAN;
+    if (R.exit_z) R.exit_z[o] = NAN;
     if (out.pixels) {
         const uint32_t pflags = (status == RT_RAY_CAPTURED)  ? RT_PIXEL_HORIZON_ABSORBED
                                 : (status == RT_RAY_ESCAPED) ? RT_PIXEL_CELESTIAL_HIT

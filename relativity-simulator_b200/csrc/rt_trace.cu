@@ -248,6 +248,25 @@ __device__ __noinline__ void finish_ray(const BundleDesc* __restrict__ Bp, Cold<
     if (R.dE) R.dE[o] = energy - 1.0;
     if (R.dLz) R.dLz[o] = lz - S.lz0[tid];
     if (R.dQ) R.dQ[o] = q - S.q0[tid];
+    if (R.exit_x) {
+        // sky-lookup direction of an escaped ray: -dx/dlambda at the terminal
+        // state, normalised (software_compute_engine.hpp:1771-1775)
+        double e[3] = {NAN, NAN, NAN};
+        if (status == RT_RAY_ESCAPED) {
+            const double sv = 1.0 + kp;
+            const double v[3] = {y[3] - 2.0 * hf * sv * kf[0], y[4] - 2.0 * hf * sv * kf[1],
+                                 y[5] - 2.0 * hf * sv * kf[2]};
+            const double inv = 1.0 / fmax(sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]), 1e-12);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) e[i] = -v[i] * inv;
+        }
+        R.exit_x[o] = e[0];
+        if (R.exit_y) R.exit_y[o] = e[1];
+        if (R.exit_z) R.exit_z[o] = e[2];
+    } else {
+        if (R.exit_y) R.exit_y[o] = NAN;
+        if (R.exit_z) R.exit_z[o] = NAN;
+    }
     if (out.pixels) {
         // GpuPixelOutput (gpu_types.hpp:1111-1130); shading is not part of this path
         const uint32_t pflags = (status == RT_RAY_CAPTURED)  ? RT_PIXEL_HORIZON_ABSORBED

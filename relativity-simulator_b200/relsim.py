@@ -78,7 +78,8 @@ class PixelOut(ctypes.Structure):
 RAY_FIELDS = [("status", np.uint32), ("flags", np.uint32), ("steps_accepted", np.uint32),
               ("steps_rejected", np.uint32), ("r", np.float64), ("theta", np.float64), ("phi", np.float64),
               ("r_hit", np.float64), ("g", np.float64), ("lambda", np.float64), ("dH", np.float64),
-              ("dE", np.float64), ("dLz", np.float64), ("dQ", np.float64)]
+              ("dE", np.float64), ("dLz", np.float64), ("dQ", np.float64), ("exit_x", np.float64),
+              ("exit_y", np.float64), ("exit_z", np.float64)]
 PIXEL_DTYPE = np.dtype([("r", "f4"), ("g", "f4"), ("b", "f4"), ("a", "f4"), ("redshift", "f4"),
                         ("affine_parameter", "f4"), ("status_flags", "u4"), ("iterations_used", "u4")])
 
