@@ -518,6 +518,8 @@ bool record_fields_ok(const rt_server* s, const rt_ray_out* rays, const rt_pixel
     void* const* hp = reinterpret_cast<void* const*>(rays);
     for (int f = 0; f < kFields; ++f)
         if (hp[f] && !(s->cfg.record_mask & (1u << f))) return false;
+    for (int f = kFields; f < kRayFields; ++f)  // exit directions: not recorded by the server
+        if (hp[f]) return false;
     return true;
 }
 

@@ -219,3 +219,13 @@ def test_epochs_budgeted_by_cost(tracer):
         assert (st.peak_epoch_rays, st.epochs) == (peak, epochs), floor
         for k in FIELDS:
             assert same(out[k], ref[k]), k
+
+
+def test_exit_directions_are_refused():
+    """The server does not record exit directions: a request asking for them is
+    refused rather than left unwritten."""
+    cam = config_cam("c2", width=32, height=32)
+    with _server() as srv:
+        with pytest.raises(relsim.RelsimError) as e:
+            srv.submit(cam, FIELDS + ("exit_x",))
+        assert e.value.status == 1
