@@ -75,3 +75,22 @@ def test_schwarzschild_shadow_edge():
     edge = ang[captured].max()
     expected = np.arcsin(3 * np.sqrt(3) * np.sqrt(1 - 2 / r_obs) / r_obs)
     assert abs(edge - expected) < 0.05 * expected
+
+
+def test_exit_directions_of_escaped_rays():
+    """The oracle's sky-lookup direction of an escaped ray, -dx/dlambda
+    normalised at the escape radius: unit length; the trace steps with h < 0,
+    as the reference's image path does (dt = -|dt|, software_compute_engine.hpp:
+    1683), so at r = 1000 M, where the backward ray moves almost radially
+    outwards, -dx/dlambda is close to r_hat of the terminal point; NaN for rays
+    that did not escape."""
+    cam = config_camera("c1", width=48, height=48, fov_deg=60.0)
+    rays = O.trace(cam)
+    esc = rays["status"] == O.ESCAPED
+    assert esc.sum() > 1000
+    e = rays["exit_dir"][esc]
+    np.testing.assert_allclose(np.linalg.norm(e, axis=1), 1.0, atol=1e-14)
+    th, ph = rays["theta"][esc], rays["phi"][esc]
+    r_hat = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], 1)
+    assert np.min(np.sum(e * r_hat, axis=1)) > 0.99
+    assert np.all(np.isnan(rays["exit_dir"][~esc]))
