@@ -186,11 +186,12 @@ typedef struct rt_ray_out {
     double* dE;      /* -p_t recomputed from the null condition at the end, minus 1 */
     double* dLz;     /* L_z(end) - L_z(start) */
     double* dQ;      /* Carter Q(end) - Q(start) */
-    /* escaped Kerr-Schild rays (KS tracers): unit direction (x, y, z) of travel at
-     * the escape radius, -dx/dlambda / |dx/dlambda| at the terminal state, the
-     * direction the reference's sky lookup takes (software_compute_engine.hpp:
-     * 1771-1775); NaN for other rays and for the Boyer-Lindquist and
-     * multi-source tracers.  Not recorded by the request server. */
+    /* escaped rays: unit Cartesian direction (x, y, z) at the escape radius that
+     * the reference's sky lookup takes: -dx/dlambda / |dx/dlambda| of the
+     * Kerr-Schild state (software_compute_engine.hpp:1771-1775), or the
+     * orthonormal-frame velocity of the Boyer-Lindquist state mapped to a
+     * direction of travel (:1581-1589).  NaN for other rays and for the
+     * multi-source tracer.  Not recorded by the request server. */
     double* exit_x;
     double* exit_y;
     double* exit_z;

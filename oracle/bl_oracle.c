@@ -636,7 +636,30 @@ static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, ui
     out->dLz = (iv[1] - inv0[1]) / E0;
     out->dQ = (iv[2] - inv0[2]) / (E0 * E0);
     out->db_shadow = db0;
+    /* sky-lookup direction of an escaped ray (software_compute_engine.hpp:
+     * 1581-1589 with local_frame_to_travel_direction, :1148-1168): the
+     * orthonormal-frame velocity mapped to a Cartesian direction of travel */
     out->exit_dir[0] = out->exit_dir[1] = out->exit_dir[2] = NAN;
+    if (status == ORC_RAY_ESCAPED) {
+        kn_geom G;
+        kn_geometry(m, a, q2, y[0], y[1], &G);
+        const double* gm = G.g;
+        const double st = sin(y[1]), ct = cos(y[1]), sp = sin(y[2]), cp = cos(y[2]);
+        const double lr = sqrt(fmax(gm[2], 0.0)) * y[4], lt = sqrt(fmax(gm[3], 0.0)) * y[5],
+                     lp = sqrt(fmax(gm[4], 0.0)) * y[6];
+        const double x = -(lr * st * cp + lt * ct * cp - lp * sp);
+        const double yy = -(lr * st * sp + lt * ct * sp + lp * cp);
+        const double z = -(lr * ct - lt * st);
+        const double len = sqrt(x * x + yy * yy + z * z);
+        if (len <= 1e-12) {
+            out->exit_dir[0] = 1.0;
+            out->exit_dir[1] = out->exit_dir[2] = 0.0;
+        } else {
+            out->exit_dir[0] = x / len;
+            out->exit_dir[1] = yy / len;
+            out->exit_dir[2] = z / len;
+        }
+    }
 }
 
 typedef struct {

@@ -92,9 +92,11 @@ typedef struct orc_ray {
     double dLz;                  /* L_z(end) - L_z(start) */
     double dQ;                   /* Q(end) - Q(start) */
     double db_shadow;            /* signed distance to the critical curve (M) */
-    double exit_dir[3];          /* escaped Kerr-Schild rays: -dx/dlambda / |dx/dlambda| at the
-                                    terminal state (software_compute_engine.hpp:1771-1775); NaN
-                                    otherwise and in the other tracer forms */
+    double exit_dir[3];          /* escaped rays: the sky-lookup direction at the terminal state
+                                    (Kerr-Schild: -dx/dlambda normalised, software_compute_engine.hpp:
+                                    1771-1775; Boyer-Lindquist: the local-frame velocity as a
+                                    direction of travel, :1581-1589); NaN otherwise and in the
+                                    multi-source form */
 } orc_ray;
 
 /* --- single-function checks (pinned against the reference) --- */

@@ -362,9 +362,38 @@ __device__ __noinline__ void bl_finish(const BlDesc* __restrict__ Bp, BlCold<BLO
     if (R.dE) R.dE[o] = E / e0 - 1.0;
     if (R.dLz) R.dLz[o] = (L - S.l0[tid]) / e0;
     if (R.dQ) R.dQ[o] = (Q - S.q0[tid]) / (e0 * e0);
-    if (R.exit_x) R.exit_x[o] = NAN;  // exit directions: Kerr-Schild tracers only
-    if (R.exit_y) R.exit_y[o] = NAN;
-    if (R.exit_z) R.exit_z[o] = NAN;
+    if (R.exit_x || R.exit_y || R.exit_z) {
+        // sky-lookup direction of an escaped ray: the orthonormal-frame velocity
+        // (sqrt(g_rr) u^r, sqrt(g_thth) u^th, sqrt(g_phph) u^ph) mapped to a
+        // Cartesian direction of travel (software_compute_engine.hpp:1581-1589,
+        // local_frame_to_travel_direction :1148-1168)
+        double e[3] = {NAN, NAN, NAN};
+        if (status == RT_RAY_ESCAPED) {
+            const double r = y[0], st = sin(y[1]), ct = cos(y[1]), sp = sin(y[2]), cp = cos(y[2]);
+            const double a2 = B.a * B.a, r2a2 = r * r + a2;
+            const double sigma = r * r + a2 * ct * ct;
+            const double delta = r * r - 2.0 * B.m * r + a2 + B.q2;
+            const double g_rr = sigma / delta;
+            const double g_pp = (r2a2 * r2a2 - a2 * delta * st * st) * st * st / sigma;
+            const double lr = sqrt(fmax(g_rr, 0.0)) * y[4], lt = sqrt(fmax(sigma, 0.0)) * y[5],
+                         lp = sqrt(fmax(g_pp, 0.0)) * y[6];
+            const double x = -(lr * st * cp + lt * ct * cp - lp * sp);
+            const double yy = -(lr * st * sp + lt * ct * sp + lp * cp);
+            const double z = -(lr * ct - lt * st);
+            const double len = sqrt(x * x + yy * yy + z * z);
+            if (len <= 1e-12) {
+                e[0] = 1.0;
+                e[1] = e[2] = 0.0;
+            } else {
+                e[0] = x / len;
+                e[1] = yy / len;
+                e[2] = z / len;
+            }
+        }
+        if (R.exit_x) R.exit_x[o] = e[0];
+        if (R.exit_y) R.exit_y[o] = e[1];
+        if (R.exit_z) R.exit_z[o] = e[2];
+    }
     if (out.pixels) {
         const uint32_t pflags = (status == RT_RAY_CAPTURED)  ? RT_PIXEL_HORIZON_ABSORBED
                                 : (status == RT_RAY_ESCAPED) ? RT_PIXEL_CELESTIAL_HIT

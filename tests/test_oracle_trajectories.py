@@ -94,3 +94,17 @@ def test_exit_directions_of_escaped_rays():
     r_hat = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], 1)
     assert np.min(np.sum(e * r_hat, axis=1)) > 0.99
     assert np.all(np.isnan(rays["exit_dir"][~esc]))
+    # the Boyer-Lindquist form (the reference's local-frame formula) points the same way
+    import relsim
+
+    bl = relsim.make_camera(spin=0.9, r_obs=50.0, incl_deg=75.0, fov_deg=60.0, width=24, height=24,
+                            metric_form=relsim.METRIC_BOYER_LINDQUIST, charge=0.3)
+    rays = O.bl_trace(relsim.camera_dict(bl), 0.3)
+    esc = rays["status"] == O.ESCAPED
+    assert esc.sum() > 300
+    e = rays["exit_dir"][esc]
+    np.testing.assert_allclose(np.linalg.norm(e, axis=1), 1.0, atol=1e-14)
+    th, ph = rays["theta"][esc], rays["phi"][esc]
+    r_hat = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], 1)
+    assert np.min(np.sum(e * r_hat, axis=1)) > 0.99
+    assert np.all(np.isnan(rays["exit_dir"][~esc]))
