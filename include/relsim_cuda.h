@@ -188,10 +188,10 @@ typedef struct rt_ray_out {
     double* dQ;      /* Carter Q(end) - Q(start) */
     /* escaped rays: unit Cartesian direction (x, y, z) at the escape radius that
      * the reference's sky lookup takes: -dx/dlambda / |dx/dlambda| of the
-     * Kerr-Schild state (software_compute_engine.hpp:1771-1775), or the
-     * orthonormal-frame velocity of the Boyer-Lindquist state mapped to a
-     * direction of travel (:1581-1589).  NaN for other rays and for the
-     * multi-source tracer.  Not recorded by the request server. */
+     * Kerr-Schild state (software_compute_engine.hpp:1771-1775; the superposed
+     * flow for multi-source scenes, :3220-3224), or the orthonormal-frame
+     * velocity of the Boyer-Lindquist state mapped to a direction of travel
+     * (:1581-1589).  NaN for other rays.  Not recorded by the request server. */
     double* exit_x;
     double* exit_y;
     double* exit_z;

@@ -94,9 +94,9 @@ typedef struct orc_ray {
     double db_shadow;            /* signed distance to the critical curve (M) */
     double exit_dir[3];          /* escaped rays: the sky-lookup direction at the terminal state
                                     (Kerr-Schild: -dx/dlambda normalised, software_compute_engine.hpp:
-                                    1771-1775; Boyer-Lindquist: the local-frame velocity as a
-                                    direction of travel, :1581-1589); NaN otherwise and in the
-                                    multi-source form */
+                                    1771-1775; multi-source: the superposed flow, :3220-3224;
+                                    Boyer-Lindquist: the local-frame velocity as a direction of
+                                    travel, :1581-1589); NaN otherwise */
 } orc_ray;
 
 /* --- single-function checks (pinned against the reference) --- */

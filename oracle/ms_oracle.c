@@ -588,7 +588,21 @@ static void trace_one(const orc_camera* cam, const orc_ms_table* t, uint32_t px,
     out->dLz = NAN;
     out->dQ = NAN;
     out->db_shadow = NAN;
+    /* sky-lookup direction of an escaped ray: minus the normalised flow of the
+     * superposed RHS at the terminal state, (0, 0, -1) where it vanishes
+     * (software_compute_engine.hpp:3220-3224) */
     out->exit_dir[0] = out->exit_dir[1] = out->exit_dir[2] = NAN;
+    if (status == ORC_RAY_ESCAPED) {
+        double dy[6];
+        orc_ms_rhs(t, y, dy);
+        const double len = sqrt(dy[0] * dy[0] + dy[1] * dy[1] + dy[2] * dy[2]);
+        if (len > 1e-12) {
+            for (int i = 0; i < 3; ++i) out->exit_dir[i] = -dy[i] / len;
+        } else {
+            out->exit_dir[0] = out->exit_dir[1] = 0.0;
+            out->exit_dir[2] = -1.0;
+        }
+    }
 }
 
 typedef struct {

@@ -356,7 +356,8 @@ __device__ __noinline__ void ms_init_ray(const MsDesc* __restrict__ Bp, const Ms
 }
 
 template <int BLOCK>
-__device__ __noinline__ void ms_finish(const MsDesc* __restrict__ Bp, MsCold<BLOCK>& S, int tid, const double* y,
+__device__ __noinline__ void ms_finish(const MsDesc* __restrict__ Bp, const MsSource* __restrict__ src,
+                                       MsCold<BLOCK>& S, int tid, const double* y,
                                        uint32_t status, uint32_t flags, uint32_t acc, uint32_t rej, double r_hit,
                                        double g, const OutPtrs& out) {
     const double r = sqrt(dot3(y, y));
@@ -377,9 +378,28 @@ __device__ __noinline__ void ms_finish(const MsDesc* __restrict__ Bp, MsCold<BLO
     if (R.dE) R.dE[o] = NAN;
     if (R.dLz) R.dLz[o] = NAN;
     if (R.dQ) R.dQ[o] = NAN;
-    if (R.exit_x) R.exit_x[o] = NAN;  // exit directions: single-hole Kerr-Schild tracers only
-    if (R.exit_y) R.exit_y[o] = NAN;
-    if (R.exit_z) R.exit_z[o] = NAN;
+    if (R.exit_x || R.exit_y || R.exit_z) {
+        // sky-lookup direction of an escaped ray: minus the normalised flow of the
+        // superposed RHS at the terminal state, (0, 0, -1) where it vanishes
+        // (software_compute_engine.hpp:3220-3224)
+        double e[3] = {NAN, NAN, NAN};
+        if (status == RT_RAY_ESCAPED) {
+            double dy[6];
+            int ins;
+            ms_rhs(src, Bp->src_count, y, dy, Bp->capture_scale, ins);
+            const double len = sqrt(dot3(dy, dy));
+            if (len > 1e-12) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) e[i] = -dy[i] / len;
+            } else {
+                e[0] = e[1] = 0.0;
+                e[2] = -1.0;
+            }
+        }
+        if (R.exit_x) R.exit_x[o] = e[0];
+        if (R.exit_y) R.exit_y[o] = e[1];
+        if (R.exit_z) R.exit_z[o] = e[2];
+    }
     if (out.pixels) {
         const uint32_t pflags = (status == RT_RAY_CAPTURED)  ? RT_PIXEL_HORIZON_ABSORBED
                                 : (status == RT_RAY_ESCAPED) ? RT_PIXEL_CELESTIAL_HIT
@@ -513,7 +533,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
             }
         }
         if (term) {
-            ms_finish<BLOCK>(Bp, S, tid, y, term & 15u, flags, acc, rej, NAN, 1.0, args.out);
+            ms_finish<BLOCK>(Bp, src, S, tid, y, term & 15u, flags, acc, rej, NAN, 1.0, args.out);
             mode = MS_IDLE;
             continue;
         }
@@ -552,7 +572,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
 #pragma unroll
         for (int i = 0; i < 6; ++i) finite = finite && isfinite(y5[i]);
         if (!finite) {
-            ms_finish<BLOCK>(Bp, S, tid, y, RT_RAY_CAPTURED, flags | RT_RAYFLAG_NONFINITE, acc, rej, NAN, 1.0,
+            ms_finish<BLOCK>(Bp, src, S, tid, y, RT_RAY_CAPTURED, flags | RT_RAYFLAG_NONFINITE, acc, rej, NAN, 1.0,
                              args.out);
             mode = MS_IDLE;
             continue;
@@ -603,7 +623,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
                 ms_unwrap(ph, yr);
                 S.phi[tid] = ph;
                 const MsSource& s = src[best_i];
-                ms_finish<BLOCK>(Bp, S, tid, yr, RT_RAY_DISK, flags, acc, rej, best_r,
+                ms_finish<BLOCK>(Bp, src, S, tid, yr, RT_RAY_DISK, flags, acc, rej, best_r,
                                  disk_redshift(s.m, s.a, best_r, best_lz), args.out);
                 mode = MS_IDLE;
                 continue;
@@ -614,7 +634,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
             double ph = S.phi[tid];
             ms_unwrap(ph, y5);
             S.phi[tid] = ph;
-            ms_finish<BLOCK>(Bp, S, tid, y5, RT_RAY_CAPTURED, flags, acc, rej, NAN, 1.0, args.out);
+            ms_finish<BLOCK>(Bp, src, S, tid, y5, RT_RAY_CAPTURED, flags, acc, rej, NAN, 1.0, args.out);
             mode = MS_IDLE;
             continue;
         }
@@ -626,7 +646,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
             double ph = S.phi[tid];
             ms_unwrap(ph, yt);
             S.phi[tid] = ph;
-            ms_finish<BLOCK>(Bp, S, tid, yt, RT_RAY_ESCAPED, flags, acc, rej, NAN, 1.0, args.out);
+            ms_finish<BLOCK>(Bp, src, S, tid, yt, RT_RAY_ESCAPED, flags, acc, rej, NAN, 1.0, args.out);
             mode = MS_IDLE;
             continue;
         }

@@ -31,7 +31,8 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-FIELDS = ["status", "flags", "steps_accepted", "steps_rejected", "r", "theta", "phi", "r_hit", "g", "lambda"]
+FIELDS = ["status", "flags", "steps_accepted", "steps_rejected", "r", "theta", "phi", "r_hit", "g", "lambda",
+          "exit_x", "exit_y", "exit_z"]
 
 
 def _oracle_sources(srcs):
@@ -67,6 +68,12 @@ def _compare(tracer, cam, srcs):
         rel = np.abs(out[f][disk] - ref[f][disk]) / ref[f][disk]
         assert share_within(rel, 1e-9) >= 0.995, (f, share_within(rel, 1e-9))
         assert share_within(rel, 1e-6) >= 0.999, (f, share_within(rel, 1e-6))
+    # sky-lookup directions of escaped rays (the superposed flow), same bars
+    esc = same & (rst == O.ESCAPED)
+    e = np.stack([out["exit_x"], out["exit_y"], out["exit_z"]], 1)
+    de = np.max(np.abs(e[esc] - ref["exit_dir"][esc]), axis=1) if esc.any() else np.zeros(0)
+    assert share_within(de, 1e-9) >= 0.995 and share_within(de, 1e-6) >= 0.999
+    assert np.all(np.isnan(e[st != O.ESCAPED]))
     assert np.all(out["status"] != relsim.RAY_UNFINISHED)
     return out, ref
 
