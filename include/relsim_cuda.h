@@ -430,7 +430,11 @@ rt_status rt_server_set_shading(rt_server* s, const rt_shading* shading);
  * every ray of the table is written.
  *
  * The first call on a device does its set-up (scratch address lookup, kernel
- * loading); make it before any stream capture that is to contain this call.
+ * loading).  The call cannot be captured into a CUDA graph: it uploads the
+ * bundle table from its own stack frame, which a replay could not read again,
+ * so on a stream that is capturing it returns RT_ERR_INVALID_ARG before
+ * enqueuing anything (the capture stays valid).  The caller's current device
+ * is restored before the call returns.
  * Calls that overlap in time on one device share the one scratch array and
  * race: serialise them (one stream, or events between streams).
  *

@@ -1028,6 +1028,14 @@ struct NoAllocDevice {
     int sm_count = 0;
 };
 
+// Puts the caller's current device back when the entry point returns.
+struct DeviceRestore {
+    int prev = -1;
+    ~DeviceRestore() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 std::mutex g_noalloc_mutex;
 NoAllocDevice g_noalloc_devices[kNoAllocMaxDevices];
 
@@ -1117,7 +1125,19 @@ extern "C" rt_status rt_trace_bundles_noalloc(int device_ordinal, const rt_camer
     if (e != cudaSuccess) return noalloc_cuda_fail(error, error_len, e, "cudaGetDeviceCount");
     if (device_ordinal < 0 || device_ordinal >= n_dev || device_ordinal >= kNoAllocMaxDevices)
         return noalloc_fail(error, error_len, RT_ERR_DEVICE, "no such device");
+    // the caller's current device is put back on every return path
+    DeviceRestore restore;
+    if ((e = cudaGetDevice(&restore.prev)) != cudaSuccess) return noalloc_cuda_fail(error, error_len, e, "cudaGetDevice");
     if ((e = cudaSetDevice(device_ordinal)) != cudaSuccess) return noalloc_cuda_fail(error, error_len, e, "cudaSetDevice");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the bundle table is uploaded from this call's stack frame, which a graph
+    // replay could not read again: refuse capture before anything is enqueued
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(s, &capture)) != cudaSuccess)
+        return noalloc_cuda_fail(error, error_len, e, "stream capture check");
+    if (capture != cudaStreamCaptureStatusNone)
+        return noalloc_fail(error, error_len, RT_ERR_INVALID_ARG, "stream is capturing",
+                            "the allocation-free call cannot be captured into a CUDA graph");
     NoAllocDevice dev;
     rt_status st = noalloc_setup(device_ordinal, dev, error, error_len);
     if (st != RT_OK) return st;
@@ -1127,7 +1147,6 @@ extern "C" rt_status rt_trace_bundles_noalloc(int device_ordinal, const rt_camer
     if (cfg) shape.cfg = *cfg;
     const rt_launch_config c = effective_cfg(&shape, mixed);
 
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned char* table_dev = dev.scratch + kNoAllocCounterBytes;
     // pageable source: the copy is staged before the call returns, after the stream's earlier work
     if ((e = cudaMemcpyAsync(table_dev, table, sizeof(BundleDesc) * n_bundles, cudaMemcpyHostToDevice, s)) !=

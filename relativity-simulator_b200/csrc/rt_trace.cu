@@ -248,9 +248,10 @@ __device__ __noinline__ void finish_ray(const BundleDesc* __restrict__ Bp, Cold<
     if (R.dE) R.dE[o] = energy - 1.0;
     if (R.dLz) R.dLz[o] = lz - S.lz0[tid];
     if (R.dQ) R.dQ[o] = q - S.q0[tid];
-    if (R.exit_x) {
+    if (R.exit_x || R.exit_y || R.exit_z) {
         // sky-lookup direction of an escaped ray: -dx/dlambda at the terminal
-        // state, normalised (software_compute_engine.hpp:1771-1775)
+        // state, normalised (software_compute_engine.hpp:1771-1775); each
+        // component is written only where the caller asked for it
         double e[3] = {NAN, NAN, NAN};
         if (status == RT_RAY_ESCAPED) {
             const double sv = 1.0 + kp;
@@ -260,12 +261,9 @@ __device__ __noinline__ void finish_ray(const BundleDesc* __restrict__ Bp, Cold<
 #pragma unroll
             for (int i = 0; i < 3; ++i) e[i] = -v[i] * inv;
         }
-        R.exit_x[o] = e[0];
+        if (R.exit_x) R.exit_x[o] = e[0];
         if (R.exit_y) R.exit_y[o] = e[1];
         if (R.exit_z) R.exit_z[o] = e[2];
-    } else {
-        if (R.exit_y) R.exit_y[o] = NAN;
-        if (R.exit_z) R.exit_z[o] = NAN;
     }
     if (out.pixels) {
         // GpuPixelOutput (gpu_types.hpp:1111-1130); shading is not part of this path

@@ -20,7 +20,8 @@ import relsim
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SRC = os.path.join(ROOT, "tests", "native", "adapter_main.cpp")
 LIBDIR = os.path.dirname(relsim.LIB_PATH)
-REFERENCE_INCLUDE = "/root/reference/include"
+# the reference source tree, as oracle/Makefile takes it (REF_ROOT)
+REFERENCE_INCLUDE = os.path.join(os.environ.get("REF_ROOT", "/root/reference"), "include")
 
 
 def _build(tmp_path, extra=()):

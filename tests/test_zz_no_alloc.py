@@ -6,7 +6,9 @@ handle-owned buffers.  Two calls in a row must each reproduce
 rt_trace_bundles_device on the same bundle table (every call clears the
 counters that must start at zero), repeated calls must leave the device's free
 memory unchanged, and a bundle table longer than the static scratch holds is
-rejected with a message before any device work.
+rejected with a message before any device work.  The call cannot be captured
+into a CUDA graph (it uploads the bundle table from its own stack frame), so on
+a capturing stream it is refused before anything is enqueued.
 
 This file is collected last so that it also runs after every other GPU test.
 """
@@ -18,7 +20,8 @@ import pytest
 import relsim
 from cameras import config_cam
 
-FIELDS = ["status", "flags", "steps_accepted", "steps_rejected", "r", "theta", "phi", "r_hit", "g", "lambda"]
+FIELDS = [name for name, _ in relsim.RAY_FIELDS]  # every record field, the drifts and exit directions too
+FLOAT_FIELDS = [name for name, dt in relsim.RAY_FIELDS if dt == np.float64]
 REL = 1e-12  # same kernel, same inputs: the records agree to rounding of the last digit at most
 
 
@@ -46,7 +49,7 @@ def _host(t, pix):
 def _assert_same(a, b):
     for k in ("status", "flags", "steps_accepted", "steps_rejected"):
         assert np.array_equal(a[k], b[k]), k
-    for k in ("r", "theta", "phi", "r_hit", "g", "lambda"):
+    for k in FLOAT_FIELDS:
         x, y = a[k], b[k]
         nan = np.isnan(y)
         assert np.array_equal(np.isnan(x), nan), k
@@ -131,3 +134,27 @@ def test_noalloc_reports_bad_arguments():
         relsim.trace_bundles_noalloc(cams, ro, pix.data_ptr(), n, device=1 << 20)
     with pytest.raises(relsim.RelsimError, match="16-byte"):
         relsim.trace_bundles_noalloc(cams, ro, pix.data_ptr() + 4, n)
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_stream_capture():
+    """A capturing stream is refused before anything is enqueued: the capture
+    stays valid (it ends as an empty graph) and the caller's current device is
+    unchanged."""
+    import torch
+    cams = _cams(relsim.PRECISION_FP64)
+    n = relsim.bundle_rays(cams)
+    ro, t, pix = _outputs(n)
+    relsim.trace_bundles_noalloc(cams, ro, pix.data_ptr(), n)  # set-up call outside the capture
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        with pytest.raises(relsim.RelsimError, match="capturing") as e:
+            relsim.trace_bundles_noalloc(cams, ro, pix.data_ptr(), n, stream=stream.cuda_stream)
+    assert e.value.status == 1
+    assert torch.cuda.current_device() == 0
+    # the entry point still works on an ordinary stream afterwards
+    relsim.trace_bundles_noalloc(cams, ro, pix.data_ptr(), n, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    assert np.all(t["status"].cpu().numpy() != relsim.RAY_UNFINISHED)
