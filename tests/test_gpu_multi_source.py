@@ -19,7 +19,12 @@ Hamiltonian, rtol = atol = 1e-10).  Bars:
   - accepted step counts within one of each other for 99 % of escaped and
     disk rays (with up to 16 sources summed, a last-bit difference now and then
     moves an acceptance decision at err = 1 by one step, about one ray in ten;
-    the outcome stays within the bars above).
+    the outcome stays within the bars above);
+  - the per-ray constraint drift dH (the largest |H| of the superposed
+    Hamiltonian before a projection; the Kerr invariants E, L_z, Q do not exist
+    for a superposition and are NaN on both sides) within 1e-12 of the
+    oracle's for 99.9 % of escaped and disk rays (measured on B200: 9e-16 at
+    most over three stream scenes, with dH itself up to 5e-4).
 """
 import numpy as np
 import pytest
@@ -32,7 +37,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 FIELDS = ["status", "flags", "steps_accepted", "steps_rejected", "r", "theta", "phi", "r_hit", "g", "lambda",
-          "exit_x", "exit_y", "exit_z"]
+          "dH", "dE", "dLz", "dQ", "exit_x", "exit_y", "exit_z"]
 
 
 def _oracle_sources(srcs):
@@ -68,6 +73,10 @@ def _compare(tracer, cam, srcs):
         rel = np.abs(out[f][disk] - ref[f][disk]) / ref[f][disk]
         assert share_within(rel, 1e-9) >= 0.995, (f, share_within(rel, 1e-9))
         assert share_within(rel, 1e-6) >= 0.999, (f, share_within(rel, 1e-6))
+    dh = np.abs(out["dH"][same] - ref["dH"][same])
+    assert share_within(dh, 1e-12) >= 0.999, share_within(dh, 1e-12)
+    for f in ("dE", "dLz", "dQ"):
+        assert np.all(np.isnan(out[f])), f
     # sky-lookup directions of escaped rays (the superposed flow), same bars
     esc = same & (rst == O.ESCAPED)
     e = np.stack([out["exit_x"], out["exit_y"], out["exit_z"]], 1)
