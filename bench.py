@@ -370,7 +370,7 @@ def bl_camera(relsim, side: int):
     return relsim.make_camera(width=side, height=side, metric_form=relsim.METRIC_BOYER_LINDQUIST, **BL_CAMERA)
 
 
-def time_boyer_lindquist(tr, relsim, side, ro, pix, flush, steps, warmup, fp64_peak, ws, device) -> dict:
+def time_boyer_lindquist(tr, relsim, side, ro, pix, flush, steps, warmup, fp64_peak, fp32_peak, ws, device) -> dict:
     """The Boyer-Lindquist Kerr-Newman tracer on its own workload: device time with
     resident outputs (L2 flushed between steps) and end to end through rt_dispatch."""
     cam = bl_camera(relsim, side)
@@ -399,7 +399,8 @@ def time_boyer_lindquist(tr, relsim, side, ro, pix, flush, steps, warmup, fp64_p
         "roofline": {"bound": "fp64 pipe", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak, "flop_per_attempt": BL_FLOP_PER_ATTEMPT,
                      "peak_source": "measured in this run: register FMA-chain kernel (rt_measure_fma_peak)",
-                     "traffic": committed_traffic("bl")},
+                     "traffic": committed_traffic("bl"),
+                     "executed": executed_roofline("bl", d["attempts"], own_ms, fp64_peak, fp32_peak)},
     }
 
 
@@ -529,8 +530,8 @@ def ours(args) -> None:
 
     bl = None
     if not args.no_bl:
-        bl = time_boyer_lindquist(tr, relsim, args.side, ro, pix, flush, args.steps, args.warmup, fp64_peak, ws,
-                                  f"cuda:{local}")
+        bl = time_boyer_lindquist(tr, relsim, args.side, ro, pix, flush, args.steps, args.warmup, fp64_peak, fp32_peak,
+                                  ws, f"cuda:{local}")
         if rank == 0 and ws == 1 and not args.no_cpu_baseline:
             bl["cpu_baseline"] = bl_cpu_baselines(args.side, args.cpu_seconds)
 
@@ -551,7 +552,8 @@ def ours(args) -> None:
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": "measured in this run: register FMA-chain kernel (rt_measure_fma_peak)",
                          "flop_per_attempt": FLOP_PER_ATTEMPT,
-                         "traffic": committed_traffic(prec)},
+                         "traffic": committed_traffic(prec),
+                         "executed": executed_roofline(prec, d["attempts"], own_ms, fp64_peak, fp32_peak)},
         }
 
     # the plain FP64 tracer at the mixed tracer's tolerance: the equal-tolerance comparison
@@ -654,6 +656,25 @@ def ours(args) -> None:
 
 def vars_of(c) -> dict:
     return {f: getattr(c, f) for f, _ in c._fields_}
+
+
+def executed_roofline(key, attempts, ms, fp64_peak, fp32_peak):
+    """Executed floating-point work against the pipe peaks: per-attempt FP32 and
+    FP64 FLOP counts from the committed ncu instruction mix of the same kernels
+    (profiles/instruction_mix.json: FFMA and packed FFMA2 count 2 and 4 FLOP,
+    FMUL/FADD 1 and 2, DFMA 2, DMUL/DADD 1), times the attempts of this run,
+    over its device time.  None when no mix is committed for `key`."""
+    path = os.path.join(ROOT, "profiles", "instruction_mix.json")
+    try:
+        with open(path) as f:
+            mix = json.load(f)[key]
+    except (OSError, ValueError, KeyError):
+        return None
+    sec = ms * 1e-3
+    f32 = attempts * mix["fp32_flop_per_attempt"] / sec / 1e12
+    f64 = attempts * mix["fp64_flop_per_attempt"] / sec / 1e12
+    return {"fp32_tflops": f32, "fp32_frac": f32 / fp32_peak, "fp64_tflops": f64, "fp64_frac": f64 / fp64_peak,
+            "pipe_frac": f32 / fp32_peak + f64 / fp64_peak, "source": f"profiles/instruction_mix.json[{key}]"}
 
 
 def committed_traffic(precision):
