@@ -253,6 +253,7 @@ struct SlotState {
     uint32_t acc, rej, flags, guard, bidx, ray;
     int mode, wind, can_early;
     bool has_hist;
+    bool critical;  // near-critical: goes to the FP64 near pass at its first step
 };
 
 }  // namespace
@@ -287,6 +288,7 @@ __global__ void __launch_bounds__(BLOCK, WARPS_PER_SM * 32 / BLOCK) far_pair_ker
         st[s].mode = MODE_IDLE;
         st[s].wind = st[s].can_early = 0;
         st[s].has_hist = false;
+        st[s].critical = false;
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i) dx1[i] = kp1[i] = bc(0.0f);
@@ -328,7 +330,8 @@ __global__ void __launch_bounds__(BLOCK, WARPS_PER_SM * 32 / BLOCK) far_pair_ker
                         for (int i = 0; i < 6; ++i) xch[i] = st[s].y[i];
                         xch[6] = st[s].h;
                         const uint32_t misc = (st[s].has_hist ? PM_HAS_HIST : 0u) |
-                                              (static_cast<uint32_t>(st[s].can_early + 1) << PM_EARLY_SHIFT);
+                                              (static_cast<uint32_t>(st[s].can_early + 1) << PM_EARLY_SHIFT) |
+                                              (st[s].critical ? PM_CRITICAL : 0u);
                         const uint32_t uch[PU_COUNT] = {st[s].acc,   st[s].rej,  st[s].flags,
                                                         st[s].guard, static_cast<uint32_t>(st[s].wind),
                                                         misc,        __float_as_uint(st[s].lnp)};
@@ -394,6 +397,7 @@ __global__ void __launch_bounds__(BLOCK, WARPS_PER_SM * 32 / BLOCK) far_pair_ker
                         q.has_hist = (uch[PU_MISC] & PM_HAS_HIST) != 0u;
                         q.can_early = static_cast<int>((uch[PU_MISC] >> PM_EARLY_SHIFT) & 3u) - 1;
                         q.lnp = __uint_as_float(uch[PU_LNP]);
+                        q.critical = false;
                     } else {
                         const InitResult ir = init_ray(Bp, rix - Bp->ray_begin, S, tid + s * BLOCK, xch);
                         q.r = static_cast<float>(ir.r);
@@ -404,6 +408,15 @@ __global__ void __launch_bounds__(BLOCK, WARPS_PER_SM * 32 / BLOCK) far_pair_ker
                         q.acc = q.rej = q.flags = 0u;
                         q.wind = Bp->wind0;
                         q.guard = 0u;
+                        q.critical = false;
+                        if (args.opts & TO_CRITICAL_FP64) {
+                            // distance of the ray's constants from the critical curve; the
+                            // Carter early-capture decision comes from the same value
+                            const double db = shadow_distance(Bp->m, Bp->a, 0.0, Bp->rh, S.lz0[tid + s * BLOCK],
+                                                              S.q0[tid + s * BLOCK]);
+                            if (q.can_early < 0) q.can_early = db > kEarlyCaptureMargin;
+                            q.critical = fabs(db) < kCriticalBand * Bp->m;
+                        }
                         ++n_rays;
                     }
                     ++n_rhs;
@@ -465,7 +478,7 @@ __global__ void __launch_bounds__(BLOCK, WARPS_PER_SM * 32 / BLOCK) far_pair_ker
                     term = RT_RAY_CAPTURED;
                 }
             }
-            if (!term && (r < Bp->fp64_radius || r >= kFp32MaxRadius)) {
+            if (!term && (q.critical || r < Bp->fp64_radius || r >= kFp32MaxRadius)) {
                 q.mode = MODE_PARK;  // into the FP64 zone: the near pass takes it
                 continue;
             }

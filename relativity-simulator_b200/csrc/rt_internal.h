@@ -70,7 +70,8 @@ enum ParkU : int { PU_ACC = 0, PU_REJ, PU_FLAGS, PU_GUARD, PU_WIND, PU_MISC, PU_
 // PU_MISC bits
 enum : uint32_t {
     PM_HAS_HIST = 1u,    // bit 0: PI30 history present
-    PM_EARLY_SHIFT = 2u  // bits 2..3: Carter early-capture state + 1
+    PM_EARLY_SHIFT = 2u, // bits 2..3: Carter early-capture state + 1
+    PM_CRITICAL = 16u    // bit 4: near-critical ray, traced in FP64 at the tightened tolerance
 };
 
 struct ParkBuf {
@@ -84,12 +85,17 @@ struct ParkBuf {
 // near-zone pass; rays move between them through queues of launch indices.
 enum TracePass : int { PASS_SINGLE = 0, PASS_FAR = 1, PASS_NEAR = 2 };
 
+// TraceArgs.opts
+enum : uint32_t {
+    TO_CRITICAL_FP64 = 1u  // far pass: near-critical rays go to the FP64 near pass at their first step
+};
+
 struct TraceArgs {
     const BundleDesc* bundles;
     uint32_t n_bundles;
     uint32_t refill_threshold;
     uint32_t claim;             // rays a warp claims per global atomic
-    uint32_t pad;
+    uint32_t opts;              // TO_* bits
     uint64_t total_rays;
     unsigned long long* queue;  // [0]: next unclaimed ray (or queue entry)
     unsigned long long* stats;  // [ST_COUNT]

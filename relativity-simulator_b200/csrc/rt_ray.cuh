@@ -353,6 +353,15 @@ __device__ __noinline__ double dense_disk_root(const double* __restrict__ y0, co
 // multiple of the FP64 radius (hysteresis against ping-pong at the boundary).
 constexpr double kNearExitFactor = 1.25;
 
+// Near-critical rays of the mixed tracer: a ray whose impact parameter lies
+// within kCriticalBand M of the critical curve (|d_b| from the Kerr radial
+// potential, shadow_distance) orbits the photon region, where any step error
+// is amplified about as 1/|d_b|.  The mixed tracer sends such a ray to the
+// FP64 near pass at its first step and keeps it there to its end, at the
+// camera's tolerance times kCriticalTolScale.
+constexpr double kCriticalBand = 0.05;
+constexpr double kCriticalTolScale = 1e-2;
+
 // Largest r_BL at which the FP32 stages are used (keeps r^4 and 1/r^4 in range).
 constexpr double kFp32MaxRadius = 1e6;
 

@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     uint32_t acc = 0, rej = 0, flags = 0, bidx = 0;
     int mode = MODE_IDLE, wind = 0, can_early = 0;
     bool has_hist = false;
+    bool critical = false;  // near pass: a near-critical ray (FP64 to its end, tightened tolerance)
     bool k1_fp32 = false;  // k1 came from an FP32 far-zone stage (mixed mode)
     uint32_t guard = 0;    // loop iterations spent on the current ray
     uint64_t ray = 0;        // launch index of the lane's ray
@@ -287,7 +288,8 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                     for (int i = 0; i < 6; ++i) xch[i] = y[i];
                     xch[6] = h;
                     const uint32_t misc =
-                        (has_hist ? PM_HAS_HIST : 0u) | (static_cast<uint32_t>(can_early + 1) << PM_EARLY_SHIFT);
+                        (has_hist ? PM_HAS_HIST : 0u) | (static_cast<uint32_t>(can_early + 1) << PM_EARLY_SHIFT) |
+                        (critical ? PM_CRITICAL : 0u);
                     const uint32_t uch[PU_COUNT] = {acc, rej, flags, guard, static_cast<uint32_t>(wind), misc,
                                                     __float_as_uint(lnp)};
                     park_ray(args.park, ray, S, tid, xch, uch);
@@ -356,6 +358,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                             wind = static_cast<int>(uch[PU_WIND]);
                             has_hist = (uch[PU_MISC] & PM_HAS_HIST) != 0u;
                             can_early = static_cast<int>((uch[PU_MISC] >> PM_EARLY_SHIFT) & 3u) - 1;
+                            critical = (uch[PU_MISC] & PM_CRITICAL) != 0u;
                             lnp = __uint_as_float(uch[PU_LNP]);
                             k1_fp32 = false;
                             mode = MODE_STEP;
@@ -462,7 +465,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 }
             }
             if constexpr (NEAR_PASS) {
-                if (args.allow_exit != 0u && r >= kNearExitFactor * Bp->fp64_radius &&
+                if (args.allow_exit != 0u && !critical && r >= kNearExitFactor * Bp->fp64_radius &&
                     r < kFp32MaxRadius) {  // back out of the FP64 zone
                     mode = MODE_PARK;
                     continue;
@@ -601,7 +604,8 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
         double err;
         {
             double num = 0.0, den = 1.0;
-            const double rtol = Bp->rtol, atol = Bp->atol;
+            const double tol_scale = (NEAR_PASS && critical) ? kCriticalTolScale : 1.0;
+            const double rtol = Bp->rtol * tol_scale, atol = Bp->atol * tol_scale;
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
                 const double sc = rtol * fmax(fabs(y[i]), fabs(y5[i])) + atol;
@@ -870,6 +874,15 @@ const void* far_pair_kernel_for(uint32_t block, int warps_per_sm);  // rt_far.cu
 
 namespace {
 // far-pass form: 0 single-slot kernel, 2 two-slot kernel at 12 warps/SM, 3 at 8 warps/SM
+// near-critical rays to the FP64 near pass (paired far pass only): RELSIM_CRITICAL=1
+uint32_t trace_opts() {
+    static const uint32_t o = [] {
+        const char* v = std::getenv("RELSIM_CRITICAL");
+        return (v && v[0] == '1') ? TO_CRITICAL_FP64 : 0u;
+    }();
+    return o;
+}
+
 int far_form() {
     static const int form = [] {
         const char* v = std::getenv("RELSIM_FAR_FORM");
@@ -941,6 +954,7 @@ cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t beg
         args.queue = reinterpret_cast<unsigned long long*>(qb);
         args.refill_threshold = far_refill;
         args.from_pixels = (round == 0) ? 1u : 0u;
+        args.opts = trace_opts();
         args.allow_exit = 0;
         args.in_queue = far_q;
         args.in_count = reinterpret_cast<const uint32_t*>(qb + 12);
