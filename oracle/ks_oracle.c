@@ -536,7 +536,15 @@ static inline float pi30f(float le, float lp, float order_p1)
     return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));
 }
 
-static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, uint32_t py, orc_ray* out)
+/* cont == NULL: the ray ends at its first disk hit (the north-star record).
+ * cont != NULL: the translucent-disk continuation of the reference's image
+ * path (software_compute_engine.hpp:1734-1765): every crossing on the disk is
+ * recorded (radius, azimuth, g) and the ray goes on to its capture or escape,
+ * up to ORC_MAX_CROSSINGS crossings; the record `out` still describes the
+ * first hit, and cont holds the crossings, the ray's final class and its
+ * exit direction. */
+static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, uint32_t py, orc_ray* out,
+                      orc_cont* cont)
 {
     const double m = c->m, a = c->a;
     double y[6];
@@ -558,6 +566,15 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
     uint32_t acc = 0, rej = 0, status = ORC_RAY_UNFINISHED, flags = 0;
     double r_hit = NAN, g = 1.0;
     double yn[6];
+    /* continuation: the first hit's record (status, point, lambda, counts, flags, azimuth reference) */
+    int hit = 0;
+    double y_hit[6], lambda_hit = 0.0, phi_ref_hit = 0.0;
+    uint32_t acc_hit = 0, rej_hit = 0, flags_hit = 0;
+    if (cont) {
+        cont->n_cross = 0;
+        cont->fate = ORC_RAY_UNFINISHED;
+        cont->exit_dir[0] = cont->exit_dir[1] = cont->exit_dir[2] = NAN;
+    }
     /* Certain capture (the CertainAbsorption early-out of
      * carter_ray_classifier.hpp:146-150, used by software_compute_engine.hpp:1356-1368):
      * with no turning point outside r_+ and below the disk's inner edge, an
@@ -613,12 +630,33 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
                     const double t = disk_root(m, a, y, h, k[0], y[2], yn[2], yr);
                     const double rr = bl_radius(yr, a);
                     if (rr >= c->r_in && rr <= c->r_out && rr > c->rh * 1.02) {
-                        status = ORC_RAY_DISK;
-                        r_hit = rr;
-                        g = orc_redshift_at(m, a, rr, lz0);
-                        lambda += t * h;
-                        memcpy(y, yr, sizeof yr);
-                        break;
+                        if (!cont) {
+                            status = ORC_RAY_DISK;
+                            r_hit = rr;
+                            g = orc_redshift_at(m, a, rr, lz0);
+                            lambda += t * h;
+                            memcpy(y, yr, sizeof yr);
+                            break;
+                        }
+                        /* record the crossing and go on through the disk */
+                        double bl[3];
+                        orc_bl_from_ks(yr, a, phi_unwrapped, bl);
+                        const uint32_t kx = cont->n_cross++;
+                        cont->cross_r[kx] = rr;
+                        cont->cross_phi[kx] = bl[2];
+                        cont->cross_g[kx] = orc_redshift_at(m, a, rr, lz0);
+                        if (!hit) {
+                            hit = 1;
+                            r_hit = rr;
+                            g = cont->cross_g[kx];
+                            memcpy(y_hit, yr, sizeof yr);
+                            lambda_hit = lambda + t * h;
+                            phi_ref_hit = phi_unwrapped;
+                            acc_hit = acc;
+                            rej_hit = rej;
+                            flags_hit = flags;
+                        }
+                        if (cont->n_cross >= ORC_MAX_CROSSINGS) break;
                     }
                 }
             }
@@ -691,6 +729,26 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
         }
     }
 
+    if (cont) {
+        cont->fate = status;
+        if (status == ORC_RAY_ESCAPED) {
+            double dy[6];
+            ks_rhs(y, m, a, dy);
+            const double len = sqrt(dy[0] * dy[0] + dy[1] * dy[1] + dy[2] * dy[2]);
+            const double inv = 1.0 / max_d(len, 1e-12);
+            for (int i = 0; i < 3; ++i) cont->exit_dir[i] = -dy[i] * inv;
+        }
+        if (hit) {
+            /* the record describes the first hit */
+            status = ORC_RAY_DISK;
+            memcpy(y, y_hit, sizeof y_hit);
+            lambda = lambda_hit;
+            phi_unwrapped = phi_ref_hit;
+            acc = acc_hit;
+            rej = rej_hit;
+            flags = flags_hit;
+        }
+    }
     double bl[3];
     orc_bl_from_ks(y, a, phi_unwrapped, bl);
     out->status = status;
@@ -726,6 +784,7 @@ typedef struct {
     const uint64_t* idx;
     uint64_t first, count;
     orc_ray* out;
+    orc_cont* cont;
     atomic_ullong next;
 } work_t;
 
@@ -741,14 +800,29 @@ static void* worker(void* arg)
             const uint64_t pix = w->idx ? w->idx[i] : w->first + i;
             const uint32_t px = (uint32_t)(pix % w->cam->screen_width);
             const uint32_t py = (uint32_t)(pix / w->cam->screen_width);
-            trace_one(w->cam, w->c, px, py, &w->out[i]);
+            trace_one(w->cam, w->c, px, py, &w->out[i], w->cont ? &w->cont[i] : NULL);
         }
     }
     return NULL;
 }
 
+static void trace_range(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
+                        orc_ray* out, orc_cont* cont, int threads);
+
 void orc_trace(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count, orc_ray* out,
                int threads)
+{
+    trace_range(cam, pixel_index, first, count, out, NULL, threads);
+}
+
+void orc_trace_cont(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
+                    orc_ray* out, orc_cont* cont, int threads)
+{
+    trace_range(cam, pixel_index, first, count, out, cont, threads);
+}
+
+static void trace_range(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
+                        orc_ray* out, orc_cont* cont, int threads)
 {
     cam_consts c;
     camera_consts(cam, &c);
@@ -761,6 +835,7 @@ void orc_trace(const orc_camera* cam, const uint64_t* pixel_index, uint64_t firs
     w.first = first;
     w.count = count;
     w.out = out;
+    w.cont = cont;
     atomic_init(&w.next, 0);
     if (threads == 1) {
         worker(&w);

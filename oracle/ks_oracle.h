@@ -99,6 +99,20 @@ typedef struct orc_ray {
                                     travel, :1581-1589); NaN otherwise */
 } orc_ray;
 
+/* Translucent-disk continuation of a ray (software_compute_engine.hpp:1734-1765,
+ * :1771-1795): the reference's image path does not end a ray at the disk; each
+ * crossing adds the disk's radiance at the remaining throughput and the ray
+ * goes on to its capture or escape, where the sky behind adds in. */
+#define ORC_MAX_CROSSINGS 8
+typedef struct orc_cont {
+    uint32_t n_cross;            /* disk crossings recorded, in order along the backward ray */
+    uint32_t fate;               /* class at the ray's end (ORC_RAY_*) */
+    double cross_r[ORC_MAX_CROSSINGS];
+    double cross_phi[ORC_MAX_CROSSINGS];
+    double cross_g[ORC_MAX_CROSSINGS];
+    double exit_dir[3];          /* escaped at its end: the sky-lookup direction; NaN otherwise */
+} orc_cont;
+
 /* --- single-function checks (pinned against the reference) --- */
 void orc_ks_field(const double x[3], double mass, double spin, double* r, double* h, double k[3]);
 void orc_ks_rhs(const double y[6], double mass, double spin, double dy[6]);
@@ -124,6 +138,10 @@ double orc_dp45_attempt(const orc_camera* cam, const double y[6], double h, doub
  * threads <= 0 uses all online cores. */
 void orc_trace(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
                orc_ray* out, int threads);
+/* The same with the translucent-disk continuation: `out` describes each ray's
+ * first hit as orc_trace does, `cont` its crossings and end. */
+void orc_trace_cont(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
+                    orc_ray* out, orc_cont* cont, int threads);
 
 /* --- multi-source Kerr-Schild superposition (ms_oracle.c) --- */
 #define ORC_MS_MAX_SOURCES 16

@@ -54,6 +54,13 @@ RAY_DTYPE = np.dtype([
 
 CAPTURED, ESCAPED, DISK, UNFINISHED = 1, 2, 3, 0
 
+# orc_cont: the translucent-disk continuation of a ray (ks_oracle.h)
+MAX_CROSSINGS = 8
+CONT_DTYPE = np.dtype([
+    ("n_cross", "u4"), ("fate", "u4"), ("cross_r", "f8", MAX_CROSSINGS), ("cross_phi", "f8", MAX_CROSSINGS),
+    ("cross_g", "f8", MAX_CROSSINGS), ("exit_dir", "f8", (3,)),
+])
+
 # orc_source: a black-hole body beside the camera's hole (ms_oracle.c)
 SOURCE_DTYPE = np.dtype([
     ("position", "f8", 3), ("mass", "f8"), ("spin_parameter", "f8"), ("axis", "f8", 3),
@@ -92,6 +99,8 @@ def lib() -> ctypes.CDLL:
         d = ctypes.c_double
         L.orc_trace.argtypes = [v, v, ctypes.c_uint64, ctypes.c_uint64, v, ctypes.c_int]
         L.orc_trace.restype = None
+        L.orc_trace_cont.argtypes = [v, v, ctypes.c_uint64, ctypes.c_uint64, v, v, ctypes.c_int]
+        L.orc_trace_cont.restype = None
         L.orc_ray_initial_state.argtypes = [v, ctypes.c_uint32, ctypes.c_uint32, v]
         L.orc_ray_initial_state.restype = d
         L.orc_dp45_attempt.argtypes = [v, v, d, v]
@@ -218,6 +227,22 @@ def trace(cam: dict, pixels: np.ndarray | None = None, first: int = 0, count: in
         out = np.zeros(n, dtype=RAY_DTYPE)
         lib().orc_trace(_p(c), None, first, n, _p(out), threads)
     return out
+
+
+def trace_cont(cam: dict, pixels: np.ndarray | None = None, threads: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Trace pixels with the translucent-disk continuation: (records of the
+    first hit, as trace() gives them; CONT_DTYPE crossings and ends)."""
+    c = to_camera(cam)
+    if pixels is None:
+        n = int(cam["screen_width"]) * int(cam["screen_height"])
+        idx = None
+    else:
+        idx = np.ascontiguousarray(pixels, dtype=np.uint64)
+        n = idx.size
+    out = np.zeros(n, dtype=RAY_DTYPE)
+    cont = np.zeros(n, dtype=CONT_DTYPE)
+    lib().orc_trace_cont(_p(c), _p(idx) if idx is not None else None, 0, n, _p(out), _p(cont), threads)
+    return out, cont
 
 
 def initial_state(cam: dict, px: int, py: int) -> tuple[np.ndarray, float]:
