@@ -485,7 +485,12 @@ static inline float pi30f(float le, float lp, float order_p1)
     return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));
 }
 
-static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, uint32_t py, orc_ray* out)
+/* cont != NULL: the translucent-disk continuation (as orc_trace_cont in
+ * ks_oracle.c; software_compute_engine.hpp:1538-1560 for this path): every
+ * crossing on the disk is recorded at the reflected root point and the ray
+ * goes on; `out` still describes the first hit. */
+static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, uint32_t py, orc_ray* out,
+                      orc_cont* cont)
 {
     const double m = c->m, a = c->a, q2 = c->q2;
     double y[NB];
@@ -506,6 +511,14 @@ static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, ui
     const double db0 = orc_kn_shadow_distance(m, a, sqrt(q2), xi, eta);
     const int can_early = cam->early_capture && db0 > ORC_EARLY_CAPTURE_MARGIN;
     const double r_early = c->disk ? c->r_in : INFINITY;
+    int hit = 0;
+    double y_hit[NB], lambda_hit = 0.0;
+    uint32_t acc_hit = 0, rej_hit = 0, flags_hit = 0;
+    if (cont) {
+        cont->n_cross = 0;
+        cont->fate = ORC_RAY_UNFINISHED;
+        cont->exit_dir[0] = cont->exit_dir[1] = cont->exit_dir[2] = NAN;
+    }
 
     for (uint32_t attempt = 0;; ++attempt) {
         const double r = y[0];
@@ -564,12 +577,33 @@ static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, ui
                     if (rr >= c->r_in && rr <= c->r_out && rr > c->rh * 1.02) {
                         double iv[3];
                         invariants(m, a, q2, yr, iv);
-                        status = ORC_RAY_DISK;
-                        r_hit = rr;
-                        g = orc_redshift_at(m, a, rr, iv[1] / iv[0]);
-                        lambda += t * h;
-                        memcpy(y, yr, sizeof yr);
-                        break;
+                        const double gg = orc_redshift_at(m, a, rr, iv[1] / iv[0]);
+                        if (!cont) {
+                            status = ORC_RAY_DISK;
+                            r_hit = rr;
+                            g = gg;
+                            lambda += t * h;
+                            memcpy(y, yr, sizeof yr);
+                            break;
+                        }
+                        double yp[NB];
+                        memcpy(yp, yr, sizeof yr);
+                        reflect_pole(yp, NULL);
+                        const uint32_t kx = cont->n_cross++;
+                        cont->cross_r[kx] = rr;
+                        cont->cross_phi[kx] = yp[2];
+                        cont->cross_g[kx] = gg;
+                        if (!hit) {
+                            hit = 1;
+                            r_hit = rr;
+                            g = gg;
+                            memcpy(y_hit, yr, sizeof yr);
+                            lambda_hit = lambda + t * h;
+                            acc_hit = acc;
+                            rej_hit = rej;
+                            flags_hit = flags;
+                        }
+                        if (cont->n_cross >= ORC_MAX_CROSSINGS) break;
                     }
                 }
             }
@@ -618,6 +652,17 @@ static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, ui
         h = -clamp_d(fabs(h) * clamp_d(0.9 * factor, 0.2, 5.0), 1e-8, 1e13);
     }
 
+    if (cont) {
+        cont->fate = status;
+        if (hit) {
+            status = ORC_RAY_DISK;
+            memcpy(y, y_hit, sizeof y_hit);
+            lambda = lambda_hit;
+            acc = acc_hit;
+            rej = rej_hit;
+            flags = flags_hit;
+        }
+    }
     reflect_pole(y, NULL);
     double iv[3];
     invariants(m, a, q2, y, iv);
@@ -668,6 +713,7 @@ typedef struct {
     const uint64_t* idx;
     uint64_t first, count;
     orc_ray* out;
+    orc_cont* cont;
     atomic_ullong next;
 } work_t;
 
@@ -682,14 +728,29 @@ static void* worker(void* arg)
         for (uint64_t i = b; i < e; ++i) {
             const uint64_t pix = w->idx ? w->idx[i] : w->first + i;
             trace_one(w->cam, w->c, (uint32_t)(pix % w->cam->screen_width), (uint32_t)(pix / w->cam->screen_width),
-                      &w->out[i]);
+                      &w->out[i], w->cont ? &w->cont[i] : NULL);
         }
     }
     return NULL;
 }
 
+static void bl_trace_range(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first,
+                           uint64_t count, orc_ray* out, orc_cont* cont, int threads);
+
 void orc_bl_trace(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first, uint64_t count,
                   orc_ray* out, int threads)
+{
+    bl_trace_range(cam, charge, pixel_index, first, count, out, NULL, threads);
+}
+
+void orc_bl_trace_cont(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first,
+                       uint64_t count, orc_ray* out, orc_cont* cont, int threads)
+{
+    bl_trace_range(cam, charge, pixel_index, first, count, out, cont, threads);
+}
+
+static void bl_trace_range(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first,
+                           uint64_t count, orc_ray* out, orc_cont* cont, int threads)
 {
     bl_consts c;
     bl_camera_consts(cam, charge, &c);
@@ -702,6 +763,7 @@ void orc_bl_trace(const orc_camera* cam, double charge, const uint64_t* pixel_in
     w.first = first;
     w.count = count;
     w.out = out;
+    w.cont = cont;
     atomic_init(&w.next, 0);
     if (threads == 1) {
         worker(&w);

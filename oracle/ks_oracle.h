@@ -205,6 +205,9 @@ void orc_bl_zamo_ray(double mass, double spin, double charge, double r, double t
 void orc_bl_initial_state(const orc_camera* cam, double charge, uint32_t px, uint32_t py, double y0[7]);
 void orc_bl_trace(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first, uint64_t count,
                   orc_ray* out, int threads);
+/* The same with the translucent-disk continuation (as orc_trace_cont). */
+void orc_bl_trace_cont(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first,
+                       uint64_t count, orc_ray* out, orc_cont* cont, int threads);
 
 /* --- pixel shading tail (shade_oracle.c) ---
  * Disk profiles are GpuDiskProfile's 32 floats in declaration order.  A
@@ -221,6 +224,10 @@ void orc_shade_pixel(const float resolved_profile[32], uint32_t hydro_model, flo
                      uint32_t tonemap_mode, double exposure_ev, double mass, double disk_spin, double inner,
                      double outer, double time, double detail, uint32_t status, double r_hit, double phi, double g,
                      float out[3]);
+void orc_shade_cont(const float resolved_profile[32], uint32_t hydro_model, float accretion_rate_scale,
+                    uint32_t tonemap_mode, double exposure_ev, double mass, double disk_spin, double inner,
+                    double outer, double time, double detail, uint32_t n_cross, const double* cross_r,
+                    const double* cross_phi, const double* cross_g, float out[3]);
 
 #ifdef __cplusplus
 }

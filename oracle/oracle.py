@@ -146,6 +146,8 @@ def lib() -> ctypes.CDLL:
         L.orc_bl_initial_state.argtypes = [v, d, ctypes.c_uint32, ctypes.c_uint32, v]
         L.orc_bl_trace.argtypes = [v, d, v, ctypes.c_uint64, ctypes.c_uint64, v, ctypes.c_int]
         L.orc_bl_trace.restype = None
+        L.orc_bl_trace_cont.argtypes = [v, d, v, ctypes.c_uint64, ctypes.c_uint64, v, v, ctypes.c_int]
+        L.orc_bl_trace_cont.restype = None
         f = ctypes.c_float
         L.orc_planck_xyz.argtypes = [d, v]
         L.orc_blackbody_rgb.argtypes = [d, d, v]
@@ -153,6 +155,8 @@ def lib() -> ctypes.CDLL:
         L.orc_nt_context.argtypes = [d, d, d, d, f, v]
         L.orc_disk_shade.argtypes = [v, v, ctypes.c_uint32, f, v]
         L.orc_tonemap.argtypes = [v, ctypes.c_uint32, d, v]
+        L.orc_shade_cont.argtypes = [v, ctypes.c_uint32, f, ctypes.c_uint32, d, d, d, d, d, d, d, ctypes.c_uint32,
+                                     v, v, v, v]
         L.orc_shade_pixel.argtypes = [v, ctypes.c_uint32, f, ctypes.c_uint32, d, d, d, d, d, d, d, ctypes.c_uint32,
                                       d, d, d, v]
         _lib = L
@@ -313,3 +317,20 @@ def bl_trace(cam: dict, charge: float, pixels: np.ndarray | None = None, threads
         out = np.zeros(idx.size, dtype=RAY_DTYPE)
         lib().orc_bl_trace(_p(c), charge, _p(idx), 0, idx.size, _p(out), threads)
     return out
+
+
+def bl_trace_cont(cam: dict, charge: float, pixels: np.ndarray | None = None,
+                  threads: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Boyer-Lindquist trace with the translucent-disk continuation: (records of
+    the first hit, CONT_DTYPE crossings and ends)."""
+    c = to_camera(cam)
+    if pixels is None:
+        n = int(cam["screen_width"]) * int(cam["screen_height"])
+        idx = None
+    else:
+        idx = np.ascontiguousarray(pixels, dtype=np.uint64)
+        n = idx.size
+    out = np.zeros(n, dtype=RAY_DTYPE)
+    cont = np.zeros(n, dtype=CONT_DTYPE)
+    lib().orc_bl_trace_cont(_p(c), charge, _p(idx) if idx is not None else None, 0, n, _p(out), _p(cont), threads)
+    return out, cont

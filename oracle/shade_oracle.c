@@ -407,3 +407,27 @@ void orc_shade_pixel(const float resolved_profile[32], uint32_t hydro_model, flo
     }
     orc_tonemap(accum, tonemap_mode, exposure_ev, out);
 }
+
+/* Pixel colour of a ray followed through the translucent disk
+ * (software_compute_engine.hpp:1743-1765, 1777-1795; sky disabled): each
+ * recorded crossing k adds the disk's radiance at the throughput left,
+ * T_k = prod_{j<k} (1 - opacity_j), while T > 0.01 (the reference's loop
+ * condition); with the sky disabled the ray's end adds nothing. */
+void orc_shade_cont(const float resolved_profile[32], uint32_t hydro_model, float accretion_rate_scale,
+                    uint32_t tonemap_mode, double exposure_ev, double mass, double disk_spin, double inner,
+                    double outer, double time, double detail, uint32_t n_cross, const double* cross_r,
+                    const double* cross_phi, const double* cross_g, float out[3])
+{
+    double accum[3] = {0.0, 0.0, 0.0};
+    double throughput = 1.0;
+    for (uint32_t k = 0; k < n_cross && throughput > 0.01; ++k) {
+        const double pt[9] = {mass, disk_spin, inner, outer, cross_r[k], cross_phi[k], cross_g[k], time, detail};
+        double sh[4];
+        orc_disk_shade(resolved_profile, pt, hydro_model, accretion_rate_scale, sh);
+        accum[0] += throughput * sh[0];
+        accum[1] += throughput * sh[1];
+        accum[2] += throughput * sh[2];
+        throughput *= 1.0 - sh[3];
+    }
+    orc_tonemap(accum, tonemap_mode, exposure_ev, out);
+}
