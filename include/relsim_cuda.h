@@ -147,11 +147,16 @@ typedef struct rt_disk_profile {
 } rt_disk_profile;
 
 /* Pixel shading of GpuPixelOutput's colour (the reference's shading tail,
- * software_compute_engine.hpp:1538-1611): a disk hit is shaded as the thin
- * disk at (r_hit, phi, g) -- temperature profile, rings, spiral arms,
- * turbulence, blackbody colour, Doppler beaming, grading -- then tonemapped
- * to sRGB; escaped and captured rays are black (the procedural sky is not
- * part of this library: sky_enabled must be 0).  Fields as in
+ * software_compute_engine.hpp:1538-1611, 1734-1808): each disk crossing is
+ * shaded as the thin disk at (r, phi, g) -- temperature profile, rings,
+ * spiral arms, turbulence, blackbody colour, Doppler beaming, grading -- and
+ * the disk is translucent, as in the reference: a crossing adds its radiance
+ * at the throughput left and lowers the throughput by its opacity, and the
+ * ray is followed on while more than 0.01 is left (the per-ray record still
+ * describes the first hit; a disk pixel's flags add how the ray ended and its
+ * redshift is the last crossing's).  The sum is tonemapped to sRGB.  The
+ * procedural sky is not part of this library (sky_enabled must be 0), so the
+ * sky behind a ray adds nothing.  Fields as in
  * GpuCameraPushConstants (gpu_types.hpp:990-1106); the profile is resolved as
  * AccretionDiskModel::resolve_primary_profile does. */
 typedef struct rt_shading {
@@ -403,7 +408,8 @@ rt_status rt_server_poll(rt_server* s, rt_request_done* done, uint32_t max_done,
 rt_status rt_server_get_stats(rt_server* s, rt_server_stats* stats);
 const char* rt_server_last_error(const rt_server* s);
 /* Shade the pixels of requests that finish from now on (single-hole cameras of
- * both metric forms; multi-source requests keep r = g = b = 0), as
+ * both metric forms, at their first disk crossing -- the server's epochs hold
+ * no continuation state; multi-source requests keep r = g = b = 0), as
  * rt_set_shading does for a handle; NULL turns it off.  The server's
  * record_mask must hold status, phi, r_hit, g and the pixels, else
  * RT_ERR_INVALID_ARG. */

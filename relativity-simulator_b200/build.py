@@ -20,7 +20,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "librelsim_cuda.so")
 BUILD = os.path.join(HERE, "_build")
 
-SOURCES = ["rt_trace.cu", "rt_far.cu", "rt_multi.cu", "rt_bl.cu", "rt_shade.cu", "rt_api.cu", "rt_server.cu", "rt_peak.cu", "rt_bundle.cpp"]
+SOURCES = ["rt_trace.cu", "rt_multi.cu", "rt_bl.cu", "rt_shade.cu", "rt_api.cu", "rt_server.cu", "rt_peak.cu", "rt_bundle.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -52,6 +52,11 @@ struct rt_handle {
     DevBuf band_desc, band_queue;        // banded single-kernel host dispatches: per-band camera and counter
     DevBuf shade_desc;                   // pixel shading constants of the last shaded camera
     bool shade_on = false;               // rt_set_shading
+    // translucent-disk continuation of a shaded Kerr-Schild dispatch: accumulated
+    // radiance, throughput and last g per ray, and what the launches pass the tracer
+    DevBuf cont;
+    const ShadeDesc* cur_shade = nullptr;
+    ContOut cur_cont{};
     rt_shading shading{};
     DevBuf ray_fields[kRayFields];
     DevBuf pixels;
@@ -193,6 +198,8 @@ rt_status launch_two_pass(rt_handle* h, uint32_t n_bundles, uint64_t total, cons
     args.total_rays = total;
     args.stats = static_cast<unsigned long long*>(h->stats.ptr);
     args.out = out;
+    args.shade = h->cur_shade;
+    args.cont = h->cur_cont;
     TwoPassBuffers buf{};
     buf.park = ParkBuf{static_cast<double*>(h->park_d.ptr), static_cast<uint32_t*>(h->park_u.ptr), total};
     buf.queues = static_cast<uint32_t*>(h->pass_queues.ptr);
@@ -227,6 +234,8 @@ rt_status launch(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs
     args.queue = static_cast<unsigned long long*>(h->queue.ptr);
     args.stats = static_cast<unsigned long long*>(h->stats.ptr);
     args.out = out;
+    args.shade = h->cur_shade;
+    args.cont = h->cur_cont;
     RT_CUDA(h, cudaMemsetAsync(h->queue.ptr, 0, sizeof(unsigned long long), s));
     RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
     const uint32_t grid = static_cast<uint32_t>(h->sm_count) * c.ctas_per_sm;
@@ -313,12 +322,35 @@ rt_status shade_prepare(rt_handle* h, const rt_camera* cam, cudaStream_t s) {
     return RT_OK;
 }
 
+// Turn on the translucent-disk continuation for the Kerr-Schild launches of a
+// shaded dispatch of n rays (the shading constants already uploaded): the
+// tracers shade each disk crossing and follow the ray on through the disk.
+rt_status begin_continuation(rt_handle* h, size_t n) {
+    const rt_status st = ensure(h, h->cont, sizeof(double) * CF_COUNT * n);
+    if (st != RT_OK) return st;
+    h->cur_shade = static_cast<const ShadeDesc*>(h->shade_desc.ptr);
+    h->cur_cont = ContOut{static_cast<double*>(h->cont.ptr), n};
+    return RT_OK;
+}
+
+void end_continuation_state(rt_handle* h) {
+    h->cur_shade = nullptr;
+    h->cur_cont = ContOut{};
+}
+
+// Turns the continuation off when a dispatch returns, on every path.
+struct ContinuationScope {
+    rt_handle* h;
+    ~ContinuationScope() { end_continuation_state(h); }
+};
+
 // Enqueue the shading pass over n traced rays (after the trace, same stream).
 rt_status shade_launch(rt_handle* h, const rt_camera* cam, const rt_ray_out& dev, rt_pixel_out* pixels, size_t n,
-                       cudaStream_t s) {
+                       cudaStream_t s, bool prepared = false) {
     rt_status st;
-    if ((st = shade_prepare(h, cam, s)) != RT_OK) return st;
-    launch_shade(static_cast<const ShadeDesc*>(h->shade_desc.ptr), dev.status, dev.r_hit, dev.phi, dev.g, pixels, n, s);
+    if (!prepared && (st = shade_prepare(h, cam, s)) != RT_OK) return st;
+    launch_shade(static_cast<const ShadeDesc*>(h->shade_desc.ptr), dev.status, dev.r_hit, dev.phi, dev.g, h->cur_cont,
+                 pixels, n, s);
     RT_CUDA(h, cudaGetLastError());
     return RT_OK;
 }
@@ -336,6 +368,7 @@ struct BandCopyCtx {
     uint64_t offset;  // output element of the launch's first ray
     bool shade;
     uint32_t band;    // next band event
+    ContOut cont;     // translucent-disk continuation outputs (rgb null: none)
 };
 
 int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
@@ -344,7 +377,8 @@ int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
     const uint64_t o = c.offset + begin;
     if (c.shade && c.dpix) {
         launch_shade(static_cast<const ShadeDesc*>(c.h->shade_desc.ptr), c.dev.status + o, c.dev.r_hit + o,
-                     c.dev.phi + o, c.dev.g + o, c.dpix + o, count, s);
+                     c.dev.phi + o, c.dev.g + o, ContOut{c.cont.rgb ? c.cont.rgb + o : nullptr, c.cont.stride},
+                     c.dpix + o, count, s);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return static_cast<int>(e);
     }
@@ -396,8 +430,10 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
         dpix = static_cast<rt_pixel_out*>(h->pixels.ptr);
     }
     const bool shade = h->shade_on && pixels;
+    ContinuationScope cont_scope{h};
     if (shade && (st = add_shade_fields(h, dev, n)) != RT_OK) return st;
     if (shade && (st = shade_prepare(h, cam, h->stream)) != RT_OK) return st;
+    if (shade && (st = begin_continuation(h, n)) != RT_OK) return st;
     // bands of at most 2^24 rays; the cancel flag is polled between bands.  Each
     // band's shading and copies follow its trace; on the two-pass tracer a band
     // is traced in sub-bands whose copies overlap the next sub-band's trace.
@@ -407,7 +443,7 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
         const uint32_t rows = static_cast<uint32_t>(std::min<uint64_t>(band_rows, nrows - r));
         const uint64_t offset = static_cast<uint64_t>(r) * ncols;
         const uint64_t launch_rays = static_cast<uint64_t>(rows) * ncols;
-        BandCopyCtx ctx{h, rays, dev, pixels, dpix, offset, shade, 0};
+        BandCopyCtx ctx{h, rays, dev, pixels, dpix, offset, shade, 0, h->cur_cont};
         const bool two_pass = !is_bl(cam) && uses_two_pass(effective_cfg(h, cam->precision_mode == RT_PRECISION_MIXED),
                                                           cam->precision_mode == RT_PRECISION_MIXED, launch_rays);
         if (!two_pass && launch_rays >= kBandedMinRays && rows >= kCopyBands) {
@@ -512,6 +548,8 @@ rt_status bl_launch(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t 
     args.queue = static_cast<unsigned long long*>(h->queue.ptr);
     args.stats = static_cast<unsigned long long*>(h->stats.ptr);
     args.out = out;
+    args.shade = h->cur_shade;
+    args.cont = h->cur_cont;
     RT_CUDA(h, cudaEventRecord(h->ev0, s));
     launch_bl_trace(args, bl_trace_grid(h->sm_count), s);
     RT_CUDA(h, cudaGetLastError());
@@ -565,6 +603,8 @@ rt_status launch_banded_single(rt_handle* h, const rt_camera* cam, uint32_t col0
             args.queue = q;
             args.stats = static_cast<unsigned long long*>(h->stats.ptr);
             args.out = out;
+            args.shade = h->cur_shade;
+            args.cont = h->cur_cont;
             launch_bl_trace(args, bl_trace_grid(h->sm_count), sb);
         } else {
             BundleDesc d;
@@ -579,6 +619,8 @@ rt_status launch_banded_single(rt_handle* h, const rt_camera* cam, uint32_t col0
             args.queue = q;
             args.stats = static_cast<unsigned long long*>(h->stats.ptr);
             args.out = out;
+            args.shade = h->cur_shade;
+            args.cont = h->cur_cont;
             launch_trace(args, static_cast<uint32_t>(h->sm_count) * c.ctas_per_sm, c.block_size, mixed,
                          c.fp64_rolled != 0, sb);
         }
@@ -852,10 +894,15 @@ rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* p
     rt_ray_out dev = rays ? *rays : rt_ray_out{};
     const bool shade = h->shade_on && pixels;
     rt_status st;
+    ContinuationScope cont_scope{h};
     if (shade && (st = add_shade_fields(h, dev, n)) != RT_OK) return st;
     if (is_bl(cam)) {
+        // shaded: the shading constants go up before the trace, which follows each
+        // ray through the translucent disk
+        if (shade && (st = shade_prepare(h, cam, s)) != RT_OK) return st;
+        if (shade && (st = begin_continuation(h, n)) != RT_OK) return st;
         if ((st = bl_launch(h, cam, 0, cam->screen_width, row0, nrows, 0, OutPtrs{pixels, dev}, s)) != RT_OK) return st;
-        return shade ? shade_launch(h, cam, dev, pixels, n, s) : RT_OK;
+        return shade ? shade_launch(h, cam, dev, pixels, n, s, true) : RT_OK;
     }
     if ((st = ensure_host_bundles(h, 1)) != RT_OK) return st;
     if ((st = ensure(h, h->bundles, sizeof(BundleDesc))) != RT_OK) return st;
@@ -863,8 +910,12 @@ rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* p
     RT_CUDA(h, cudaStreamSynchronize(s));
     build_bundle(*cam, 0, cam->screen_width, row0, nrows, 0, 0, h->host_bundles[0]);
     RT_CUDA(h, cudaMemcpyAsync(h->bundles.ptr, h->host_bundles, sizeof(BundleDesc), cudaMemcpyHostToDevice, s));
+    // shaded: the shading constants go up before the trace, which follows each
+    // ray through the translucent disk
+    if (shade && (st = shade_prepare(h, cam, s)) != RT_OK) return st;
+    if (shade && (st = begin_continuation(h, n)) != RT_OK) return st;
     if ((st = launch(h, 1, n, OutPtrs{pixels, dev}, cam->precision_mode == RT_PRECISION_MIXED, s)) != RT_OK) return st;
-    return shade ? shade_launch(h, cam, dev, pixels, n, s) : RT_OK;
+    return shade ? shade_launch(h, cam, dev, pixels, n, s, true) : RT_OK;
 }
 
 uint64_t rt_bundle_rays(const rt_camera* cams, uint32_t n) {

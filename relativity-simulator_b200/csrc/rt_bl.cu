@@ -29,6 +29,7 @@
 
 #include "rt_device.cuh"
 #include "rt_internal.h"
+#include "rt_shade.cuh"
 
 namespace relsim {
 
@@ -420,6 +421,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
     bool has_hist = false;
     int can_early = 0;  // -1: undecided (Carter test when first inside r_early)
     uint32_t acc = 0, rej = 0, flags = 0, bidx = 0, guard = 0;
+    uint32_t n_cross = 0;  // disk crossings so far (translucent-disk continuation)
     int mode = BL_IDLE;
 #pragma unroll
     for (int i = 0; i < NB; ++i) y[i] = k1[i] = 0.0;
@@ -469,6 +471,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
                     lnp = 0.0f;
                     has_hist = false;
                     can_early = (Bp->flags & BF_EARLY_CAPTURE) ? -1 : 0;
+                    n_cross = 0;
                     acc = rej = flags = guard = 0;
                     mode = BL_STEP;
                     ++n_rays;
@@ -511,7 +514,9 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
             }
         }
         if (term) {
-            bl_finish<BLOCK>(Bp, S, tid, y, term & 15u, flags, acc, rej, NAN, 1.0, args.out);
+            if (n_cross == 0) bl_finish<BLOCK>(Bp, S, tid, y, term & 15u, flags, acc, rej, NAN, 1.0, args.out);
+            if (args.cont.rgb)
+                cont_end(args.cont, args.out.pixels, B.out_offset + S.local[tid], n_cross, term & 15u, y[0], B.m);
             mode = BL_IDLE;
             continue;
         }
@@ -539,8 +544,11 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
 #pragma unroll
         for (int i = 0; i < NB; ++i) finite = finite && isfinite(y5[i]);
         if (!finite) {
-            bl_finish<BLOCK>(Bp, S, tid, y, RT_RAY_CAPTURED, flags | RT_RAYFLAG_NONFINITE, acc, rej, NAN, 1.0,
-                             args.out);
+            if (n_cross == 0)
+                bl_finish<BLOCK>(Bp, S, tid, y, RT_RAY_CAPTURED, flags | RT_RAYFLAG_NONFINITE, acc, rej, NAN, 1.0,
+                                 args.out);
+            if (args.cont.rgb)
+                cont_end(args.cont, args.out.pixels, B.out_offset + S.local[tid], n_cross, RT_RAY_CAPTURED, y[0], B.m);
             mode = BL_IDLE;
             continue;
         }
@@ -562,11 +570,30 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
                     if (rr >= B.r_in && rr <= B.r_out && rr > B.rh * 1.02) {
                         double E, L, Q;
                         bl_invariants(B, yr, E, L, Q);
-                        S.lambda[tid] += t * hh;
-                        bl_finish<BLOCK>(Bp, S, tid, yr, RT_RAY_DISK, flags, acc, rej, rr,
-                                         disk_redshift(B.m, B.a, rr, L / E), args.out);
+                        const double g = disk_redshift(B.m, B.a, rr, L / E);
+                        if (n_cross == 0) {
+                            // lambda at the root, one rounding with or without the continuation
+                            const double lambda_step = S.lambda[tid];
+                            S.lambda[tid] = fma(t, hh, lambda_step);
+                            bl_finish<BLOCK>(Bp, S, tid, yr, RT_RAY_DISK, flags, acc, rej, rr, g, args.out);
+                            S.lambda[tid] = lambda_step;
+                        }
                         mode = BL_IDLE;
-                        continue;
+                        if (!args.shade) continue;
+                        // translucent disk: shade the crossing (at the record's azimuth,
+                        // that of the reflected root point) and go on through it
+                        double yp[NB];
+#pragma unroll
+                        for (int i = 0; i < NB; ++i) yp[i] = yr[i];
+                        bl_reflect(yp, nullptr);
+                        const uint64_t o = B.out_offset + S.local[tid];
+                        const double thr = cont_crossing(*args.shade, args.cont, o, n_cross, rr, yp[2], g);
+                        ++n_cross;
+                        if (!(thr > kMinThroughput && n_cross < kMaxCrossings)) {
+                            cont_end(args.cont, args.out.pixels, o, n_cross, RT_RAY_UNFINISHED, rr, B.m);
+                            continue;
+                        }
+                        mode = BL_STEP;
                     }
                 }
             }
@@ -611,7 +638,9 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
                     for (int i = 0; i < NB; ++i) yt[i] = y5[i];
                     S.lambda[tid] += hh;
                 }
-                bl_finish<BLOCK>(Bp, S, tid, yt, tterm, flags, acc, rej, NAN, 1.0, args.out);
+                if (n_cross == 0) bl_finish<BLOCK>(Bp, S, tid, yt, tterm, flags, acc, rej, NAN, 1.0, args.out);
+                if (args.cont.rgb)
+                    cont_end(args.cont, args.out.pixels, B.out_offset + S.local[tid], n_cross, tterm, yt[0], B.m);
                 mode = BL_IDLE;
                 continue;
             }

@@ -60,6 +60,16 @@ struct OutPtrs {
     rt_ray_out rays;
 };
 
+// Translucent-disk continuation outputs (structure of arrays, `stride`
+// elements each, indexed like the record): the radiance accumulated over the
+// ray's disk crossings (r, g, b), the throughput left, and the redshift of the
+// last crossing.  rgb == nullptr: the tracer ends a ray at its first disk hit.
+enum ContField : int { CF_R = 0, CF_G, CF_B, CF_THROUGHPUT, CF_LAST_G, CF_COUNT };
+struct ContOut {
+    double* rgb;      // [CF_COUNT][stride]
+    uint64_t stride;
+};
+
 // Device counters of one launch.
 enum StatIndex { ST_RAYS = 0, ST_ATTEMPTS, ST_ACCEPTED, ST_RHS, ST_FP64_ATTEMPTS, ST_COUNT };
 
@@ -71,7 +81,8 @@ enum ParkU : int { PU_ACC = 0, PU_REJ, PU_FLAGS, PU_GUARD, PU_WIND, PU_MISC, PU_
 enum : uint32_t {
     PM_HAS_HIST = 1u,    // bit 0: PI30 history present
     PM_EARLY_SHIFT = 2u, // bits 2..3: Carter early-capture state + 1
-    PM_CRITICAL = 16u    // bit 4: near-critical ray, traced in FP64 at the tightened tolerance
+    PM_CRITICAL = 16u,   // bit 4: near-critical ray, traced in FP64 at the tightened tolerance
+    PM_CROSS_SHIFT = 5u  // bits 5..9: disk crossings so far (translucent-disk continuation)
 };
 
 struct ParkBuf {
@@ -84,6 +95,8 @@ struct ParkBuf {
 // The two-pass mixed tracer alternates an FP32 far-zone pass and an FP64
 // near-zone pass; rays move between them through queues of launch indices.
 enum TracePass : int { PASS_SINGLE = 0, PASS_FAR = 1, PASS_NEAR = 2 };
+
+struct ShadeDesc;
 
 // TraceArgs.opts
 enum : uint32_t {
@@ -111,6 +124,11 @@ struct TraceArgs {
     uint32_t* finish_queue;     // disk hits parked with their root point for the finish pass
     uint32_t* finish_count;
     ParkBuf park;
+    // translucent-disk continuation (single-camera launches with shading): the
+    // camera's shading constants and the continuation outputs; null: off
+    const ShadeDesc* shade;
+    ContOut cont;
+    float critical_band;        // TO_CRITICAL_FP64: |d_b| / M below which a ray is near-critical
 };
 
 // Multi-source Kerr-Schild superposition: per-source frame (source 0 is the
@@ -180,6 +198,10 @@ struct BlArgs {
     unsigned long long* queue;
     unsigned long long* stats;
     OutPtrs out;
+    // translucent-disk continuation (shaded dispatches): shading constants and
+    // continuation outputs; null: off
+    const ShadeDesc* shade;
+    ContOut cont;
 };
 
 // Per-camera constants of the pixel shading pass (rt_shade.cu): the resolved
@@ -202,7 +224,7 @@ struct alignas(16) ShadeDesc {
 bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d);
 // Shade n rays: pixels[i].rgba from the record's status, r_hit, phi and g.
 void launch_shade(const ShadeDesc* desc, const uint32_t* status, const double* r_hit, const double* phi,
-                  const double* g, rt_pixel_out* pixels, uint64_t n, void* stream);
+                  const double* g, ContOut cont, rt_pixel_out* pixels, uint64_t n, void* stream);
 
 // Host-side helpers implemented in rt_bundle.cpp.
 // Boyer-Lindquist bundle of a camera window (metric_form RT_METRIC_BOYER_LINDQUIST).

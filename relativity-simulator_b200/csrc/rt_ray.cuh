@@ -1,7 +1,7 @@
 // rt_ray.cuh -- per-ray pieces shared by the Kerr-Schild tracer kernels
-// (rt_trace.cu: single kernel, far/near passes, finish pass; rt_far.cu: the
-// paired far pass): ray generation, termination records, the parked-ray
-// format of the two-pass tracer and the dense-output disk root.
+// (rt_trace.cu: single kernel, far/near passes, finish pass): ray generation,
+// termination records, the parked-ray format of the two-pass tracer, the
+// dense-output disk root and the translucent-disk continuation.
 //
 // The cold per-lane state is passed as any structure with the SoA arrays
 // lambda, dH, lz0, q0 and local, indexed by the caller's lane slot.
@@ -14,6 +14,7 @@
 
 #include "rt_device.cuh"
 #include "rt_internal.h"
+#include "rt_shade.cuh"
 
 namespace relsim {
 
@@ -35,17 +36,6 @@ struct Cold {
     double lo[BLOCK], hi[BLOCK], flo[BLOCK], fhi[BLOCK], troot[BLOCK];
     uint64_t local[BLOCK];
     int side[BLOCK], rit[BLOCK];
-};
-
-// The cold state the far and finish passes need (no root bracket), one entry
-// per ray slot.
-template <int SLOTS>
-struct ColdSlots {
-    double lambda[SLOTS];
-    double dH[SLOTS];
-    double lz0[SLOTS];
-    double q0[SLOTS];
-    uint64_t local[SLOTS];
 };
 
 // Carter constant with E = 1, mu = 0 (kerr_invariants.hpp:45-48); BL p_theta
@@ -347,6 +337,44 @@ __device__ __noinline__ double dense_disk_root(const double* __restrict__ y0, co
 #pragma unroll
     for (int i = 0; i < 6; ++i) out[i] = y0[i] + t * (d[i] + (1.0 - t) * (b[i] + t * (c[i] + (1.0 - t) * e[i])));
     return t;
+}
+
+// Shade a Kerr-Schild disk crossing at the root point yr (winding wind_root
+// along the ray) for the translucent-disk continuation (rt_shade.cuh).
+// Returns the throughput left.
+template <class ColdT>
+__device__ __forceinline__ double shade_crossing(const TraceArgs& args, const BundleDesc* __restrict__ Bp, ColdT& S,
+                                                 int j, uint32_t n_cross, const double* __restrict__ yr, int wind_root) {
+    const double a = Bp->a;
+    const double r = sqrt(bl_r2<double>(yr[0], yr[1], yr[2], a * a));
+    const double phi = atan2(yr[1], yr[0]) - atan2(a, r) + kTwoPi * static_cast<double>(wind_root);
+    return cont_crossing(*args.shade, args.cont, Bp->out_offset + S.local[j], n_cross, r, phi,
+                         disk_redshift(Bp->m, a, r, S.lz0[j]));
+}
+
+// End of a Kerr-Schild ray's trace with the continuation on; y its last point.
+template <class ColdT>
+__device__ __forceinline__ void end_continuation(const TraceArgs& args, const BundleDesc* __restrict__ Bp, ColdT& S,
+                                                 int j, uint32_t n_cross, uint32_t status, const double* __restrict__ y) {
+    cont_end(args.cont, args.out.pixels, Bp->out_offset + S.local[j], n_cross, status,
+             sqrt(bl_r2<double>(y[0], y[1], y[2], Bp->a * Bp->a)), Bp->m);
+}
+
+// A ray's end (capture, escape, unfinished): its record and pixel unless it
+// crossed the disk before (they describe the first hit, written then), and its
+// continuation outputs when the continuation is on.  xch as finish_ray takes
+// it; the ray's last point is xch[12..17] with interp_target > 0, else xch[0..5].
+template <bool CONT, class ColdT>
+__device__ __forceinline__ void end_ray(const TraceArgs& args, const BundleDesc* __restrict__ Bp, ColdT& S, int j,
+                                        uint32_t n_cross, uint32_t status, uint32_t flags, uint32_t acc, uint32_t rej,
+                                        int wind, double interp_target, double hh, const double* __restrict__ xch) {
+    if constexpr (CONT) {
+        if (n_cross == 0)
+            finish_ray(Bp, S, j, status, flags, acc, rej, wind, interp_target, hh, NAN, 1.0, args.out, xch);
+        end_continuation(args, Bp, S, j, n_cross, status, xch + (interp_target > 0.0 ? 12 : 0));
+    } else {
+        finish_ray(Bp, S, j, status, flags, acc, rej, wind, interp_target, hh, NAN, 1.0, args.out, xch);
+    }
 }
 
 // A ray in the near pass returns to the far pass once r_BL exceeds this

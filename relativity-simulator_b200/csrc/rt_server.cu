@@ -259,7 +259,7 @@ bool start_copy(rt_server* s, Request* r) {
             const uint64_t b = r->base;
             launch_shade(slot, static_cast<const uint32_t*>(s->field_base[0]) + b,
                          static_cast<const double*>(s->field_base[7]) + b, static_cast<const double*>(s->field_base[6]) + b,
-                         static_cast<const double*>(s->field_base[8]) + b, s->pixel_base + b, r->rays, cs);
+                         static_cast<const double*>(s->field_base[8]) + b, ContOut{}, s->pixel_base + b, r->rays, cs);
             e = cudaGetLastError();
             if (e != cudaSuccess) return fail_server(s, "shade launch", e), false;
         }

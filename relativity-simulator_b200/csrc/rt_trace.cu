@@ -224,7 +224,7 @@ __device__ __forceinline__ void fp64_stages_rolled(const double* __restrict__ y,
 // which rays share its warp.
 // Every form runs 12 warps per SM (168 registers); the pass kernels spill a
 // little there, which measured faster than 8 warps without spills.
-template <int BLOCK, bool MIXED, bool ROLLED, int PASS = PASS_SINGLE>
+template <int BLOCK, bool MIXED, bool ROLLED, int PASS = PASS_SINGLE, bool CONT = false>
 __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs args) {
     __shared__ Cold<BLOCK> S;
     __shared__ KStore<ROLLED ? BLOCK : 1> K;
@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     bool critical = false;  // near pass: a near-critical ray (FP64 to its end, tightened tolerance)
     bool k1_fp32 = false;  // k1 came from an FP32 far-zone stage (mixed mode)
     uint32_t guard = 0;    // loop iterations spent on the current ray
+    uint32_t n_cross = 0;  // disk crossings so far (translucent-disk continuation)
     uint64_t ray = 0;        // launch index of the lane's ray
 #pragma unroll
     for (int i = 0; i < 6; ++i) y[i] = k1[i] = 0.0;
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                     xch[6] = h;
                     const uint32_t misc =
                         (has_hist ? PM_HAS_HIST : 0u) | (static_cast<uint32_t>(can_early + 1) << PM_EARLY_SHIFT) |
-                        (critical ? PM_CRITICAL : 0u);
+                        (critical ? PM_CRITICAL : 0u) | (n_cross << PM_CROSS_SHIFT);
                     const uint32_t uch[PU_COUNT] = {acc, rej, flags, guard, static_cast<uint32_t>(wind), misc,
                                                     __float_as_uint(lnp)};
                     park_ray(args.park, ray, S, tid, xch, uch);
@@ -359,6 +360,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                             has_hist = (uch[PU_MISC] & PM_HAS_HIST) != 0u;
                             can_early = static_cast<int>((uch[PU_MISC] >> PM_EARLY_SHIFT) & 3u) - 1;
                             critical = (uch[PU_MISC] & PM_CRITICAL) != 0u;
+                            if constexpr (CONT) n_cross = (uch[PU_MISC] >> PM_CROSS_SHIFT) & 31u;
                             lnp = __uint_as_float(uch[PU_LNP]);
                             k1_fp32 = false;
                             mode = MODE_STEP;
@@ -384,6 +386,18 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                         wind = args.bundles[lo].wind0;
                         k1_fp32 = false;
                         guard = 0;
+                        n_cross = 0;
+                        critical = false;
+                        if constexpr (FAR_PASS) {
+                            if (args.opts & TO_CRITICAL_FP64) {
+                                // distance of the ray's constants from the critical curve; the
+                                // Carter early-capture decision comes from the same value
+                                const BundleDesc* Bc = args.bundles + lo;
+                                const double db = shadow_distance(Bc->m, Bc->a, 0.0, Bc->rh, S.lz0[tid], S.q0[tid]);
+                                if (can_early < 0) can_early = db > kEarlyCaptureMargin;
+                                critical = fabs(db) < static_cast<double>(args.critical_band) * Bc->m;
+                            }
+                        }
                         mode = MODE_STEP;
                         ++n_rays;
                         ++n_rhs;
@@ -427,7 +441,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
             double xch[6];
 #pragma unroll
             for (int i = 0; i < 6; ++i) xch[i] = y[i];
-            finish_ray(Bp, S, tid, RT_RAY_UNFINISHED, flags, acc, rej, wind, 0.0, 0.0, NAN, 1.0, args.out, xch);
+            end_ray<CONT>(args, Bp, S, tid, n_cross, RT_RAY_UNFINISHED, flags, acc, rej, wind, 0.0, 0.0, xch);
             mode = MODE_IDLE;
             continue;
         }
@@ -454,12 +468,12 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 double xch[6];
 #pragma unroll
                 for (int i = 0; i < 6; ++i) xch[i] = y[i];
-                finish_ray(Bp, S, tid, term & 15u, flags, acc, rej, wind, 0.0, 0.0, NAN, 1.0, args.out, xch);
+                end_ray<CONT>(args, Bp, S, tid, n_cross, term & 15u, flags, acc, rej, wind, 0.0, 0.0, xch);
                 mode = MODE_IDLE;
                 continue;
             }
             if constexpr (FAR_PASS) {
-                if (r < Bp->fp64_radius || r >= kFp32MaxRadius) {  // into the FP64 zone
+                if (critical || r < Bp->fp64_radius || r >= kFp32MaxRadius) {  // into the FP64 zone
                     mode = MODE_PARK;
                     continue;
                 }
@@ -568,16 +582,31 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
             if (done) {
                 const double rr = sqrt(bl_r2<double>(y5[0], y5[1], y5[2], a * a));
                 if (rr >= Bp->r_in && rr <= Bp->r_out && rr > Bp->rh * 1.02) {
-                    S.lambda[tid] += S.troot[tid] * h;
+                    // lambda at the root, one rounding in every kernel variant
+                    const double lambda_step = S.lambda[tid];
+                    S.lambda[tid] = fma(S.troot[tid], h, lambda_step);
                     double xch[18];
 #pragma unroll
                     for (int i = 0; i < 6; ++i) {
                         xch[i] = y[i];
                         xch[12 + i] = y5[i];
                     }
-                    finish_ray(Bp, S, tid, RT_RAY_DISK, flags, acc, rej, wind, 0.0, 0.0, rr,
-                                      disk_redshift(M, a, rr, S.lz0[tid]), args.out, xch);
+                    if (n_cross == 0)
+                        finish_ray(Bp, S, tid, RT_RAY_DISK, flags, acc, rej, wind, 0.0, 0.0, rr,
+                                   disk_redshift(M, a, rr, S.lz0[tid]), args.out, xch);
                     mode = MODE_IDLE;
+                    if constexpr (CONT) {
+                        // translucent disk: shade the crossing and go on through it
+                        const double thr = shade_crossing(args, Bp, S, tid, n_cross, y5,
+                                                          wind + branch_winding(y[0], y[1], y5[0], y5[1]));
+                        ++n_cross;
+                        if (thr > kMinThroughput && n_cross < kMaxCrossings) {
+                            S.lambda[tid] = lambda_step;
+                            mode = MODE_REDO;  // the full step again, accepted as it stands
+                        } else {
+                            end_continuation(args, Bp, S, tid, n_cross, RT_RAY_UNFINISHED, y5);
+                        }
+                    }
                 } else {
                     mode = MODE_REDO;  // not on the disk: take the full step again
                 }
@@ -640,8 +669,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 double xch[6];
 #pragma unroll
                 for (int i = 0; i < 6; ++i) xch[i] = y[i];
-                finish_ray(Bp, S, tid, RT_RAY_CAPTURED, flags, acc, rej, wind, 0.0, 0.0, NAN, 1.0, args.out,
-                                  xch);
+                end_ray<CONT>(args, Bp, S, tid, n_cross, RT_RAY_CAPTURED, flags, acc, rej, wind, 0.0, 0.0, xch);
                 mode = MODE_IDLE;
                 continue;
             }
@@ -660,15 +688,37 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                         const double t = dense_disk_root(y, k1, y5, kA, dense5, hh, xr + 12);
                         const double rr = sqrt(bl_r2<double>(xr[12], xr[13], xr[14], a * a));
                         if (rr >= Bp->r_in && rr <= Bp->r_out && rr > Bp->rh * 1.02) {
-                            // a disk hit: park the root point (r_hit in the step slot) for
-                            // the finish pass, which writes the record in lockstep
-                            S.lambda[tid] += t * hh;
-                            wind += branch_winding(y[0], y[1], xr[12], xr[13]);
+                            const int wroot = wind + branch_winding(y[0], y[1], xr[12], xr[13]);
+                            if constexpr (!CONT) {
+                                // a disk hit: park the root point (r_hit in the step slot) for
+                                // the finish pass, which writes the record in lockstep
+                                S.lambda[tid] = fma(t, hh, S.lambda[tid]);
+                                wind = wroot;
 #pragma unroll
-                            for (int i = 0; i < 6; ++i) y[i] = xr[12 + i];
-                            h = rr;
-                            mode = MODE_FINISHQ;
-                            continue;
+                                for (int i = 0; i < 6; ++i) y[i] = xr[12 + i];
+                                h = rr;
+                                mode = MODE_FINISHQ;
+                                continue;
+                            }
+                            // translucent disk: the first hit's record now, the crossing
+                            // shaded, and the step accepted as it stands
+                            if (n_cross == 0) {
+                                // finish_ray takes the root point in xr[0..5] and xr[12..17]
+#pragma unroll
+                                for (int i = 0; i < 6; ++i) xr[i] = xr[12 + i];
+                                const double lambda_step = S.lambda[tid];
+                                S.lambda[tid] = fma(t, hh, lambda_step);
+                                finish_ray(Bp, S, tid, RT_RAY_DISK, flags, acc, rej, wroot, 0.0, 0.0, rr,
+                                           disk_redshift(M, a, rr, S.lz0[tid]), args.out, xr);
+                                S.lambda[tid] = lambda_step;
+                            }
+                            const double thr = shade_crossing(args, Bp, S, tid, n_cross, xr + 12, wroot);
+                            ++n_cross;
+                            if (!(thr > kMinThroughput && n_cross < kMaxCrossings)) {
+                                end_continuation(args, Bp, S, tid, n_cross, RT_RAY_UNFINISHED, xr + 12);
+                                mode = MODE_IDLE;
+                                continue;
+                            }
                         }
                     } else {
                         mode = MODE_ROOT;
@@ -719,7 +769,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                     xch[12 + i] = y5[i];
                     xch[18 + i] = kA[i];
                 }
-                finish_ray(Bp, S, tid, term, flags, acc, rej, wind, target, hh, NAN, 1.0, args.out, xch);
+                end_ray<CONT>(args, Bp, S, tid, n_cross, term, flags, acc, rej, wind, target, hh, xch);
                 mode = MODE_IDLE;
                 continue;
             }
@@ -788,6 +838,8 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     }
 }
 
+// unshaded launches (CONT = false) and shaded ones that follow rays through the
+// translucent disk (CONT = true)
 template __global__ void trace_kernel_t<64, false, false>(TraceArgs);
 template __global__ void trace_kernel_t<128, false, false>(TraceArgs);
 template __global__ void trace_kernel_t<256, false, false>(TraceArgs);
@@ -799,25 +851,41 @@ template __global__ void trace_kernel_t<64, true, false, PASS_FAR>(TraceArgs);
 template __global__ void trace_kernel_t<128, true, false, PASS_FAR>(TraceArgs);
 template __global__ void trace_kernel_t<64, false, false, PASS_NEAR>(TraceArgs);
 template __global__ void trace_kernel_t<128, false, false, PASS_NEAR>(TraceArgs);
+template __global__ void trace_kernel_t<64, false, false, PASS_SINGLE, true>(TraceArgs);
+template __global__ void trace_kernel_t<128, false, false, PASS_SINGLE, true>(TraceArgs);
+template __global__ void trace_kernel_t<256, false, false, PASS_SINGLE, true>(TraceArgs);
+template __global__ void trace_kernel_t<64, false, true, PASS_SINGLE, true>(TraceArgs);
+template __global__ void trace_kernel_t<128, false, true, PASS_SINGLE, true>(TraceArgs);
+template __global__ void trace_kernel_t<64, true, true, PASS_SINGLE, true>(TraceArgs);
+template __global__ void trace_kernel_t<128, true, true, PASS_SINGLE, true>(TraceArgs);
+template __global__ void trace_kernel_t<64, true, false, PASS_FAR, true>(TraceArgs);
+template __global__ void trace_kernel_t<128, true, false, PASS_FAR, true>(TraceArgs);
+template __global__ void trace_kernel_t<64, false, false, PASS_NEAR, true>(TraceArgs);
+template __global__ void trace_kernel_t<128, false, false, PASS_NEAR, true>(TraceArgs);
 
 namespace {
 // Mixed precision always uses the rolled FP64 step (its FP64 steps are a
 // minority; the rolled form keeps the loop small).  Rolled kernels exist for
 // 64- and 128-thread blocks (their stage store is 36 KB of shared memory at 128).
-const void* kernel_for(uint32_t block, bool mixed, bool rolled) {
+template <bool CONT>
+const void* kernel_for_t(uint32_t block, bool mixed, bool rolled) {
     if (mixed) {
-        return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, true, true>)
-                             : reinterpret_cast<const void*>(&trace_kernel_t<128, true, true>);
+        return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, true, true, PASS_SINGLE, CONT>)
+                             : reinterpret_cast<const void*>(&trace_kernel_t<128, true, true, PASS_SINGLE, CONT>);
     }
     if (rolled) {
-        return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, false, true>)
-                             : reinterpret_cast<const void*>(&trace_kernel_t<128, false, true>);
+        return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, false, true, PASS_SINGLE, CONT>)
+                             : reinterpret_cast<const void*>(&trace_kernel_t<128, false, true, PASS_SINGLE, CONT>);
     }
     switch (block) {
-        case 64: return reinterpret_cast<const void*>(&trace_kernel_t<64, false, false>);
-        case 256: return reinterpret_cast<const void*>(&trace_kernel_t<256, false, false>);
-        default: return reinterpret_cast<const void*>(&trace_kernel_t<128, false, false>);
+        case 64: return reinterpret_cast<const void*>(&trace_kernel_t<64, false, false, PASS_SINGLE, CONT>);
+        case 256: return reinterpret_cast<const void*>(&trace_kernel_t<256, false, false, PASS_SINGLE, CONT>);
+        default: return reinterpret_cast<const void*>(&trace_kernel_t<128, false, false, PASS_SINGLE, CONT>);
     }
+}
+
+const void* kernel_for(uint32_t block, bool mixed, bool rolled, bool cont = false) {
+    return cont ? kernel_for_t<true>(block, mixed, rolled) : kernel_for_t<false>(block, mixed, rolled);
 }
 }  // namespace
 
@@ -870,11 +938,17 @@ __global__ void __launch_bounds__(BLOCK) finish_kernel_t(TraceArgs args) {
 }
 template __global__ void finish_kernel_t<128>(TraceArgs);
 
-const void* far_pair_kernel_for(uint32_t block, int warps_per_sm);  // rt_far.cu
-
 namespace {
-// far-pass form: 0 single-slot kernel, 2 two-slot kernel at 12 warps/SM, 3 at 8 warps/SM
-// near-critical rays to the FP64 near pass (paired far pass only): RELSIM_CRITICAL=1
+// Near-critical band of the mixed tracer (|d_b| / M); RELSIM_CRITICAL_BAND overrides it
+float critical_band() {
+    static const float b = [] {
+        const char* v = std::getenv("RELSIM_CRITICAL_BAND");
+        return v ? static_cast<float>(std::atof(v)) : static_cast<float>(kCriticalBand);
+    }();
+    return b;
+}
+
+// near-critical rays to the FP64 near pass: RELSIM_CRITICAL=1
 uint32_t trace_opts() {
     static const uint32_t o = [] {
         const char* v = std::getenv("RELSIM_CRITICAL");
@@ -883,21 +957,17 @@ uint32_t trace_opts() {
     return o;
 }
 
-int far_form() {
-    static const int form = [] {
-        const char* v = std::getenv("RELSIM_FAR_FORM");
-        return (v && v[0] >= '0' && v[0] <= '3') ? v[0] - '0' : 0;
-    }();
-    return form;
+template <bool CONT>
+const void* pass_kernel_t(int pass, uint32_t block) {
+    if (pass == PASS_FAR)
+        return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, true, false, PASS_FAR, CONT>)
+                             : reinterpret_cast<const void*>(&trace_kernel_t<128, true, false, PASS_FAR, CONT>);
+    return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, false, false, PASS_NEAR, CONT>)
+                         : reinterpret_cast<const void*>(&trace_kernel_t<128, false, false, PASS_NEAR, CONT>);
 }
 
-const void* pass_kernel(int pass, uint32_t block) {
-    if (pass == PASS_FAR && far_form() >= 2) return far_pair_kernel_for(block, far_form() == 3 ? 8 : 12);
-    if (pass == PASS_FAR)
-        return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, true, false, PASS_FAR>)
-                             : reinterpret_cast<const void*>(&trace_kernel_t<128, true, false, PASS_FAR>);
-    return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, false, false, PASS_NEAR>)
-                         : reinterpret_cast<const void*>(&trace_kernel_t<128, false, false, PASS_NEAR>);
+const void* pass_kernel(int pass, uint32_t block, bool cont = false) {
+    return cont ? pass_kernel_t<true>(pass, block) : pass_kernel_t<false>(pass, block);
 }
 }  // namespace
 
@@ -915,7 +985,8 @@ int trace_pass_occupancy(int pass, uint32_t block) {
 void launch_trace_pass(const TraceArgs& args, int pass, uint32_t grid, uint32_t block, void* stream) {
     void* params[] = {const_cast<TraceArgs*>(&args)};
     block = (block == 64) ? 64u : 128u;
-    cudaLaunchKernel(pass_kernel(pass, block), dim3(grid), dim3(block), params, 0, static_cast<cudaStream_t>(stream));
+    cudaLaunchKernel(pass_kernel(pass, block, args.shade != nullptr), dim3(grid), dim3(block), params, 0,
+                     static_cast<cudaStream_t>(stream));
 }
 
 // Rounds of the two-pass mixed tracer: far pass (FP32) then near pass (FP64),
@@ -955,6 +1026,7 @@ cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t beg
         args.refill_threshold = far_refill;
         args.from_pixels = (round == 0) ? 1u : 0u;
         args.opts = trace_opts();
+        args.critical_band = critical_band();
         args.allow_exit = 0;
         args.in_queue = far_q;
         args.in_count = reinterpret_cast<const uint32_t*>(qb + 12);
@@ -1034,7 +1106,7 @@ int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_co
 void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled, void* stream) {
     void* params[] = {const_cast<TraceArgs*>(&args)};
     block = kernel_block(block, mixed, rolled);
-    cudaLaunchKernel(kernel_for(block, mixed, rolled), dim3(grid), dim3(block), params, 0,
+    cudaLaunchKernel(kernel_for(block, mixed, rolled, args.shade != nullptr), dim3(grid), dim3(block), params, 0,
                      static_cast<cudaStream_t>(stream));
 }
 

@@ -2,7 +2,7 @@
 
     python relativity-simulator_b200/trace_once.py [--side 512] [--spin 0.94] [--r-obs 100]
         [--incl 17] [--fov 12] [--precision fp64|mixed] [--repeat 1]
-        [--metric ks|bl] [--charge 0] [--sources N]
+        [--metric ks|bl] [--charge 0] [--sources N] [--device] [--shade]
 """
 from __future__ import annotations
 
@@ -41,6 +41,10 @@ def main() -> None:
     ap.add_argument("--sources", type=int, default=0,
                     help="multi-source scene: the first request of the seeded stream with this many bodies beside "
                          "the camera's hole (its camera, at --side), traced by the multi-source tracer")
+    ap.add_argument("--device", action="store_true",
+                    help="device-resident outputs (rt_dispatch_device: one set of launches, no host bands)")
+    ap.add_argument("--shade", action="store_true",
+                    help="shade the pixels (rt_set_shading defaults): rays are followed through the translucent disk")
     ap.add_argument("--record", choices=["minimal", "bench"], default="minimal",
                     help="outputs written: class and step counts, or the bench's record (class, r, theta, "
                          "phi, r_hit, g) plus the 32-byte pixels")
@@ -61,8 +65,21 @@ def main() -> None:
         srcs = scenes.rt_sources(req.sources)
     with relsim.Tracer(0) as tr:
         tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread, a.fp64_rolled, a.mixed_single)
+        if a.shade:
+            tr.set_shading(relsim.shading())
+        dev = None
+        if a.device:
+            import torch
+
+            n = cam.screen_width * cam.screen_height
+            fields = ["status", "r", "theta", "phi", "r_hit", "g"] if a.record == "bench" else ["status"]
+            dev = relsim.device_ray_out(n, fields) + (torch.empty(n * 32, dtype=torch.uint8, device="cuda"),)
         for _ in range(a.repeat):
-            if srcs is not None:
+            if dev is not None:
+                tr.dispatch_device(cam, dev[0], dev[2].data_ptr(), cam.screen_width * cam.screen_height)
+                tr.synchronize()
+                out = {"status": dev[1]["status"].cpu().numpy().view(np.uint32)}
+            elif srcs is not None:
                 out = tr.dispatch_multi(cam, srcs, fields=["status", "steps_accepted", "steps_rejected"],
                                         pixels=False)
             elif a.record == "bench":

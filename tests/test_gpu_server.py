@@ -149,19 +149,20 @@ def test_multi_source_request_matches_direct_trace(tracer):
 
 def test_shaded_requests_match_shaded_dispatch(tracer):
     """With rt_server_set_shading, a finished single-hole request's pixels are
-    shaded (disk colour, tonemapping) exactly as a shaded rt_dispatch of the same
-    camera; a multi-source request keeps black pixels; a server that does not
-    record the fields the shading reads refuses it."""
+    shaded (disk colour, tonemapping) at the first disk crossing -- the
+    server's epochs hold no translucent-disk continuation -- as the shading
+    oracle shades the request's own record, within 1e-6 sRGB; the rest of each
+    pixel equals an unshaded rt_dispatch of the same camera; a multi-source
+    request keeps black pixels; a server that does not record the fields the
+    shading reads refuses it."""
+    from test_gpu_shading import oracle_pixels
+
     sh = relsim.shading(tonemapping_mode=1, hydro_model=1)
     cams = [config_cam("c2", width=128, height=96, precision=relsim.PRECISION_MIXED),
             relsim.make_camera(spin=0.9, r_obs=50.0, incl_deg=75.0, fov_deg=30.0, width=96, height=64,
                                metric_form=relsim.METRIC_BOYER_LINDQUIST, charge=0.3)]
     tracer.set_launch_config()
-    tracer.set_shading(sh)
-    try:
-        ref = [tracer.dispatch(c, fields=list(FIELDS), pixels=True) for c in cams]
-    finally:
-        tracer.set_shading(None)
+    ref = [tracer.dispatch(c, fields=list(FIELDS), pixels=True) for c in cams]
     req = [r for r in scenes.request_stream() if r.multi_source][0]
     mcam = req.bundle.camera(relsim.PRECISION_FP64)
     mcam.screen_width = mcam.screen_height = 32
@@ -170,9 +171,15 @@ def test_shaded_requests_match_shaded_dispatch(tracer):
         subs = [srv.submit(c, FIELDS, pixels=True) for c in cams]
         mid, mout = srv.submit(mcam, FIELDS, pixels=True, sources=scenes.rt_sources(req.sources))
         done = srv.wait([i for i, _ in subs] + [mid])
-    for (rid, out), r in zip(subs, ref):
+    for (rid, out), r, c in zip(subs, ref, cams):
         assert done[rid].status == relsim.RT_OK
-        assert np.array_equal(out["pixels"], r["pixels"])
+        for f in ("status", "r_hit", "phi", "g"):
+            assert np.array_equal(out[f], r[f], equal_nan=(out[f].dtype.kind == "f")), f
+        want = oracle_pixels(c, sh, out["status"], out["r_hit"], out["phi"], out["g"])
+        rgb = np.stack([out["pixels"]["r"], out["pixels"]["g"], out["pixels"]["b"]], 1)
+        assert np.abs(rgb - want).max() < 1e-6
+        for f in ("a", "redshift", "affine_parameter", "status_flags", "iterations_used"):
+            assert np.array_equal(out["pixels"][f], r["pixels"][f]), f
         assert out["pixels"]["r"].max() > 0.0
     assert done[mid].status == relsim.RT_OK
     assert np.all(mout["pixels"]["r"] == 0.0) and np.all(mout["pixels"]["a"] == 1.0)
