@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define RT_ABI_VERSION 3
+#define RT_ABI_VERSION 4
 
 typedef enum rt_status {
     RT_OK = 0,
@@ -110,6 +110,10 @@ typedef struct rt_camera {
     double projection_tol;       /* project onto H = 0 when |H| >= tol */
     double mixed_fp64_radius;    /* MIXED: FP64 stages inside this r_BL (<= 0: max(3 r_+, 5 M)) */
     double metric_charge;        /* Q (G = c = k_e = 1), RT_METRIC_BOYER_LINDQUIST only */
+    double mixed_critical_band;  /* MIXED: a ray whose constants lie within this distance (M, in impact
+                                    parameter) of the critical curve orbits the photon region, where step
+                                    errors grow about as 1/distance; it is traced in FP64 at a hundredth of
+                                    rtol and atol from its first step (0: 1 M; < 0: none) */
     uint32_t screen_width;
     uint32_t screen_height;
     uint32_t max_integration_steps; /* step attempts per ray, accepted + rejected */

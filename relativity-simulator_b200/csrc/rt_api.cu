@@ -52,10 +52,9 @@ struct rt_handle {
     DevBuf band_desc, band_queue;        // banded single-kernel host dispatches: per-band camera and counter
     DevBuf shade_desc;                   // pixel shading constants of the last shaded camera
     bool shade_on = false;               // rt_set_shading
-    // translucent-disk continuation of a shaded Kerr-Schild dispatch: accumulated
-    // radiance, throughput and last g per ray, and what the launches pass the tracer
-    DevBuf cont;
-    const ShadeDesc* cur_shade = nullptr;
+    // translucent-disk continuation of a shaded dispatch: each ray's disk crossings
+    // and how it ended, and what the launches pass the tracer
+    DevBuf cont_cross, cont_info;
     ContOut cur_cont{};
     rt_shading shading{};
     DevBuf ray_fields[kRayFields];
@@ -161,6 +160,7 @@ bool camera_valid(const rt_camera* c) {
            c->step_cap_fraction > 0.0 && c->initial_step_fraction > 0.0 && c->capture_scale >= 1.0 &&
            c->max_integration_steps > 0 && std::isfinite(c->observer_position[1]) &&
            std::isfinite(c->observer_position[2]) && std::isfinite(c->observer_position[3]) &&
+           !std::isnan(c->mixed_critical_band) &&
            (c->precision_mode == RT_PRECISION_FP64 || c->precision_mode == RT_PRECISION_MIXED);
 }
 
@@ -198,7 +198,6 @@ rt_status launch_two_pass(rt_handle* h, uint32_t n_bundles, uint64_t total, cons
     args.total_rays = total;
     args.stats = static_cast<unsigned long long*>(h->stats.ptr);
     args.out = out;
-    args.shade = h->cur_shade;
     args.cont = h->cur_cont;
     TwoPassBuffers buf{};
     buf.park = ParkBuf{static_cast<double*>(h->park_d.ptr), static_cast<uint32_t*>(h->park_u.ptr), total};
@@ -234,7 +233,6 @@ rt_status launch(rt_handle* h, uint32_t n_bundles, uint64_t total, const OutPtrs
     args.queue = static_cast<unsigned long long*>(h->queue.ptr);
     args.stats = static_cast<unsigned long long*>(h->stats.ptr);
     args.out = out;
-    args.shade = h->cur_shade;
     args.cont = h->cur_cont;
     RT_CUDA(h, cudaMemsetAsync(h->queue.ptr, 0, sizeof(unsigned long long), s));
     RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
@@ -322,21 +320,18 @@ rt_status shade_prepare(rt_handle* h, const rt_camera* cam, cudaStream_t s) {
     return RT_OK;
 }
 
-// Turn on the translucent-disk continuation for the Kerr-Schild launches of a
-// shaded dispatch of n rays (the shading constants already uploaded): the
-// tracers shade each disk crossing and follow the ray on through the disk.
+// Turn on the translucent-disk continuation for the launches of a shaded
+// dispatch of n rays: the tracers record each disk crossing and follow the ray
+// on through the disk; the shading pass composes the crossings.
 rt_status begin_continuation(rt_handle* h, size_t n) {
-    const rt_status st = ensure(h, h->cont, sizeof(double) * CF_COUNT * n);
+    rt_status st = ensure(h, h->cont_cross, sizeof(double) * 3 * kMaxCrossings * n);
+    if (st == RT_OK) st = ensure(h, h->cont_info, sizeof(uint32_t) * n);
     if (st != RT_OK) return st;
-    h->cur_shade = static_cast<const ShadeDesc*>(h->shade_desc.ptr);
-    h->cur_cont = ContOut{static_cast<double*>(h->cont.ptr), n};
+    h->cur_cont = ContOut{static_cast<double*>(h->cont_cross.ptr), static_cast<uint32_t*>(h->cont_info.ptr), n};
     return RT_OK;
 }
 
-void end_continuation_state(rt_handle* h) {
-    h->cur_shade = nullptr;
-    h->cur_cont = ContOut{};
-}
+void end_continuation_state(rt_handle* h) { h->cur_cont = ContOut{}; }
 
 // Turns the continuation off when a dispatch returns, on every path.
 struct ContinuationScope {
@@ -377,7 +372,8 @@ int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
     const uint64_t o = c.offset + begin;
     if (c.shade && c.dpix) {
         launch_shade(static_cast<const ShadeDesc*>(c.h->shade_desc.ptr), c.dev.status + o, c.dev.r_hit + o,
-                     c.dev.phi + o, c.dev.g + o, ContOut{c.cont.rgb ? c.cont.rgb + o : nullptr, c.cont.stride},
+                     c.dev.phi + o, c.dev.g + o,
+                     c.cont.cross ? ContOut{c.cont.cross + o, c.cont.info + o, c.cont.stride} : ContOut{},
                      c.dpix + o, count, s);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return static_cast<int>(e);
@@ -548,7 +544,6 @@ rt_status bl_launch(rt_handle* h, const rt_camera* cam, uint32_t col0, uint32_t 
     args.queue = static_cast<unsigned long long*>(h->queue.ptr);
     args.stats = static_cast<unsigned long long*>(h->stats.ptr);
     args.out = out;
-    args.shade = h->cur_shade;
     args.cont = h->cur_cont;
     RT_CUDA(h, cudaEventRecord(h->ev0, s));
     launch_bl_trace(args, bl_trace_grid(h->sm_count), s);
@@ -603,7 +598,6 @@ rt_status launch_banded_single(rt_handle* h, const rt_camera* cam, uint32_t col0
             args.queue = q;
             args.stats = static_cast<unsigned long long*>(h->stats.ptr);
             args.out = out;
-            args.shade = h->cur_shade;
             args.cont = h->cur_cont;
             launch_bl_trace(args, bl_trace_grid(h->sm_count), sb);
         } else {
@@ -619,7 +613,6 @@ rt_status launch_banded_single(rt_handle* h, const rt_camera* cam, uint32_t col0
             args.queue = q;
             args.stats = static_cast<unsigned long long*>(h->stats.ptr);
             args.out = out;
-            args.shade = h->cur_shade;
             args.cont = h->cur_cont;
             launch_trace(args, static_cast<uint32_t>(h->sm_count) * c.ctas_per_sm, c.block_size, mixed,
                          c.fp64_rolled != 0, sb);
@@ -788,6 +781,7 @@ void rt_camera_defaults(rt_camera* c) {
     c->initial_step_fraction = 0.01;
     c->projection_tol = 1e-12;
     c->mixed_fp64_radius = 0.0;
+    c->mixed_critical_band = 0.0;
     c->screen_width = 2048;
     c->screen_height = 2048;
     c->max_integration_steps = 20000;

@@ -515,8 +515,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
         }
         if (term) {
             if (n_cross == 0) bl_finish<BLOCK>(Bp, S, tid, y, term & 15u, flags, acc, rej, NAN, 1.0, args.out);
-            if (args.cont.rgb)
-                cont_end(args.cont, args.out.pixels, B.out_offset + S.local[tid], n_cross, term & 15u, y[0], B.m);
+            if (args.cont.cross) cont_finish(args.cont, B.out_offset + S.local[tid], n_cross, term & 15u, y[0], B.m);
             mode = BL_IDLE;
             continue;
         }
@@ -547,8 +546,8 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
             if (n_cross == 0)
                 bl_finish<BLOCK>(Bp, S, tid, y, RT_RAY_CAPTURED, flags | RT_RAYFLAG_NONFINITE, acc, rej, NAN, 1.0,
                                  args.out);
-            if (args.cont.rgb)
-                cont_end(args.cont, args.out.pixels, B.out_offset + S.local[tid], n_cross, RT_RAY_CAPTURED, y[0], B.m);
+            if (args.cont.cross)
+                cont_finish(args.cont, B.out_offset + S.local[tid], n_cross, RT_RAY_CAPTURED, y[0], B.m);
             mode = BL_IDLE;
             continue;
         }
@@ -579,18 +578,18 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
                             S.lambda[tid] = lambda_step;
                         }
                         mode = BL_IDLE;
-                        if (!args.shade) continue;
-                        // translucent disk: shade the crossing (at the record's azimuth,
+                        if (!args.cont.cross) continue;
+                        // translucent disk: record the crossing (at the record's azimuth,
                         // that of the reflected root point) and go on through it
                         double yp[NB];
 #pragma unroll
                         for (int i = 0; i < NB; ++i) yp[i] = yr[i];
                         bl_reflect(yp, nullptr);
                         const uint64_t o = B.out_offset + S.local[tid];
-                        const double thr = cont_crossing(*args.shade, args.cont, o, n_cross, rr, yp[2], g);
+                        cont_record(args.cont, o, n_cross, rr, yp[2], g);
                         ++n_cross;
-                        if (!(thr > kMinThroughput && n_cross < kMaxCrossings)) {
-                            cont_end(args.cont, args.out.pixels, o, n_cross, RT_RAY_UNFINISHED, rr, B.m);
+                        if (n_cross >= kMaxCrossings) {
+                            cont_finish(args.cont, o, n_cross, RT_RAY_UNFINISHED, rr, B.m);
                             continue;
                         }
                         mode = BL_STEP;
@@ -639,8 +638,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
                     S.lambda[tid] += hh;
                 }
                 if (n_cross == 0) bl_finish<BLOCK>(Bp, S, tid, yt, tterm, flags, acc, rej, NAN, 1.0, args.out);
-                if (args.cont.rgb)
-                    cont_end(args.cont, args.out.pixels, B.out_offset + S.local[tid], n_cross, tterm, yt[0], B.m);
+                if (args.cont.cross) cont_finish(args.cont, B.out_offset + S.local[tid], n_cross, tterm, yt[0], B.m);
                 mode = BL_IDLE;
                 continue;
             }

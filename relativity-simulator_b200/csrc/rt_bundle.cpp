@@ -127,6 +127,9 @@ void build_bundle(const rt_camera& cam, uint32_t col0, uint32_t ncols, uint32_t 
     b.h0 = cam.initial_step_fraction * r_obs;
     b.proj_tol = cam.projection_tol;
     b.fp64_radius = (cam.mixed_fp64_radius > 0.0) ? cam.mixed_fp64_radius : std::max(3.0 * rh, 5.0 * m);
+    b.critical_band = (cam.mixed_critical_band < 0.0)   ? 0.0f
+                      : (cam.mixed_critical_band > 0.0) ? static_cast<float>(cam.mixed_critical_band)
+                                                        : kDefaultCriticalBand;
     b.flags = (disk ? BF_DISK : 0u) | (cam.early_capture ? BF_EARLY_CAPTURE : 0u) |
               (cam.precision_mode == RT_PRECISION_MIXED ? BF_MIXED : 0u);
 }

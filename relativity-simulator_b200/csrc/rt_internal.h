@@ -21,6 +21,13 @@ enum : uint32_t {
     BF_MIXED = 1u << 2          // mixed-precision stages
 };
 
+// Mixed mode: the near-critical band (M, distance of a ray's constants from
+// the critical curve) of a camera that does not set one.  Rays inside it are
+// traced in FP64 at a tightened tolerance from their first step; measured on
+// the 512-bundle table, a band of 1 M keeps every disk radius within 1e-6 of
+// the FP64 tracer's.
+constexpr float kDefaultCriticalBand = 1.0f;
+
 // Per-camera constants, precomputed once on the host in FP64 (the same
 // operations the reference performs per pixel that do not depend on the pixel:
 // software_compute_engine.hpp:3790-3803 and :3902-3912, the observer's
@@ -46,7 +53,7 @@ struct alignas(16) BundleDesc {
     double phi_start;       // unwrapped azimuth at the observer
     double raw_phi0;        // atan2(y, x) - atan2(a, r) at the observer
     int32_t wind0;          // phi_start = raw_phi0 + 2 pi wind0
-    int32_t pad0;
+    float critical_band;    // mixed mode: near-critical band in M (<= 0: none)
     // metric and integration
     double m, a, rh;
     double r_capture, r_esc, r_in, r_out, r_early;
@@ -61,12 +68,20 @@ struct OutPtrs {
 };
 
 // Translucent-disk continuation outputs (structure of arrays, `stride`
-// elements each, indexed like the record): the radiance accumulated over the
-// ray's disk crossings (r, g, b), the throughput left, and the redshift of the
-// last crossing.  rgb == nullptr: the tracer ends a ray at its first disk hit.
-enum ContField : int { CF_R = 0, CF_G, CF_B, CF_THROUGHPUT, CF_LAST_G, CF_COUNT };
+// elements each, indexed like the record): the tracer records each disk
+// crossing k < kMaxCrossings of a ray (r, phi, g at the crossing), and in
+// info how many crossings it recorded, the class the ray ended with and
+// whether its last point lay inside 3 r_s; the shading pass composes the
+// pixel from them.  cross == nullptr: the tracer ends a ray at its first hit.
+constexpr uint32_t kMaxCrossings = 8;
+enum : uint32_t {
+    CI_COUNT_MASK = 0xffu,  // bits 0..7: crossings recorded
+    CI_FATE_SHIFT = 8u,     // bits 8..11: RT_RAY_* class at the ray's end
+    CI_INSIDE_3RS = 1u << 12  // last point inside 3 r_s (6 M)
+};
 struct ContOut {
-    double* rgb;      // [CF_COUNT][stride]
+    double* cross;    // [3 * kMaxCrossings][stride]: r_k at [3k], phi_k at [3k + 1], g_k at [3k + 2]
+    uint32_t* info;   // [stride]
     uint64_t stride;
 };
 
@@ -96,19 +111,12 @@ struct ParkBuf {
 // near-zone pass; rays move between them through queues of launch indices.
 enum TracePass : int { PASS_SINGLE = 0, PASS_FAR = 1, PASS_NEAR = 2 };
 
-struct ShadeDesc;
-
-// TraceArgs.opts
-enum : uint32_t {
-    TO_CRITICAL_FP64 = 1u  // far pass: near-critical rays go to the FP64 near pass at their first step
-};
-
 struct TraceArgs {
     const BundleDesc* bundles;
     uint32_t n_bundles;
     uint32_t refill_threshold;
     uint32_t claim;             // rays a warp claims per global atomic
-    uint32_t opts;              // TO_* bits
+    uint32_t pad;
     uint64_t total_rays;
     unsigned long long* queue;  // [0]: next unclaimed ray (or queue entry)
     unsigned long long* stats;  // [ST_COUNT]
@@ -125,10 +133,8 @@ struct TraceArgs {
     uint32_t* finish_count;
     ParkBuf park;
     // translucent-disk continuation (single-camera launches with shading): the
-    // camera's shading constants and the continuation outputs; null: off
-    const ShadeDesc* shade;
+    // crossings' outputs; cross null: off
     ContOut cont;
-    float critical_band;        // TO_CRITICAL_FP64: |d_b| / M below which a ray is near-critical
 };
 
 // Multi-source Kerr-Schild superposition: per-source frame (source 0 is the
@@ -198,9 +204,8 @@ struct BlArgs {
     unsigned long long* queue;
     unsigned long long* stats;
     OutPtrs out;
-    // translucent-disk continuation (shaded dispatches): shading constants and
-    // continuation outputs; null: off
-    const ShadeDesc* shade;
+    // translucent-disk continuation (shaded dispatches): the crossings' outputs;
+    // cross null: off
     ContOut cont;
 };
 

@@ -339,25 +339,24 @@ __device__ __noinline__ double dense_disk_root(const double* __restrict__ y0, co
     return t;
 }
 
-// Shade a Kerr-Schild disk crossing at the root point yr (winding wind_root
-// along the ray) for the translucent-disk continuation (rt_shade.cuh).
-// Returns the throughput left.
+// Record crossing k of a Kerr-Schild ray at the root point yr (winding
+// wind_root along the ray) for the translucent-disk continuation: r_BL, the
+// unwrapped azimuth and g, as the first hit's record has them.
 template <class ColdT>
-__device__ __forceinline__ double shade_crossing(const TraceArgs& args, const BundleDesc* __restrict__ Bp, ColdT& S,
-                                                 int j, uint32_t n_cross, const double* __restrict__ yr, int wind_root) {
+__device__ __forceinline__ void record_crossing(const TraceArgs& args, const BundleDesc* __restrict__ Bp, ColdT& S,
+                                                int j, uint32_t k, const double* __restrict__ yr, int wind_root) {
     const double a = Bp->a;
     const double r = sqrt(bl_r2<double>(yr[0], yr[1], yr[2], a * a));
     const double phi = atan2(yr[1], yr[0]) - atan2(a, r) + kTwoPi * static_cast<double>(wind_root);
-    return cont_crossing(*args.shade, args.cont, Bp->out_offset + S.local[j], n_cross, r, phi,
-                         disk_redshift(Bp->m, a, r, S.lz0[j]));
+    cont_record(args.cont, Bp->out_offset + S.local[j], k, r, phi, disk_redshift(Bp->m, a, r, S.lz0[j]));
 }
 
 // End of a Kerr-Schild ray's trace with the continuation on; y its last point.
 template <class ColdT>
 __device__ __forceinline__ void end_continuation(const TraceArgs& args, const BundleDesc* __restrict__ Bp, ColdT& S,
                                                  int j, uint32_t n_cross, uint32_t status, const double* __restrict__ y) {
-    cont_end(args.cont, args.out.pixels, Bp->out_offset + S.local[j], n_cross, status,
-             sqrt(bl_r2<double>(y[0], y[1], y[2], Bp->a * Bp->a)), Bp->m);
+    cont_finish(args.cont, Bp->out_offset + S.local[j], n_cross, status,
+                sqrt(bl_r2<double>(y[0], y[1], y[2], Bp->a * Bp->a)), Bp->m);
 }
 
 // A ray's end (capture, escape, unfinished): its record and pixel unless it
@@ -382,12 +381,11 @@ __device__ __forceinline__ void end_ray(const TraceArgs& args, const BundleDesc*
 constexpr double kNearExitFactor = 1.25;
 
 // Near-critical rays of the mixed tracer: a ray whose impact parameter lies
-// within kCriticalBand M of the critical curve (|d_b| from the Kerr radial
-// potential, shadow_distance) orbits the photon region, where any step error
-// is amplified about as 1/|d_b|.  The mixed tracer sends such a ray to the
-// FP64 near pass at its first step and keeps it there to its end, at the
-// camera's tolerance times kCriticalTolScale.
-constexpr double kCriticalBand = 0.05;
+// within the camera's band (BundleDesc::critical_band, M) of the critical
+// curve (|d_b| from the Kerr radial potential, shadow_distance) orbits the
+// photon region, where any step error is amplified about as 1/|d_b|.  The
+// far pass sends such a ray to the FP64 near pass at its first step, which
+// keeps it to its end at the camera's tolerance times kCriticalTolScale.
 constexpr double kCriticalTolScale = 1e-2;
 
 // Largest r_BL at which the FP32 stages are used (keeps r^4 and 1/r^4 in range).

@@ -63,14 +63,42 @@ __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict_
     const ShadeDesc& D = *Dp;
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        if (cont.rgb) {
-            // translucent-disk continuation: the tracer accumulated the crossings
-            acc[0] = cont.rgb[i];
-            acc[1] = cont.rgb[cont.stride + i];
-            acc[2] = cont.rgb[2 * cont.stride + i];
+        double acc[3] = {0.0, 0.0, 0.0};
+        if (cont.cross) {
+            // translucent disk (software_compute_engine.hpp:1660, 1743-1796): the
+            // crossings in order, each at the throughput left, while more than 0.01
+            // is left; the pixel's redshift is the last crossing's and its flags add
+            // the way the ray ended, if the throughput lasted to the end
+            const uint32_t info = cont.info[i];
+            const uint32_t n_cross = info & CI_COUNT_MASK;
+            double thr = 1.0, last_g = 1.0;
+            for (uint32_t k = 0; k < n_cross && thr > kMinThroughput; ++k) {
+                double sh[4];
+                const double gk = cont.cross[(3 * k + 2) * cont.stride + i];
+                disk_radiance(D, cont.cross[(3 * k) * cont.stride + i], cont.cross[(3 * k + 1) * cont.stride + i], gk,
+                              sh);
+                acc[0] += thr * sh[0];
+                acc[1] += thr * sh[1];
+                acc[2] += thr * sh[2];
+                thr *= 1.0 - sh[3];
+                last_g = gk;
+            }
+            if (n_cross > 0) {
+                const uint32_t fate = (info >> CI_FATE_SHIFT) & 15u;
+                uint32_t add = 0;
+                if (thr > kMinThroughput) {
+                    if (fate == RT_RAY_CAPTURED) add = RT_PIXEL_HORIZON_ABSORBED;
+                    else if (fate == RT_RAY_ESCAPED || !(info & CI_INSIDE_3RS)) add = RT_PIXEL_CELESTIAL_HIT;
+                }
+                pixels[i].status_flags |= add;
+                pixels[i].redshift = static_cast<float>(last_g);
+            }
         } else if (status[i] == RT_RAY_DISK) {
-            disk_radiance(D, r_hit[i], phi[i], g[i], acc);
+            double sh[4];
+            disk_radiance(D, r_hit[i], phi[i], g[i], sh);
+            acc[0] = sh[0];
+            acc[1] = sh[1];
+            acc[2] = sh[2];
         }
         // apply_tonemapping (software_compute_engine.hpp:3461-3516)
         const double k = exp2(D.exposure);

@@ -224,60 +224,25 @@ __device__ __noinline__ void disk_radiance(const ShadeDesc& D, double radius_in,
 // (software_compute_engine.hpp:1660, 1743-1765): each crossing adds the disk's
 // radiance at the throughput left and lowers the throughput by the crossing's
 // opacity, and the ray goes on while the throughput exceeds 0.01 (the loop
-// condition there), to its capture or escape.  The tracers record the first
-// hit as before and follow a ray for at most kMaxCrossings crossings; the
-// accumulated radiance, the throughput left and the last crossing's g go to
-// the continuation outputs (ContOut), which the shading pass tonemaps.
-constexpr uint32_t kMaxCrossings = 8;
+// condition there), to its capture or escape.  The tracers record each
+// crossing (cont_record) and the ray's end (cont_finish) and follow a ray for
+// at most kMaxCrossings crossings; the shading pass shades the crossings in
+// order with the throughput rule, in parallel over rays (shading a crossing
+// where it is found would run it one lane at a time while the warp waits).
 constexpr double kMinThroughput = 0.01;
 
-// Shade one crossing at (r, phi, g) into element o of the continuation outputs
-// (set up at the ray's first crossing, n_cross == 0).  Returns the throughput left.
-__device__ __noinline__ double cont_crossing(const ShadeDesc& D, const ContOut& C, uint64_t o, uint32_t n_cross,
-                                             double r, double phi, double g) {
-    double sh[4];
-    disk_radiance(D, r, phi, g, sh);
-    const uint64_t st = C.stride;
-    double* c = C.rgb;
-    const double t = (n_cross == 0) ? 1.0 : c[CF_THROUGHPUT * st + o];
-    const double r0 = (n_cross == 0) ? 0.0 : c[CF_R * st + o];
-    const double g0 = (n_cross == 0) ? 0.0 : c[CF_G * st + o];
-    const double b0 = (n_cross == 0) ? 0.0 : c[CF_B * st + o];
-    c[CF_R * st + o] = r0 + t * sh[0];
-    c[CF_G * st + o] = g0 + t * sh[1];
-    c[CF_B * st + o] = b0 + t * sh[2];
-    const double left = t * (1.0 - sh[3]);
-    c[CF_THROUGHPUT * st + o] = left;
-    c[CF_LAST_G * st + o] = g;
-    return left;
+__device__ __forceinline__ void cont_record(const ContOut& C, uint64_t o, uint32_t k, double r, double phi,
+                                            double g) {
+    C.cross[(3 * k) * C.stride + o] = r;
+    C.cross[(3 * k + 1) * C.stride + o] = phi;
+    C.cross[(3 * k + 2) * C.stride + o] = g;
 }
 
-// End of a ray's trace with the continuation on.  A ray that never crossed the
-// disk gets empty continuation outputs; for one that did, its pixel's flags
-// gain the way the ray ended (the record and pixel of the first hit were
-// written at the crossing) and its redshift becomes the last crossing's:
-// absorbed at the horizon, or the sky branch -- escaped, or throughput left
-// above 0.01 outside 3 r_s = 6 M (software_compute_engine.hpp:1660-1673,
-// 1768-1796).  status: the class at the end (UNFINISHED also when the
-// throughput ran out); r_last: r_BL of the last point.
-__device__ __noinline__ void cont_end(const ContOut& C, rt_pixel_out* pixels, uint64_t o, uint32_t n_cross,
-                                      uint32_t status, double r_last, double m) {
-    const uint64_t st = C.stride;
-    double* c = C.rgb;
-    if (n_cross == 0) {
-        c[CF_R * st + o] = c[CF_G * st + o] = c[CF_B * st + o] = 0.0;
-        c[CF_THROUGHPUT * st + o] = 1.0;
-        c[CF_LAST_G * st + o] = 1.0;
-        return;
-    }
-    if (!pixels) return;
-    uint32_t add = 0;
-    if (status == RT_RAY_CAPTURED) add = RT_PIXEL_HORIZON_ABSORBED;
-    else if (status == RT_RAY_ESCAPED) add = RT_PIXEL_CELESTIAL_HIT;
-    else if (c[CF_THROUGHPUT * st + o] > kMinThroughput && !(r_last < 6.0 * m)) add = RT_PIXEL_CELESTIAL_HIT;
-    rt_pixel_out& px = pixels[o];
-    px.status_flags |= add;
-    px.redshift = static_cast<float>(c[CF_LAST_G * st + o]);
+// End of a ray's trace: crossings recorded, its class at the end (UNFINISHED
+// also when it stopped at kMaxCrossings) and whether r_last lies inside 3 r_s.
+__device__ __forceinline__ void cont_finish(const ContOut& C, uint64_t o, uint32_t n_cross, uint32_t status,
+                                            double r_last, double m) {
+    C.info[o] = n_cross | (status << CI_FATE_SHIFT) | ((r_last < 6.0 * m) ? CI_INSIDE_3RS : 0u);
 }
 
 }  // namespace

@@ -36,7 +36,6 @@
 
 #include <cmath>
 #include <cstdint>
-#include <cstdlib>
 
 #include "rt_device.cuh"
 #include "rt_internal.h"
@@ -389,13 +388,13 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                         n_cross = 0;
                         critical = false;
                         if constexpr (FAR_PASS) {
-                            if (args.opts & TO_CRITICAL_FP64) {
+                            const BundleDesc* Bc = args.bundles + lo;
+                            if (Bc->critical_band > 0.0f) {
                                 // distance of the ray's constants from the critical curve; the
                                 // Carter early-capture decision comes from the same value
-                                const BundleDesc* Bc = args.bundles + lo;
                                 const double db = shadow_distance(Bc->m, Bc->a, 0.0, Bc->rh, S.lz0[tid], S.q0[tid]);
                                 if (can_early < 0) can_early = db > kEarlyCaptureMargin;
-                                critical = fabs(db) < static_cast<double>(args.critical_band) * Bc->m;
+                                critical = fabs(db) < static_cast<double>(Bc->critical_band) * Bc->m;
                             }
                         }
                         mode = MODE_STEP;
@@ -596,11 +595,11 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                                    disk_redshift(M, a, rr, S.lz0[tid]), args.out, xch);
                     mode = MODE_IDLE;
                     if constexpr (CONT) {
-                        // translucent disk: shade the crossing and go on through it
-                        const double thr = shade_crossing(args, Bp, S, tid, n_cross, y5,
-                                                          wind + branch_winding(y[0], y[1], y5[0], y5[1]));
+                        // translucent disk: record the crossing and go on through it
+                        record_crossing(args, Bp, S, tid, n_cross, y5,
+                                        wind + branch_winding(y[0], y[1], y5[0], y5[1]));
                         ++n_cross;
-                        if (thr > kMinThroughput && n_cross < kMaxCrossings) {
+                        if (n_cross < kMaxCrossings) {
                             S.lambda[tid] = lambda_step;
                             mode = MODE_REDO;  // the full step again, accepted as it stands
                         } else {
@@ -701,7 +700,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                                 continue;
                             }
                             // translucent disk: the first hit's record now, the crossing
-                            // shaded, and the step accepted as it stands
+                            // recorded, and the step accepted as it stands
                             if (n_cross == 0) {
                                 // finish_ray takes the root point in xr[0..5] and xr[12..17]
 #pragma unroll
@@ -712,9 +711,9 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                                            disk_redshift(M, a, rr, S.lz0[tid]), args.out, xr);
                                 S.lambda[tid] = lambda_step;
                             }
-                            const double thr = shade_crossing(args, Bp, S, tid, n_cross, xr + 12, wroot);
+                            record_crossing(args, Bp, S, tid, n_cross, xr + 12, wroot);
                             ++n_cross;
-                            if (!(thr > kMinThroughput && n_cross < kMaxCrossings)) {
+                            if (n_cross >= kMaxCrossings) {
                                 end_continuation(args, Bp, S, tid, n_cross, RT_RAY_UNFINISHED, xr + 12);
                                 mode = MODE_IDLE;
                                 continue;
@@ -939,24 +938,6 @@ __global__ void __launch_bounds__(BLOCK) finish_kernel_t(TraceArgs args) {
 template __global__ void finish_kernel_t<128>(TraceArgs);
 
 namespace {
-// Near-critical band of the mixed tracer (|d_b| / M); RELSIM_CRITICAL_BAND overrides it
-float critical_band() {
-    static const float b = [] {
-        const char* v = std::getenv("RELSIM_CRITICAL_BAND");
-        return v ? static_cast<float>(std::atof(v)) : static_cast<float>(kCriticalBand);
-    }();
-    return b;
-}
-
-// near-critical rays to the FP64 near pass: RELSIM_CRITICAL=1
-uint32_t trace_opts() {
-    static const uint32_t o = [] {
-        const char* v = std::getenv("RELSIM_CRITICAL");
-        return (v && v[0] == '1') ? TO_CRITICAL_FP64 : 0u;
-    }();
-    return o;
-}
-
 template <bool CONT>
 const void* pass_kernel_t(int pass, uint32_t block) {
     if (pass == PASS_FAR)
@@ -985,7 +966,7 @@ int trace_pass_occupancy(int pass, uint32_t block) {
 void launch_trace_pass(const TraceArgs& args, int pass, uint32_t grid, uint32_t block, void* stream) {
     void* params[] = {const_cast<TraceArgs*>(&args)};
     block = (block == 64) ? 64u : 128u;
-    cudaLaunchKernel(pass_kernel(pass, block, args.shade != nullptr), dim3(grid), dim3(block), params, 0,
+    cudaLaunchKernel(pass_kernel(pass, block, args.cont.cross != nullptr), dim3(grid), dim3(block), params, 0,
                      static_cast<cudaStream_t>(stream));
 }
 
@@ -1025,8 +1006,6 @@ cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t beg
         args.queue = reinterpret_cast<unsigned long long*>(qb);
         args.refill_threshold = far_refill;
         args.from_pixels = (round == 0) ? 1u : 0u;
-        args.opts = trace_opts();
-        args.critical_band = critical_band();
         args.allow_exit = 0;
         args.in_queue = far_q;
         args.in_count = reinterpret_cast<const uint32_t*>(qb + 12);
@@ -1106,7 +1085,7 @@ int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_co
 void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled, void* stream) {
     void* params[] = {const_cast<TraceArgs*>(&args)};
     block = kernel_block(block, mixed, rolled);
-    cudaLaunchKernel(kernel_for(block, mixed, rolled, args.shade != nullptr), dim3(grid), dim3(block), params, 0,
+    cudaLaunchKernel(kernel_for(block, mixed, rolled, args.cont.cross != nullptr), dim3(grid), dim3(block), params, 0,
                      static_cast<cudaStream_t>(stream));
 }
 

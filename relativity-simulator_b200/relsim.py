@@ -42,7 +42,7 @@ class Camera(ctypes.Structure):
         ("field_of_view_rad", _d), ("metric_mass", _d), ("metric_spin", _d), ("escape_radius", _d),
         ("capture_scale", _d), ("disk_inner_radius", _d), ("disk_outer_radius", _d), ("rtol", _d), ("atol", _d),
         ("step_cap_fraction", _d), ("initial_step_fraction", _d), ("projection_tol", _d), ("mixed_fp64_radius", _d),
-        ("metric_charge", _d),
+        ("metric_charge", _d), ("mixed_critical_band", _d),
         ("screen_width", _u32), ("screen_height", _u32), ("max_integration_steps", _u32), ("early_capture", _u32),
         ("precision_mode", _u32), ("dispatch_row_offset", _u32), ("dispatch_row_count", _u32),
         ("tile_origin_x", _u32), ("tile_origin_y", _u32), ("tile_extent_x", _u32), ("tile_extent_y", _u32),
@@ -219,11 +219,16 @@ def make_camera(*, spin: float = 0.94, mass: float = 1.0, r_obs: float = 100.0, 
                 max_steps: int = 20000,
                 step_cap: float = 0.1, h0: float = 0.01, projection_tol: float = 1e-12, early_capture: bool = True,
                 precision: int = PRECISION_FP64, mixed_fp64_radius: float = 0.0, row_offset: int = 0,
-                row_count: int = 0, metric_form: int = METRIC_KERR_SCHILD, charge: float = 0.0) -> Camera:
+                row_count: int = 0, metric_form: int = METRIC_KERR_SCHILD, charge: float = 0.0,
+                critical_band: float = 0.0) -> Camera:
     """A camera looking at the hole from (r_obs, incl, phi_obs) with a static-observer tetrad.
 
     metric_form METRIC_BOYER_LINDQUIST traces the Kerr-Newman metric of the
     given charge in Boyer-Lindquist coordinates (FP64, ZAMO observer).
+
+    critical_band (mixed mode): rays whose constants lie within this many M of
+    the critical curve are traced in FP64 from their first step (0: 1 M,
+    negative: none).
 
     Tolerances default to rtol = atol = 1e-10 for FP64 and 1e-8 for the mixed
     precision mode (whose FP32 stages carry ~1e-7 relative increments)."""
@@ -238,7 +243,7 @@ def make_camera(*, spin: float = 0.94, mass: float = 1.0, r_obs: float = 100.0, 
     c.disk_inner_radius, c.disk_outer_radius = disk_inner, disk_outer
     c.rtol, c.atol = rtol, atol
     c.step_cap_fraction, c.initial_step_fraction, c.projection_tol = step_cap, h0, projection_tol
-    c.mixed_fp64_radius = mixed_fp64_radius
+    c.mixed_fp64_radius, c.mixed_critical_band = mixed_fp64_radius, critical_band
     c.screen_width, c.screen_height = width, height
     c.max_integration_steps = max_steps
     c.early_capture = 1 if early_capture else 0

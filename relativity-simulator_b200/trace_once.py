@@ -33,6 +33,8 @@ def main() -> None:
     ap.add_argument("--fp64-rolled", type=int, default=0)
     ap.add_argument("--rtol", type=float, default=None)
     ap.add_argument("--fp64-radius", type=float, default=0.0)
+    ap.add_argument("--critical-band", type=float, default=0.0,
+                    help="mixed precision: near-critical band in M traced in FP64 (0: 1 M, negative: none)")
     ap.add_argument("--mixed-single", type=int, default=0,
                     help="mixed precision: 1 = the single-kernel form instead of far/near passes")
     ap.add_argument("--metric", choices=["ks", "bl"], default="ks",
@@ -52,7 +54,7 @@ def main() -> None:
     cam = relsim.make_camera(spin=a.spin, r_obs=a.r_obs, incl_deg=a.incl, fov_deg=a.fov, width=a.side,
                              height=a.side,
                              precision=relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64,
-                             rtol=a.rtol, mixed_fp64_radius=a.fp64_radius,
+                             rtol=a.rtol, mixed_fp64_radius=a.fp64_radius, critical_band=a.critical_band,
                              metric_form=relsim.METRIC_BOYER_LINDQUIST if a.metric == "bl" else relsim.METRIC_KERR_SCHILD,
                              charge=a.charge)
     srcs = None

@@ -33,10 +33,11 @@ def test_every_declared_symbol_is_exported():
 def test_layouts_match_header(tmp_path):
     prog = tmp_path / "sizes.c"
     prog.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "relsim_cuda.h"\nint main(void){'
-                    'printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(rt_camera), sizeof(rt_pixel_out),'
+                    'printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(rt_camera), sizeof(rt_pixel_out),'
                     ' sizeof(rt_ray_out), sizeof(rt_launch_config), sizeof(rt_stats),'
                     ' offsetof(rt_camera, screen_width), offsetof(rt_camera, metric_form),'
-                    ' offsetof(rt_camera, metric_charge), offsetof(rt_pixel_out, status_flags));'
+                    ' offsetof(rt_camera, metric_charge), offsetof(rt_camera, mixed_critical_band),'
+                    ' offsetof(rt_pixel_out, status_flags));'
                     'return 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
@@ -44,7 +45,7 @@ def test_layouts_match_header(tmp_path):
     exp = [ctypes.sizeof(relsim.Camera), ctypes.sizeof(relsim.PixelOut), ctypes.sizeof(relsim.RayOut),
            ctypes.sizeof(relsim.LaunchConfig), ctypes.sizeof(relsim.Stats),
            relsim.Camera.screen_width.offset, relsim.Camera.metric_form.offset, relsim.Camera.metric_charge.offset,
-           relsim.PixelOut.status_flags.offset]
+           relsim.Camera.mixed_critical_band.offset, relsim.PixelOut.status_flags.offset]
     assert got == exp
     assert got[1] == 32  # GpuPixelOutput (gpu_types.hpp:1111-1121)
     assert relsim.PIXEL_DTYPE.itemsize == 32
@@ -97,10 +98,10 @@ def test_server_config_defaults_and_no_device():
 
 def test_host_only_entry_points():
     L = relsim.lib()
-    assert L.rt_abi_version() == 3
+    assert L.rt_abi_version() == 4
     c = relsim.Camera()
     L.rt_camera_defaults(ctypes.byref(c))
-    assert c.screen_width == 2048 and c.metric_spin == 0.94 and c.rtol == 1e-10
+    assert c.screen_width == 2048 and c.metric_spin == 0.94 and c.rtol == 1e-10 and c.mixed_critical_band == 0.0
     # the default camera looks at the hole from r=100, 17 deg: forward = -e_r
     th = np.radians(17.0)
     np.testing.assert_allclose(list(c.tetrad_e1)[1:], [-np.sin(th), 0.0, -np.cos(th)], atol=1e-15)
