@@ -23,9 +23,8 @@ enum : uint32_t {
 
 // Mixed mode: the near-critical band (M, distance of a ray's constants from
 // the critical curve) of a camera that does not set one.  Rays inside it are
-// traced in FP64 at a tightened tolerance from their first step; measured on
-// the 512-bundle table, a band of 1 M keeps every disk radius within 1e-6 of
-// the FP64 tracer's.
+// traced in FP64 from their first step, at a tolerance graded with their
+// distance from the curve.
 constexpr float kDefaultCriticalBand = 1.0f;
 
 // Per-camera constants, precomputed once on the host in FP64 (the same
@@ -96,7 +95,6 @@ enum ParkU : int { PU_ACC = 0, PU_REJ, PU_FLAGS, PU_GUARD, PU_WIND, PU_MISC, PU_
 enum : uint32_t {
     PM_HAS_HIST = 1u,    // bit 0: PI30 history present
     PM_EARLY_SHIFT = 2u, // bits 2..3: Carter early-capture state + 1
-    PM_CRITICAL = 16u,   // bit 4: near-critical ray, traced in FP64 at the tightened tolerance
     PM_CROSS_SHIFT = 5u  // bits 5..9: disk crossings so far (translucent-disk continuation)
 };
 
@@ -131,6 +129,8 @@ struct TraceArgs {
     uint32_t* out_count;
     uint32_t* finish_queue;     // disk hits parked with their root point for the finish pass
     uint32_t* finish_count;
+    uint32_t* crit_queue;       // first far pass: near-critical rays, for the critical pass
+    uint32_t* crit_count;
     ParkBuf park;
     // translucent-disk continuation (single-camera launches with shading): the
     // crossings' outputs; cross null: off

@@ -24,7 +24,15 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr double kTwoPi = 2.0 * kPi;
 constexpr double kEarlyCaptureMargin = 1e-4;  // M, distance to the critical curve
 
-enum LaneMode : int { MODE_IDLE = 0, MODE_STEP = 1, MODE_ROOT = 2, MODE_REDO = 3, MODE_PARK = 4, MODE_FINISHQ = 5 };
+enum LaneMode : int {
+    MODE_IDLE = 0,
+    MODE_STEP = 1,
+    MODE_ROOT = 2,
+    MODE_REDO = 3,
+    MODE_PARK = 4,     // two-pass: to the other pass, state parked
+    MODE_FINISHQ = 5,  // two-pass: a disk hit, root point parked for the finish pass
+    MODE_CRITQ = 6     // far pass: a near-critical ray, to the critical pass (no state)
+};
 
 // Cold per-lane state, structure of arrays indexed by threadIdx.x.
 template <int BLOCK>
@@ -383,10 +391,19 @@ constexpr double kNearExitFactor = 1.25;
 // Near-critical rays of the mixed tracer: a ray whose impact parameter lies
 // within the camera's band (BundleDesc::critical_band, M) of the critical
 // curve (|d_b| from the Kerr radial potential, shadow_distance) orbits the
-// photon region, where any step error is amplified about as 1/|d_b|.  The
-// far pass sends such a ray to the FP64 near pass at its first step, which
-// keeps it to its end at the camera's tolerance times kCriticalTolScale.
-constexpr double kCriticalTolScale = 1e-2;
+// photon region, where a step error grows about as 1/|d_b|.  The two-pass
+// tracer hands such a ray, before its first step, to the critical pass: the
+// FP64 kernel over a queue of those rays, at the camera's tolerance times
+// critical_tol_scale.  The single-kernel form keeps such a lane in FP64.
+constexpr double kCriticalTolScale = 1e-2;  // the smallest tolerance factor
+
+// Tolerance factor of a near-critical ray: (|d_b| / band)^2, at least
+// kCriticalTolScale; 1 at the band's edge, where the FP32 stages' error
+// already meets the stated bound.
+__device__ __forceinline__ float critical_tol_scale(double db, double band) {
+    const double u = fabs(db) / band;
+    return static_cast<float>(fmin(1.0, fmax(kCriticalTolScale, u * u)));
+}
 
 // Largest r_BL at which the FP32 stages are used (keeps r^4 and 1/r^4 in range).
 constexpr double kFp32MaxRadius = 1e6;

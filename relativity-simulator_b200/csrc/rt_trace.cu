@@ -236,7 +236,9 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     static_assert(!FAR_PASS || MIXED, "the far pass runs the FP32 stages");
     static_assert(!NEAR_PASS || !MIXED, "the near pass runs FP64 stages");
     // rays of this launch: pixels (single kernel, first far pass) or queue entries
-    const bool from_queue = (PASS != PASS_SINGLE) && !(FAR_PASS && args.from_pixels != 0);
+    // (later passes; the single kernel as the critical pass of a two-pass launch)
+    const bool from_queue =
+        (PASS == PASS_SINGLE) ? (args.in_queue != nullptr) : !(FAR_PASS && args.from_pixels != 0);
     const uint64_t total = from_queue ? static_cast<uint64_t>(*args.in_count) : args.total_rays;
 
     // hot lane state
@@ -246,7 +248,8 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     uint32_t acc = 0, rej = 0, flags = 0, bidx = 0;
     int mode = MODE_IDLE, wind = 0, can_early = 0;
     bool has_hist = false;
-    bool critical = false;  // near pass: a near-critical ray (FP64 to its end, tightened tolerance)
+    bool critical = false;  // mixed mode: a near-critical ray (FP64 from its first step)
+    float tol_sc = 1.0f;    // tolerance factor of the ray (critical_tol_scale for near-critical rays)
     bool k1_fp32 = false;  // k1 came from an FP32 far-zone stage (mixed mode)
     uint32_t guard = 0;    // loop iterations spent on the current ray
     uint32_t n_cross = 0;  // disk crossings so far (translucent-disk continuation)
@@ -287,13 +290,28 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
 #pragma unroll
                     for (int i = 0; i < 6; ++i) xch[i] = y[i];
                     xch[6] = h;
-                    const uint32_t misc =
-                        (has_hist ? PM_HAS_HIST : 0u) | (static_cast<uint32_t>(can_early + 1) << PM_EARLY_SHIFT) |
-                        (critical ? PM_CRITICAL : 0u) | (n_cross << PM_CROSS_SHIFT);
+                    const uint32_t misc = (has_hist ? PM_HAS_HIST : 0u) |
+                                          (static_cast<uint32_t>(can_early + 1) << PM_EARLY_SHIFT) |
+                                          (n_cross << PM_CROSS_SHIFT);
                     const uint32_t uch[PU_COUNT] = {acc, rej, flags, guard, static_cast<uint32_t>(wind), misc,
                                                     __float_as_uint(lnp)};
                     park_ray(args.park, ray, S, tid, xch, uch);
                     mode = MODE_IDLE;
+                }
+            }
+            if constexpr (FAR_PASS) {
+                // near-critical rays to the critical pass, before their first step
+                const unsigned cmask = __ballot_sync(FULL, mode == MODE_CRITQ);
+                if (cmask) {
+                    const int leader = __ffs(cmask) - 1;
+                    uint32_t cbase = 0;
+                    if (lane == leader) cbase = atomicAdd(args.crit_count, static_cast<uint32_t>(__popc(cmask)));
+                    cbase = __shfl_sync(FULL, cbase, leader);
+                    if (mode == MODE_CRITQ) {
+                        args.crit_queue[cbase + static_cast<uint32_t>(__popc(cmask & lt_mask))] =
+                            static_cast<uint32_t>(ray);
+                        mode = MODE_IDLE;
+                    }
                 }
             }
         }
@@ -329,6 +347,8 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                     uint64_t rix = rid;
                     if constexpr (PASS != PASS_SINGLE) {
                         rix = from_queue ? static_cast<uint64_t>(args.in_queue[rid]) : args.ray_base + rid;
+                    } else {
+                        if (from_queue) rix = args.in_queue[rid];
                     }
                     // bundle of this ray: last bundle whose ray_begin <= rix
                     uint32_t lo = 0, hi = args.n_bundles;
@@ -358,7 +378,6 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                             wind = static_cast<int>(uch[PU_WIND]);
                             has_hist = (uch[PU_MISC] & PM_HAS_HIST) != 0u;
                             can_early = static_cast<int>((uch[PU_MISC] >> PM_EARLY_SHIFT) & 3u) - 1;
-                            critical = (uch[PU_MISC] & PM_CRITICAL) != 0u;
                             if constexpr (CONT) n_cross = (uch[PU_MISC] >> PM_CROSS_SHIFT) & 31u;
                             lnp = __uint_as_float(uch[PU_LNP]);
                             k1_fp32 = false;
@@ -387,18 +406,21 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                         guard = 0;
                         n_cross = 0;
                         critical = false;
-                        if constexpr (FAR_PASS) {
-                            const BundleDesc* Bc = args.bundles + lo;
-                            if (Bc->critical_band > 0.0f) {
-                                // distance of the ray's constants from the critical curve; the
-                                // Carter early-capture decision comes from the same value
-                                const double db = shadow_distance(Bc->m, Bc->a, 0.0, Bc->rh, S.lz0[tid], S.q0[tid]);
-                                if (can_early < 0) can_early = db > kEarlyCaptureMargin;
-                                critical = fabs(db) < static_cast<double>(Bc->critical_band) * Bc->m;
-                            }
+                        tol_sc = 1.0f;
+                        const BundleDesc* Bc = args.bundles + lo;
+                        // mixed mode: the distance of the ray's constants from the critical
+                        // curve decides whether it is near-critical (and the Carter early
+                        // capture, from the same value); the critical pass grades its
+                        // tolerance with it
+                        if ((MIXED && Bc->critical_band > 0.0f) || (PASS == PASS_SINGLE && !MIXED && from_queue)) {
+                            const double db = shadow_distance(Bc->m, Bc->a, 0.0, Bc->rh, S.lz0[tid], S.q0[tid]);
+                            if (can_early < 0) can_early = db > kEarlyCaptureMargin;
+                            const double band = static_cast<double>(Bc->critical_band) * Bc->m;
+                            critical = fabs(db) < band;
+                            if (critical && PASS == PASS_SINGLE) tol_sc = critical_tol_scale(db, band);
                         }
                         mode = MODE_STEP;
-                        ++n_rays;
+                        if (!(PASS == PASS_SINGLE && from_queue)) ++n_rays;  // counted by the far pass
                         ++n_rhs;
                     }
                 }
@@ -424,7 +446,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
         } else if constexpr (MIXED) {
             const bool stepping = (mode == MODE_STEP || mode == MODE_REDO);
             const BundleDesc* Bz = args.bundles + bidx;
-            const bool lane_far = stepping && r >= Bz->fp64_radius && r < kFp32MaxRadius;
+            const bool lane_far = stepping && !critical && r >= Bz->fp64_radius && r < kFp32MaxRadius;
             // every lane executes the ballot (no short-circuit around a full-mask sync)
             const unsigned near_lanes = __ballot_sync(FULL, stepping && !lane_far);
             far = lane_far && near_lanes == 0u;
@@ -473,12 +495,12 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
             }
             if constexpr (FAR_PASS) {
                 if (critical || r < Bp->fp64_radius || r >= kFp32MaxRadius) {  // into the FP64 zone
-                    mode = MODE_PARK;
+                    mode = critical ? MODE_CRITQ : MODE_PARK;
                     continue;
                 }
             }
             if constexpr (NEAR_PASS) {
-                if (args.allow_exit != 0u && !critical && r >= kNearExitFactor * Bp->fp64_radius &&
+                if (args.allow_exit != 0u && r >= kNearExitFactor * Bp->fp64_radius &&
                     r < kFp32MaxRadius) {  // back out of the FP64 zone
                     mode = MODE_PARK;
                     continue;
@@ -632,8 +654,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
         double err;
         {
             double num = 0.0, den = 1.0;
-            const double tol_scale = (NEAR_PASS && critical) ? kCriticalTolScale : 1.0;
-            const double rtol = Bp->rtol * tol_scale, atol = Bp->atol * tol_scale;
+            const double rtol = Bp->rtol * static_cast<double>(tol_sc), atol = Bp->atol * static_cast<double>(tol_sc);
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
                 const double sc = rtol * fmax(fabs(y[i]), fabs(y5[i])) + atol;
@@ -979,6 +1000,8 @@ constexpr int kMixedRounds = 4;
 // loads and one RHS), so refilling a partly idle warp is cheap, while the
 // near-zone work per ray (disk root, photon-region orbits) varies widely.
 constexpr uint32_t kNearRefill = 16;  // measured best of 1, 4, 8, 16, 32
+// Block of the critical pass (the FP64 kernel's default shape).
+constexpr uint32_t kCriticalBlock = 128;
 
 uint64_t two_pass_state_bytes(uint64_t n) {
     return n * (sizeof(double) * PD_COUNT + sizeof(uint32_t) * PU_COUNT + 3 * sizeof(uint32_t));
@@ -986,11 +1009,14 @@ uint64_t two_pass_state_bytes(uint64_t n) {
 
 // Per-band queue counters (32 bytes): [0] far-pass claim (u64), [8] near queue
 // count (u32), [12] far queue count (u32), [16] near-pass claim (u64), zeroed
-// pairwise before each pass; [24] finish queue count (u32), zeroed once.
+// pairwise before each pass; [24] finish queue count (u32), zeroed once.  The
+// first far pass also counts the near-critical rays in [12] (their queue is
+// the far queue's storage, free until the first near pass) and the critical
+// pass claims them through [16].
 namespace {
 cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t begin, uint64_t count, char* qb,
                          uint32_t far_grid, uint32_t far_block, uint32_t near_grid, uint32_t finish_grid,
-                         cudaStream_t s) {
+                         uint32_t crit_grid, cudaStream_t s) {
     uint32_t* near_q = buf.queues + 3 * begin;
     uint32_t* far_q = near_q + count;
     args.park = buf.park;
@@ -1002,7 +1028,7 @@ cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t beg
     cudaError_t e = cudaMemsetAsync(qb + 24, 0, 8, s);
     for (int round = 0; e == cudaSuccess && round < kMixedRounds; ++round) {
         // far pass: pixels (first round) or the far queue -> near queue
-        if ((e = cudaMemsetAsync(qb, 0, 12, s)) != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(qb, 0, round == 0 ? 24 : 12, s)) != cudaSuccess) break;
         args.queue = reinterpret_cast<unsigned long long*>(qb);
         args.refill_threshold = far_refill;
         args.from_pixels = (round == 0) ? 1u : 0u;
@@ -1011,8 +1037,23 @@ cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t beg
         args.in_count = reinterpret_cast<const uint32_t*>(qb + 12);
         args.out_queue = near_q;
         args.out_count = reinterpret_cast<uint32_t*>(qb + 8);
+        args.crit_queue = (round == 0) ? far_q : nullptr;
+        args.crit_count = (round == 0) ? reinterpret_cast<uint32_t*>(qb + 12) : nullptr;
         launch_trace_pass(args, PASS_FAR, far_grid, far_block, s);
         if ((e = cudaGetLastError()) != cudaSuccess) break;
+        if (round == 0) {
+            // critical pass: the near-critical rays, FP64 from their pixels to their
+            // end at their graded tolerance (the single FP64 kernel over a queue)
+            TraceArgs c = args;
+            c.queue = reinterpret_cast<unsigned long long*>(qb + 16);
+            c.refill_threshold = 32;
+            c.in_queue = far_q;
+            c.in_count = reinterpret_cast<const uint32_t*>(qb + 12);
+            c.out_queue = c.finish_queue = c.crit_queue = nullptr;
+            c.out_count = c.finish_count = c.crit_count = nullptr;
+            launch_trace(c, crit_grid, kCriticalBlock, false, false, s);
+            if ((e = cudaGetLastError()) != cudaSuccess) break;
+        }
         // near pass: near queue -> far queue (the last one keeps its rays)
         if ((e = cudaMemsetAsync(qb + 12, 0, 12, s)) != cudaSuccess) break;
         args.queue = reinterpret_cast<unsigned long long*>(qb + 16);
@@ -1050,6 +1091,8 @@ int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_co
     const uint32_t far_grid = static_cast<uint32_t>(sm_count) * static_cast<uint32_t>(far_occ > 1 ? far_occ : 1);
     const uint32_t near_grid = static_cast<uint32_t>(sm_count) * static_cast<uint32_t>(near_occ > 1 ? near_occ : 1);
     const uint32_t finish_grid = static_cast<uint32_t>(sm_count) * 8u;
+    const int crit_occ = trace_occupancy(kCriticalBlock, false, false);
+    const uint32_t crit_grid = static_cast<uint32_t>(sm_count) * static_cast<uint32_t>(crit_occ > 1 ? crit_occ : 1);
     cudaError_t e = cudaSuccess;
     if (bands > 1) {
         if ((e = cudaEventRecord(static_cast<cudaEvent_t>(fork), s)) != cudaSuccess) return static_cast<int>(e);
@@ -1063,7 +1106,7 @@ int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_co
     for (uint32_t b = 0; b < bands && begin < n && e == cudaSuccess; ++b) {
         const uint64_t count = (n - begin < per) ? n - begin : per;
         cudaStream_t sb = (b & 1u) ? s2 : s;
-        e = enqueue_band(base, buf, begin, count, buf.counters + 32 * b, far_grid, far_block, near_grid, finish_grid,
+        e = enqueue_band(base, buf, begin, count, buf.counters + 32 * b, far_grid, far_block, near_grid, finish_grid, crit_grid,
                          sb);
         if (e == cudaSuccess && after_band && prev_stream)
             e = static_cast<cudaError_t>(after_band(hook_ctx, prev_begin, prev_count, prev_stream));

@@ -91,6 +91,7 @@ def test_c4_sample_against_fp64_oracle(c4):
             g = out["g"][begins[b] + pix][both]
             worst_r = max(worst_r, float(np.max(np.abs(rh - ref["r_hit"][both]) / ref["r_hit"][both])))
             worst_g = max(worst_g, float(np.max(np.abs(g - ref["g"][both]) / ref["g"][both])))
+    print(f"c4 sample: r_hit rel max {worst_r:.2e}, g rel max {worst_g:.2e}")
     assert worst_r < 1e-5 and worst_g < 1e-5, (worst_r, worst_g)
 
 

@@ -153,3 +153,46 @@ def test_banded_host_dispatch_equals_device_dispatch(tracer):
     np.testing.assert_array_equal(bare, dp)
     np.testing.assert_array_equal(part["pixels"], host["pixels"][300 * 1024:400 * 1024])
     assert host["pixels"]["r"].max() > 0.0
+
+
+def test_critical_band_default_is_one_m(tracer):
+    """mixed_critical_band = 0 means 1 M: bit-identical records; a negative band
+    routes no ray, so fewer attempts run in FP64."""
+    fields = ["status", "steps_accepted", "steps_rejected", "r", "theta", "phi", "r_hit", "g"]
+    tracer.set_launch_config()
+    outs, fp64 = {}, {}
+    for band in (0.0, 1.0, -1.0):
+        cam = config_cam("c2", width=256, height=256, precision=relsim.PRECISION_MIXED)
+        cam.mixed_critical_band = band
+        outs[band] = tracer.dispatch(cam, fields=fields, pixels=False)
+        fp64[band] = tracer.stats().fp64_attempts
+    for f in fields:
+        np.testing.assert_array_equal(outs[0.0][f], outs[1.0][f])
+    assert fp64[-1.0] < fp64[1.0]
+
+
+def test_critical_band_covering_the_image_traces_fp64(tracer):
+    """A band wider than the image hands every ray with a turning point (every
+    disk ray) to the critical pass before its first step: the FP64 kernel,
+    at a hundredth of the mixed tolerance (rtol = atol = 1e-10, the oracle's)
+    this far inside the band.  Classes exact outside the 1e-6 M band, disk
+    radius and g within CRIT_BAR of the FP64 oracle (the same algorithm and
+    tolerance; the bar is the FP64 tracer's parity bar)."""
+    CRIT_BAR = 1e-9
+    cam = config_cam("c2", width=96, height=96, precision=relsim.PRECISION_MIXED)
+    cam.mixed_critical_band = 1e6
+    tracer.set_launch_config()
+    out = tracer.dispatch(cam, fields=["status", "r_hit", "g"], pixels=False)
+    st = tracer.stats()
+    # rays without a turning point (no minimum of the radial potential outside
+    # the horizon: plunging) stay in the FP32 far pass
+    assert st.fp64_attempts > 0.9 * st.attempts
+    ref = O.trace(relsim.camera_dict(config_cam("c2", width=96, height=96)))
+    r_in = O.lib().orc_isco_radius(1.0, cam.metric_spin)
+    band = O.boundary_band(ref, r_in, cam.disk_outer_radius, 1e-6)
+    assert not ((out["status"] != ref["status"]) & ~band).any()
+    both = (out["status"] == O.DISK) & (ref["status"] == O.DISK)
+    rel = np.abs(out["r_hit"][both] - ref["r_hit"][both]) / ref["r_hit"][both]
+    relg = np.abs(out["g"][both] - ref["g"][both]) / ref["g"][both]
+    print(f"band 1e6 M: {both.sum()} disk rays, r_hit rel max {rel.max():.2e}, g rel max {relg.max():.2e}")
+    assert rel.max() < CRIT_BAR and relg.max() < CRIT_BAR

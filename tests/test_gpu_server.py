@@ -119,17 +119,22 @@ def test_stream_replay_serves_every_request():
     assert res["latency_ms_p99"] >= res["latency_ms_p50"] > 0.0
     from oracle import oracle as O
     rng = np.random.default_rng(4)
+    worst_r = worst_g = 0.0
+    n_disk = 0
     for idx, (r, out) in sorted(res["kept"].items()):
         cam = r.bundle.camera(relsim.PRECISION_FP64)
-        pix = rng.choice(r.rays, min(r.rays, 60), replace=False)
-        ref = O.trace(relsim.camera_dict(cam), pixels=pix.astype(np.uint64))
+        pix = rng.choice(r.rays, min(r.rays, 500), replace=False)
+        ref = O.trace(relsim.camera_dict(cam), pixels=pix.astype(np.uint64), threads=0)
         st = out["status"][pix].astype(np.uint32)
         band = O.boundary_band(ref, O.lib().orc_isco_radius(1.0, cam.metric_spin), cam.disk_outer_radius, 1e-6)
         assert not ((st != ref["status"]) & ~band).any(), idx
         both = (st == O.DISK) & (ref["status"] == O.DISK)
         if both.any():
-            assert np.max(np.abs(out["r_hit"][pix][both] - ref["r_hit"][both]) / ref["r_hit"][both]) < 1e-5
-            assert np.max(np.abs(out["g"][pix][both] - ref["g"][both]) / ref["g"][both]) < 1e-5
+            n_disk += int(both.sum())
+            worst_r = max(worst_r, float(np.max(np.abs(out["r_hit"][pix][both] - ref["r_hit"][both]) / ref["r_hit"][both])))
+            worst_g = max(worst_g, float(np.max(np.abs(out["g"][pix][both] - ref["g"][both]) / ref["g"][both])))
+    print(f"stream sample vs oracle: {n_disk} disk rays, r_hit rel max {worst_r:.2e}, g rel max {worst_g:.2e}")
+    assert worst_r < 1e-5 and worst_g < 1e-5
 
 
 def test_multi_source_request_matches_direct_trace(tracer):
