@@ -553,7 +553,8 @@ def ours(args) -> None:
                          "peak_source": "measured in this run: register FMA-chain kernel (rt_measure_fma_peak)",
                          "flop_per_attempt": FLOP_PER_ATTEMPT,
                          "traffic": committed_traffic(prec),
-                         "executed": executed_roofline(prec, d["attempts"], own_ms, fp64_peak, fp32_peak)},
+                         "executed": executed_roofline(prec, d["attempts"], own_ms, fp64_peak, fp32_peak,
+                                                       d["fp64_attempts"])},
         }
 
     # the plain FP64 tracer at the mixed tracer's tolerance: the equal-tolerance comparison
@@ -658,12 +659,14 @@ def vars_of(c) -> dict:
     return {f: getattr(c, f) for f, _ in c._fields_}
 
 
-def executed_roofline(key, attempts, ms, fp64_peak, fp32_peak):
+def executed_roofline(key, attempts, ms, fp64_peak, fp32_peak, fp64_attempts=None):
     """Executed floating-point work against the pipe peaks: per-attempt FP32 and
     FP64 FLOP counts from the committed ncu instruction mix of the same kernels
     (profiles/instruction_mix.json: FFMA and packed FFMA2 count 2 and 4 FLOP,
     FMUL/FADD 1 and 2, DFMA 2, DMUL/DADD 1), times the attempts of this run,
-    over its device time.  None when no mix is committed for `key`."""
+    over its device time.  The mixed tracer's attempts are weighted by pass:
+    its FP32 attempts at the far pass's mix, its FP64 attempts (critical and
+    near passes) at the near pass's.  None when no mix is committed for `key`."""
     path = os.path.join(ROOT, "profiles", "instruction_mix.json")
     try:
         with open(path) as f:
@@ -671,8 +674,16 @@ def executed_roofline(key, attempts, ms, fp64_peak, fp32_peak):
     except (OSError, ValueError, KeyError):
         return None
     sec = ms * 1e-3
-    f32 = attempts * mix["fp32_flop_per_attempt"] / sec / 1e12
-    f64 = attempts * mix["fp64_flop_per_attempt"] / sec / 1e12
+    if "passes" in mix and fp64_attempts is not None:
+        far, near = mix["passes"]["far"], mix["passes"]["near"]
+        n32 = attempts - fp64_attempts
+        f32_flop = n32 * far["fp32_flop_per_attempt"] + fp64_attempts * near["fp32_flop_per_attempt"]
+        f64_flop = n32 * far["fp64_flop_per_attempt"] + fp64_attempts * near["fp64_flop_per_attempt"]
+    else:
+        f32_flop = attempts * mix["fp32_flop_per_attempt"]
+        f64_flop = attempts * mix["fp64_flop_per_attempt"]
+    f32 = f32_flop / sec / 1e12
+    f64 = f64_flop / sec / 1e12
     return {"fp32_tflops": f32, "fp32_frac": f32 / fp32_peak, "fp64_tflops": f64, "fp64_frac": f64 / fp64_peak,
             "pipe_frac": f32 / fp32_peak + f64 / fp64_peak, "source": f"profiles/instruction_mix.json[{key}]"}
 

@@ -92,7 +92,17 @@ def main() -> None:
     print(json.dumps({"rays": int(s.rays), "attempts": int(s.attempts), "accepted": int(s.accepted),
                       "fp64_attempts": int(s.fp64_attempts), "rhs_evals": int(s.rhs_evals),
                       "kernel_ms": s.kernel_ms, "mrays_per_s": s.rays / s.kernel_ms / 1e3 if s.kernel_ms > 0 else None,
-                      "classes": np.bincount(out["status"], minlength=4).tolist()}))
+                      "classes": np.bincount(out["status"], minlength=4).tolist(),
+                      **attempt_tail(out)}))
+
+
+def attempt_tail(out: dict) -> dict:
+    """Largest and 99.9th-percentile step attempts of one ray (host records with step counts)."""
+    if "steps_accepted" not in out:
+        return {}
+    att = out["steps_accepted"].astype(np.int64) + out["steps_rejected"]
+    return {"ray_attempts_max": int(att.max()), "ray_attempts_p999": float(np.percentile(att, 99.9)),
+            "ray_attempts_mean": float(att.mean())}
 
 
 if __name__ == "__main__":
