@@ -204,7 +204,14 @@ typedef struct rt_ray_out {
     double* exit_x;
     double* exit_y;
     double* exit_z;
+    /* the body the ray ended on: for a disk hit the source whose disk it hit
+     * first, for a capture the source that captured it (0: the camera's hole,
+     * k: the k-th rt_source of a multi-source scene); RT_BODY_NONE for escaped
+     * and unfinished rays and for captures in a horizon-like region of the
+     * summed fields (RT_RAYFLAG_DIVERGED).  Not recorded by the request server. */
+    uint32_t* body;
 } rt_ray_out;
+#define RT_BODY_NONE 0xFFFFFFFFu
 
 /* Launch shape of the persistent tracer (set by the autotuner). */
 typedef struct rt_launch_config {
@@ -253,7 +260,16 @@ int rt_abi_version(void);
  * region of the summed fields), escaped at |x| > escape_radius, disk hit at a
  * source's first equatorial crossing on its disk (g from that source's disk).
  * The record's r, theta, phi are spherical about the origin; dE, dLz, dQ are
- * NaN (no Kerr invariants for the superposition). */
+ * NaN (no Kerr invariants for the superposition); body names the source of the
+ * first disk hit or of the capture.  Shaded (rt_set_shading, pixels
+ * requested), every ray is followed through the translucent disks of all
+ * sources, each step's crossings in order along the ray, and each crossing is
+ * shaded with its source's disk: the camera's hole with rt_shading.disk
+ * resolved, a body with rt_source.disk as it stands, both by the thin
+ * procedural model at detail 1 (software_compute_engine.hpp:3150-3191); a ray
+ * that ends within 6 m of a source with throughput left adds no sky
+ * (:3207-3216).  The camera's rtol and atol apply (the mixed mode's 1e-8 for a
+ * mixed-mode camera; the stages stay FP64). */
 #define RT_MAX_SOURCES 16        /* the camera's hole and up to 15 sources */
 #define RT_RAYFLAG_DIVERGED (1u << 4)
 
@@ -266,11 +282,13 @@ typedef struct rt_source {
     double disk_enabled;    /* > 0.5: thin disk */
     double disk_inner_scale;/* inner radius = max(scale, 1) * r_ISCO of the source */
     double disk_outer_units;/* outer radius = max(units * mass, 1.05 * inner) */
+    rt_disk_profile disk;   /* the body's disk appearance (GpuBodyData::disk), used as it stands when
+                               shading; the camera's hole uses rt_shading.disk */
 } rt_source;
 
 /* Trace the row window of a multi-source scene (host buffers, as rt_dispatch).
  * The camera's metric_mass / metric_spin / disk describe the hole at the
- * origin; n_sources <= RT_MAX_SOURCES - 1 more.  FP64 only. */
+ * origin; n_sources <= RT_MAX_SOURCES - 1 more.  FP64 stages. */
 rt_status rt_dispatch_multi(rt_handle* h, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
                             rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity);
 /* Device-resident form: device outputs, enqueued on `stream` (NULL: the handle's). */
@@ -403,7 +421,7 @@ void rt_server_destroy(rt_server* s);
  * RT_ERR_INVALID_ARG also for a row wider than epoch_rays. */
 rt_status rt_server_submit(rt_server* s, const rt_camera* cam, rt_pixel_out* pixels, const rt_ray_out* rays,
                            size_t capacity, uint64_t* id);
-/* Queue a multi-source scene (see rt_dispatch_multi; traced in FP64). */
+/* Queue a multi-source scene (see rt_dispatch_multi; FP64 stages). */
 rt_status rt_server_submit_multi(rt_server* s, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
                                  rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity, uint64_t* id);
 /* Up to max_done finished requests, waiting at most timeout_ms for the first. */

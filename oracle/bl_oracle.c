@@ -681,6 +681,7 @@ static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, ui
     out->dLz = (iv[1] - inv0[1]) / E0;
     out->dQ = (iv[2] - inv0[2]) / (E0 * E0);
     out->db_shadow = db0;
+    out->body = (status == ORC_RAY_DISK || status == ORC_RAY_CAPTURED) ? 0u : ORC_BODY_NONE;
     /* sky-lookup direction of an escaped ray (software_compute_engine.hpp:
      * 1581-1589 with local_frame_to_travel_direction, :1148-1168): the
      * orthonormal-frame velocity mapped to a Cartesian direction of travel */

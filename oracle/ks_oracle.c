@@ -766,6 +766,7 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
     out->dLz = (y[0] * y[4] - y[1] * y[3]) - lz0;
     out->dQ = orc_carter_q(y, m, a) - q0;
     out->db_shadow = db0;
+    out->body = (status == ORC_RAY_DISK || status == ORC_RAY_CAPTURED) ? 0u : ORC_BODY_NONE;
     /* sky-lookup direction of an escaped ray: minus the normalised dx/dlambda of
      * the terminal state (software_compute_engine.hpp:1771-1775) */
     out->exit_dir[0] = out->exit_dir[1] = out->exit_dir[2] = NAN;

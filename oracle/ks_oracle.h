@@ -97,7 +97,11 @@ typedef struct orc_ray {
                                     1771-1775; multi-source: the superposed flow, :3220-3224;
                                     Boyer-Lindquist: the local-frame velocity as a direction of
                                     travel, :1581-1589); NaN otherwise */
+    uint32_t body;               /* the body the ray ended on: the source of its first disk hit or of
+                                    its capture (0: the camera's hole); ORC_BODY_NONE otherwise */
+    uint32_t pad;
 } orc_ray;
+#define ORC_BODY_NONE 0xFFFFFFFFu
 
 /* Translucent-disk continuation of a ray (software_compute_engine.hpp:1734-1765,
  * :1771-1795): the reference's image path does not end a ray at the disk; each
@@ -111,6 +115,9 @@ typedef struct orc_cont {
     double cross_phi[ORC_MAX_CROSSINGS];
     double cross_g[ORC_MAX_CROSSINGS];
     double exit_dir[3];          /* escaped at its end: the sky-lookup direction; NaN otherwise */
+    uint32_t cross_src[ORC_MAX_CROSSINGS]; /* multi-source: the source whose disk crossing k is on (else 0) */
+    uint32_t near_source;        /* multi-source: the end point lies within 6 m of a source */
+    uint32_t pad;
 } orc_cont;
 
 /* --- single-function checks (pinned against the reference) --- */
@@ -183,6 +190,12 @@ double orc_ms_hamiltonian(const orc_ms_table* t, const double y[6]);
 void orc_ms_initial_momentum(const orc_ms_table* t, const double x[3], const double outward[3], double p[3]);
 int orc_ms_inside_horizon(const orc_ms_table* t, const double x[3]);
 void orc_ms_initial_state(const orc_camera* cam, const orc_ms_table* t, uint32_t px, uint32_t py, double y0[6]);
+/* The same with the translucent-disk continuation (trace_multi_source,
+ * software_compute_engine.hpp:3150-3216): every crossing of a step in order
+ * along the ray, each on the disk of cross_src[k]; `out` describes the first
+ * hit, `cont` the crossings and the end. */
+void orc_ms_trace_cont(const orc_camera* cam, const orc_ms_table* t, const uint64_t* pixel_index, uint64_t first,
+                       uint64_t count, orc_ray* out, orc_cont* cont, int threads);
 void orc_ms_trace(const orc_camera* cam, const orc_ms_table* t, const uint64_t* pixel_index, uint64_t first,
                   uint64_t count, orc_ray* out, int threads);
 

@@ -415,7 +415,17 @@ void orc_ms_initial_state(const orc_camera* cam, const orc_ms_table* t, uint32_t
     orc_ms_initial_momentum(t, y0, d, y0 + 3);
 }
 
-static void trace_one(const orc_camera* cam, const orc_ms_table* t, uint32_t px, uint32_t py, orc_ray* out)
+static inline void unwrap_to(double* phi, const double* y)
+{
+    double d = atan2(y[1], y[0]) - *phi;
+    d -= 2.0 * ORC_PI * floor(d / (2.0 * ORC_PI) + 0.5);
+    *phi += d;
+}
+
+/* One ray; with `cont`, the translucent-disk continuation (crossings recorded
+ * in order along the ray, the record describing the first hit). */
+static void trace_one(const orc_camera* cam, const orc_ms_table* t, uint32_t px, uint32_t py, orc_ray* out,
+                      orc_cont* cont)
 {
     double y[6];
     orc_ms_initial_state(cam, t, px, py, y);
@@ -429,9 +439,20 @@ static void trace_one(const orc_camera* cam, const orc_ms_table* t, uint32_t px,
     uint32_t acc = 0, rej = 0, status = ORC_RAY_UNFINISHED, flags = 0;
     double phi = atan2(y[1], y[0]);
     double yn[6];
+    uint32_t body = ORC_BODY_NONE;
+    /* continuation: the first hit's record */
+    int hit = 0;
+    double y_hit[6], lambda_hit = 0.0, phi_hit = 0.0, r_hit1 = NAN, g_hit1 = 1.0;
+    uint32_t acc_hit = 0, rej_hit = 0, flags_hit = 0, body_hit = 0;
+    if (cont) {
+        memset(cont, 0, sizeof *cont);
+        cont->fate = ORC_RAY_UNFINISHED;
+        cont->exit_dir[0] = cont->exit_dir[1] = cont->exit_dir[2] = NAN;
+    }
     for (uint32_t attempt = 0;; ++attempt) {
         if (inside >= 0) {
             status = ORC_RAY_CAPTURED;
+            body = (uint32_t)inside;
             break;
         }
         if (dot3(y + 3, y + 3) > ORC_MS_MAX_MOMENTUM * ORC_MS_MAX_MOMENTUM) {
@@ -473,52 +494,85 @@ static void trace_one(const orc_camera* cam, const orc_ms_table* t, uint32_t px,
                 flags |= ORC_FLAG_NONFINITE;
                 break;
             }
-            /* disk crossings: the earliest local z = 0 root on a disk */
-            double best = 2.0, best_r = 0.0, best_g = 1.0, best_y[6];
-            for (uint32_t i = 0; i < t->count; ++i) {
-                if (t->disk_in[i] < 0.0) continue;
-                const double r0[3] = {y[0] - t->pos[i][0], y[1] - t->pos[i][1], y[2] - t->pos[i][2]};
-                const double r1[3] = {yn[0] - t->pos[i][0], yn[1] - t->pos[i][1], yn[2] - t->pos[i][2]};
-                const double z0 = dot3(r0, t->axis[i]), z1 = dot3(r1, t->axis[i]);
-                if (!(z0 * z1 <= 0.0) || z0 == z1) continue;
-                /* linear estimate with a margin before the root solve */
-                const double sl = z0 / (z0 - z1);
-                double ce[3], le[3];
-                for (int q = 0; q < 3; ++q) ce[q] = r0[q] + sl * (r1[q] - r0[q]);
-                to_local(t, i, ce, le);
-                const double a = t->spin[i];
-                const double re = sqrt(max_d(le[0] * le[0] + le[1] * le[1] - a * a, 0.0));
-                const double margin = 0.05 * re + 0.5 * t->mass[i];
-                if (re < t->disk_in[i] - margin || re > t->disk_out[i] + margin) continue;
-                const double th = local_z_root(t, i, y, yn, k, h, z0, z1);
-                if (!(th < best)) continue;
-                double yr[6];
-                dense(y, yn, k, h, th, yr);
-                const double rel[3] = {yr[0] - t->pos[i][0], yr[1] - t->pos[i][1], yr[2] - t->pos[i][2]};
-                double c[3], pl[3];
-                to_local(t, i, rel, c);
-                to_local(t, i, yr + 3, pl);
-                const double rr = sqrt(max_d(c[0] * c[0] + c[1] * c[1] - a * a, 0.0));
-                if (rr < t->disk_in[i] || rr > t->disk_out[i] || rr <= t->rh[i] * 1.02) continue;
-                const double lz = (c[0] * pl[1] - c[1] * pl[0]) / max_d(sqrt(dot3(pl, pl)), 1e-30);
-                best = th;
-                best_r = rr;
-                best_g = orc_redshift_at(t->mass[i], a, rr, lz);
-                memcpy(best_y, yr, sizeof yr);
-            }
-            if (best <= 1.0) {
-                status = ORC_RAY_DISK;
-                r_hit = best_r;
-                g = best_g;
-                lambda += best * h;
-                {
-                    double d = atan2(best_y[1], best_y[0]) - phi;
-                    d -= 2.0 * ORC_PI * floor(d / (2.0 * ORC_PI) + 0.5);
-                    phi += d;
+            /* disk crossings of the step in order along the ray: the earliest
+             * local z = 0 root on a disk after the previous one */
+            int ended = 0;
+            double t_prev = -1.0;
+            for (uint32_t pass = 0; pass < t->count; ++pass) {
+                double best = 2.0, best_r = 0.0, best_g = 1.0, best_az = 0.0, best_y[6];
+                uint32_t best_i = 0;
+                for (uint32_t i = 0; i < t->count; ++i) {
+                    if (t->disk_in[i] < 0.0) continue;
+                    const double r0[3] = {y[0] - t->pos[i][0], y[1] - t->pos[i][1], y[2] - t->pos[i][2]};
+                    const double r1[3] = {yn[0] - t->pos[i][0], yn[1] - t->pos[i][1], yn[2] - t->pos[i][2]};
+                    const double z0 = dot3(r0, t->axis[i]), z1 = dot3(r1, t->axis[i]);
+                    if (!(z0 * z1 <= 0.0) || z0 == z1) continue;
+                    /* linear estimate with a margin before the root solve */
+                    const double sl = z0 / (z0 - z1);
+                    double ce[3], le[3];
+                    for (int q = 0; q < 3; ++q) ce[q] = r0[q] + sl * (r1[q] - r0[q]);
+                    to_local(t, i, ce, le);
+                    const double a = t->spin[i];
+                    const double re = sqrt(max_d(le[0] * le[0] + le[1] * le[1] - a * a, 0.0));
+                    const double margin = 0.05 * re + 0.5 * t->mass[i];
+                    if (re < t->disk_in[i] - margin || re > t->disk_out[i] + margin) continue;
+                    const double th = local_z_root(t, i, y, yn, k, h, z0, z1);
+                    if (!(th < best) || !(th > t_prev)) continue;
+                    double yr[6];
+                    dense(y, yn, k, h, th, yr);
+                    const double rel[3] = {yr[0] - t->pos[i][0], yr[1] - t->pos[i][1], yr[2] - t->pos[i][2]};
+                    double c[3], pl[3];
+                    to_local(t, i, rel, c);
+                    to_local(t, i, yr + 3, pl);
+                    const double rr = sqrt(max_d(c[0] * c[0] + c[1] * c[1] - a * a, 0.0));
+                    if (rr < t->disk_in[i] || rr > t->disk_out[i] || rr <= t->rh[i] * 1.02) continue;
+                    const double lz = (c[0] * pl[1] - c[1] * pl[0]) / max_d(sqrt(dot3(pl, pl)), 1e-30);
+                    best = th;
+                    best_r = rr;
+                    best_g = orc_redshift_at(t->mass[i], a, rr, lz);
+                    /* local azimuth of the crossing (ms_disk_crossing, software_compute_engine.hpp:3037) */
+                    best_az = atan2(c[1], c[0]) - atan2(a, rr);
+                    best_i = i;
+                    memcpy(best_y, yr, sizeof yr);
                 }
-                memcpy(y, best_y, sizeof best_y);
-                break;
+                if (best > 1.0) break;
+                if (!cont) {
+                    status = ORC_RAY_DISK;
+                    body = best_i;
+                    r_hit = best_r;
+                    g = best_g;
+                    lambda += best * h;
+                    unwrap_to(&phi, best_y);
+                    memcpy(y, best_y, sizeof best_y);
+                    ended = 1;
+                    break;
+                }
+                const uint32_t kx = cont->n_cross++;
+                cont->cross_r[kx] = best_r;
+                cont->cross_phi[kx] = best_az;
+                cont->cross_g[kx] = best_g;
+                cont->cross_src[kx] = best_i;
+                if (!hit) {
+                    hit = 1;
+                    memcpy(y_hit, best_y, sizeof best_y);
+                    lambda_hit = lambda + best * h;
+                    phi_hit = phi;
+                    unwrap_to(&phi_hit, best_y);
+                    r_hit1 = best_r;
+                    g_hit1 = best_g;
+                    acc_hit = acc;
+                    rej_hit = rej;
+                    flags_hit = flags;
+                    body_hit = best_i;
+                }
+                t_prev = best;
+                if (cont->n_cross >= ORC_MAX_CROSSINGS) {
+                    memcpy(y, best_y, sizeof best_y);
+                    ended = 1;
+                    break;
+                }
             }
+            if (ended) break;
             if (inside_n >= 0) { /* captured inside this step: the end point */
                 lambda += h;
                 {
@@ -528,6 +582,7 @@ static void trace_one(const orc_camera* cam, const orc_ms_table* t, uint32_t px,
                 }
                 memcpy(y, yn, sizeof yn);
                 status = ORC_RAY_CAPTURED;
+                body = (uint32_t)inside_n;
                 break;
             }
             if (sqrt(dot3(yn, yn)) > cam->escape_radius) { /* escaped: interpolated to the escape radius */
@@ -572,7 +627,40 @@ static void trace_one(const orc_camera* cam, const orc_ms_table* t, uint32_t px,
             h = -fabs(h) * clamp_d(0.9 * factor, 0.1, 0.9);
         }
     }
+    if (cont) {
+        cont->fate = status;
+        cont->near_source = 0;
+        for (uint32_t i = 0; i < t->count; ++i) {
+            const double d[3] = {y[0] - t->pos[i][0], y[1] - t->pos[i][1], y[2] - t->pos[i][2]};
+            if (sqrt(dot3(d, d)) < 6.0 * t->mass[i]) cont->near_source = 1;
+        }
+        if (status == ORC_RAY_ESCAPED) {
+            double dy[6];
+            orc_ms_rhs(t, y, dy);
+            const double len = sqrt(dy[0] * dy[0] + dy[1] * dy[1] + dy[2] * dy[2]);
+            if (len > 1e-12) {
+                for (int i = 0; i < 3; ++i) cont->exit_dir[i] = -dy[i] / len;
+            } else {
+                cont->exit_dir[0] = cont->exit_dir[1] = 0.0;
+                cont->exit_dir[2] = -1.0;
+            }
+        }
+        if (hit) {
+            /* the record describes the first hit */
+            status = ORC_RAY_DISK;
+            memcpy(y, y_hit, sizeof y_hit);
+            lambda = lambda_hit;
+            phi = phi_hit;
+            r_hit = r_hit1;
+            g = g_hit1;
+            acc = acc_hit;
+            rej = rej_hit;
+            flags = flags_hit;
+            body = body_hit;
+        }
+    }
     const double rr = sqrt(dot3(y, y));
+    out->body = body;
     out->status = status;
     out->flags = flags;
     out->steps_accepted = acc;
@@ -611,6 +699,7 @@ typedef struct {
     const uint64_t* idx;
     uint64_t first, count;
     orc_ray* out;
+    orc_cont* cont;
     atomic_ullong next;
 } work_t;
 
@@ -624,14 +713,14 @@ static void* worker(void* arg)
         for (uint64_t i = b; i < e; ++i) {
             const uint64_t pix = w->idx ? w->idx[i] : w->first + i;
             trace_one(w->cam, w->t, (uint32_t)(pix % w->cam->screen_width), (uint32_t)(pix / w->cam->screen_width),
-                      &w->out[i]);
+                      &w->out[i], w->cont ? &w->cont[i] : NULL);
         }
     }
     return NULL;
 }
 
-void orc_ms_trace(const orc_camera* cam, const orc_ms_table* t, const uint64_t* pixel_index, uint64_t first,
-                  uint64_t count, orc_ray* out, int threads)
+static void run(const orc_camera* cam, const orc_ms_table* t, const uint64_t* pixel_index, uint64_t first,
+                uint64_t count, orc_ray* out, orc_cont* cont, int threads)
 {
     if (threads <= 0) threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
     if (threads < 1) threads = 1;
@@ -642,6 +731,7 @@ void orc_ms_trace(const orc_camera* cam, const orc_ms_table* t, const uint64_t* 
     w.first = first;
     w.count = count;
     w.out = out;
+    w.cont = cont;
     atomic_init(&w.next, 0);
     pthread_t* tid = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)threads);
     int started = 0;
@@ -650,4 +740,16 @@ void orc_ms_trace(const orc_camera* cam, const orc_ms_table* t, const uint64_t* 
     if (started == 0) worker(&w);
     for (int i = 0; i < started; ++i) pthread_join(tid[i], NULL);
     free(tid);
+}
+
+void orc_ms_trace(const orc_camera* cam, const orc_ms_table* t, const uint64_t* pixel_index, uint64_t first,
+                  uint64_t count, orc_ray* out, int threads)
+{
+    run(cam, t, pixel_index, first, count, out, NULL, threads);
+}
+
+void orc_ms_trace_cont(const orc_camera* cam, const orc_ms_table* t, const uint64_t* pixel_index, uint64_t first,
+                       uint64_t count, orc_ray* out, orc_cont* cont, int threads)
+{
+    run(cam, t, pixel_index, first, count, out, cont, threads);
 }

@@ -50,7 +50,9 @@ RAY_DTYPE = np.dtype([
     ("status", "u4"), ("flags", "u4"), ("steps_accepted", "u4"), ("steps_rejected", "u4"),
     ("r", "f8"), ("theta", "f8"), ("phi", "f8"), ("r_hit", "f8"), ("g", "f8"), ("lambda", "f8"),
     ("dH", "f8"), ("dE", "f8"), ("dLz", "f8"), ("dQ", "f8"), ("db_shadow", "f8"), ("exit_dir", "f8", (3,)),
+    ("body", "u4"), ("pad", "u4"),
 ])
+BODY_NONE = 0xFFFFFFFF
 
 CAPTURED, ESCAPED, DISK, UNFINISHED = 1, 2, 3, 0
 
@@ -58,7 +60,8 @@ CAPTURED, ESCAPED, DISK, UNFINISHED = 1, 2, 3, 0
 MAX_CROSSINGS = 8
 CONT_DTYPE = np.dtype([
     ("n_cross", "u4"), ("fate", "u4"), ("cross_r", "f8", MAX_CROSSINGS), ("cross_phi", "f8", MAX_CROSSINGS),
-    ("cross_g", "f8", MAX_CROSSINGS), ("exit_dir", "f8", (3,)),
+    ("cross_g", "f8", MAX_CROSSINGS), ("exit_dir", "f8", (3,)), ("cross_src", "u4", MAX_CROSSINGS),
+    ("near_source", "u4"), ("pad", "u4"),
 ])
 
 # orc_source: a black-hole body beside the camera's hole (ms_oracle.c)
@@ -132,6 +135,8 @@ def lib() -> ctypes.CDLL:
         L.orc_ms_initial_state.argtypes = [v, v, ctypes.c_uint32, ctypes.c_uint32, v]
         L.orc_ms_trace.argtypes = [v, v, v, ctypes.c_uint64, ctypes.c_uint64, v, ctypes.c_int]
         L.orc_ms_trace.restype = None
+        L.orc_ms_trace_cont.argtypes = [v, v, v, ctypes.c_uint64, ctypes.c_uint64, v, v, ctypes.c_int]
+        L.orc_ms_trace_cont.restype = None
         L.orc_kn_horizon.argtypes = [d, d, d]
         L.orc_kn_horizon.restype = d
         L.orc_kn_metric.argtypes = [d, d, d, d, d, v]
@@ -295,6 +300,20 @@ def ms_trace(cam: dict, sources, pixels: np.ndarray | None = None, threads: int 
         out = np.zeros(idx.size, dtype=RAY_DTYPE)
         lib().orc_ms_trace(_p(c), _p(t), _p(idx), 0, idx.size, _p(out), threads)
     return out
+
+
+def ms_trace_cont(cam: dict, sources, pixels: np.ndarray | None = None,
+                  threads: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Multi-source trace with the translucent-disk continuation: (records of the
+    first hits, continuation records with each crossing's source)."""
+    c = to_camera(cam)
+    t = ms_table(cam, sources)
+    idx = None if pixels is None else np.ascontiguousarray(pixels, dtype=np.uint64)
+    n = int(cam["screen_width"]) * int(cam["screen_height"]) if idx is None else idx.size
+    out = np.zeros(n, dtype=RAY_DTYPE)
+    cont = np.zeros(n, dtype=CONT_DTYPE)
+    lib().orc_ms_trace_cont(_p(c), _p(t), None if idx is None else _p(idx), 0, n, _p(out), _p(cont), threads)
+    return out, cont
 
 
 def bl_initial_state(cam: dict, charge: float, px: int, py: int) -> np.ndarray:

@@ -54,7 +54,8 @@ struct rt_handle {
     bool shade_on = false;               // rt_set_shading
     // translucent-disk continuation of a shaded dispatch: each ray's disk crossings
     // and how it ended, and what the launches pass the tracer
-    DevBuf cont_cross, cont_info;
+    DevBuf cont_cross, cont_info, cont_body;
+    DevBuf ms_shade;  // multi-source shading: one descriptor per source
     ContOut cur_cont{};
     rt_shading shading{};
     DevBuf ray_fields[kRayFields];
@@ -323,11 +324,13 @@ rt_status shade_prepare(rt_handle* h, const rt_camera* cam, cudaStream_t s) {
 // Turn on the translucent-disk continuation for the launches of a shaded
 // dispatch of n rays: the tracers record each disk crossing and follow the ray
 // on through the disk; the shading pass composes the crossings.
-rt_status begin_continuation(rt_handle* h, size_t n) {
+rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false) {
     rt_status st = ensure(h, h->cont_cross, sizeof(double) * 3 * kMaxCrossings * n);
     if (st == RT_OK) st = ensure(h, h->cont_info, sizeof(uint32_t) * n);
+    if (st == RT_OK && bodies) st = ensure(h, h->cont_body, sizeof(uint32_t) * n);
     if (st != RT_OK) return st;
-    h->cur_cont = ContOut{static_cast<double*>(h->cont_cross.ptr), static_cast<uint32_t*>(h->cont_info.ptr), n};
+    h->cur_cont = ContOut{static_cast<double*>(h->cont_cross.ptr), static_cast<uint32_t*>(h->cont_info.ptr), n,
+                          bodies ? static_cast<uint32_t*>(h->cont_body.ptr) : nullptr};
     return RT_OK;
 }
 
@@ -502,6 +505,7 @@ rt_status ms_launch(rt_handle* h, const rt_camera* cam, const rt_source* src, ui
     args.queue = static_cast<unsigned long long*>(h->queue.ptr);
     args.stats = static_cast<unsigned long long*>(h->stats.ptr);
     args.out = out;
+    args.cont = h->cur_cont;
     RT_CUDA(h, cudaEventRecord(h->ev0, s));
     launch_ms_trace(args, ms_trace_grid(h->sm_count), s);
     RT_CUDA(h, cudaGetLastError());
@@ -637,6 +641,48 @@ extern "C" {
 
 int rt_abi_version(void) { return RT_ABI_VERSION; }
 
+// Shading descriptors of a multi-source scene: the camera's hole with
+// rt_shading's resolved disk, each body with its own disk profile; every
+// source shaded by the thin procedural model at detail 1 (trace_multi_source,
+// software_compute_engine.hpp:3172-3185).
+rt_status ms_shade_prepare(rt_handle* h, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
+                           cudaStream_t s) {
+    MsSource table[kMaxSources];
+    const uint32_t count = build_ms_sources(*cam, sources, n_sources, table);
+    ShadeDesc d[kMaxSources];
+    ShadeDesc base;
+    if (!build_shade_desc(*cam, h->shading, base)) return fail(h, RT_ERR_INVALID_ARG, "unsupported shading settings");
+    build_source_shade_desc(base, nullptr, table[0].m, table[0].a, table[0].disk_in, table[0].disk_out, d[0]);
+    for (uint32_t i = 1; i < count; ++i)
+        build_source_shade_desc(base, reinterpret_cast<const float*>(&sources[i - 1].disk), table[i].m, table[i].a,
+                                table[i].disk_in, table[i].disk_out, d[i]);
+    rt_status st;
+    if ((st = ensure(h, h->ms_shade, sizeof(ShadeDesc) * kMaxSources)) != RT_OK) return st;
+    // pageable descriptors: the copy is staged before the call returns
+    RT_CUDA(h, cudaMemcpyAsync(h->ms_shade.ptr, d, sizeof(ShadeDesc) * count, cudaMemcpyHostToDevice, s));
+    return RT_OK;
+}
+
+// Trace a multi-source window into device outputs; shaded (handle shading on,
+// pixels requested): every ray followed through the translucent disks and its
+// crossings composed by the shading pass.
+rt_status ms_dispatch_window(rt_handle* h, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
+                             uint32_t row0, uint32_t nrows, const OutPtrs& out, cudaStream_t s) {
+    const size_t n = static_cast<size_t>(cam->screen_width) * nrows;
+    const bool shade = h->shade_on && out.pixels;
+    rt_status st;
+    ContinuationScope cont_scope{h};
+    if (shade && (st = ms_shade_prepare(h, cam, sources, n_sources, s)) != RT_OK) return st;
+    if (shade && (st = begin_continuation(h, n, true)) != RT_OK) return st;
+    if ((st = ms_launch(h, cam, sources, n_sources, row0, nrows, out, s)) != RT_OK) return st;
+    if (shade) {
+        launch_shade(static_cast<const ShadeDesc*>(h->ms_shade.ptr), nullptr, nullptr, nullptr, nullptr, h->cur_cont,
+                     out.pixels, n, s);
+        RT_CUDA(h, cudaGetLastError());
+    }
+    return RT_OK;
+}
+
 rt_status rt_dispatch_multi(rt_handle* h, const rt_camera* cam, const rt_source* sources, uint32_t n_sources,
                             rt_pixel_out* pixels, const rt_ray_out* rays, size_t capacity) {
     if (!h) return RT_ERR_INVALID_ARG;
@@ -655,7 +701,8 @@ rt_status rt_dispatch_multi(rt_handle* h, const rt_camera* cam, const rt_source*
         if ((st = ensure(h, h->pixels, n * sizeof(rt_pixel_out))) != RT_OK) return st;
         dpix = static_cast<rt_pixel_out*>(h->pixels.ptr);
     }
-    if ((st = ms_launch(h, cam, sources, n_sources, row0, nrows, OutPtrs{dpix, dev}, h->stream)) != RT_OK) return st;
+    if ((st = ms_dispatch_window(h, cam, sources, n_sources, row0, nrows, OutPtrs{dpix, dev}, h->stream)) != RT_OK)
+        return st;
     if ((st = copy_back(h, rays, dev, pixels, dpix, n, h->stream)) != RT_OK) return st;
     return wait_stream(h, h->stream, 0.0);
 }
@@ -673,7 +720,8 @@ rt_status rt_dispatch_multi_device(rt_handle* h, const rt_camera* cam, const rt_
     if (capacity < n) return fail(h, RT_ERR_INVALID_ARG, "capacity smaller than the window");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
     RT_CUDA(h, cudaSetDevice(h->device));
-    return ms_launch(h, cam, sources, n_sources, row0, nrows, OutPtrs{pixels, rays ? *rays : rt_ray_out{}}, s);
+    return ms_dispatch_window(h, cam, sources, n_sources, row0, nrows, OutPtrs{pixels, rays ? *rays : rt_ray_out{}},
+                              s);
 }
 
 double rt_kerr_isco_radius(double mass, double spin) { return kerr_isco_radius(mass, spin); }
@@ -741,6 +789,10 @@ void rt_destroy(rt_handle* h) {
     release(h->band_desc);
     release(h->band_queue);
     release(h->shade_desc);
+    release(h->ms_shade);
+    release(h->cont_cross);
+    release(h->cont_info);
+    release(h->cont_body);
     release(h->park_d);
     release(h->park_u);
     release(h->pass_queues);

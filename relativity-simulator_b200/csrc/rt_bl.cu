@@ -363,6 +363,7 @@ __device__ __noinline__ void bl_finish(const BlDesc* __restrict__ Bp, BlCold<BLO
     if (R.dE) R.dE[o] = E / e0 - 1.0;
     if (R.dLz) R.dLz[o] = (L - S.l0[tid]) / e0;
     if (R.dQ) R.dQ[o] = (Q - S.q0[tid]) / (e0 * e0);
+    if (R.body) R.body[o] = (status == RT_RAY_DISK || status == RT_RAY_CAPTURED) ? 0u : RT_BODY_NONE;
     if (R.exit_x || R.exit_y || R.exit_z) {
         // sky-lookup direction of an escaped ray: the orthonormal-frame velocity
         // (sqrt(g_rr) u^r, sqrt(g_thth) u^th, sqrt(g_phph) u^ph) mapped to a

@@ -10,8 +10,8 @@ namespace relsim {
 
 // rt_ray_out as an array of pointers: its fields in declaration order and their
 // element sizes
-constexpr int kRayFields = 17;
-constexpr size_t kRayFieldBytes[kRayFields] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8};
+constexpr int kRayFields = 18;
+constexpr size_t kRayFieldBytes[kRayFields] = {4, 4, 4, 4, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 4};
 static_assert(sizeof(rt_ray_out) == kRayFields * sizeof(void*), "rt_ray_out is an array of pointers");
 
 // Bundle flags.
@@ -76,12 +76,13 @@ constexpr uint32_t kMaxCrossings = 8;
 enum : uint32_t {
     CI_COUNT_MASK = 0xffu,  // bits 0..7: crossings recorded
     CI_FATE_SHIFT = 8u,     // bits 8..11: RT_RAY_* class at the ray's end
-    CI_INSIDE_3RS = 1u << 12  // last point inside 3 r_s (6 M)
+    CI_INSIDE_3RS = 1u << 12  // last point inside 3 r_s (6 M; multi-source: within 6 m of a source)
 };
 struct ContOut {
     double* cross;    // [3 * kMaxCrossings][stride]: r_k at [3k], phi_k at [3k + 1], g_k at [3k + 2]
     uint32_t* info;   // [stride]
     uint64_t stride;
+    uint32_t* body;   // multi-source: [stride], source of crossing k in bits 4k..4k+3 (else null)
 };
 
 // Device counters of one launch.
@@ -173,6 +174,7 @@ struct MsArgs {
     unsigned long long* queue;
     unsigned long long* stats;
     OutPtrs out;
+    ContOut cont;  // translucent-disk continuation (shaded dispatches), else null
 };
 
 // Per-camera constants of the Boyer-Lindquist Kerr-Newman tracer, precomputed
@@ -227,6 +229,8 @@ struct alignas(16) ShadeDesc {
 // Build the shading constants of a camera; false if the settings are not
 // supported (hydro model 2, sky enabled).
 bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d);
+void build_source_shade_desc(const ShadeDesc& base, const float* profile, double mass, double spin, double inner,
+                             double outer, ShadeDesc& d);
 // Shade n rays: pixels[i].rgba from the record's status, r_hit, phi and g.
 void launch_shade(const ShadeDesc* desc, const uint32_t* status, const double* r_hit, const double* phi,
                   const double* g, ContOut cont, rt_pixel_out* pixels, uint64_t n, void* stream);

@@ -359,7 +359,7 @@ template <int BLOCK>
 __device__ __noinline__ void ms_finish(const MsDesc* __restrict__ Bp, const MsSource* __restrict__ src,
                                        MsCold<BLOCK>& S, int tid, const double* y,
                                        uint32_t status, uint32_t flags, uint32_t acc, uint32_t rej, double r_hit,
-                                       double g, const OutPtrs& out) {
+                                       double g, uint32_t body, const OutPtrs& out) {
     const double r = sqrt(dot3(y, y));
     const double theta = acos(fmin(fmax(y[2] / fmax(r, 1e-300), -1.0), 1.0));
     const uint64_t o = Bp->out_offset + S.local[tid];
@@ -378,6 +378,7 @@ __device__ __noinline__ void ms_finish(const MsDesc* __restrict__ Bp, const MsSo
     if (R.dE) R.dE[o] = NAN;
     if (R.dLz) R.dLz[o] = NAN;
     if (R.dQ) R.dQ[o] = NAN;
+    if (R.body) R.body[o] = body;
     if (R.exit_x || R.exit_y || R.exit_z) {
         // sky-lookup direction of an escaped ray: minus the normalised flow of the
         // superposed RHS at the terminal state, (0, 0, -1) where it vanishes
@@ -412,13 +413,38 @@ __device__ __noinline__ void ms_finish(const MsDesc* __restrict__ Bp, const MsSo
     }
 }
 
+// Translucent-disk continuation of a multi-source ray (trace_multi_source,
+// software_compute_engine.hpp:3150-3191): every disk crossing recorded in
+// order along the ray (radius, local azimuth, g and the source), the ray
+// followed to its end.  End record: crossings, class at the end, and whether
+// the end point lies within 6 m of a source (where the reference drops the
+// remaining throughput instead of adding the sky, :3207-3216).
+__device__ __forceinline__ void ms_cont_record(const ContOut& C, uint64_t o, uint32_t k, double r, double az,
+                                               double g) {
+    C.cross[(3 * k) * C.stride + o] = r;
+    C.cross[(3 * k + 1) * C.stride + o] = az;
+    C.cross[(3 * k + 2) * C.stride + o] = g;
+}
+
+__device__ __noinline__ void ms_cont_finish(const ContOut& C, uint64_t o, uint32_t n_cross, uint32_t bodies,
+                                            uint32_t status, const MsSource* __restrict__ src, uint32_t n,
+                                            const double* x) {
+    bool near = false;
+    for (uint32_t i = 0; i < n; ++i) {
+        const double d[3] = {x[0] - src[i].pos[0], x[1] - src[i].pos[1], x[2] - src[i].pos[2]};
+        near = near || sqrt(dot3(d, d)) < 6.0 * src[i].m;
+    }
+    C.info[o] = n_cross | (status << CI_FATE_SHIFT) | (near ? CI_INSIDE_3RS : 0u);
+    C.body[o] = bodies;
+}
+
 __device__ __forceinline__ void ms_unwrap(double& phi, const double* y) {
     double d = atan2(y[1], y[0]) - phi;
     d -= kTwoPi * floor(d / kTwoPi + 0.5);
     phi += d;
 }
 
-template <int BLOCK>
+template <int BLOCK, bool CONT>
 __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs args) {
     __shared__ MsCold<BLOCK> S;
     const unsigned FULL = 0xffffffffu;
@@ -433,6 +459,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
     int inside = -1;
     uint32_t acc = 0, rej = 0, flags = 0, bidx = 0, guard = 0;
     int mode = MS_IDLE;
+    uint32_t n_cross = 0, bodies = 0;  // continuation: crossings so far, their sources
 #pragma unroll
     for (int i = 0; i < 6; ++i) y[i] = k1[i] = 0.0;
     bool queue_open = true;
@@ -488,6 +515,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
                     S.lambda[tid] = 0.0;
                     S.dH[tid] = 0.0;
                     S.phi[tid] = Bp->phi0;
+                    n_cross = bodies = 0;
                     mode = MS_STEP;
                     ++n_rays;
                 }
@@ -509,6 +537,15 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
         const MsDesc* Bp = args.bundles + bidx;
         const MsSource* src = args.sources + Bp->src_begin;
         const uint32_t ns = Bp->src_count;
+        // the end of a ray: its record (with the continuation only when it crossed
+        // no disk: the record describes the first hit) and its continuation end
+        auto end_ray = [&](const double* yend, uint32_t status, uint32_t fl, uint32_t body) {
+            if (!CONT || n_cross == 0)
+                ms_finish<BLOCK>(Bp, src, S, tid, yend, status, fl, acc, rej, NAN, 1.0, body, args.out);
+            if constexpr (CONT)
+                ms_cont_finish(args.cont, Bp->out_offset + S.local[tid], n_cross, bodies, status, src, ns, yend);
+            mode = MS_IDLE;
+        };
         // backstop on loop iterations per ray (one attempt per iteration)
         uint32_t term = 0;
         if (++guard > Bp->max_steps + 64u) {
@@ -533,8 +570,9 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
             }
         }
         if (term) {
-            ms_finish<BLOCK>(Bp, src, S, tid, y, term & 15u, flags, acc, rej, NAN, 1.0, args.out);
-            mode = MS_IDLE;
+            const uint32_t cls = term & 15u;
+            end_ray(y, cls, flags,
+                    (cls == RT_RAY_CAPTURED && inside >= 0) ? static_cast<uint32_t>(inside) : RT_BODY_NONE);
             continue;
         }
 
@@ -572,70 +610,97 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
 #pragma unroll
         for (int i = 0; i < 6; ++i) finite = finite && isfinite(y5[i]);
         if (!finite) {
-            ms_finish<BLOCK>(Bp, src, S, tid, y, RT_RAY_CAPTURED, flags | RT_RAYFLAG_NONFINITE, acc, rej, NAN, 1.0,
-                             args.out);
-            mode = MS_IDLE;
+            end_ray(y, RT_RAY_CAPTURED, flags | RT_RAYFLAG_NONFINITE, RT_BODY_NONE);
             continue;
         }
-        // disk crossings: the earliest local equator crossing on a disk
+        // disk crossings of this step in order along the ray, each the earliest
+        // local-equator crossing on a disk after the previous one: the first ends
+        // the ray; under the continuation each is recorded and the ray goes on
         {
-            double best = 2.0, best_r = 0.0, best_lz = 0.0;
-            uint32_t best_i = 0;
+            bool ended = false;
+            double t_prev = -1.0;
 #pragma unroll 1
-            for (uint32_t i = 0; i < ns; ++i) {
-                const MsSource& s = src[i];
-                if (s.disk_in < 0.0) continue;
-                const double r0[3] = {y[0] - s.pos[0], y[1] - s.pos[1], y[2] - s.pos[2]};
-                const double r1[3] = {y5[0] - s.pos[0], y5[1] - s.pos[1], y5[2] - s.pos[2]};
-                const double z0 = dot3(r0, s.axis), z1 = dot3(r1, s.axis);
-                if (!(z0 * z1 <= 0.0) || z0 == z1) continue;
-                const double sl = z0 / (z0 - z1);
-                const double ce[3] = {r0[0] + sl * (r1[0] - r0[0]), r0[1] + sl * (r1[1] - r0[1]),
-                                      r0[2] + sl * (r1[2] - r0[2])};
-                const double lxe = dot3(ce, s.fx), lye = dot3(ce, s.fy);
-                const double re = sqrt(fmax(lxe * lxe + lye * lye - s.a * s.a, 0.0));
-                const double margin = 0.05 * re + 0.5 * s.m;
-                if (re < s.disk_in - margin || re > s.disk_out + margin) continue;
-                double co[4][6];
-                ms_dense_coeffs<BLOCK>(y, y5, k1, k7, hh, S, tid, co);
-                const double t = ms_local_z_root(s, y, co, z0, z1);
-                if (!(t < best)) continue;
-                double yr[6];
+            for (uint32_t pass = 0; pass < ns; ++pass) {
+                double best = 2.0, best_r = 0.0, best_lz = 0.0, best_az = 0.0;
+                uint32_t best_i = 0;
+#pragma unroll 1
+                for (uint32_t i = 0; i < ns; ++i) {
+                    const MsSource& s = src[i];
+                    if (s.disk_in < 0.0) continue;
+                    const double r0[3] = {y[0] - s.pos[0], y[1] - s.pos[1], y[2] - s.pos[2]};
+                    const double r1[3] = {y5[0] - s.pos[0], y5[1] - s.pos[1], y5[2] - s.pos[2]};
+                    const double z0 = dot3(r0, s.axis), z1 = dot3(r1, s.axis);
+                    if (!(z0 * z1 <= 0.0) || z0 == z1) continue;
+                    const double sl = z0 / (z0 - z1);
+                    const double ce[3] = {r0[0] + sl * (r1[0] - r0[0]), r0[1] + sl * (r1[1] - r0[1]),
+                                          r0[2] + sl * (r1[2] - r0[2])};
+                    const double lxe = dot3(ce, s.fx), lye = dot3(ce, s.fy);
+                    const double re = sqrt(fmax(lxe * lxe + lye * lye - s.a * s.a, 0.0));
+                    const double margin = 0.05 * re + 0.5 * s.m;
+                    if (re < s.disk_in - margin || re > s.disk_out + margin) continue;
+                    double co[4][6];
+                    ms_dense_coeffs<BLOCK>(y, y5, k1, k7, hh, S, tid, co);
+                    const double t = ms_local_z_root(s, y, co, z0, z1);
+                    if (!(t < best) || !(t > t_prev)) continue;
+                    double yr[6];
 #pragma unroll
-                for (int q = 0; q < 6; ++q) yr[q] = ms_dense_at(y, co, q, t);
-                const double rel[3] = {yr[0] - s.pos[0], yr[1] - s.pos[1], yr[2] - s.pos[2]};
-                const double c0 = dot3(rel, s.fx), c1 = dot3(rel, s.fy);
-                const double pl[3] = {dot3(yr + 3, s.fx), dot3(yr + 3, s.fy), dot3(yr + 3, s.axis)};
-                const double rr = sqrt(fmax(c0 * c0 + c1 * c1 - s.a * s.a, 0.0));
-                if (rr < s.disk_in || rr > s.disk_out || rr <= s.rh * 1.02) continue;
-                best = t;
-                best_r = rr;
-                best_i = i;
-                best_lz = (c0 * pl[1] - c1 * pl[0]) / fmax(sqrt(dot3(pl, pl)), 1e-30);
-            }
-            if (best <= 1.0) {
+                    for (int q = 0; q < 6; ++q) yr[q] = ms_dense_at(y, co, q, t);
+                    const double rel[3] = {yr[0] - s.pos[0], yr[1] - s.pos[1], yr[2] - s.pos[2]};
+                    const double c0 = dot3(rel, s.fx), c1 = dot3(rel, s.fy);
+                    const double pl[3] = {dot3(yr + 3, s.fx), dot3(yr + 3, s.fy), dot3(yr + 3, s.axis)};
+                    const double rr = sqrt(fmax(c0 * c0 + c1 * c1 - s.a * s.a, 0.0));
+                    if (rr < s.disk_in || rr > s.disk_out || rr <= s.rh * 1.02) continue;
+                    best = t;
+                    best_r = rr;
+                    best_i = i;
+                    best_lz = (c0 * pl[1] - c1 * pl[0]) / fmax(sqrt(dot3(pl, pl)), 1e-30);
+                    // local azimuth of the crossing (ms_disk_crossing, :3037)
+                    best_az = atan2(c1, c0) - atan2(s.a, rr);
+                }
+                if (best > 1.0) break;
                 double co[4][6], yr[6];
                 ms_dense_coeffs<BLOCK>(y, y5, k1, k7, hh, S, tid, co);
 #pragma unroll
                 for (int q = 0; q < 6; ++q) yr[q] = ms_dense_at(y, co, q, best);
-                S.lambda[tid] += best * hh;
-                double ph = S.phi[tid];
-                ms_unwrap(ph, yr);
-                S.phi[tid] = ph;
                 const MsSource& s = src[best_i];
-                ms_finish<BLOCK>(Bp, src, S, tid, yr, RT_RAY_DISK, flags, acc, rej, best_r,
-                                 disk_redshift(s.m, s.a, best_r, best_lz), args.out);
-                mode = MS_IDLE;
-                continue;
+                const double g = disk_redshift(s.m, s.a, best_r, best_lz);
+                const double lam = S.lambda[tid], ph0 = S.phi[tid];
+                if (!CONT || n_cross == 0) {
+                    S.lambda[tid] = lam + best * hh;
+                    double ph = ph0;
+                    ms_unwrap(ph, yr);
+                    S.phi[tid] = ph;
+                    ms_finish<BLOCK>(Bp, src, S, tid, yr, RT_RAY_DISK, flags, acc, rej, best_r, g, best_i, args.out);
+                }
+                if constexpr (!CONT) {
+                    mode = MS_IDLE;
+                    ended = true;
+                    break;
+                } else {
+                    // the crossing recorded; the ray goes on through the disk
+                    S.lambda[tid] = lam;
+                    S.phi[tid] = ph0;
+                    ms_cont_record(args.cont, Bp->out_offset + S.local[tid], n_cross, best_r, best_az, g);
+                    bodies |= best_i << (4u * n_cross);
+                    ++n_cross;
+                    t_prev = best;
+                    if (n_cross >= kMaxCrossings) {
+                        ms_cont_finish(args.cont, Bp->out_offset + S.local[tid], n_cross, bodies, RT_RAY_UNFINISHED,
+                                       src, ns, yr);
+                        mode = MS_IDLE;
+                        ended = true;
+                        break;
+                    }
+                }
             }
+            if (ended) continue;
         }
         if (inside5 >= 0) {  // captured inside this step: its end point
             S.lambda[tid] += hh;
             double ph = S.phi[tid];
             ms_unwrap(ph, y5);
             S.phi[tid] = ph;
-            ms_finish<BLOCK>(Bp, src, S, tid, y5, RT_RAY_CAPTURED, flags, acc, rej, NAN, 1.0, args.out);
-            mode = MS_IDLE;
+            end_ray(y5, RT_RAY_CAPTURED, flags, static_cast<uint32_t>(inside5));
             continue;
         }
         if (dot3(y5, y5) > Bp->r_esc * Bp->r_esc) {  // escaped: interpolated to the escape radius
@@ -646,8 +711,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
             double ph = S.phi[tid];
             ms_unwrap(ph, yt);
             S.phi[tid] = ph;
-            ms_finish<BLOCK>(Bp, src, S, tid, yt, RT_RAY_ESCAPED, flags, acc, rej, NAN, 1.0, args.out);
-            mode = MS_IDLE;
+            end_ray(yt, RT_RAY_ESCAPED, flags, RT_BODY_NONE);
             continue;
         }
         S.dH[tid] = fmax(S.dH[tid], ms_project(src, ns, y5, Bp->proj_tol));
@@ -688,13 +752,14 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) ms_trace_kernel(MsArgs arg
     }
 }
 
-template __global__ void ms_trace_kernel<128>(MsArgs);
+template __global__ void ms_trace_kernel<128, false>(MsArgs);
+template __global__ void ms_trace_kernel<128, true>(MsArgs);
 
 }  // namespace
 
 uint32_t ms_trace_grid(int sm_count) {
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ms_trace_kernel<128>, 128, 0) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ms_trace_kernel<128, false>, 128, 0) != cudaSuccess) {
         cudaGetLastError();
         occ = 1;
     }
@@ -702,7 +767,10 @@ uint32_t ms_trace_grid(int sm_count) {
 }
 
 void launch_ms_trace(const MsArgs& args, uint32_t grid, void* stream) {
-    ms_trace_kernel<128><<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(args);
+    if (args.cont.cross)
+        ms_trace_kernel<128, true><<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(args);
+    else
+        ms_trace_kernel<128, false><<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(args);
 }
 
 }  // namespace relsim

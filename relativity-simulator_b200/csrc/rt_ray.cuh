@@ -230,6 +230,7 @@ __device__ __noinline__ void finish_ray(const BundleDesc* __restrict__ Bp, ColdT
     if (R.dE) R.dE[o] = energy - 1.0;
     if (R.dLz) R.dLz[o] = lz - S.lz0[tid];
     if (R.dQ) R.dQ[o] = q - S.q0[tid];
+    if (R.body) R.body[o] = (status == RT_RAY_DISK || status == RT_RAY_CAPTURED) ? 0u : RT_BODY_NONE;
     if (R.exit_x || R.exit_y || R.exit_z) {
         // sky-lookup direction of an escaped ray: -dx/dlambda at the terminal
         // state, normalised (software_compute_engine.hpp:1771-1775); each

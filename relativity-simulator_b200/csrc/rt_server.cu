@@ -121,12 +121,13 @@ struct Request {
         return static_cast<int>(cam.precision_mode);
     }
     // GPU time of one ray in units of a mixed-precision Kerr-Schild ray (measured
-    // on B200: mixed 194 Mrays/s, FP64 105, Boyer-Lindquist 47, multi-source about
-    // 39 / holes); epochs are budgeted in these units so that an epoch of slow
+    // on B200: mixed 160 Mrays/s, FP64 105, Boyer-Lindquist 47; multi-source
+    // about 90 / holes at rtol 1e-8, the mixed mode's tolerance, and 40 / holes
+    // at 1e-10); epochs are budgeted in these units so that an epoch of slow
     // rays does not hold the GPU much longer than one of fast rays
     uint64_t cost() const {
         switch (kind()) {
-            case 2: return 5ull * n_sources;
+            case 2: return (cam.rtol >= 1e-9 ? 2ull : 4ull) * n_sources;
             case 3: return 4;
             case RT_PRECISION_MIXED: return 1;
             default: return 2;

@@ -2,12 +2,13 @@
 //
 // After a trace, one thread per ray turns the ray's radiance into the pixel's
 // sRGB colour, as the reference's CPU image path does
-// (software_compute_engine.hpp:1538-1611, 1734-1808).  With the
-// translucent-disk continuation (the handle's dispatches) the tracers have
-// already shaded every disk crossing at the throughput left (rt_shade.cuh) and
-// this pass reads the accumulated radiance; without it (the server) the record's
-// first hit (class, r_hit, phi, g) is shaded here as the thin disk at the
-// crossing (AccretionDiskModel::shade,
+// (software_compute_engine.hpp:1538-1611, 1734-1808, 3150-3252).  With the
+// translucent-disk continuation (the handle's dispatches) the tracers record
+// every disk crossing of a ray and this pass shades them in order at the
+// throughput left, each with the descriptor of the source whose disk it
+// crossed (multi-source scenes: one per source); without it (the server) the
+// record's first hit (class, r_hit, phi, g) is shaded here as the thin disk at
+// the crossing (AccretionDiskModel::shade,
 // render/accretion_disk/accretion_disk_model.hpp:245-316, with the
 // Novikov-Thorne base temperature of hydro model 1,
 // render/accretion_disk/hydro_disk_shading.hpp:160-171).  The radiance is
@@ -60,7 +61,7 @@ __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict_
                                                     const double* __restrict__ phi,
                                                     const double* __restrict__ g, ContOut cont,
                                                     rt_pixel_out* __restrict__ pixels, uint64_t n) {
-    const ShadeDesc& D = *Dp;
+    const ShadeDesc& D = *Dp;  // the camera's hole (and the tonemap)
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         double acc[3] = {0.0, 0.0, 0.0};
@@ -71,12 +72,13 @@ __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict_
             // the way the ray ended, if the throughput lasted to the end
             const uint32_t info = cont.info[i];
             const uint32_t n_cross = info & CI_COUNT_MASK;
+            const uint32_t bodies = cont.body ? cont.body[i] : 0u;  // source of each crossing
             double thr = 1.0, last_g = 1.0;
             for (uint32_t k = 0; k < n_cross && thr > kMinThroughput; ++k) {
                 double sh[4];
                 const double gk = cont.cross[(3 * k + 2) * cont.stride + i];
-                disk_radiance(D, cont.cross[(3 * k) * cont.stride + i], cont.cross[(3 * k + 1) * cont.stride + i], gk,
-                              sh);
+                disk_radiance(Dp[(bodies >> (4u * k)) & 15u], cont.cross[(3 * k) * cont.stride + i],
+                              cont.cross[(3 * k + 1) * cont.stride + i], gk, sh);
                 acc[0] += thr * sh[0];
                 acc[1] += thr * sh[1];
                 acc[2] += thr * sh[2];
@@ -216,6 +218,23 @@ bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d) {
         d.nt_rate_factor = std::pow(mxd(static_cast<double>(s.accretion_rate_scale), 1e-6), 0.25);
     }
     return true;
+}
+
+// A multi-source body's descriptor from the scene's base descriptor: its disk
+// profile as it stands (GpuBodyData::disk), its geometry; the thin procedural
+// model at detail 1, as trace_multi_source shades every source
+// (software_compute_engine.hpp:3172-3185).
+void build_source_shade_desc(const ShadeDesc& base, const float* profile, double mass, double spin, double inner,
+                             double outer, ShadeDesc& d) {
+    d = base;
+    if (profile) std::copy_n(profile, 32, d.profile);
+    d.mass = mxd(mass, 1e-9);
+    d.disk_spin = spin;
+    d.inner = mxd(inner, 1e-9);
+    d.outer = mxd(outer, d.inner * 1.0001);
+    d.detail = 1.0;
+    d.hydro_model = 0u;
+    d.pattern_omega = orbital_omega(d.mass, spin, std::sqrt(d.inner * d.outer));
 }
 
 void launch_shade(const ShadeDesc* desc, const uint32_t* status, const double* r_hit, const double* phi,

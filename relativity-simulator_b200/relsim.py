@@ -79,7 +79,8 @@ RAY_FIELDS = [("status", np.uint32), ("flags", np.uint32), ("steps_accepted", np
               ("steps_rejected", np.uint32), ("r", np.float64), ("theta", np.float64), ("phi", np.float64),
               ("r_hit", np.float64), ("g", np.float64), ("lambda", np.float64), ("dH", np.float64),
               ("dE", np.float64), ("dLz", np.float64), ("dQ", np.float64), ("exit_x", np.float64),
-              ("exit_y", np.float64), ("exit_z", np.float64)]
+              ("exit_y", np.float64), ("exit_z", np.float64), ("body", np.uint32)]
+BODY_NONE = 0xFFFFFFFF  # RT_BODY_NONE
 PIXEL_DTYPE = np.dtype([("r", "f4"), ("g", "f4"), ("b", "f4"), ("a", "f4"), ("redshift", "f4"),
                         ("affine_parameter", "f4"), ("status_flags", "u4"), ("iterations_used", "u4")])
 
@@ -101,7 +102,7 @@ class Stats(ctypes.Structure):
 class Source(ctypes.Structure):
     """rt_source: a black-hole body beside the camera's hole (multi-source scenes)."""
     _fields_ = [("position", _d * 3), ("mass", _d), ("spin_parameter", _d), ("axis", _d * 3), ("disk_enabled", _d),
-                ("disk_inner_scale", _d), ("disk_outer_units", _d)]
+                ("disk_inner_scale", _d), ("disk_outer_units", _d), ("disk", DiskProfile)]
 
 
 MAX_SOURCES = 16  # RT_MAX_SOURCES: the camera's hole and up to 15 sources
@@ -109,9 +110,13 @@ RAYFLAG_DIVERGED = 16
 
 
 def make_source(position, mass: float = 1.0, spin_parameter: float = 0.0, axis=(0.0, 0.0, 1.0), disk: bool = True,
-                disk_inner_scale: float = 1.0, disk_outer_units: float = 20.0) -> Source:
+                disk_inner_scale: float = 1.0, disk_outer_units: float = 20.0,
+                profile: "DiskProfile | None" = None) -> Source:
+    """A body; its disk appearance defaults to GpuDiskProfile's defaults (rt_shading_defaults' disk)."""
+    if profile is None:
+        profile = shading().disk
     return Source((_d * 3)(*position), mass, spin_parameter, (_d * 3)(*axis), 1.0 if disk else 0.0, disk_inner_scale,
-                  disk_outer_units)
+                  disk_outer_units, profile)
 
 
 class ServerConfig(ctypes.Structure):

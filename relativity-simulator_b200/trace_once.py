@@ -42,7 +42,7 @@ def main() -> None:
     ap.add_argument("--charge", type=float, default=0.0, help="Kerr-Newman charge Q (--metric bl)")
     ap.add_argument("--sources", type=int, default=0,
                     help="multi-source scene: the first request of the seeded stream with this many bodies beside "
-                         "the camera's hole (its camera, at --side), traced by the multi-source tracer")
+                         "the camera's hole (its camera at --side and --precision), traced by the multi-source tracer")
     ap.add_argument("--device", action="store_true",
                     help="device-resident outputs (rt_dispatch_device: one set of launches, no host bands)")
     ap.add_argument("--shade", action="store_true",
@@ -62,8 +62,10 @@ def main() -> None:
         import scenes
 
         req = [r for r in scenes.request_stream() if r.multi_source and len(r.sources) == a.sources][0]
-        cam = req.bundle.camera(relsim.PRECISION_FP64)
+        cam = req.bundle.camera(relsim.PRECISION_MIXED if a.precision == "mixed" else relsim.PRECISION_FP64)
         cam.screen_width = cam.screen_height = a.side
+        if a.rtol is not None:
+            cam.rtol = cam.atol = a.rtol
         srcs = scenes.rt_sources(req.sources)
     with relsim.Tracer(0) as tr:
         tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread, a.fp64_rolled, a.mixed_single)
