@@ -38,6 +38,8 @@ struct rt_handle {
     bool ready = false;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;          // second stream of banded host dispatches
+    cudaStream_t stream3 = nullptr;          // the mixed tracer's critical pass, beside its near passes
+    cudaEvent_t ev_cfork = nullptr, ev_cjoin = nullptr;
     cudaStream_t copy_stream = nullptr;      // their device-to-host copies
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -173,7 +175,7 @@ rt_status ensure_two_pass(rt_handle* h, uint64_t total) {
     rt_status st;
     if ((st = ensure(h, h->park_d, sizeof(double) * PD_COUNT * total)) != RT_OK) return st;
     if ((st = ensure(h, h->park_u, sizeof(uint32_t) * PU_COUNT * total)) != RT_OK) return st;
-    return ensure(h, h->pass_queues, sizeof(uint32_t) * 3 * total);
+    return ensure(h, h->pass_queues, sizeof(uint32_t) * 4 * total);
 }
 
 bool uses_two_pass(const rt_launch_config& c, bool mixed, uint64_t total) {
@@ -188,7 +190,7 @@ rt_status launch_two_pass(rt_handle* h, uint32_t n_bundles, uint64_t total, cons
         if (st != RT_OK) return st;
     } else if (h->park_d.bytes < sizeof(double) * PD_COUNT * total ||
                h->park_u.bytes < sizeof(uint32_t) * PU_COUNT * total ||
-               h->pass_queues.bytes < sizeof(uint32_t) * 3 * total) {
+               h->pass_queues.bytes < sizeof(uint32_t) * 4 * total) {
         return fail(h, RT_ERR_INVALID_ARG, "two-pass buffers not reserved before capture");
     }
     TraceArgs args{};
@@ -204,6 +206,9 @@ rt_status launch_two_pass(rt_handle* h, uint32_t n_bundles, uint64_t total, cons
     buf.park = ParkBuf{static_cast<double*>(h->park_d.ptr), static_cast<uint32_t*>(h->park_u.ptr), total};
     buf.queues = static_cast<uint32_t*>(h->pass_queues.ptr);
     buf.counters = static_cast<char*>(h->queue.ptr);
+    buf.crit_stream = h->stream3;
+    buf.crit_fork = h->ev_cfork;
+    buf.crit_join = h->ev_cjoin;
     RT_CUDA(h, cudaMemsetAsync(h->stats.ptr, 0, sizeof(unsigned long long) * ST_COUNT, s));
     if (!capturing) RT_CUDA(h, cudaEventRecord(h->ev0, s));
     const bool banded = bands > 1 && !capturing;
@@ -760,6 +765,9 @@ rt_status rt_create(rt_handle** out, int device_ordinal) {
     h->sm_count = p.multiProcessorCount;
     if (cudaSetDevice(device_ordinal) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->stream3, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_cfork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_cjoin, cudaEventDisableTiming) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
@@ -768,7 +776,7 @@ rt_status rt_create(rt_handle** out, int device_ordinal) {
         rt_destroy(h);
         return RT_ERR_DEVICE;
     }
-    if (ensure(h, h->queue, 256) != RT_OK || ensure(h, h->stats, 256) != RT_OK) {
+    if (ensure(h, h->queue, kBandCounterBytes * kMaxBands) != RT_OK || ensure(h, h->stats, 256) != RT_OK) {
         rt_destroy(h);
         return RT_ERR_OOM;
     }
@@ -804,11 +812,14 @@ void rt_destroy(rt_handle* h) {
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_cfork) cudaEventDestroy(h->ev_cfork);
+    if (h->ev_cjoin) cudaEventDestroy(h->ev_cjoin);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
     for (cudaEvent_t& e : h->band_ev)
         if (e) cudaEventDestroy(e);
     if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     if (h->stream2) cudaStreamDestroy(h->stream2);
+    if (h->stream3) cudaStreamDestroy(h->stream3);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }

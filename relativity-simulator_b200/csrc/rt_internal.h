@@ -262,9 +262,15 @@ int trace_pass_occupancy(int pass, uint32_t block);
 // Device buffers of the two-pass mixed tracer for n rays.
 struct TwoPassBuffers {
     ParkBuf park;       // parked state, n slots
-    uint32_t* queues;   // 3n entries: per band near, far and finish queues
-    char* counters;     // 32 bytes per band (up to kMaxBands): claim counters and queue counts
+    uint32_t* queues;   // 4n entries: per band near, far, finish and near-critical queues
+    char* counters;     // kBandCounterBytes per band (up to kMaxBands): claim counters and queue counts
+    // one band: the critical pass runs on this stream beside the near pass
+    // (forked and joined with the two events); null: after it, on the band's
+    void* crit_stream = nullptr;
+    void* crit_fork = nullptr;
+    void* crit_join = nullptr;
 };
+constexpr uint32_t kBandCounterBytes = 64;
 constexpr uint32_t kMaxBands = 8;
 // Bytes of park.d, park.u and queues for n rays.
 uint64_t two_pass_state_bytes(uint64_t n);

@@ -597,7 +597,7 @@ rt_status rt_server_create(rt_server** out, int device_ordinal, const rt_server_
         ok = ok && cudaMalloc(&slot.dev_table, sizeof(BundleDesc) * cfg->max_epoch_bundles) == cudaSuccess;
         ok = ok && cudaMalloc(&slot.counters, 256) == cudaSuccess;
         ok = ok && cudaMalloc(&slot.pass_state, two_pass_state_bytes(cfg->epoch_rays)) == cudaSuccess;
-        ok = ok && cudaMalloc(&slot.pass_counters, 256) == cudaSuccess;
+        ok = ok && cudaMalloc(&slot.pass_counters, kBandCounterBytes * kMaxBands) == cudaSuccess;
         ok = ok && cudaMallocHost(&slot.host_ms, sizeof(MsDesc) * cfg->max_epoch_bundles) == cudaSuccess;
         ok = ok && cudaMalloc(&slot.dev_ms, sizeof(MsDesc) * cfg->max_epoch_bundles) == cudaSuccess;
         ok = ok && cudaMallocHost(&slot.host_src, sizeof(MsSource) * kMaxSources * cfg->max_epoch_bundles) ==

@@ -1004,31 +1004,31 @@ constexpr uint32_t kNearRefill = 16;  // measured best of 1, 4, 8, 16, 32
 constexpr uint32_t kCriticalBlock = 128;
 
 uint64_t two_pass_state_bytes(uint64_t n) {
-    return n * (sizeof(double) * PD_COUNT + sizeof(uint32_t) * PU_COUNT + 3 * sizeof(uint32_t));
+    return n * (sizeof(double) * PD_COUNT + sizeof(uint32_t) * PU_COUNT + 4 * sizeof(uint32_t));
 }
 
-// Per-band queue counters (32 bytes): [0] far-pass claim (u64), [8] near queue
-// count (u32), [12] far queue count (u32), [16] near-pass claim (u64), zeroed
-// pairwise before each pass; [24] finish queue count (u32), zeroed once.  The
-// first far pass also counts the near-critical rays in [12] (their queue is
-// the far queue's storage, free until the first near pass) and the critical
-// pass claims them through [16].
+// Per-band queue counters (kBandCounterBytes): [0] far-pass claim (u64), [8]
+// near queue count (u32), [12] far queue count (u32), [16] near-pass claim
+// (u64), zeroed pairwise before each pass; [24] finish queue count (u32), [32]
+// near-critical queue count (u32) and [40] the critical pass's claim (u64),
+// zeroed once.
 namespace {
 cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t begin, uint64_t count, char* qb,
                          uint32_t far_grid, uint32_t far_block, uint32_t near_grid, uint32_t finish_grid,
-                         uint32_t crit_grid, cudaStream_t s) {
-    uint32_t* near_q = buf.queues + 3 * begin;
+                         uint32_t crit_grid, bool crit_beside, cudaStream_t s) {
+    uint32_t* near_q = buf.queues + 4 * begin;
     uint32_t* far_q = near_q + count;
+    uint32_t* crit_q = far_q + 2 * count;
     args.park = buf.park;
     args.total_rays = count;
     args.ray_base = begin;
     args.finish_queue = far_q + count;
     args.finish_count = reinterpret_cast<uint32_t*>(qb + 24);
     const uint32_t far_refill = args.refill_threshold;
-    cudaError_t e = cudaMemsetAsync(qb + 24, 0, 8, s);
+    cudaError_t e = cudaMemsetAsync(qb + 24, 0, 24, s);
     for (int round = 0; e == cudaSuccess && round < kMixedRounds; ++round) {
         // far pass: pixels (first round) or the far queue -> near queue
-        if ((e = cudaMemsetAsync(qb, 0, round == 0 ? 24 : 12, s)) != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(qb, 0, 12, s)) != cudaSuccess) break;
         args.queue = reinterpret_cast<unsigned long long*>(qb);
         args.refill_threshold = far_refill;
         args.from_pixels = (round == 0) ? 1u : 0u;
@@ -1037,22 +1037,31 @@ cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t beg
         args.in_count = reinterpret_cast<const uint32_t*>(qb + 12);
         args.out_queue = near_q;
         args.out_count = reinterpret_cast<uint32_t*>(qb + 8);
-        args.crit_queue = (round == 0) ? far_q : nullptr;
-        args.crit_count = (round == 0) ? reinterpret_cast<uint32_t*>(qb + 12) : nullptr;
+        args.crit_queue = (round == 0) ? crit_q : nullptr;
+        args.crit_count = (round == 0) ? reinterpret_cast<uint32_t*>(qb + 32) : nullptr;
         launch_trace_pass(args, PASS_FAR, far_grid, far_block, s);
         if ((e = cudaGetLastError()) != cudaSuccess) break;
         if (round == 0) {
             // critical pass: the near-critical rays, FP64 from their pixels to their
-            // end at their graded tolerance (the single FP64 kernel over a queue)
+            // end at their graded tolerance (the single FP64 kernel over a queue);
+            // on its own stream it runs beside the near passes, each filling the
+            // SMs the other's tail leaves idle
             TraceArgs c = args;
-            c.queue = reinterpret_cast<unsigned long long*>(qb + 16);
+            c.queue = reinterpret_cast<unsigned long long*>(qb + 40);
             c.refill_threshold = 32;
-            c.in_queue = far_q;
-            c.in_count = reinterpret_cast<const uint32_t*>(qb + 12);
+            c.in_queue = crit_q;
+            c.in_count = reinterpret_cast<const uint32_t*>(qb + 32);
             c.out_queue = c.finish_queue = c.crit_queue = nullptr;
             c.out_count = c.finish_count = c.crit_count = nullptr;
-            launch_trace(c, crit_grid, kCriticalBlock, false, false, s);
+            cudaStream_t cs = s;
+            if (crit_beside) {
+                cs = static_cast<cudaStream_t>(buf.crit_stream);
+                if ((e = cudaEventRecord(static_cast<cudaEvent_t>(buf.crit_fork), s)) != cudaSuccess) break;
+                if ((e = cudaStreamWaitEvent(cs, static_cast<cudaEvent_t>(buf.crit_fork), 0)) != cudaSuccess) break;
+            }
+            launch_trace(c, crit_grid, kCriticalBlock, false, false, cs);
             if ((e = cudaGetLastError()) != cudaSuccess) break;
+            if (crit_beside && (e = cudaEventRecord(static_cast<cudaEvent_t>(buf.crit_join), cs)) != cudaSuccess) break;
         }
         // near pass: near queue -> far queue (the last one keeps its rays)
         if ((e = cudaMemsetAsync(qb + 12, 0, 12, s)) != cudaSuccess) break;
@@ -1072,7 +1081,9 @@ cudaError_t enqueue_band(TraceArgs args, const TwoPassBuffers& buf, uint64_t beg
     args.in_queue = args.finish_queue;
     args.in_count = args.finish_count;
     finish_kernel_t<128><<<finish_grid, 128, 0, s>>>(args);
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (crit_beside) e = cudaStreamWaitEvent(s, static_cast<cudaEvent_t>(buf.crit_join), 0);
+    return e;
 }
 }  // namespace
 
@@ -1106,8 +1117,9 @@ int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_co
     for (uint32_t b = 0; b < bands && begin < n && e == cudaSuccess; ++b) {
         const uint64_t count = (n - begin < per) ? n - begin : per;
         cudaStream_t sb = (b & 1u) ? s2 : s;
-        e = enqueue_band(base, buf, begin, count, buf.counters + 32 * b, far_grid, far_block, near_grid, finish_grid, crit_grid,
-                         sb);
+        const bool crit_beside = bands == 1 && buf.crit_stream && buf.crit_fork && buf.crit_join;
+        e = enqueue_band(base, buf, begin, count, buf.counters + kBandCounterBytes * b, far_grid, far_block, near_grid,
+                         finish_grid, crit_grid, crit_beside, sb);
         if (e == cudaSuccess && after_band && prev_stream)
             e = static_cast<cudaError_t>(after_band(hook_ctx, prev_begin, prev_count, prev_stream));
         prev_begin = begin;
