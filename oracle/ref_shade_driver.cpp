@@ -126,6 +126,23 @@ void ref_blackbody_rgb(double temperature_k, double reference_luminance, double 
 	out[2] = c[2];
 }
 
+// The procedural sky (SkyboxRenderer::sample_sky) in direction (x, y, z) for
+// a GpuSkyProfile image (1808 bytes), a field of view and a scene time.
+void ref_sample_sky(const void* profile, double x, double y, double z, double fov, double time, float out[3]) {
+	R::GpuSkyProfile p;
+	std::memcpy(&p, profile, sizeof p);
+	const auto c = R::SkyboxRenderer::sample_sky(x, y, z, p.to_settings(), fov, time);
+	out[0] = c[0];
+	out[1] = c[1];
+	out[2] = c[2];
+}
+
+// The default GpuSkyProfile image.
+void ref_sky_profile_defaults(void* out) {
+	const R::GpuSkyProfile p{};
+	std::memcpy(out, &p, sizeof p);
+}
+
 void ref_tonemap(const double rgb[3], uint32_t mode, double exposure_ev, float out[3]) {
 	const auto c = R::SoftwareComputeEngine::apply_tonemapping({rgb[0], rgb[1], rgb[2]}, mode, exposure_ev);
 	out[0] = c[0];
