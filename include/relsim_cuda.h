@@ -158,11 +158,21 @@ typedef struct rt_disk_profile {
  * at the throughput left and lowers the throughput by its opacity, and the
  * ray is followed on while more than 0.01 is left (the per-ray record still
  * describes the first hit; a disk pixel's flags add how the ray ended and its
- * redshift is the last crossing's).  The sum is tonemapped to sRGB.  The
- * procedural sky is not part of this library (sky_enabled must be 0), so the
- * sky behind a ray adds nothing.  Fields as in
- * GpuCameraPushConstants (gpu_types.hpp:990-1106); the profile is resolved as
- * AccretionDiskModel::resolve_primary_profile does. */
+ * redshift is the last crossing's).  A ray that escapes, or ends with more
+ * than 0.01 of its throughput outside 3 r_s, adds the procedural sky
+ * (SkyboxRenderer, render/skybox_renderer.hpp) at its exit direction times
+ * the throughput left when sky_enabled is 1 (software_compute_engine.hpp:
+ * 1766-1795).  The sum is tonemapped to sRGB.  Fields as in
+ * GpuCameraPushConstants (gpu_types.hpp:990-1106); the disk profile is
+ * resolved as AccretionDiskModel::resolve_primary_profile does. */
+/* The procedural sky's settings: the byte image of GpuSkyProfile
+ * (gpu_types.hpp:273-964), so a GpuSkyProfile copies in directly.
+ * rt_sky_profile_defaults gives its defaults; rt_sky_profile_set / _get read
+ * and write a field by its GpuSkyProfile name ("star_density", "seed",
+ * "nebula_emission_color[1]", "grid_cell_colors[3][0]"). */
+typedef struct rt_sky_profile {
+    unsigned char bytes[1808];
+} rt_sky_profile;
 typedef struct rt_shading {
     rt_disk_profile disk;                 /* primary_disk */
     double disk_temperature_scale_k;      /* overrides disk.peak_temperature_k */
@@ -174,7 +184,11 @@ typedef struct rt_shading {
     uint32_t tonemapping_mode;            /* 0 clamp, 1 ACES fit, 2 log luminance, 3 extended Reinhard */
     uint32_t hydro_model;                 /* hydro_disk.model: 0 procedural profile, 1 Novikov-Thorne flux */
     float accretion_rate_scale;           /* hydro_disk.accretion_rate_scale (Novikov-Thorne) */
-    uint32_t sky_enabled;                 /* must be 0 */
+    uint32_t sky_enabled;                 /* 1: the procedural sky behind escaped rays (sky.enabled
+                                             switches it off as well); the reference's image
+                                             panoramas (sky_background_source != 0) are not part of
+                                             this library */
+    rt_sky_profile sky;                   /* sky (GpuSkyProfile) */
 } rt_shading;
 
 /* Per-ray record, structure of arrays.  Any pointer may be NULL (not written).
@@ -337,13 +351,18 @@ uint64_t rt_bundle_rays(const rt_camera* cams, uint32_t n_bundles);
 /* Launch configuration (the autotuner writes it; zeros select defaults). */
 rt_status rt_set_launch_config(rt_handle* h, const rt_launch_config* cfg);
 
-/* Shade the pixels of later rt_dispatch, rt_dispatch_tile and
- * rt_dispatch_device calls on this handle (single-hole cameras, both metric
- * forms); NULL turns shading off (r = g = b = 0, a = 1, the default).
- * RT_ERR_INVALID_ARG for hydro_model 2 (the Fishbone-Moncrief torus) or
- * sky_enabled != 0. */
+/* Shade the pixels of later rt_dispatch, rt_dispatch_tile, rt_dispatch_device
+ * and rt_dispatch_multi* calls on this handle; NULL turns shading off
+ * (r = g = b = 0, a = 1, the default).  RT_ERR_INVALID_ARG for hydro_model 2
+ * (the Fishbone-Moncrief torus) or sky_enabled > 1.  rt_shading_defaults
+ * gives the reference's defaults, the sky off. */
 void rt_shading_defaults(rt_shading* s);
 rt_status rt_set_shading(rt_handle* h, const rt_shading* s);
+/* GpuSkyProfile's defaults, and one field by name (see rt_sky_profile):
+ * RT_ERR_INVALID_ARG for an unknown name or index. */
+void rt_sky_profile_defaults(rt_sky_profile* p);
+rt_status rt_sky_profile_set(rt_sky_profile* p, const char* field, double value);
+rt_status rt_sky_profile_get(const rt_sky_profile* p, const char* field, double* value);
 rt_status rt_get_launch_config(const rt_handle* h, rt_launch_config* cfg);
 
 /* Counters of the last dispatch; waits for it to finish. */
@@ -431,10 +450,10 @@ rt_status rt_server_get_stats(rt_server* s, rt_server_stats* stats);
 const char* rt_server_last_error(const rt_server* s);
 /* Shade the pixels of requests that finish from now on (single-hole cameras of
  * both metric forms, at their first disk crossing -- the server's epochs hold
- * no continuation state; multi-source requests keep r = g = b = 0), as
- * rt_set_shading does for a handle; NULL turns it off.  The server's
- * record_mask must hold status, phi, r_hit, g and the pixels, else
- * RT_ERR_INVALID_ARG. */
+ * no continuation state; multi-source requests keep r = g = b = 0; no sky:
+ * sky_enabled must be 0), as rt_set_shading does for a handle; NULL turns it
+ * off.  The server's record_mask must hold status, phi, r_hit, g and the
+ * pixels, else RT_ERR_INVALID_ARG. */
 rt_status rt_server_set_shading(rt_server* s, const rt_shading* shading);
 
 /* Allocation-free bundle trace.  No counterpart in the reference: its compute

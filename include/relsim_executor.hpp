@@ -104,8 +104,10 @@ rt_camera camera_from_push_constants(const PushConstants& p, const TraceSettings
 // rt_shading from the reference's push constants: primary_disk (a
 // GpuDiskProfile, copied as it lies), the disk temperature, saturation and
 // beaming overrides, time, exposure, tonemapping mode, and the hydro disk
-// model and accretion rate.  The procedural sky (params.sky) is not part of
-// the library and is left out: rays that escape stay black.
+// model and accretion rate, and the procedural sky (params.sky, a
+// GpuSkyProfile copied as it lies).  The reference's image panoramas
+// (sky_background_source != 0) are not part of the library: such a scene
+// keeps the procedural sky.
 template <class PushConstants>
 rt_shading shading_from_push_constants(const PushConstants& p) {
     rt_shading s;
@@ -121,7 +123,9 @@ rt_shading shading_from_push_constants(const PushConstants& p) {
     s.tonemapping_mode = p.tonemapping_mode;
     s.hydro_model = p.hydro_disk.model;
     s.accretion_rate_scale = p.hydro_disk.accretion_rate_scale;
-    s.sky_enabled = 0;
+    static_assert(sizeof(p.sky) == sizeof(rt_sky_profile), "GpuSkyProfile layout");
+    std::memcpy(&s.sky, &p.sky, sizeof s.sky);
+    s.sky_enabled = 1;
     return s;
 }
 
@@ -215,7 +219,7 @@ private:
         adv(o.status), adv(o.flags), adv(o.steps_accepted), adv(o.steps_rejected);
         adv(o.r), adv(o.theta), adv(o.phi), adv(o.r_hit), adv(o.g), adv(o.lambda);
         adv(o.dH), adv(o.dE), adv(o.dLz), adv(o.dQ);
-        adv(o.exit_x), adv(o.exit_y), adv(o.exit_z);
+        adv(o.exit_x), adv(o.exit_y), adv(o.exit_z), adv(o.body);
         return o;
     }
 

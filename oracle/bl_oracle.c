@@ -489,6 +489,30 @@ static inline float pi30f(float le, float lp, float order_p1)
  * ks_oracle.c; software_compute_engine.hpp:1538-1560 for this path): every
  * crossing on the disk is recorded at the reflected root point and the ray
  * goes on; `out` still describes the first hit. */
+/* Sky-lookup direction of a (pole-reflected) state: the orthonormal-frame
+ * velocity mapped to a Cartesian direction of travel (software_compute_engine.hpp:
+ * 1581-1589 with local_frame_to_travel_direction, :1148-1168). */
+static void exit_direction(double m, double a, double q2, const double* y, double* e)
+{
+    kn_geom G;
+    kn_geometry(m, a, q2, y[0], y[1], &G);
+    const double* gm = G.g;
+    const double st = sin(y[1]), ct = cos(y[1]), sp = sin(y[2]), cp = cos(y[2]);
+    const double lr = sqrt(fmax(gm[2], 0.0)) * y[4], lt = sqrt(fmax(gm[3], 0.0)) * y[5], lp = sqrt(fmax(gm[4], 0.0)) * y[6];
+    const double x = -(lr * st * cp + lt * ct * cp - lp * sp);
+    const double yy = -(lr * st * sp + lt * ct * sp + lp * cp);
+    const double z = -(lr * ct - lt * st);
+    const double len = sqrt(x * x + yy * yy + z * z);
+    if (len <= 1e-12) {
+        e[0] = 1.0;
+        e[1] = e[2] = 0.0;
+    } else {
+        e[0] = x / len;
+        e[1] = yy / len;
+        e[2] = z / len;
+    }
+}
+
 static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, uint32_t py, orc_ray* out,
                       orc_cont* cont)
 {
@@ -654,6 +678,13 @@ static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, ui
 
     if (cont) {
         cont->fate = status;
+        {
+            /* the sky-lookup direction at the ray's end */
+            double yr[7];
+            memcpy(yr, y, sizeof yr);
+            reflect_pole(yr, NULL);
+            exit_direction(m, a, q2, yr, cont->exit_dir);
+        }
         if (hit) {
             status = ORC_RAY_DISK;
             memcpy(y, y_hit, sizeof y_hit);
@@ -686,26 +717,7 @@ static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, ui
      * 1581-1589 with local_frame_to_travel_direction, :1148-1168): the
      * orthonormal-frame velocity mapped to a Cartesian direction of travel */
     out->exit_dir[0] = out->exit_dir[1] = out->exit_dir[2] = NAN;
-    if (status == ORC_RAY_ESCAPED) {
-        kn_geom G;
-        kn_geometry(m, a, q2, y[0], y[1], &G);
-        const double* gm = G.g;
-        const double st = sin(y[1]), ct = cos(y[1]), sp = sin(y[2]), cp = cos(y[2]);
-        const double lr = sqrt(fmax(gm[2], 0.0)) * y[4], lt = sqrt(fmax(gm[3], 0.0)) * y[5],
-                     lp = sqrt(fmax(gm[4], 0.0)) * y[6];
-        const double x = -(lr * st * cp + lt * ct * cp - lp * sp);
-        const double yy = -(lr * st * sp + lt * ct * sp + lp * cp);
-        const double z = -(lr * ct - lt * st);
-        const double len = sqrt(x * x + yy * yy + z * z);
-        if (len <= 1e-12) {
-            out->exit_dir[0] = 1.0;
-            out->exit_dir[1] = out->exit_dir[2] = 0.0;
-        } else {
-            out->exit_dir[0] = x / len;
-            out->exit_dir[1] = yy / len;
-            out->exit_dir[2] = z / len;
-        }
-    }
+    if (status == ORC_RAY_ESCAPED) exit_direction(m, a, q2, y, out->exit_dir);
 }
 
 typedef struct {

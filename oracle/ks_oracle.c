@@ -731,7 +731,7 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
 
     if (cont) {
         cont->fate = status;
-        if (status == ORC_RAY_ESCAPED) {
+        {  /* the sky-lookup direction at the ray's end */
             double dy[6];
             ks_rhs(y, m, a, dy);
             const double len = sqrt(dy[0] * dy[0] + dy[1] * dy[1] + dy[2] * dy[2]);

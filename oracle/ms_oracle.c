@@ -634,7 +634,7 @@ static void trace_one(const orc_camera* cam, const orc_ms_table* t, uint32_t px,
             const double d[3] = {y[0] - t->pos[i][0], y[1] - t->pos[i][1], y[2] - t->pos[i][2]};
             if (sqrt(dot3(d, d)) < 6.0 * t->mass[i]) cont->near_source = 1;
         }
-        if (status == ORC_RAY_ESCAPED) {
+        {  /* the sky-lookup direction at the ray's end */
             double dy[6];
             orc_ms_rhs(t, y, dy);
             const double len = sqrt(dy[0] * dy[0] + dy[1] * dy[1] + dy[2] * dy[2]);

@@ -56,7 +56,7 @@ struct rt_handle {
     bool shade_on = false;               // rt_set_shading
     // translucent-disk continuation of a shaded dispatch: each ray's disk crossings
     // and how it ended, and what the launches pass the tracer
-    DevBuf cont_cross, cont_info, cont_body;
+    DevBuf cont_cross, cont_info, cont_body, cont_exit;
     DevBuf ms_shade;  // multi-source shading: one descriptor per source
     ContOut cur_cont{};
     rt_shading shading{};
@@ -330,12 +330,18 @@ rt_status shade_prepare(rt_handle* h, const rt_camera* cam, cudaStream_t s) {
 // dispatch of n rays: the tracers record each disk crossing and follow the ray
 // on through the disk; the shading pass composes the crossings.
 rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false) {
+    // the sky needs each ray's direction at its end
+    double sky_enabled = 0.0;
+    rt_sky_profile_get(&h->shading.sky, "enabled", &sky_enabled);
+    const bool sky = h->shading.sky_enabled == 1u && sky_enabled != 0.0;
     rt_status st = ensure(h, h->cont_cross, sizeof(double) * 3 * kMaxCrossings * n);
     if (st == RT_OK) st = ensure(h, h->cont_info, sizeof(uint32_t) * n);
     if (st == RT_OK && bodies) st = ensure(h, h->cont_body, sizeof(uint32_t) * n);
+    if (st == RT_OK && sky) st = ensure(h, h->cont_exit, sizeof(double) * 3 * n);
     if (st != RT_OK) return st;
     h->cur_cont = ContOut{static_cast<double*>(h->cont_cross.ptr), static_cast<uint32_t*>(h->cont_info.ptr), n,
-                          bodies ? static_cast<uint32_t*>(h->cont_body.ptr) : nullptr};
+                          bodies ? static_cast<uint32_t*>(h->cont_body.ptr) : nullptr,
+                          sky ? static_cast<double*>(h->cont_exit.ptr) : nullptr};
     return RT_OK;
 }
 
@@ -381,7 +387,10 @@ int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
     if (c.shade && c.dpix) {
         launch_shade(static_cast<const ShadeDesc*>(c.h->shade_desc.ptr), c.dev.status + o, c.dev.r_hit + o,
                      c.dev.phi + o, c.dev.g + o,
-                     c.cont.cross ? ContOut{c.cont.cross + o, c.cont.info + o, c.cont.stride} : ContOut{},
+                     c.cont.cross ? ContOut{c.cont.cross + o, c.cont.info + o, c.cont.stride,
+                                            c.cont.body ? c.cont.body + o : nullptr,
+                                            c.cont.exit ? c.cont.exit + o : nullptr}
+                                  : ContOut{},
                      c.dpix + o, count, s);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return static_cast<int>(e);
@@ -801,6 +810,7 @@ void rt_destroy(rt_handle* h) {
     release(h->cont_cross);
     release(h->cont_info);
     release(h->cont_body);
+    release(h->cont_exit);
     release(h->park_d);
     release(h->park_u);
     release(h->pass_queues);
@@ -890,6 +900,77 @@ void rt_shading_defaults(rt_shading* s) {
     s->hydro_model = 0;
     s->accretion_rate_scale = 1.0f;
     s->sky_enabled = 0;
+    rt_sky_profile_defaults(&s->sky);
+}
+
+void rt_sky_profile_defaults(rt_sky_profile* p) {
+    if (!p) return;
+    const SkyProfile d{};
+    std::memcpy(p, &d, sizeof d);
+}
+
+namespace {
+// Address and type of a sky-profile field by its GpuSkyProfile name: a scalar,
+// "name[k]" of a three-float vector, or "grid_cell_colors[c][k]".
+void* sky_field(SkyProfile& p, const char* field, int& kind) {
+    if (!field) return nullptr;
+#define RT_SKY_FIND(T, N, D)                       \
+    if (std::strcmp(field, #N) == 0) {             \
+        kind = (sizeof(T) == 8) ? 1 : 0;           \
+        return &p.N;                               \
+    }
+    RT_SKY_U32_FIELDS(RT_SKY_FIND)
+    RT_SKY_F64_FIELDS(RT_SKY_FIND)
+#undef RT_SKY_FIND
+    kind = 2;
+    const char* br = std::strchr(field, '[');
+    if (!br) return nullptr;
+    const std::string name(field, br);
+    unsigned a = 0, b = 0;
+    char tail = 0;
+    if (name == "grid_cell_colors") {
+        if (std::sscanf(br, "[%u][%u]%c", &a, &b, &tail) != 2 || a >= 16 || b >= 3) return nullptr;
+        return &p.grid_cell_colors[a][b];
+    }
+    if (std::sscanf(br, "[%u]%c", &a, &tail) != 1 || a >= 3) return nullptr;
+#define RT_SKY_FINDV(N, A, B, C) \
+    if (name == #N) return &p.N[a];
+    RT_SKY_VEC_FIELDS(RT_SKY_FINDV)
+#undef RT_SKY_FINDV
+    return nullptr;
+}
+}  // namespace
+
+rt_status rt_sky_profile_set(rt_sky_profile* p, const char* field, double value) {
+    if (!p) return RT_ERR_INVALID_ARG;
+    SkyProfile s;
+    std::memcpy(&s, p, sizeof s);
+    int kind = 0;
+    void* f = sky_field(s, field, kind);
+    if (!f) return RT_ERR_INVALID_ARG;
+    if (kind == 0) {
+        if (!(value >= 0.0 && value <= 4294967295.0)) return RT_ERR_INVALID_ARG;
+        *static_cast<uint32_t*>(f) = static_cast<uint32_t>(value);
+    } else if (kind == 1) {
+        *static_cast<double*>(f) = value;
+    } else {
+        *static_cast<float*>(f) = static_cast<float>(value);
+    }
+    std::memcpy(p, &s, sizeof s);
+    return RT_OK;
+}
+
+rt_status rt_sky_profile_get(const rt_sky_profile* p, const char* field, double* value) {
+    if (!p || !value) return RT_ERR_INVALID_ARG;
+    SkyProfile s;
+    std::memcpy(&s, p, sizeof s);
+    int kind = 0;
+    const void* f = sky_field(s, field, kind);
+    if (!f) return RT_ERR_INVALID_ARG;
+    *value = (kind == 0) ? static_cast<double>(*static_cast<const uint32_t*>(f))
+             : (kind == 1) ? *static_cast<const double*>(f)
+                           : static_cast<double>(*static_cast<const float*>(f));
+    return RT_OK;
 }
 
 rt_status rt_set_shading(rt_handle* h, const rt_shading* s) {
@@ -902,7 +983,7 @@ rt_status rt_set_shading(rt_handle* h, const rt_shading* s) {
     rt_camera_defaults(&probe);
     ShadeDesc d;
     if (!build_shade_desc(probe, *s, d))
-        return fail(h, RT_ERR_INVALID_ARG, "shading: hydro_model 0 or 1, tonemapping_mode 0..3, sky_enabled 0");
+        return fail(h, RT_ERR_INVALID_ARG, "shading: hydro_model 0 or 1, tonemapping_mode 0..3, sky_enabled 0 or 1");
     h->shading = *s;
     h->shade_on = true;
     return RT_OK;

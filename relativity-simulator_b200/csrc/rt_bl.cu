@@ -335,6 +335,48 @@ __device__ __noinline__ void bl_init_ray(const BlDesc* __restrict__ Bp, uint64_t
     S.local[tid] = local;
 }
 
+// Sky-lookup direction of a (reflected) Boyer-Lindquist state: the
+// orthonormal-frame velocity (sqrt(g_rr) u^r, sqrt(g_thth) u^th, sqrt(g_phph)
+// u^ph) mapped to a Cartesian direction of travel (software_compute_engine.hpp:
+// 1581-1589, local_frame_to_travel_direction :1148-1168).
+__device__ void bl_exit_direction(const BlDesc& B, const double* y, double* e) {
+    const double r = y[0], st = sin(y[1]), ct = cos(y[1]), sp = sin(y[2]), cp = cos(y[2]);
+    const double a2 = B.a * B.a, r2a2 = r * r + a2;
+    const double sigma = r * r + a2 * ct * ct;
+    const double delta = r * r - 2.0 * B.m * r + a2 + B.q2;
+    const double g_rr = sigma / delta;
+    const double g_pp = (r2a2 * r2a2 - a2 * delta * st * st) * st * st / sigma;
+    const double lr = sqrt(fmax(g_rr, 0.0)) * y[4], lt = sqrt(fmax(sigma, 0.0)) * y[5], lp = sqrt(fmax(g_pp, 0.0)) * y[6];
+    const double x = -(lr * st * cp + lt * ct * cp - lp * sp);
+    const double yy = -(lr * st * sp + lt * ct * sp + lp * cp);
+    const double z = -(lr * ct - lt * st);
+    const double len = sqrt(x * x + yy * yy + z * z);
+    if (len <= 1e-12) {
+        e[0] = 1.0;
+        e[1] = e[2] = 0.0;
+    } else {
+        e[0] = x / len;
+        e[1] = yy / len;
+        e[2] = z / len;
+    }
+}
+
+// Continuation end of a Boyer-Lindquist ray at state yin (unreflected), with
+// the sky-lookup direction there when the sky is on.
+__device__ __noinline__ void bl_cont_finish(const ContOut& C, const BlDesc& B, uint64_t o, uint32_t n_cross,
+                                            uint32_t status, const double* yin) {
+    double e[3];
+    const double* ep = nullptr;
+    if (C.exit) {
+        double y[NB];
+        for (int i = 0; i < NB; ++i) y[i] = yin[i];
+        bl_reflect(y, nullptr);
+        bl_exit_direction(B, y, e);
+        ep = e;
+    }
+    cont_finish(C, o, n_cross, status, yin[0], B.m, ep);
+}
+
 template <int BLOCK>
 __device__ __noinline__ void bl_finish(const BlDesc* __restrict__ Bp, BlCold<BLOCK>& S, int tid, const double* yin,
                                        uint32_t status, uint32_t flags, uint32_t acc, uint32_t rej, double r_hit,
@@ -365,33 +407,8 @@ __device__ __noinline__ void bl_finish(const BlDesc* __restrict__ Bp, BlCold<BLO
     if (R.dQ) R.dQ[o] = (Q - S.q0[tid]) / (e0 * e0);
     if (R.body) R.body[o] = (status == RT_RAY_DISK || status == RT_RAY_CAPTURED) ? 0u : RT_BODY_NONE;
     if (R.exit_x || R.exit_y || R.exit_z) {
-        // sky-lookup direction of an escaped ray: the orthonormal-frame velocity
-        // (sqrt(g_rr) u^r, sqrt(g_thth) u^th, sqrt(g_phph) u^ph) mapped to a
-        // Cartesian direction of travel (software_compute_engine.hpp:1581-1589,
-        // local_frame_to_travel_direction :1148-1168)
         double e[3] = {NAN, NAN, NAN};
-        if (status == RT_RAY_ESCAPED) {
-            const double r = y[0], st = sin(y[1]), ct = cos(y[1]), sp = sin(y[2]), cp = cos(y[2]);
-            const double a2 = B.a * B.a, r2a2 = r * r + a2;
-            const double sigma = r * r + a2 * ct * ct;
-            const double delta = r * r - 2.0 * B.m * r + a2 + B.q2;
-            const double g_rr = sigma / delta;
-            const double g_pp = (r2a2 * r2a2 - a2 * delta * st * st) * st * st / sigma;
-            const double lr = sqrt(fmax(g_rr, 0.0)) * y[4], lt = sqrt(fmax(sigma, 0.0)) * y[5],
-                         lp = sqrt(fmax(g_pp, 0.0)) * y[6];
-            const double x = -(lr * st * cp + lt * ct * cp - lp * sp);
-            const double yy = -(lr * st * sp + lt * ct * sp + lp * cp);
-            const double z = -(lr * ct - lt * st);
-            const double len = sqrt(x * x + yy * yy + z * z);
-            if (len <= 1e-12) {
-                e[0] = 1.0;
-                e[1] = e[2] = 0.0;
-            } else {
-                e[0] = x / len;
-                e[1] = yy / len;
-                e[2] = z / len;
-            }
-        }
+        if (status == RT_RAY_ESCAPED) bl_exit_direction(B, y, e);
         if (R.exit_x) R.exit_x[o] = e[0];
         if (R.exit_y) R.exit_y[o] = e[1];
         if (R.exit_z) R.exit_z[o] = e[2];
@@ -516,7 +533,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
         }
         if (term) {
             if (n_cross == 0) bl_finish<BLOCK>(Bp, S, tid, y, term & 15u, flags, acc, rej, NAN, 1.0, args.out);
-            if (args.cont.cross) cont_finish(args.cont, B.out_offset + S.local[tid], n_cross, term & 15u, y[0], B.m);
+            if (args.cont.cross) bl_cont_finish(args.cont, B, B.out_offset + S.local[tid], n_cross, term & 15u, y);
             mode = BL_IDLE;
             continue;
         }
@@ -548,7 +565,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
                 bl_finish<BLOCK>(Bp, S, tid, y, RT_RAY_CAPTURED, flags | RT_RAYFLAG_NONFINITE, acc, rej, NAN, 1.0,
                                  args.out);
             if (args.cont.cross)
-                cont_finish(args.cont, B.out_offset + S.local[tid], n_cross, RT_RAY_CAPTURED, y[0], B.m);
+                bl_cont_finish(args.cont, B, B.out_offset + S.local[tid], n_cross, RT_RAY_CAPTURED, y);
             mode = BL_IDLE;
             continue;
         }
@@ -590,7 +607,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
                         cont_record(args.cont, o, n_cross, rr, yp[2], g);
                         ++n_cross;
                         if (n_cross >= kMaxCrossings) {
-                            cont_finish(args.cont, o, n_cross, RT_RAY_UNFINISHED, rr, B.m);
+                            bl_cont_finish(args.cont, B, o, n_cross, RT_RAY_UNFINISHED, yr);
                             continue;
                         }
                         mode = BL_STEP;
@@ -639,7 +656,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
                     S.lambda[tid] += hh;
                 }
                 if (n_cross == 0) bl_finish<BLOCK>(Bp, S, tid, yt, tterm, flags, acc, rej, NAN, 1.0, args.out);
-                if (args.cont.cross) cont_finish(args.cont, B.out_offset + S.local[tid], n_cross, tterm, yt[0], B.m);
+                if (args.cont.cross) bl_cont_finish(args.cont, B, B.out_offset + S.local[tid], n_cross, tterm, yt);
                 mode = BL_IDLE;
                 continue;
             }

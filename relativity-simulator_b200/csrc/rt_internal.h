@@ -5,6 +5,7 @@
 #include <cstdint>
 
 #include "relsim_cuda.h"
+#include "rt_sky_profile.h"
 
 namespace relsim {
 
@@ -83,6 +84,7 @@ struct ContOut {
     uint32_t* info;   // [stride]
     uint64_t stride;
     uint32_t* body;   // multi-source: [stride], source of crossing k in bits 4k..4k+3 (else null)
+    double* exit;     // sky on: [3][stride], the sky-lookup direction at the ray's end (else null)
 };
 
 // Device counters of one launch.
@@ -221,13 +223,15 @@ struct alignas(16) ShadeDesc {
     double pattern_omega;                 // orbital angular velocity at sqrt(inner outer)
     double nt_flux_peak, nt_rate_factor;  // Novikov-Thorne: peak flux over the disk, rate^(1/4)
     double nt_m, nt_a_star, nt_x0, nt_x1, nt_x2, nt_x3, nt_r_isco;
-    uint32_t hydro_model, tonemap, pad0, pad1;
+    uint32_t hydro_model, tonemap, sky_on, pad1;
     double lambda_um[33];
     double weight[33][3];
+    double fov;      // the camera's field of view (the sky's level of detail)
+    SkyProfile sky;  // the procedural sky, read when sky_on
 };
 
 // Build the shading constants of a camera; false if the settings are not
-// supported (hydro model 2, sky enabled).
+// supported (hydro model 2, sky_enabled above 1).
 bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d);
 void build_source_shade_desc(const ShadeDesc& base, const float* profile, double mass, double spin, double inner,
                              double outer, ShadeDesc& d);

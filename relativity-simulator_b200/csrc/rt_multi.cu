@@ -436,6 +436,19 @@ __device__ __noinline__ void ms_cont_finish(const ContOut& C, uint64_t o, uint32
     }
     C.info[o] = n_cross | (status << CI_FATE_SHIFT) | (near ? CI_INSIDE_3RS : 0u);
     C.body[o] = bodies;
+    if (C.exit) {
+        // the sky-lookup direction at the end: minus the normalised flow of the
+        // superposed RHS, (0, 0, -1) where it vanishes (:3220-3224)
+        double dy[6], e[3] = {0.0, 0.0, -1.0};
+        int ins;
+        ms_rhs(src, n, x, dy, 1.0, ins);
+        const double len = sqrt(dot3(dy, dy));
+        if (len > 1e-12)
+            for (int i = 0; i < 3; ++i) e[i] = -dy[i] / len;
+        C.exit[o] = e[0];
+        C.exit[C.stride + o] = e[1];
+        C.exit[2 * C.stride + o] = e[2];
+    }
 }
 
 __device__ __forceinline__ void ms_unwrap(double& phi, const double* y) {

@@ -364,8 +364,22 @@ __device__ __forceinline__ void record_crossing(const TraceArgs& args, const Bun
 template <class ColdT>
 __device__ __forceinline__ void end_continuation(const TraceArgs& args, const BundleDesc* __restrict__ Bp, ColdT& S,
                                                  int j, uint32_t n_cross, uint32_t status, const double* __restrict__ y) {
+    double e[3];
+    const double* ep = nullptr;
+    if (args.cont.exit) {
+        // the sky-lookup direction at the end: -dx/dlambda of the state, normalised
+        // (software_compute_engine.hpp:1771-1775)
+        double k[3], hf;
+        ks_field64(y, Bp->m, Bp->a, k, hf);
+        const double sv = 1.0 + k[0] * y[3] + k[1] * y[4] + k[2] * y[5];
+        const double v[3] = {y[3] - 2.0 * hf * sv * k[0], y[4] - 2.0 * hf * sv * k[1], y[5] - 2.0 * hf * sv * k[2]};
+        const double inv = 1.0 / fmax(sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]), 1e-12);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) e[i] = -v[i] * inv;
+        ep = e;
+    }
     cont_finish(args.cont, Bp->out_offset + S.local[j], n_cross, status,
-                sqrt(bl_r2<double>(y[0], y[1], y[2], Bp->a * Bp->a)), Bp->m);
+                sqrt(bl_r2<double>(y[0], y[1], y[2], Bp->a * Bp->a)), Bp->m, ep);
 }
 
 // A ray's end (capture, escape, unfinished): its record and pixel unless it
@@ -379,7 +393,21 @@ __device__ __forceinline__ void end_ray(const TraceArgs& args, const BundleDesc*
     if constexpr (CONT) {
         if (n_cross == 0)
             finish_ray(Bp, S, j, status, flags, acc, rej, wind, interp_target, hh, NAN, 1.0, args.out, xch);
-        end_continuation(args, Bp, S, j, n_cross, status, xch + (interp_target > 0.0 ? 12 : 0));
+        if (interp_target > 0.0 && args.cont.exit) {
+            // the end interpolated to the threshold radius, as the record's
+            double y0[6], f0[6], y1[6], f1[6], yt[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                y0[i] = xch[i];
+                f0[i] = xch[6 + i];
+                y1[i] = xch[12 + i];
+                f1[i] = xch[18 + i];
+            }
+            hermite(y0, f0, y1, f1, hh, crossing_fraction(y0, f0, y1, f1, hh, Bp->a, interp_target), 6, yt);
+            end_continuation(args, Bp, S, j, n_cross, status, yt);
+        } else {
+            end_continuation(args, Bp, S, j, n_cross, status, xch + (interp_target > 0.0 ? 12 : 0));
+        }
     } else {
         finish_ray(Bp, S, j, status, flags, acc, rej, wind, interp_target, hh, NAN, 1.0, args.out, xch);
     }

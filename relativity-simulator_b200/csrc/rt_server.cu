@@ -771,7 +771,9 @@ rt_status rt_server_set_shading(rt_server* s, const rt_shading* sh) {
     rt_camera probe;
     rt_camera_defaults(&probe);
     ShadeDesc d;
-    if (!build_shade_desc(probe, *sh, d) || (s->cfg.record_mask & kShadeMask) != kShadeMask) return RT_ERR_INVALID_ARG;
+    // no sky: the server's epochs record no exit directions
+    if (sh->sky_enabled != 0u || !build_shade_desc(probe, *sh, d) || (s->cfg.record_mask & kShadeMask) != kShadeMask)
+        return RT_ERR_INVALID_ARG;
     if (!s->dev_shade) {
         cudaSetDevice(s->device);
         if (cudaMalloc(&s->dev_shade, sizeof(ShadeDesc) * kShadeSlots) != cudaSuccess) {

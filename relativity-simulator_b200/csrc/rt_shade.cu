@@ -12,8 +12,9 @@
 // render/accretion_disk/accretion_disk_model.hpp:245-316, with the
 // Novikov-Thorne base temperature of hydro model 1,
 // render/accretion_disk/hydro_disk_shading.hpp:160-171).  The radiance is
-// tonemapped (apply_tonemapping, :3461-3516).  The procedural sky is not part
-// of this library, so the sky behind a ray adds nothing.
+// tonemapped (apply_tonemapping, :3461-3516).  With the sky on, a ray that
+// escapes, or ends outside 3 r_s with throughput left, adds the procedural sky
+// (rt_sky.cuh) at the direction the tracer recorded at its end.
 //
 // Per-camera constants (the resolved profile, the Novikov-Thorne flux
 // normalisation, the spectral table of the blackbody colour) are computed on
@@ -24,9 +25,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 
 #include "rt_internal.h"
 #include "rt_shade.cuh"
+#include "rt_sky.cuh"
 
 namespace relsim {
 
@@ -85,15 +88,23 @@ __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict_
                 thr *= 1.0 - sh[3];
                 last_g = gk;
             }
-            if (n_cross > 0) {
-                const uint32_t fate = (info >> CI_FATE_SHIFT) & 15u;
-                uint32_t add = 0;
-                if (thr > kMinThroughput) {
-                    if (fate == RT_RAY_CAPTURED) add = RT_PIXEL_HORIZON_ABSORBED;
-                    else if (fate == RT_RAY_ESCAPED || !(info & CI_INSIDE_3RS)) add = RT_PIXEL_CELESTIAL_HIT;
-                }
-                pixels[i].status_flags |= add;
-                pixels[i].redshift = static_cast<float>(last_g);
+            // how the ray ended (software_compute_engine.hpp:1766-1795): with throughput
+            // left, a capture absorbs it; an escape, or an end outside 3 r_s, sees the sky
+            const uint32_t fate = (info >> CI_FATE_SHIFT) & 15u;
+            uint32_t add = 0;
+            if (thr > kMinThroughput) {
+                if (fate == RT_RAY_CAPTURED) add = RT_PIXEL_HORIZON_ABSORBED;
+                else if (fate == RT_RAY_ESCAPED || !(info & CI_INSIDE_3RS)) add = RT_PIXEL_CELESTIAL_HIT;
+            }
+            pixels[i].status_flags |= add;
+            if (n_cross > 0) pixels[i].redshift = static_cast<float>(last_g);
+            if (D.sky_on && add == RT_PIXEL_CELESTIAL_HIT && cont.exit) {
+                float sky_rgb[3];
+                sky::sample(D.sky, cont.exit[i], cont.exit[cont.stride + i], cont.exit[2 * cont.stride + i], D.fov, D.time,
+                            sky_rgb);
+                acc[0] += thr * static_cast<double>(sky_rgb[0]);
+                acc[1] += thr * static_cast<double>(sky_rgb[1]);
+                acc[2] += thr * static_cast<double>(sky_rgb[2]);
             }
         } else if (status[i] == RT_RAY_DISK) {
             double sh[4];
@@ -145,7 +156,7 @@ double temperature_shape_peak(double exponent, double zero_torque) {
 }  // namespace
 
 bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d) {
-    if (s.hydro_model > 1u || s.sky_enabled != 0u || s.tonemapping_mode > 3u) return false;
+    if (s.hydro_model > 1u || s.sky_enabled > 1u || s.tonemapping_mode > 3u) return false;
     d = ShadeDesc{};
     // spectral table (accretion_disk_model.hpp:52-69)
     const double step = (780.0 - 380.0) / 32.0;
@@ -191,6 +202,11 @@ bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d) {
     const double pixel = cam.field_of_view_rad / mxd(static_cast<double>(cam.screen_width), 1.0);
     d.detail = cd((2.0 * rh / r_obs) / mxd(pixel * 24.0, 1e-9), 0.0, 1.0);
     d.pattern_omega = orbital_omega(d.mass, a, std::sqrt(d.inner * d.outer));
+    // the procedural sky (GpuSkyProfile image) and the camera's field of view
+    static_assert(sizeof(rt_sky_profile) == sizeof(SkyProfile), "sky profile layout");
+    std::memcpy(&d.sky, &s.sky, sizeof d.sky);
+    d.sky_on = (s.sky_enabled == 1u && d.sky.enabled != 0u) ? 1u : 0u;
+    d.fov = cam.field_of_view_rad;
 
     // Novikov-Thorne disk of (M, a): ISCO, Page-Thorne roots, peak flux over
     // 192 log-spaced radii (hydro_disk_shading.hpp:44-62)

@@ -239,10 +239,16 @@ __device__ __forceinline__ void cont_record(const ContOut& C, uint64_t o, uint32
 }
 
 // End of a ray's trace: crossings recorded, its class at the end (UNFINISHED
-// also when it stopped at kMaxCrossings) and whether r_last lies inside 3 r_s.
+// also when it stopped at kMaxCrossings) and whether r_last lies inside 3 r_s;
+// with the sky on, the sky-lookup direction e at the end.
 __device__ __forceinline__ void cont_finish(const ContOut& C, uint64_t o, uint32_t n_cross, uint32_t status,
-                                            double r_last, double m) {
+                                            double r_last, double m, const double* e = nullptr) {
     C.info[o] = n_cross | (status << CI_FATE_SHIFT) | ((r_last < 6.0 * m) ? CI_INSIDE_3RS : 0u);
+    if (C.exit && e) {
+        C.exit[o] = e[0];
+        C.exit[C.stride + o] = e[1];
+        C.exit[2 * C.stride + o] = e[2];
+    }
 }
 
 }  // namespace

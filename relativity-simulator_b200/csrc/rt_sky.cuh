@@ -306,7 +306,7 @@ RT_SKY_HD void star_tint(double t, double variation, float* out) {
 // ---- layers ----
 
 // Stars on a hashed 3-D grid around the direction (:769-913).
-RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, double* acc) {
+RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, double time, double* acc) {
     if (!s.stars_enabled || s.star_density <= 0.0) return;
     const uint64_t seed = static_cast<uint64_t>(s.seed);
     const double q = mx(s.quality_factor * s.star_quality_factor, 0.05);
@@ -357,7 +357,7 @@ RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, do
                 if (s.dynamic_motion) {
                     const double rate = s.motion_speed * 0.012;
                     const double phase = unit(h + 47ULL) * kTwoPi;
-                    const double ang = sin(s.time_seconds * 0.18 + phase) * rate;
+                    const double ang = sin(time * 0.18 + phase) * rate;
                     sd = rotate(sd, ang * (180.0 / kPi), 0.0, 0.0);
                 }
                 const double mu = dot(dir, sd);
@@ -381,7 +381,7 @@ RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, do
                              s.star_brightness;
                 if (s.dynamic_motion && s.star_scintillation > 0.0) {
                     const double tw = unit(h + 67ULL) * kTwoPi;
-                    lum *= (1.0 + s.star_scintillation * sin(s.time_seconds * 3.8 + tw));
+                    lum *= (1.0 + s.star_scintillation * sin(time * 3.8 + tw));
                 }
                 V3 u1, u2;
                 tangents(sd, u1, u2);
@@ -740,7 +740,7 @@ RT_SKY_HD_NOINLINE void quasars(const V3& dir, const SkyProfile& s, double* acc)
 }
 
 // Pulsars: swept beams and wind nebulae (:1415-1501).
-RT_SKY_HD_NOINLINE void pulsars(const V3& dir, const SkyProfile& s, double* acc) {
+RT_SKY_HD_NOINLINE void pulsars(const V3& dir, const SkyProfile& s, double time, double* acc) {
     if (!s.pulsar_enabled || s.pulsar_brightness <= 0.0) return;
     const uint64_t seed = static_cast<uint64_t>(s.seed) ^ 0x4f1bbcdcu;
     const double res = sparse_res(s.pulsar_density);
@@ -763,7 +763,7 @@ RT_SKY_HD_NOINLINE void pulsars(const V3& dir, const SkyProfile& s, double* acc)
                 const double tilt = s.pulsar_magnetic_tilt_deg * (kPi / 180.0);
                 const double jitter = exp((unit(h + 83ULL) - 0.5) * s.pulsar_frequency_spread * 2.0);
                 const double rate = s.pulsar_pulse_rate * jitter;
-                const double phase = fmod(s.time_seconds * rate + unit(h + 61ULL), 1.0) * kTwoPi;
+                const double phase = fmod(time * rate + unit(h + 61ULL), 1.0) * kTwoPi;
                 V3 u1, u2;
                 tangents(axis, u1, u2);
                 const double sti = sin(tilt), cti = cos(tilt), cph = cos(phase), sph = sin(phase);
@@ -955,22 +955,15 @@ RT_SKY_HD_NOINLINE void sample(const SkyProfile& s, double x, double y, double z
                      static_cast<double>(s.background_color[2])};
     const double fov_deg = fov * (180.0 / kPi);
     const double zoom = cl(s.adaptive_fov_reference / mx(fov_deg, 0.05), 1.0, 128.0);
-    // the layers read the scene's time
-    SkyProfile const* sp = &s;
-    SkyProfile timed;
-    if (s.time_seconds != time && (s.dynamic_motion || s.pulsar_enabled)) {
-        timed = s;
-        timed.time_seconds = time;
-        sp = &timed;
-    }
-    if (s.nebula_enabled) nebulae(d, *sp, zoom, acc);
-    if (s.dust_enabled) dust(d, *sp, acc);
-    if (s.galaxies_enabled) galaxies(d, *sp, acc);
-    if (s.clusters_enabled) clusters(d, *sp, fov, acc);
-    if (s.quasar_enabled) quasars(d, *sp, acc);
-    if (s.pulsar_enabled) pulsars(d, *sp, acc);
-    if (s.snr_enabled) remnants(d, *sp, acc);
-    if (s.stars_enabled) stars(d, *sp, fov, acc);
+    // the layers that move read the scene's time in place of the profile's
+    if (s.nebula_enabled) nebulae(d, s, zoom, acc);
+    if (s.dust_enabled) dust(d, s, acc);
+    if (s.galaxies_enabled) galaxies(d, s, acc);
+    if (s.clusters_enabled) clusters(d, s, fov, acc);
+    if (s.quasar_enabled) quasars(d, s, acc);
+    if (s.pulsar_enabled) pulsars(d, s, time, acc);
+    if (s.snr_enabled) remnants(d, s, acc);
+    if (s.stars_enabled) stars(d, s, fov, time, acc);
     const double k = mx(s.master_intensity, 0.0);
     float rgb[3] = {static_cast<float>(mx(0.0, acc[0] * k)), static_cast<float>(mx(0.0, acc[1] * k)),
                     static_cast<float>(mx(0.0, acc[2] * k))};

@@ -61,12 +61,18 @@ class DiskProfile(ctypes.Structure):
         "grain_scale", "reference_luminance", "noise_seed", "temperature_normalization", "edge_softness")]
 
 
+class SkyProfile(ctypes.Structure):
+    """rt_sky_profile: the GpuSkyProfile image (1808 bytes); fields by name through
+    sky_profile() / sky_get()."""
+    _fields_ = [("bytes", ctypes.c_uint8 * 1808)]
+
+
 class Shading(ctypes.Structure):
-    """rt_shading: the pixel shading tail (disk colour, tonemapping)."""
+    """rt_shading: the pixel shading tail (disk colour, the procedural sky, tonemapping)."""
     _fields_ = [("disk", DiskProfile), ("disk_temperature_scale_k", _d), ("disk_temperature_floor_k", _d),
                 ("disk_color_saturation", _d), ("disk_doppler_beaming_exponent", _d), ("time", _d),
                 ("camera_exposure", _d), ("tonemapping_mode", _u32), ("hydro_model", _u32),
-                ("accretion_rate_scale", ctypes.c_float), ("sky_enabled", _u32)]
+                ("accretion_rate_scale", ctypes.c_float), ("sky_enabled", _u32), ("sky", SkyProfile)]
 
 
 class PixelOut(ctypes.Structure):
@@ -152,7 +158,8 @@ EXPORTS = ["rt_create", "rt_destroy", "rt_is_ready", "rt_is_platform_supported",
            "rt_get_stats", "rt_synchronize", "rt_measure_fma_peak", "rt_trace_bundles_noalloc", "rt_kerr_isco_radius", "rt_dispatch_multi", "rt_dispatch_multi_device",
            "rt_server_config_defaults", "rt_server_create", "rt_server_destroy", "rt_server_submit",
            "rt_server_poll", "rt_server_get_stats", "rt_server_last_error", "rt_server_submit_multi",
-           "rt_shading_defaults", "rt_set_shading", "rt_server_set_shading"]
+           "rt_shading_defaults", "rt_set_shading", "rt_server_set_shading", "rt_sky_profile_defaults",
+           "rt_sky_profile_set", "rt_sky_profile_get"]
 NOALLOC_MAX_BUNDLES = 32  # RT_NOALLOC_MAX_BUNDLES
 
 
@@ -183,6 +190,12 @@ def lib() -> ctypes.CDLL:
         L.rt_set_launch_config.argtypes = [v, p(LaunchConfig)]
         L.rt_shading_defaults.argtypes = [p(Shading)]
         L.rt_shading_defaults.restype = None
+        L.rt_sky_profile_defaults.argtypes = [p(SkyProfile)]
+        L.rt_sky_profile_defaults.restype = None
+        L.rt_sky_profile_set.argtypes = [p(SkyProfile), ctypes.c_char_p, _d]
+        L.rt_sky_profile_set.restype = ctypes.c_int
+        L.rt_sky_profile_get.argtypes = [p(SkyProfile), ctypes.c_char_p, p(_d)]
+        L.rt_sky_profile_get.restype = ctypes.c_int
         L.rt_set_shading.argtypes = [v, p(Shading)]
         L.rt_server_set_shading.argtypes = [v, p(Shading)]
         L.rt_get_launch_config.argtypes = [v, p(LaunchConfig)]
@@ -433,12 +446,31 @@ def trace_bundles_noalloc(cams: list[Camera], rays: RayOut, pixels_ptr: int | No
 
 
 def shading(**kw) -> Shading:
-    """rt_shading with the reference's defaults, overridden by keyword (field names)."""
+    """rt_shading with the reference's defaults (the sky off), overridden by keyword (field names)."""
     s = Shading()
     lib().rt_shading_defaults(ctypes.byref(s))
     for k, v in kw.items():
         setattr(s, k, v)
     return s
+
+
+def sky_profile(**fields) -> SkyProfile:
+    """GpuSkyProfile's defaults with fields set by name (vector components as
+    "name[k]" through a dict: sky_profile(**{"dust_tint[0]": 0.5}))."""
+    p = SkyProfile()
+    L = lib()
+    L.rt_sky_profile_defaults(ctypes.byref(p))
+    for k, v in fields.items():
+        if L.rt_sky_profile_set(ctypes.byref(p), k.encode(), float(v)) != RT_OK:
+            raise KeyError(k)
+    return p
+
+
+def sky_get(p: SkyProfile, field: str) -> float:
+    v = _d()
+    if lib().rt_sky_profile_get(ctypes.byref(p), field.encode(), ctypes.byref(v)) != RT_OK:
+        raise KeyError(field)
+    return v.value
 
 
 def server_config(budget_bytes: int | None = None, record: Iterable[str] | None = None, **kw) -> ServerConfig:

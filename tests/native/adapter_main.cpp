@@ -43,6 +43,9 @@ struct Push {  // the fields of GpuCameraPushConstants the tracer reads (gpu_typ
     uint32_t dispatch_row_offset = 0, dispatch_row_count = 0;
     uint32_t tile_origin_x = 0, tile_origin_y = 0, tile_extent_x = 0, tile_extent_y = 0;
     DiskProfile primary_disk{};
+    struct {
+        unsigned char bytes[1808];
+    } sky{};  // a GpuSkyProfile image
 };
 #endif
 #include "relsim_executor.hpp"

@@ -54,17 +54,18 @@ def test_metric_type_routing(tmp_path):
 
 
 def test_shading_mapping(tmp_path):
-    """The push constants' disk profile, overrides, time, exposure, tonemapping
-    and hydro model become rt_shading; the sky is left out."""
+    """The push constants' disk profile, overrides, time, exposure, tonemapping,
+    hydro model and procedural sky (the GpuSkyProfile image) become rt_shading,
+    with the sky drawn."""
     out = subprocess.run([_build(tmp_path), "shade"], capture_output=True, text=True, check=True).stdout.split()
-    assert out == ["7", "15000", "3", "2.5", "-1", "1", "1", "2", "0", "1"]
+    assert out == ["7", "15000", "3", "2.5", "-1", "1", "1", "2", "1", "1"]
 
 
 @pytest.mark.skipif(not os.path.isdir(REFERENCE_INCLUDE), reason="reference headers not present")
 def test_shading_mapping_compiles_against_reference_push_constants(tmp_path):
     exe = _build(tmp_path, extra=("-std=c++23", "-DRELSIM_WITH_REFERENCE_TYPES", "-I", REFERENCE_INCLUDE))
     out = subprocess.run([exe, "shade"], capture_output=True, text=True, check=True).stdout.split()
-    assert out[:3] == ["7", "15000", "3"] and out[8] == "0"
+    assert out[:3] == ["7", "15000", "3"] and out[8] == "1"
 
 
 def test_no_device_answers(tmp_path):

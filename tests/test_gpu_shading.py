@@ -14,10 +14,19 @@ cameras end at the first crossing; there the oracle shades each ray from the
 GPU's own record (class, r_hit, phi, g), which isolates the shading
 arithmetic: CUDA's float cosf/powf/expf and FMA contraction differ from the
 host's in the last bits (bar 1e-6 sRGB, measured 1.8e-7).  Rays that are not
-disk hits are exactly black with alpha 1 (the sky is disabled).
+disk hits are exactly black with alpha 1 when the sky is off.
+
+With the sky on, a ray that escapes with throughput left adds the procedural
+sky at its exit direction; the oracle side samples the reference's own
+SkyboxRenderer::sample_sky (compiled from the reference headers into
+oracle/_ref) at the oracle's exit direction.  Bar SKY_BAR in sRGB for 99.5 %
+of those rays and SKY_MAX for every one: a point-like star's flux changes as
+theta dtheta / sigma^2 with the 1e-9 rad difference of the two traces' exit
+directions, and CUDA's transcendental functions differ from the host's.
 """
 import ctypes
 import math
+import os
 
 import numpy as np
 import pytest
@@ -218,8 +227,163 @@ def test_device_entry_point_and_tiles(tracer):
 
 def test_unsupported_settings_rejected(tracer):
     with pytest.raises(relsim.RelsimError):
-        tracer.set_shading(relsim.shading(sky_enabled=1))
+        tracer.set_shading(relsim.shading(sky_enabled=2))
     with pytest.raises(relsim.RelsimError):
         tracer.set_shading(relsim.shading(hydro_model=2))
     with pytest.raises(relsim.RelsimError):
         tracer.set_shading(relsim.shading(tonemapping_mode=4))
+
+
+
+SKY_BAR = 1e-5
+SKY_MAX = 1e-3
+
+
+@pytest.fixture(scope="module")
+def sky_sampler(tmp_path_factory):
+    """The sky the oracle side adds: the reference's SkyboxRenderer::sample_sky
+    from oracle/_ref where that library was built; else the library's own sky
+    arithmetic compiled for the host (tests/sky/sky_host.cpp), which
+    tests/test_sky_host.py pins to the reference on every layer."""
+    import subprocess
+    v, d = ctypes.c_void_p, ctypes.c_double
+    if O.ref_available():
+        fn = O.ref().ref_sample_sky
+        which = "reference"
+    else:
+        here = os.path.dirname(os.path.abspath(__file__))
+        out = tmp_path_factory.mktemp("sky") / "libsky_host.so"
+        subprocess.run(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-I",
+                        os.path.join(os.path.dirname(here), "relativity-simulator_b200", "csrc"),
+                        os.path.join(here, "sky", "sky_host.cpp"), "-o", str(out)], check=True)
+        fn = ctypes.CDLL(str(out)).host_sample_sky
+        which = "host build"
+    fn.argtypes = [v, d, d, d, d, d, v]
+    fn.restype = None
+    print(f"sky sampled by the {which}")
+    return fn
+
+
+def oracle_sky_pixels(sample, cam, sh, cont, srcs=None):
+    """Pixels of an oracle continuation trace with the sky: the crossings shaded
+    in order at the throughput left (the camera's disk, or each source's for a
+    multi-source scene), then, for a ray that escaped with more than 0.01 of
+    its throughput, the sky at the oracle's exit direction times that
+    throughput; tonemapped.  NaN for rays the oracle left unfinished."""
+    L = O.lib()
+    prof_in = np.frombuffer(bytes(sh.disk), np.float32).copy()
+    over = np.array([sh.disk_temperature_scale_k, sh.disk_temperature_floor_k, sh.disk_color_saturation,
+                     sh.disk_doppler_beaming_exponent])
+    primary = np.zeros(32, np.float32)
+    L.orc_resolve_profile(O._p(prof_in), O._p(over), O._p(primary))
+    if srcs is None:
+        m, a, inner, outer, detail = _camera_constants(cam)
+        geo, profiles, hydro = [(m, a, inner, outer)], [primary], sh.hydro_model
+    else:
+        from test_gpu_multi_source import _oracle_sources
+        t = O.ms_table(relsim.camera_dict(cam), _oracle_sources(srcs))[0]
+        geo = [(t["mass"][i], t["spin"][i], t["disk_in"][i], t["disk_out"][i]) for i in range(len(srcs) + 1)]
+        profiles = [primary] + [np.frombuffer(bytes(s.disk), np.float32).copy() for s in srcs]
+        detail, hydro = 1.0, 0
+    prof = (ctypes.c_uint8 * 1808).from_buffer_copy(bytes(sh.sky))
+    out = np.full((cont.size, 3), np.nan, np.float32)
+    px = np.zeros(3, np.float32)
+    rgb = np.zeros(3, np.float32)
+    shv = np.zeros(4)
+    for i in range(cont.size):
+        fate = int(cont["fate"][i])
+        if fate == O.UNFINISHED:
+            continue
+        acc = np.zeros(3)
+        thr = 1.0
+        for k in range(int(cont["n_cross"][i])):
+            if not thr > 0.01:
+                break
+            s_idx = int(cont["cross_src"][i][k]) if srcs is not None else 0
+            m, a, inner, outer = geo[s_idx]
+            pt = np.array([m, a, inner, outer, cont["cross_r"][i][k], cont["cross_phi"][i][k], cont["cross_g"][i][k],
+                           sh.time, detail])
+            L.orc_disk_shade(O._p(profiles[s_idx]), O._p(pt), hydro, sh.accretion_rate_scale, O._p(shv))
+            acc += thr * shv[:3]
+            thr *= 1.0 - shv[3]
+        if thr > 0.01 and fate == O.ESCAPED:
+            e = cont["exit_dir"][i]
+            sample(ctypes.addressof(prof), float(e[0]), float(e[1]), float(e[2]), cam.field_of_view_rad, sh.time,
+                   rgb.ctypes.data)
+            acc += thr * rgb.astype(np.float64)
+        L.orc_tonemap(O._p(acc), sh.tonemapping_mode, sh.camera_exposure, O._p(px))
+        out[i] = px
+    return out
+
+
+def _sky_check(got, want, what):
+    ok = ~np.isnan(want).any(1)
+    err = np.abs(got - want).max(1)[ok]
+    print(f"{what}: {ok.sum()} rays compared, sRGB within {SKY_BAR:g}: {np.mean(err < SKY_BAR):.4f}, "
+          f"max {err.max():.2e}")
+    assert ok.sum() > 0.9 * want.shape[0]
+    assert np.mean(err < SKY_BAR) >= 0.995 and err.max() < SKY_MAX
+
+
+def _shaded(tracer, sh, call):
+    tracer.set_shading(sh)
+    try:
+        return call()
+    finally:
+        tracer.set_shading(None)
+
+
+def test_sky_behind_kerr_schild_rays_matches_oracle(tracer, sky_sampler):
+    """The default procedural sky (every layer the reference turns on by
+    default) behind a Kerr-Schild image whose field of view takes in the sky
+    around the hole and the sky lensed through the translucent disk."""
+    cam = relsim.make_camera(spin=0.94, r_obs=40.0, incl_deg=70.0, fov_deg=60.0, width=64, height=64)
+    sh = relsim.shading(tonemapping_mode=1, time=1.5, sky_enabled=1)
+    out = _shaded(tracer, sh, lambda: tracer.dispatch(cam, fields=["status"], pixels=True))
+    ref, cont = O.trace_cont(relsim.camera_dict(cam))
+    want = oracle_sky_pixels(sky_sampler, cam, sh, cont)
+    want[O.boundary_band(ref, _camera_constants(cam)[2], cam.disk_outer_radius) |
+         (np.abs(ref["db_shadow"]) < 1e-3)] = np.nan
+    got = _rgb(out["pixels"])
+    _sky_check(got, want, "Kerr-Schild")
+    esc = cont["fate"] == O.ESCAPED
+    assert esc.sum() > 1000 and got[esc].max() > 0.05
+    assert (out["pixels"]["status_flags"][esc & (cont["n_cross"] == 0)] & relsim.PIXEL_CELESTIAL_HIT).all()
+
+
+def test_sky_behind_boyer_lindquist_rays_matches_oracle(tracer, sky_sampler):
+    """A Kerr-Newman Boyer-Lindquist image with a sky of other models: the
+    Airy-disk star profile, denser galaxies and the coordinate grid."""
+    cam = relsim.make_camera(spin=0.9, r_obs=50.0, incl_deg=75.0, fov_deg=40.0, width=48, height=48,
+                             metric_form=relsim.METRIC_BOYER_LINDQUIST, charge=0.3)
+    sky = relsim.sky_profile(star_profile_model=5, galaxy_density=1.5, grid_enabled=1, grid_show_equator=1)
+    sh = relsim.shading(sky_enabled=1, sky=sky, time=0.5)
+    out = _shaded(tracer, sh, lambda: tracer.dispatch(cam, fields=["status"], pixels=True))
+    ref, cont = O.bl_trace_cont(relsim.camera_dict(cam), 0.3)
+    want = oracle_sky_pixels(sky_sampler, cam, sh, cont)
+    want[O.boundary_band(ref, _camera_constants(cam)[2], cam.disk_outer_radius) |
+         (np.abs(ref["db_shadow"]) < 1e-3)] = np.nan
+    _sky_check(_rgb(out["pixels"]), want, "Boyer-Lindquist")
+
+
+def test_sky_behind_multi_source_rays_matches_oracle(tracer, sky_sampler):
+    """The default sky behind a multi-source scene: each body's disk shaded
+    with its own profile, the sky at the superposed flow's exit direction."""
+    import scenes
+    req = [r for r in scenes.request_stream() if r.multi_source][2]
+    srcs = scenes.rt_sources(req.sources)
+    cam = req.bundle.camera(relsim.PRECISION_FP64)
+    cam.screen_width = cam.screen_height = 40
+    sh = relsim.shading(sky_enabled=1, tonemapping_mode=3, time=4.0)
+    out = _shaded(tracer, sh, lambda: tracer.dispatch_multi(cam, srcs, fields=["status"], pixels=True))
+    from test_gpu_multi_source import _oracle_sources
+    ref, cont = O.ms_trace_cont(relsim.camera_dict(cam), _oracle_sources(srcs))
+    want = oracle_sky_pixels(sky_sampler, cam, sh, cont, srcs)
+    want[out["status"] != ref["status"]] = np.nan
+    _sky_check(_rgb(out["pixels"]), want, "multi-source")
+
+
+def test_server_refuses_the_sky():
+    with relsim.Server(0, relsim.server_config(1 << 26)) as srv:
+        with pytest.raises(relsim.RelsimError):
+            srv.set_shading(relsim.shading(sky_enabled=1))

@@ -108,3 +108,35 @@ def test_sky_matches_reference(libs, name):
     if CASES[name].get("star_profile_model") != 6 or "wide" in name:
         assert lit > 0, "case lights no direction"
     assert worst < 1e-5, (name, worst, where)
+
+
+def test_profile_accessors_write_the_reference_layout(libs):
+    """rt_sky_profile_defaults gives the reference's GpuSkyProfile defaults byte
+    for byte; rt_sky_profile_set/get reach each kind of field (u32, f64,
+    vector component, grid cell colour) at the reference's offsets and refuse
+    unknown names, out-of-range indices and negative or fractional-free
+    overflow of u32 fields."""
+    import relsim
+    host, ref = libs
+    p = relsim.sky_profile()
+    assert bytes(p) == _defaults(ref).tobytes()
+    q = relsim.sky_profile(star_profile_model=5, star_density=2.5, **{"dust_tint[1]": 0.25,
+                                                                      "grid_cell_colors[3][2]": 0.75})
+    want = _case(host, ref, star_profile_model=5, star_density=2.5)
+    kind = ctypes.c_int()
+    off = host.host_sky_offset(b"dust_tint", ctypes.byref(kind))
+    want[off + 4:off + 8] = np.frombuffer(np.float32(0.25).tobytes(), np.uint8)
+    off = host.host_sky_offset(b"grid_cell_colors", ctypes.byref(kind))
+    want[off + (3 * 4 + 2) * 4:off + (3 * 4 + 3) * 4] = np.frombuffer(np.float32(0.75).tobytes(), np.uint8)
+    assert bytes(q) == want.tobytes()
+    assert relsim.sky_get(q, "star_profile_model") == 5.0
+    assert relsim.sky_get(q, "star_density") == 2.5
+    assert relsim.sky_get(q, "dust_tint[1]") == 0.25
+    assert relsim.sky_get(q, "grid_cell_colors[3][2]") == 0.75
+    for bad in ("no_such_field", "dust_tint[4]", "grid_cell_colors[16][0]", "star_density[0]"):
+        with pytest.raises(KeyError):
+            relsim.sky_profile(**{bad: 1.0})
+    with pytest.raises(KeyError):
+        relsim.sky_profile(star_profile_model=-1)
+    sh = relsim.shading()
+    assert sh.sky_enabled == 0 and bytes(sh.sky) == bytes(p)
