@@ -56,7 +56,7 @@ struct rt_handle {
     bool shade_on = false;               // rt_set_shading
     // translucent-disk continuation of a shaded dispatch: each ray's disk crossings
     // and how it ended, and what the launches pass the tracer
-    DevBuf cont_cross, cont_info, cont_body, cont_exit;
+    DevBuf cont_cross, cont_info, cont_body, cont_exit, cont_tail;
     DevBuf ms_shade;  // multi-source shading: one descriptor per source
     ContOut cur_cont{};
     rt_shading shading{};
@@ -329,19 +329,24 @@ rt_status shade_prepare(rt_handle* h, const rt_camera* cam, cudaStream_t s) {
 // Turn on the translucent-disk continuation for the launches of a shaded
 // dispatch of n rays: the tracers record each disk crossing and follow the ray
 // on through the disk; the shading pass composes the crossings.
-rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false) {
-    // the sky needs each ray's direction at its end
+// The sky needs each ray's direction at its end: the Boyer-Lindquist and
+// multi-source tracers write it (exit); the Kerr-Schild tracers leave the end of
+// the trace to the shading pass (tail, `kerr_schild`).
+rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false, bool kerr_schild = false) {
     double sky_enabled = 0.0;
     rt_sky_profile_get(&h->shading.sky, "enabled", &sky_enabled);
     const bool sky = h->shading.sky_enabled == 1u && sky_enabled != 0.0;
+    const bool exit = sky && !kerr_schild, tail = sky && kerr_schild;
     rt_status st = ensure(h, h->cont_cross, sizeof(double) * 3 * kMaxCrossings * n);
     if (st == RT_OK) st = ensure(h, h->cont_info, sizeof(uint32_t) * n);
     if (st == RT_OK && bodies) st = ensure(h, h->cont_body, sizeof(uint32_t) * n);
-    if (st == RT_OK && sky) st = ensure(h, h->cont_exit, sizeof(double) * 3 * n);
+    if (st == RT_OK && exit) st = ensure(h, h->cont_exit, sizeof(double) * 3 * n);
+    if (st == RT_OK && tail) st = ensure(h, h->cont_tail, sizeof(double) * TL_COUNT * n);
     if (st != RT_OK) return st;
     h->cur_cont = ContOut{static_cast<double*>(h->cont_cross.ptr), static_cast<uint32_t*>(h->cont_info.ptr), n,
                           bodies ? static_cast<uint32_t*>(h->cont_body.ptr) : nullptr,
-                          sky ? static_cast<double*>(h->cont_exit.ptr) : nullptr};
+                          exit ? static_cast<double*>(h->cont_exit.ptr) : nullptr,
+                          tail ? static_cast<double*>(h->cont_tail.ptr) : nullptr};
     return RT_OK;
 }
 
@@ -389,7 +394,8 @@ int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
                      c.dev.phi + o, c.dev.g + o,
                      c.cont.cross ? ContOut{c.cont.cross + o, c.cont.info + o, c.cont.stride,
                                             c.cont.body ? c.cont.body + o : nullptr,
-                                            c.cont.exit ? c.cont.exit + o : nullptr}
+                                            c.cont.exit ? c.cont.exit + o : nullptr,
+                                            c.cont.tail ? c.cont.tail + o : nullptr}
                                   : ContOut{},
                      c.dpix + o, count, s);
         const cudaError_t e = cudaGetLastError();
@@ -446,7 +452,7 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
     ContinuationScope cont_scope{h};
     if (shade && (st = add_shade_fields(h, dev, n)) != RT_OK) return st;
     if (shade && (st = shade_prepare(h, cam, h->stream)) != RT_OK) return st;
-    if (shade && (st = begin_continuation(h, n)) != RT_OK) return st;
+    if (shade && (st = begin_continuation(h, n, false, !is_bl(cam))) != RT_OK) return st;
     // bands of at most 2^24 rays; the cancel flag is polled between bands.  Each
     // band's shading and copies follow its trace; on the two-pass tracer a band
     // is traced in sub-bands whose copies overlap the next sub-band's trace.
@@ -811,6 +817,7 @@ void rt_destroy(rt_handle* h) {
     release(h->cont_info);
     release(h->cont_body);
     release(h->cont_exit);
+    release(h->cont_tail);
     release(h->park_d);
     release(h->park_u);
     release(h->pass_queues);
@@ -1051,7 +1058,7 @@ rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* p
     // shaded: the shading constants go up before the trace, which follows each
     // ray through the translucent disk
     if (shade && (st = shade_prepare(h, cam, s)) != RT_OK) return st;
-    if (shade && (st = begin_continuation(h, n)) != RT_OK) return st;
+    if (shade && (st = begin_continuation(h, n, false, true)) != RT_OK) return st;
     if ((st = launch(h, 1, n, OutPtrs{pixels, dev}, cam->precision_mode == RT_PRECISION_MIXED, s)) != RT_OK) return st;
     return shade ? shade_launch(h, cam, dev, pixels, n, s, true) : RT_OK;
 }

@@ -203,6 +203,38 @@ __device__ __forceinline__ void hermite(const double* y0, const double* f0, cons
     for (int i = 0; i < n; ++i) out[i] = h00 * y0[i] + h10 * h * f0[i] + h01 * y1[i] + h11 * h * f1[i];
 }
 
+// Fraction of the step where the interpolated r_BL crosses `target`
+// (Illinois regula falsi; 1 when the end points do not bracket it).
+static __device__ double crossing_fraction(const double* y0, const double* f0, const double* y1, const double* f1, double h,
+                                    double a, double target) {
+    const double a2 = a * a;
+    double lo = 0.0, hi = 1.0;
+    double flo = sqrt(bl_r2<double>(y0[0], y0[1], y0[2], a2)) - target;
+    double fhi = sqrt(bl_r2<double>(y1[0], y1[1], y1[2], a2)) - target;
+    if (!((flo > 0.0) != (fhi > 0.0))) return 1.0;
+    int side = 0;
+    double t = 1.0, x[3];
+    for (int it = 0; it < 60; ++it) {
+        t = (lo * fhi - hi * flo) / (fhi - flo);
+        if (!(t > lo && t < hi)) t = 0.5 * (lo + hi);
+        hermite(y0, f0, y1, f1, h, t, 3, x);
+        const double ft = sqrt(bl_r2<double>(x[0], x[1], x[2], a2)) - target;
+        if (ft == 0.0 || fabs(hi - lo) < 1e-15 || fabs(ft) < 1e-13 * target) break;
+        if ((ft > 0.0) == (fhi > 0.0)) {
+            hi = t;
+            fhi = ft;
+            if (side == -1) flo *= 0.5;
+            side = -1;
+        } else {
+            lo = t;
+            flo = ft;
+            if (side == 1) fhi *= 0.5;
+            side = 1;
+        }
+    }
+    return t;
+}
+
 // PI30 factor (step_controller.hpp:51-58) from base-2 logs of the errors.
 __device__ __forceinline__ float pi30_factor(float le, float lp, float order_p1) {
     return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));

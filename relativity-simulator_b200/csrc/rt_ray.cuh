@@ -135,38 +135,6 @@ __device__ __noinline__ InitResult init_ray(const BundleDesc* __restrict__ Bp, u
     return res;
 }
 
-// Fraction of the step where the interpolated r_BL crosses `target`
-// (Illinois regula falsi; 1 when the end points do not bracket it).
-__device__ double crossing_fraction(const double* y0, const double* f0, const double* y1, const double* f1, double h,
-                                    double a, double target) {
-    const double a2 = a * a;
-    double lo = 0.0, hi = 1.0;
-    double flo = sqrt(bl_r2<double>(y0[0], y0[1], y0[2], a2)) - target;
-    double fhi = sqrt(bl_r2<double>(y1[0], y1[1], y1[2], a2)) - target;
-    if (!((flo > 0.0) != (fhi > 0.0))) return 1.0;
-    int side = 0;
-    double t = 1.0, x[3];
-    for (int it = 0; it < 60; ++it) {
-        t = (lo * fhi - hi * flo) / (fhi - flo);
-        if (!(t > lo && t < hi)) t = 0.5 * (lo + hi);
-        hermite(y0, f0, y1, f1, h, t, 3, x);
-        const double ft = sqrt(bl_r2<double>(x[0], x[1], x[2], a2)) - target;
-        if (ft == 0.0 || fabs(hi - lo) < 1e-15 || fabs(ft) < 1e-13 * target) break;
-        if ((ft > 0.0) == (fhi > 0.0)) {
-            hi = t;
-            fhi = ft;
-            if (side == -1) flo *= 0.5;
-            side = -1;
-        } else {
-            lo = t;
-            flo = ft;
-            if (side == 1) fhi *= 0.5;
-            side = 1;
-        }
-    }
-    return t;
-}
-
 // Terminal point, the ray's record and its pixel.  xch (a local array of the
 // caller) holds the last accepted point in [0..5]; with interp_target > 0 it
 // holds the step's y, k1, y5, k7 in [0..23] and the point is interpolated to
@@ -360,26 +328,32 @@ __device__ __forceinline__ void record_crossing(const TraceArgs& args, const Bun
     cont_record(args.cont, Bp->out_offset + S.local[j], k, r, phi, disk_redshift(Bp->m, a, r, S.lz0[j]));
 }
 
-// End of a Kerr-Schild ray's trace with the continuation on; y its last point.
+// End of a Kerr-Schild ray's trace with the continuation on.  xch as end_ray
+// takes it: with interp_target > 0 the last step (y0, f0, y1, f1 in xch[0..23],
+// length hh), whose end the sky direction is interpolated to the threshold
+// radius on; else the ray's last point in xch[0..5].  With the sky on, the end
+// goes to the tail record for the shading pass (ks_tail_direction).
 template <class ColdT>
 __device__ __forceinline__ void end_continuation(const TraceArgs& args, const BundleDesc* __restrict__ Bp, ColdT& S,
-                                                 int j, uint32_t n_cross, uint32_t status, const double* __restrict__ y) {
-    double e[3];
-    const double* ep = nullptr;
-    if (args.cont.exit) {
-        // the sky-lookup direction at the end: -dx/dlambda of the state, normalised
-        // (software_compute_engine.hpp:1771-1775)
-        double k[3], hf;
-        ks_field64(y, Bp->m, Bp->a, k, hf);
-        const double sv = 1.0 + k[0] * y[3] + k[1] * y[4] + k[2] * y[5];
-        const double v[3] = {y[3] - 2.0 * hf * sv * k[0], y[4] - 2.0 * hf * sv * k[1], y[5] - 2.0 * hf * sv * k[2]};
-        const double inv = 1.0 / fmax(sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]), 1e-12);
+                                                 int j, uint32_t n_cross, uint32_t status, const double* __restrict__ xch,
+                                                 double interp_target = 0.0, double hh = 0.0) {
+    const uint64_t o = Bp->out_offset + S.local[j];
+    const double* yl = xch + (interp_target > 0.0 ? 12 : 0);
+    if (double* T = args.cont.tail) {
+        const uint64_t st = args.cont.stride;
+        if (interp_target > 0.0) {
 #pragma unroll
-        for (int i = 0; i < 3; ++i) e[i] = -v[i] * inv;
-        ep = e;
+            for (int i = 0; i < 24; ++i) T[i * st + o] = xch[i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) T[(TL_Y1 + i) * st + o] = xch[i];
+        }
+        T[TL_H * st + o] = hh;
+        T[TL_TARGET * st + o] = interp_target;
+        T[TL_M * st + o] = Bp->m;
+        T[TL_A * st + o] = Bp->a;
     }
-    cont_finish(args.cont, Bp->out_offset + S.local[j], n_cross, status,
-                sqrt(bl_r2<double>(y[0], y[1], y[2], Bp->a * Bp->a)), Bp->m, ep);
+    cont_finish(args.cont, o, n_cross, status, sqrt(bl_r2<double>(yl[0], yl[1], yl[2], Bp->a * Bp->a)), Bp->m);
 }
 
 // A ray's end (capture, escape, unfinished): its record and pixel unless it
@@ -393,21 +367,7 @@ __device__ __forceinline__ void end_ray(const TraceArgs& args, const BundleDesc*
     if constexpr (CONT) {
         if (n_cross == 0)
             finish_ray(Bp, S, j, status, flags, acc, rej, wind, interp_target, hh, NAN, 1.0, args.out, xch);
-        if (interp_target > 0.0 && args.cont.exit) {
-            // the end interpolated to the threshold radius, as the record's
-            double y0[6], f0[6], y1[6], f1[6], yt[6];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) {
-                y0[i] = xch[i];
-                f0[i] = xch[6 + i];
-                y1[i] = xch[12 + i];
-                f1[i] = xch[18 + i];
-            }
-            hermite(y0, f0, y1, f1, hh, crossing_fraction(y0, f0, y1, f1, hh, Bp->a, interp_target), 6, yt);
-            end_continuation(args, Bp, S, j, n_cross, status, yt);
-        } else {
-            end_continuation(args, Bp, S, j, n_cross, status, xch + (interp_target > 0.0 ? 12 : 0));
-        }
+        end_continuation(args, Bp, S, j, n_cross, status, xch, interp_target, hh);
     } else {
         finish_ray(Bp, S, j, status, flags, acc, rej, wind, interp_target, hh, NAN, 1.0, args.out, xch);
     }

@@ -27,6 +27,7 @@
 #include <cstdint>
 #include <cstring>
 
+#include "rt_device.cuh"
 #include "rt_internal.h"
 #include "rt_shade.cuh"
 #include "rt_sky.cuh"
@@ -57,6 +58,37 @@ __device__ __forceinline__ double aces(double x) {
     return cd((x * (2.51 * x + 0.03)) / (x * (2.43 * x + 0.59) + 0.14), 0.0, 1.0);
 }
 
+
+// Sky-lookup direction at the end of a Kerr-Schild ray from its tail record
+// (TailField): the end interpolated to the threshold radius on the last step's
+// Hermite interpolant when a threshold is set, then -dx/dlambda of that state,
+// normalised (software_compute_engine.hpp:1771-1775).
+__device__ __noinline__ void ks_tail_direction(const double* __restrict__ T, uint64_t st, uint64_t i, double* e) {
+    double y[6];
+    const double target = T[TL_TARGET * st + i], M = T[TL_M * st + i], a = T[TL_A * st + i];
+    if (target > 0.0) {
+        double y0[6], f0[6], y1[6], f1[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            y0[k] = T[(TL_Y0 + k) * st + i];
+            f0[k] = T[(TL_F0 + k) * st + i];
+            y1[k] = T[(TL_Y1 + k) * st + i];
+            f1[k] = T[(TL_F1 + k) * st + i];
+        }
+        const double h = T[TL_H * st + i];
+        hermite(y0, f0, y1, f1, h, crossing_fraction(y0, f0, y1, f1, h, a, target), 6, y);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) y[k] = T[(TL_Y1 + k) * st + i];
+    }
+    double k[3], hf;
+    ks_field64(y, M, a, k, hf);
+    const double sv = 1.0 + k[0] * y[3] + k[1] * y[4] + k[2] * y[5];
+    const double v[3] = {y[3] - 2.0 * hf * sv * k[0], y[4] - 2.0 * hf * sv * k[1], y[5] - 2.0 * hf * sv * k[2]};
+    const double inv = 1.0 / fmax(sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]), 1e-12);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e[c] = -v[c] * inv;
+}
 
 __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict__ Dp,
                                                     const uint32_t* __restrict__ status,
@@ -98,10 +130,17 @@ __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict_
             }
             pixels[i].status_flags |= add;
             if (n_cross > 0) pixels[i].redshift = static_cast<float>(last_g);
-            if (D.sky_on && add == RT_PIXEL_CELESTIAL_HIT && cont.exit) {
+            if (D.sky_on && add == RT_PIXEL_CELESTIAL_HIT && (cont.exit || cont.tail)) {
+                double e[3];
+                if (cont.tail) {
+                    ks_tail_direction(cont.tail, cont.stride, i, e);
+                } else {
+                    e[0] = cont.exit[i];
+                    e[1] = cont.exit[cont.stride + i];
+                    e[2] = cont.exit[2 * cont.stride + i];
+                }
                 float sky_rgb[3];
-                sky::sample(D.sky, cont.exit[i], cont.exit[cont.stride + i], cont.exit[2 * cont.stride + i], D.fov, D.time,
-                            sky_rgb);
+                sky::sample(D.sky, e[0], e[1], e[2], D.fov, D.time, sky_rgb);
                 acc[0] += thr * static_cast<double>(sky_rgb[0]);
                 acc[1] += thr * static_cast<double>(sky_rgb[1]);
                 acc[2] += thr * static_cast<double>(sky_rgb[2]);

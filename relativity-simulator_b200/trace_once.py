@@ -47,6 +47,8 @@ def main() -> None:
                     help="device-resident outputs (rt_dispatch_device: one set of launches, no host bands)")
     ap.add_argument("--shade", action="store_true",
                     help="shade the pixels (rt_set_shading defaults): rays are followed through the translucent disk")
+    ap.add_argument("--sky", action="store_true",
+                    help="shade with the procedural sky on (the default sky profile; implies --shade)")
     ap.add_argument("--record", choices=["minimal", "bench"], default="minimal",
                     help="outputs written: class and step counts, or the bench's record (class, r, theta, "
                          "phi, r_hit, g) plus the 32-byte pixels")
@@ -69,8 +71,8 @@ def main() -> None:
         srcs = scenes.rt_sources(req.sources)
     with relsim.Tracer(0) as tr:
         tr.set_launch_config(a.block, 0, a.refill, a.rays_per_thread, a.fp64_rolled, a.mixed_single)
-        if a.shade:
-            tr.set_shading(relsim.shading())
+        if a.shade or a.sky:
+            tr.set_shading(relsim.shading(sky_enabled=1) if a.sky else relsim.shading())
         dev = None
         if a.device:
             import torch
