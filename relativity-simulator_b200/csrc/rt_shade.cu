@@ -90,17 +90,24 @@ __device__ __noinline__ void ks_tail_direction(const double* __restrict__ T, uin
     for (int c = 0; c < 3; ++c) e[c] = -v[c] * inv;
 }
 
-__global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict__ Dp,
+__global__ void __launch_bounds__(512) shade_kernel(const ShadeDesc* __restrict__ Dp,
                                                     const uint32_t* __restrict__ status,
                                                     const double* __restrict__ r_hit,
                                                     const double* __restrict__ phi,
                                                     const double* __restrict__ g, ContOut cont,
                                                     rt_pixel_out* __restrict__ pixels, uint64_t n) {
     const ShadeDesc& D = *Dp;  // the camera's hole (and the tonemap)
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    // block-uniform iterations: the sky's layers run between block barriers
+    const bool sky_pass = D.sky_on && cont.cross && (cont.exit || cont.tail);
+    for (uint64_t base = blockIdx.x * static_cast<uint64_t>(blockDim.x); base < n;
+         base += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t i = base + threadIdx.x;
+        const bool live = i < n;
         double acc[3] = {0.0, 0.0, 0.0};
-        if (cont.cross) {
+        double e[3] = {0.0, 0.0, 0.0}, thr = 1.0;
+        bool sky_here = false;
+        if (!live) {
+        } else if (cont.cross) {
             // translucent disk (software_compute_engine.hpp:1660, 1743-1796): the
             // crossings in order, each at the throughput left, while more than 0.01
             // is left; the pixel's redshift is the last crossing's and its flags add
@@ -108,7 +115,7 @@ __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict_
             const uint32_t info = cont.info[i];
             const uint32_t n_cross = info & CI_COUNT_MASK;
             const uint32_t bodies = cont.body ? cont.body[i] : 0u;  // source of each crossing
-            double thr = 1.0, last_g = 1.0;
+            double last_g = 1.0;
             for (uint32_t k = 0; k < n_cross && thr > kMinThroughput; ++k) {
                 double sh[4];
                 const double gk = cont.cross[(3 * k + 2) * cont.stride + i];
@@ -130,8 +137,8 @@ __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict_
             }
             pixels[i].status_flags |= add;
             if (n_cross > 0) pixels[i].redshift = static_cast<float>(last_g);
-            if (D.sky_on && add == RT_PIXEL_CELESTIAL_HIT && (cont.exit || cont.tail)) {
-                double e[3];
+            if (sky_pass && add == RT_PIXEL_CELESTIAL_HIT) {
+                sky_here = true;
                 if (cont.tail) {
                     ks_tail_direction(cont.tail, cont.stride, i, e);
                 } else {
@@ -139,11 +146,6 @@ __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict_
                     e[1] = cont.exit[cont.stride + i];
                     e[2] = cont.exit[2 * cont.stride + i];
                 }
-                float sky_rgb[3];
-                sky::sample(D.sky, e[0], e[1], e[2], D.fov, D.time, sky_rgb);
-                acc[0] += thr * static_cast<double>(sky_rgb[0]);
-                acc[1] += thr * static_cast<double>(sky_rgb[1]);
-                acc[2] += thr * static_cast<double>(sky_rgb[2]);
             }
         } else if (status[i] == RT_RAY_DISK) {
             double sh[4];
@@ -152,6 +154,18 @@ __global__ void __launch_bounds__(256) shade_kernel(const ShadeDesc* __restrict_
             acc[1] = sh[1];
             acc[2] = sh[2];
         }
+        // the sky behind the rays that see it, at the throughput left; every
+        // thread of the block takes the layers' barriers
+        if (sky_pass && __syncthreads_or(sky_here)) {
+            float sky_rgb[3];
+            sky::sample_phased(D.sky, e[0], e[1], e[2], D.fov, D.time, sky_here, sky_rgb, [] { __syncthreads(); });
+            if (sky_here) {
+                acc[0] += thr * static_cast<double>(sky_rgb[0]);
+                acc[1] += thr * static_cast<double>(sky_rgb[1]);
+                acc[2] += thr * static_cast<double>(sky_rgb[2]);
+            }
+        }
+        if (!live) continue;
         // apply_tonemapping (software_compute_engine.hpp:3461-3516)
         const double k = exp2(D.exposure);
         double r = mxd(0.0, acc[0] * k), gg = mxd(0.0, acc[1] * k), b = mxd(0.0, acc[2] * k);
@@ -295,8 +309,10 @@ void build_source_shade_desc(const ShadeDesc& base, const float* profile, double
 void launch_shade(const ShadeDesc* desc, const uint32_t* status, const double* r_hit, const double* phi,
                   const double* g, ContOut cont, rt_pixel_out* pixels, uint64_t n, void* stream) {
     if (n == 0) return;
-    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148ull * 16);
-    shade_kernel<<<static_cast<unsigned>(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(desc, status, r_hit,
+    // 512 threads: one block of 16 warps per SM at 128 registers, so that the
+    // warps of an SM run the same sky layer
+    const uint64_t blocks = std::min<uint64_t>((n + 511) / 512, 148ull * 8);
+    shade_kernel<<<static_cast<unsigned>(blocks), 512, 0, static_cast<cudaStream_t>(stream)>>>(desc, status, r_hit,
                                                                                                 phi, g, cont, pixels, n);
 }
 

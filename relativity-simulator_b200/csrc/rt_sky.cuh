@@ -38,6 +38,26 @@ constexpr double kTwoPi = 2.0 * kPi;
 constexpr double kHalfPi = 0.5 * kPi;
 constexpr double kDegToRad = kPi / 180.0;
 
+// The double-precision library functions the layers call, each compiled once on
+// the device: inlined at their many call sites they made the sky's code larger
+// than the instruction cache, and warps in different layers stalled on
+// instruction fetch.  Same functions, same results.
+#ifdef __CUDACC__
+#define RT_SKY_MATH __host__ __device__ __noinline__
+#else
+#define RT_SKY_MATH inline
+#endif
+RT_SKY_MATH double m_exp(double x) { return ::exp(x); }
+RT_SKY_MATH double m_pow(double x, double y) { return ::pow(x, y); }
+RT_SKY_MATH double m_sin(double x) { return ::sin(x); }
+RT_SKY_MATH double m_cos(double x) { return ::cos(x); }
+RT_SKY_MATH double m_atan2(double y, double x) { return ::atan2(y, x); }
+RT_SKY_MATH double m_log(double x) { return ::log(x); }
+RT_SKY_MATH double m_remainder(double x, double y) { return ::remainder(x, y); }
+RT_SKY_MATH double m_fmod(double x, double y) { return ::fmod(x, y); }
+RT_SKY_MATH double m_asin(double x) { return ::asin(x); }
+RT_SKY_MATH double m_tan(double x) { return ::tan(x); }
+
 // comparison forms of max, min and clamp (NaN passes through as in <algorithm>)
 template <class T>
 RT_SKY_HD T mx(T a, T b) { return (a < b) ? b : a; }
@@ -83,22 +103,22 @@ RT_SKY_HD double draw(uint32_t kind, double lo, double hi, double shape, uint64_
     switch (kind) {
         case 1: {
             const double alpha = mx(shape, 0.05);
-            if (fabs(alpha - 1.0) < 1.0e-4) return lo * pow(hi / lo, u);
+            if (fabs(alpha - 1.0) < 1.0e-4) return lo * m_pow(hi / lo, u);
             const double e = 1.0 - alpha;
-            const double t = (1.0 - u) * pow(lo, e) + u * pow(hi, e);
-            return cl(pow(mx(t, 1.0e-30), 1.0 / e), lo, hi);
+            const double t = (1.0 - u) * m_pow(lo, e) + u * m_pow(hi, e);
+            return cl(m_pow(mx(t, 1.0e-30), 1.0 / e), lo, hi);
         }
         case 2: {
             const double lambda = mx(shape, 0.1);
-            const double norm = 1.0 - exp(-lambda * (hi - lo));
-            return lo - log(mx(1.0 - u * norm, 1.0e-15)) / lambda;
+            const double norm = 1.0 - m_exp(-lambda * (hi - lo));
+            return lo - m_log(mx(1.0 - u * norm, 1.0e-15)) / lambda;
         }
         case 3: {
             const double u2 = mx(unit(h ^ 0x94d049bb133111ebULL), 1.0e-15);
-            const double z = sqrt(-2.0 * log(mx(u, 1.0e-15))) * cos(2.0 * kPi * u2);
-            const double a = log(mx(lo, 1.0e-12)), b = log(mx(hi, 1.0e-11));
+            const double z = sqrt(-2.0 * m_log(mx(u, 1.0e-15))) * m_cos(2.0 * kPi * u2);
+            const double a = m_log(mx(lo, 1.0e-12)), b = m_log(mx(hi, 1.0e-11));
             const double spread = cl(shape * 0.35, 0.05, 2.5) * (b - a);
-            return cl(exp(0.5 * (a + b) + spread * z), lo, hi);
+            return cl(m_exp(0.5 * (a + b) + spread * z), lo, hi);
         }
         case 4: {
             if (u < 0.85) return lo + (u / 0.85) * (lo + 0.12 * (hi - lo) - lo);
@@ -134,6 +154,7 @@ RT_SKY_HD float vnoise(float x, float y, float z) {
 }
 RT_SKY_HD float fbm(float x, float y, float z, int octaves, float rough) {
     float total = 0.0f, amp = 1.0f, freq = 1.0f, norm = 0.0f;
+    #pragma unroll 1
     for (int i = 0; i < octaves; ++i) {
         total += vnoise(x * freq, y * freq, z * freq) * amp;
         norm += amp;
@@ -144,6 +165,7 @@ RT_SKY_HD float fbm(float x, float y, float z, int octaves, float rough) {
 }
 RT_SKY_HD float ridged(float x, float y, float z, int octaves, float rough) {
     float total = 0.0f, amp = 1.0f, freq = 1.0f, norm = 0.0f;
+    #pragma unroll 1
     for (int i = 0; i < octaves; ++i) {
         float v = 1.0f - fabsf(vnoise(x * freq, y * freq, z * freq));
         v *= v;
@@ -157,9 +179,9 @@ RT_SKY_HD float ridged(float x, float y, float z, int octaves, float rough) {
 
 // Yaw about z, pitch about y, roll about x, in degrees (:450-477).
 RT_SKY_HD V3 rotate(const V3& v, double yaw, double pitch, double roll) {
-    const double cy = cos(yaw * kDegToRad), sy = sin(yaw * kDegToRad);
-    const double cp = cos(pitch * kDegToRad), sp = sin(pitch * kDegToRad);
-    const double cr = cos(roll * kDegToRad), sr = sin(roll * kDegToRad);
+    const double cy = m_cos(yaw * kDegToRad), sy = m_sin(yaw * kDegToRad);
+    const double cp = m_cos(pitch * kDegToRad), sp = m_sin(pitch * kDegToRad);
+    const double cr = m_cos(roll * kDegToRad), sr = m_sin(roll * kDegToRad);
     const double x1 = v.x * cy - v.y * sy, y1 = v.x * sy + v.y * cy, z1 = v.z;
     const double x2 = x1 * cp + z1 * sp, y2 = y1, z2 = -x1 * sp + z1 * cp;
     return {x2, y2 * cr - z2 * sr, y2 * sr + z2 * cr};
@@ -237,7 +259,7 @@ RT_SKY_HD double bessel_j1(double x) {
     const double y = 3.75 / ax;
     const double f0 = 0.79788456 + y * (-0.00000077 + y * (-0.00552740 + y * (0.00009512 + y * (0.00137237 - y * 0.00072805))));
     const double t0 = ax - 2.35619449 + y * (0.04411179 + y * (-0.00008449 + y * (-0.00076126 + y * (0.00009185 + y * 0.00008544))));
-    const double v = (f0 / sqrt(ax)) * cos(t0);
+    const double v = (f0 / sqrt(ax)) * m_cos(t0);
     return (x < 0.0) ? -v : v;
 }
 
@@ -248,12 +270,12 @@ RT_SKY_HD double star_psf(double theta_sq, double sigma, double eff_sq, double p
         case 6: {  // pinpoint
             const double tight = cl(s.star_dirac_concentration, 0.1, 0.999);
             const double w = mx(pix * (1.0 - tight) * 0.4, 1.0e-9);
-            return exp(-theta_sq / (2.0 * w * w));
+            return m_exp(-theta_sq / (2.0 * w * w));
         }
         case 7: {  // cinematic bloom
-            const double core = exp(-theta_sq / (2.0 * eff_sq));
+            const double core = m_exp(-theta_sq / (2.0 * eff_sq));
             const double w = mx(sigma * cl(s.star_bloom_radius, 1.0, 30.0), pix * 3.5);
-            return core + s.star_bloom_intensity * 1.8 * exp(-theta / w);
+            return core + s.star_bloom_intensity * 1.8 * m_exp(-theta / w);
         }
         case 1: {  // Lorentzian
             const double g2 = eff_sq * mx(s.star_profile_param, 0.05);
@@ -262,7 +284,7 @@ RT_SKY_HD double star_psf(double theta_sq, double sigma, double eff_sq, double p
         case 2: {  // Moffat
             const double beta = cl(s.star_profile_param, 1.05, 8.0);
             const double scale = mx(eff_sq * s.star_profile_param2, 1.0e-12);
-            return pow(1.0 + theta_sq / scale, -beta);
+            return m_pow(1.0 + theta_sq / scale, -beta);
         }
         case 3: {  // Airy
             const double v = kPi * theta / mx(sigma, 1.0e-8);
@@ -278,15 +300,15 @@ RT_SKY_HD double star_psf(double theta_sq, double sigma, double eff_sq, double p
             return 1.0 - cl((theta - (rad - edge)) / mx(2.0 * edge, 1.0e-9), 0.0, 1.0);
         }
         case 5: {  // diffraction spikes
-            const double core = exp(-theta_sq / (2.0 * eff_sq));
-            const double ang = atan2(ly, lx) + s.star_spike_angle_deg * (kPi / 180.0);
+            const double core = m_exp(-theta_sq / (2.0 * eff_sq));
+            const double ang = m_atan2(ly, lx) + s.star_spike_angle_deg * (kPi / 180.0);
             const double ns = (s.star_spike_count == 6u) ? 3.0 : ((s.star_spike_count == 8u) ? 4.0 : 2.0);
-            const double beam = pow(fabs(cos(ns * ang)), 32.0);
+            const double beam = m_pow(fabs(m_cos(ns * ang)), 32.0);
             const double len = mx(sigma * cl(s.star_spike_length, 0.5, 60.0), pix * 8.0);
-            return core + s.star_spike_intensity * 2.5 * beam * exp(-theta / len);
+            return core + s.star_spike_intensity * 2.5 * beam * m_exp(-theta / len);
         }
         default:  // Gaussian with a faint exponential wing
-            return exp(-theta_sq / (2.0 * eff_sq)) + 0.06 * exp(-theta / (4.0 * mx(sigma, 1.0e-8)));
+            return m_exp(-theta_sq / (2.0 * eff_sq)) + 0.06 * m_exp(-theta / (4.0 * mx(sigma, 1.0e-8)));
     }
 }
 
@@ -318,8 +340,11 @@ RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, do
     const int32_t cx = static_cast<int32_t>(floor(dir.x * res)), cy = static_cast<int32_t>(floor(dir.y * res)),
                   cz = static_cast<int32_t>(floor(dir.z * res));
     const double presence = cl(1.0 - (s.star_density * q) * 0.16, 0.01, 0.99);
+    #pragma unroll 1
     for (int32_t dz = -1; dz <= 1; ++dz)
+        #pragma unroll 1
         for (int32_t dy = -1; dy <= 1; ++dy)
+            #pragma unroll 1
             for (int32_t dx = -1; dx <= 1; ++dx) {
                 const int32_t ix = cx + dx, iy = cy + dy, iz = cz + dz;
                 const uint64_t h = hash_3d(ix, iy, iz, seed);
@@ -330,24 +355,24 @@ RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, do
                 // populations, 4 spiral-arm density, 5 constellation associations
                 if (s.star_placement_model == 1u) {
                     const double hp = dot(sd, plane);
-                    const double p = exp(-fabs(hp) * cl(s.star_galactic_concentration, 0.2, 20.0));
+                    const double p = m_exp(-fabs(hp) * cl(s.star_galactic_concentration, 0.2, 20.0));
                     if (unit(h + 101ULL) > (p * 0.95 + 0.05)) continue;
                 } else if (s.star_placement_model == 2u) {
                     const float n = fbm(static_cast<float>(sd.x * 3.8), static_cast<float>(sd.y * 3.8),
                                         static_cast<float>(sd.z * 3.8), 3, 0.65f);
-                    const double p = pow(cl((static_cast<double>(n) + 0.6) * 0.85, 0.0, 1.0), 3.0);
+                    const double p = m_pow(cl((static_cast<double>(n) + 0.6) * 0.85, 0.0, 1.0), 3.0);
                     if (unit(h + 102ULL) > p) continue;
                 } else if (s.star_placement_model == 3u) {
                     const double hp = dot(sd, plane);
                     if (unit(h + 103ULL) > 0.30) {
-                        const double p = exp(-fabs(hp) * cl(s.star_galactic_concentration, 0.5, 15.0));
+                        const double p = m_exp(-fabs(hp) * cl(s.star_galactic_concentration, 0.5, 15.0));
                         if (unit(h + 107ULL) > p) continue;
                     }
                 } else if (s.star_placement_model == 4u) {
                     const double hp = dot(sd, plane);
-                    const double phi = atan2(sd.y, sd.x);
-                    const double arm = sin(2.0 * phi - 4.5 * log(mx(fabs(hp) + 0.2, 0.05)));
-                    const double p = cl(exp(-fabs(hp) * 3.0) * (0.15 + 0.85 * (arm * 0.5 + 0.5)), 0.02, 1.0);
+                    const double phi = m_atan2(sd.y, sd.x);
+                    const double arm = m_sin(2.0 * phi - 4.5 * m_log(mx(fabs(hp) + 0.2, 0.05)));
+                    const double p = cl(m_exp(-fabs(hp) * 3.0) * (0.15 + 0.85 * (arm * 0.5 + 0.5)), 0.02, 1.0);
                     if (unit(h + 109ULL) > p) continue;
                 } else if (s.star_placement_model == 5u) {
                     const float a = lattice(static_cast<int32_t>(sd.x * 5.0), static_cast<int32_t>(sd.y * 5.0),
@@ -357,7 +382,7 @@ RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, do
                 if (s.dynamic_motion) {
                     const double rate = s.motion_speed * 0.012;
                     const double phase = unit(h + 47ULL) * kTwoPi;
-                    const double ang = sin(time * 0.18 + phase) * rate;
+                    const double ang = m_sin(time * 0.18 + phase) * rate;
                     sd = rotate(sd, ang * (180.0 / kPi), 0.0, 0.0);
                 }
                 const double mu = dot(dir, sd);
@@ -381,7 +406,7 @@ RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, do
                              s.star_brightness;
                 if (s.dynamic_motion && s.star_scintillation > 0.0) {
                     const double tw = unit(h + 67ULL) * kTwoPi;
-                    lum *= (1.0 + s.star_scintillation * sin(time * 3.8 + tw));
+                    lum *= (1.0 + s.star_scintillation * m_sin(time * 3.8 + tw));
                 }
                 V3 u1, u2;
                 tangents(sd, u1, u2);
@@ -404,11 +429,11 @@ RT_SKY_HD_NOINLINE void nebulae(const V3& dir, const SkyProfile& s, double zoom,
     const double hgt = dot(dir, plane);
     const double thick = mx(s.nebula_plane_thickness, 0.02);
     const double fall = cl(s.nebula_plane_falloff, 1.0, 6.0);
-    const double disc = exp(-pow(fabs(hgt) / thick, fall));
+    const double disc = m_exp(-m_pow(fabs(hgt) / thick, fall));
     const V3 asym = unit_or(s.nebula_asymmetry_dir, V3{0.7071067812, 0.0, 0.7071067812});
     const double cpsi = dot(dir, asym);
-    const double asym_env = pow(cl((1.0 + cpsi) * 0.5, 0.0, 1.0), cl(s.nebula_asymmetry * 2.5 + 0.1, 0.1, 8.0));
-    const double glow = s.nebula_core_glow * exp(-2.5 * mx(0.0, 1.0 - cpsi));
+    const double asym_env = m_pow(cl((1.0 + cpsi) * 0.5, 0.0, 1.0), cl(s.nebula_asymmetry * 2.5 + 0.1, 0.1, 8.0));
+    const double glow = s.nebula_core_glow * m_exp(-2.5 * mx(0.0, 1.0 - cpsi));
     const double q = mx(s.quality_factor * s.nebula_quality_factor, 0.05);
     int oct = cl(static_cast<int>(static_cast<double>(s.nebula_octaves) * sqrt(q)), 1, 8);
     if (s.adaptive_fov_quality && zoom > 1.2) oct = mn(8, oct + static_cast<int>(floor(log2(zoom))));
@@ -437,6 +462,7 @@ RT_SKY_HD_NOINLINE void nebulae(const V3& dir, const SkyProfile& s, double zoom,
     const float* c1 = s.nebula_emission_color;
     const float* c2 = s.nebula_secondary_color;
     const float* c3 = s.nebula_tertiary_color;
+    #pragma unroll 1
     for (uint32_t L = 0; L < layers; ++L) {
         const float off = static_cast<float>(L) * 17.3f * static_cast<float>(s.nebula_layer_spread);
         const float sc = 1.0f + static_cast<float>(L) * 0.75f * static_cast<float>(s.nebula_layer_spread);
@@ -457,7 +483,7 @@ RT_SKY_HD_NOINLINE void nebulae(const V3& dir, const SkyProfile& s, double zoom,
     }
     const float nd = ridged(dx * freq * 2.6f + 71.3f, dy * freq * 2.6f - 39.4f, dz * freq * 2.6f + sf, oct, 0.6f);
     const float tau = mx(0.0f, nd - 0.26f) * static_cast<float>(s.nebula_absorption_density * 2.6);
-    const double ext = exp(-static_cast<double>(tau));
+    const double ext = m_exp(-static_cast<double>(tau));
     const double env = (disc * asym_env + glow) * ext * (s.nebula_intensity * s.nebula_quality_factor);
     acc[0] += er * env;
     acc[1] += eg * env;
@@ -470,9 +496,9 @@ RT_SKY_HD V3 ring_cell_centre(uint32_t r, uint32_t s, uint32_t rings, uint32_t s
     const double zc = -1.0 + (2.0 * static_cast<double>(r) + 1.0) / static_cast<double>(rings);
     const double pc = kTwoPi * (static_cast<double>(s) + 0.5) / static_cast<double>(sectors);
     const double z = cl(zc + (unit(h + kz) - 0.5) * (1.6 / static_cast<double>(rings)), -1.0, 1.0);
-    const double p = remainder(pc + (unit(h + kp) - 0.5) * (1.6 * kTwoPi / static_cast<double>(sectors)), kTwoPi);
+    const double p = m_remainder(pc + (unit(h + kp) - 0.5) * (1.6 * kTwoPi / static_cast<double>(sectors)), kTwoPi);
     const double rxy = sqrt(mx(1.0 - z * z, 0.0));
-    return {rxy * cos(p), rxy * sin(p), z};
+    return {rxy * m_cos(p), rxy * m_sin(p), z};
 }
 
 // Galaxies (:1010-1174).
@@ -482,15 +508,17 @@ RT_SKY_HD_NOINLINE void galaxies(const V3& dir, const SkyProfile& s, double* acc
     const uint32_t rings = static_cast<uint32_t>(cl(round(14.0 * sqrt(s.galaxy_density)), 4.0, 36.0));
     const uint32_t rc = cl(static_cast<uint32_t>((cl(dir.z, -1.0, 1.0) + 1.0) * 0.5 * static_cast<double>(rings)), 0u,
                            rings - 1u);
-    double pd = atan2(dir.y, dir.x);
+    double pd = m_atan2(dir.y, dir.x);
     if (pd < 0.0) pd += kTwoPi;
     const double presence = cl(1.0 - s.galaxy_density * 0.25, 0.02, 0.99);
+    #pragma unroll 1
     for (int dr = -1; dr <= 1; ++dr) {
         const int rcand = static_cast<int>(rc) + dr;
         if (rcand < 0 || rcand >= static_cast<int>(rings)) continue;
         const uint32_t ri = static_cast<uint32_t>(rcand);
         const uint32_t ns = sectors_of_ring(ri, rings);
         const uint32_t sc = cl(static_cast<uint32_t>(pd / kTwoPi * static_cast<double>(ns)), 0u, ns - 1u);
+        #pragma unroll 1
         for (int ds = -1; ds <= 1; ++ds) {
             const uint32_t si = (sc + ns + ds) % ns;
             const uint64_t h = hash_coords(ri, si, seed);
@@ -505,7 +533,7 @@ RT_SKY_HD_NOINLINE void galaxies(const V3& dir, const SkyProfile& s, double* acc
             V3 t1, t2;
             tangents(g, t1, t2);
             const double pa = unit(h + 17ULL) * kTwoPi;
-            const double cpa = cos(pa), spa = sin(pa);
+            const double cpa = m_cos(pa), spa = m_sin(pa);
             const V3 u1{t1.x * cpa + t2.x * spa, t1.y * cpa + t2.y * spa, t1.z * cpa + t2.z * spa};
             const V3 u2{-t1.x * spa + t2.x * cpa, -t1.y * spa + t2.y * cpa, -t1.z * spa + t2.z * cpa};
             const double cinc = cl(1.0 - unit(h + 23ULL) * s.galaxy_inclination_variance, 0.12, 1.0);
@@ -515,7 +543,7 @@ RT_SKY_HD_NOINLINE void galaxies(const V3& dir, const SkyProfile& s, double* acc
             const double yo = dot(d, u2) / mx(size, 1.0e-6);
             const double xd = xo, yd = yo / cinc;
             const double rd = sqrt(xd * xd + yd * yd);
-            const double phd = atan2(yd, xd);
+            const double phd = m_atan2(yd, xd);
             uint32_t morph = s.galaxy_morphology_model;
             if (morph == 0u) {
                 const double w1 = mx(s.galaxy_weight_grand_design, 0.0), w2 = mx(s.galaxy_weight_flocculent, 0.0),
@@ -535,41 +563,41 @@ RT_SKY_HD_NOINLINE void galaxies(const V3& dir, const SkyProfile& s, double* acc
             double tc[3] = {1.25, 1.05, 0.70}, td[3] = {0.65, 0.85, 1.35};
             if (morph == 4u) {  // elliptical: Sersic bulge
                 const double b = 2.0 * s.galaxy_bulge_sersic_index - 0.333333;
-                core = exp(-cl(b * pow(rd, 1.0 / s.galaxy_bulge_sersic_index), 0.0, 30.0));
+                core = m_exp(-cl(b * m_pow(rd, 1.0 / s.galaxy_bulge_sersic_index), 0.0, 30.0));
                 tc[0] = 1.35; tc[1] = 1.00; tc[2] = 0.65;
             } else if (morph == 5u) {  // lenticular with a dust ring
-                core = exp(-rd * 3.5);
-                disk = exp(-rd * 1.8);
+                core = m_exp(-rd * 3.5);
+                disk = m_exp(-rd * 1.8);
                 const double rdist = fabs(rd - 0.65);
-                disk *= (1.0 - (1.0 - exp(-rdist * rdist / 0.008)) * s.galaxy_dust_lane_opacity);
+                disk *= (1.0 - (1.0 - m_exp(-rdist * rdist / 0.008)) * s.galaxy_dust_lane_opacity);
                 tc[0] = 1.20; tc[1] = 1.05; tc[2] = 0.80;
                 td[0] = 0.95; td[1] = 0.95; td[2] = 0.90;
             } else if (morph == 3u) {  // barred spiral
-                core = exp(-rd * rd * 6.0);
+                core = m_exp(-rd * rd * 6.0);
                 const double bl = 0.55 * cl(s.galaxy_bar_strength, 0.1, 2.0), bw = 0.15;
-                const double bar = exp(-(xd * xd) / (2.0 * bl * bl) - (yd * yd) / (2.0 * bw * bw));
-                const double arms = 0.5 + 0.5 * cos(2.0 * (phd - rd * 3.5 * s.galaxy_pitch_angle));
-                disk = (bar * 0.7 + exp(-rd * 2.2) * arms * 0.5);
+                const double bar = m_exp(-(xd * xd) / (2.0 * bl * bl) - (yd * yd) / (2.0 * bw * bw));
+                const double arms = 0.5 + 0.5 * m_cos(2.0 * (phd - rd * 3.5 * s.galaxy_pitch_angle));
+                disk = (bar * 0.7 + m_exp(-rd * 2.2) * arms * 0.5);
             } else if (morph == 2u) {  // flocculent
-                core = exp(-rd * 4.0);
+                core = m_exp(-rd * 4.0);
                 const float cn = fbm(static_cast<float>(xd * 6.0), static_cast<float>(yd * 6.0), static_cast<float>(h & 0xFFu),
                                      3, 0.6f);
-                const double arms = 0.5 + 0.5 * cos(6.0 * phd - rd * 7.0 * s.galaxy_pitch_angle + static_cast<double>(cn) * 2.5);
-                disk = exp(-rd * 2.5) * arms * (1.0 + s.galaxy_clumpiness * static_cast<double>(cn));
+                const double arms = 0.5 + 0.5 * m_cos(6.0 * phd - rd * 7.0 * s.galaxy_pitch_angle + static_cast<double>(cn) * 2.5);
+                disk = m_exp(-rd * 2.5) * arms * (1.0 + s.galaxy_clumpiness * static_cast<double>(cn));
             } else if (morph == 6u) {  // ring
-                core = exp(-rd * rd * 8.0) * 1.2;
+                core = m_exp(-rd * rd * 8.0) * 1.2;
                 const double diff = fabs(rd - 0.70);
-                disk = exp(-(diff * diff) / (2.0 * 0.12 * 0.12)) * 1.4;
+                disk = m_exp(-(diff * diff) / (2.0 * 0.12 * 0.12)) * 1.4;
                 td[0] = 0.45; td[1] = 0.80; td[2] = 1.65;
             } else {  // grand-design spiral
-                core = exp(-rd * rd * 4.0);
-                const double arms = 0.5 + 0.5 * cos(s.galaxy_spiral_arms * phd - rd * 4.8 * s.galaxy_pitch_angle);
-                disk = exp(-rd * 2.2) * arms;
+                core = m_exp(-rd * rd * 4.0);
+                const double arms = 0.5 + 0.5 * m_cos(s.galaxy_spiral_arms * phd - rd * 4.8 * s.galaxy_pitch_angle);
+                disk = m_exp(-rd * 2.2) * arms;
             }
             if (morph != 4u && s.galaxy_dust_lane_opacity > 0.0) {
                 const double near = yo * sinc;
                 if (near > 0.0) {
-                    const double lane = exp(-fabs(near - 0.18) * 9.0) * s.galaxy_dust_lane_opacity;
+                    const double lane = m_exp(-fabs(near - 0.18) * 9.0) * s.galaxy_dust_lane_opacity;
                     core *= (1.0 - lane * 0.85);
                     disk *= (1.0 - lane * 0.65);
                 }
@@ -592,19 +620,21 @@ RT_SKY_HD_NOINLINE void clusters(const V3& dir, const SkyProfile& s, double fov,
     const uint32_t rings = static_cast<uint32_t>(cl(round(10.0 * sqrt(dens)), 3.0, 36.0));
     const uint32_t rc = cl(static_cast<uint32_t>((cl(dir.z, -1.0, 1.0) + 1.0) * 0.5 * static_cast<double>(rings)), 0u,
                            rings - 1u);
-    double pd = atan2(dir.y, dir.x);
+    double pd = m_atan2(dir.y, dir.x);
     if (pd < 0.0) pd += kTwoPi;
     const double presence = cl(1.0 - dens * 0.16, 0.01, 0.99);
     const V3 plane = unit_or(s.nebula_plane_normal, V3{0.0, 0.4472135955, 0.894427191});
     const V3 asym = unit_or(s.nebula_asymmetry_dir, V3{0.7071067812, 0.0, 0.7071067812});
     const double pix = fov / 1080.0;
     const uint32_t mprof = s.cluster_inherit_star_profile ? s.star_profile_model : s.cluster_star_profile_model;
+    #pragma unroll 1
     for (int dr = -1; dr <= 1; ++dr) {
         const int rcand = static_cast<int>(rc) + dr;
         if (rcand < 0 || rcand >= static_cast<int>(rings)) continue;
         const uint32_t ri = static_cast<uint32_t>(rcand);
         const uint32_t ns = sectors_of_ring(ri, rings);
         const uint32_t sc = cl(static_cast<uint32_t>(pd / kTwoPi * static_cast<double>(ns)), 0u, ns - 1u);
+        #pragma unroll 1
         for (int ds = -1; ds <= 1; ++ds) {
             const uint32_t si = (sc + ns + ds) % ns;
             const uint64_t h = hash_coords(ri, si, seed);
@@ -616,7 +646,7 @@ RT_SKY_HD_NOINLINE void clusters(const V3& dir, const SkyProfile& s, double fov,
                 if (unit(h + 99ULL) > p) continue;
             } else if (s.cluster_placement_model == 1u) {  // open clusters near the plane
                 const double hc = dot(c, plane);
-                const double p = exp(-(hc * hc) / mx(s.cluster_plane_scale_height * s.cluster_plane_scale_height, 0.005));
+                const double p = m_exp(-(hc * hc) / mx(s.cluster_plane_scale_height * s.cluster_plane_scale_height, 0.005));
                 if (unit(h + 99ULL) > p) continue;
             }
             const double mu = dot(dir, c);
@@ -628,7 +658,7 @@ RT_SKY_HD_NOINLINE void clusters(const V3& dir, const SkyProfile& s, double fov,
             if (sep2 > 9.0 * r2) continue;
             if (s.cluster_halo_intensity > 0.0) {
                 const double cd = r2 * 0.40 * mx(s.cluster_spread_factor, 0.1);
-                const double plummer = 1.0 / pow(1.0 + sep2 / mx(cd, 1.0e-7), s.cluster_concentration);
+                const double plummer = 1.0 / m_pow(1.0 + sep2 / mx(cd, 1.0e-7), s.cluster_concentration);
                 const double f = plummer * s.cluster_brightness * cl(s.cluster_halo_intensity, 0.0, 2.0) * 0.75;
                 acc[0] += f * static_cast<double>(s.cluster_core_tint[0]);
                 acc[1] += f * static_cast<double>(s.cluster_core_tint[1]);
@@ -640,13 +670,14 @@ RT_SKY_HD_NOINLINE void clusters(const V3& dir, const SkyProfile& s, double fov,
                 const uint32_t members =
                     cl(static_cast<uint32_t>(static_cast<double>(s.cluster_member_count) * s.cluster_quality_factor), 4u, 256u);
                 const double rcore = crad * 0.50 * mx(s.cluster_spread_factor, 0.1);
+                #pragma unroll 1
                 for (uint32_t m = 0; m < members; ++m) {
                     const uint64_t mh = hash_coords(ri * 1000u + si, m, seed ^ 0x3c6ef372fe94f82bULL);
                     const double ur = cl(unit(mh), 0.001, 0.96);
-                    const double p23 = pow(ur, 2.0 / 3.0);
-                    const double rm = rcore * sqrt(p23 / mx(1.0 - pow(ur, 2.0 / 3.0), 1.0e-4));
+                    const double p23 = m_pow(ur, 2.0 / 3.0);
+                    const double rm = rcore * sqrt(p23 / mx(1.0 - m_pow(ur, 2.0 / 3.0), 1.0e-4));
                     const double pm = kTwoPi * unit(mh + 13ULL);
-                    const double dxm = rm * cos(pm), dym = rm * sin(pm);
+                    const double dxm = rm * m_cos(pm), dym = rm * m_sin(pm);
                     const double px = c.x + u1.x * dxm + u2.x * dym, py = c.y + u1.y * dxm + u2.y * dym,
                                  pz = c.z + u1.z * dxm + u2.z * dym;
                     const double ml = sqrt(px * px + py * py + pz * pz);
@@ -701,8 +732,11 @@ RT_SKY_HD_NOINLINE void quasars(const V3& dir, const SkyProfile& s, double* acc)
     const int32_t cx = static_cast<int32_t>(floor(dir.x * res)), cy = static_cast<int32_t>(floor(dir.y * res)),
                   cz = static_cast<int32_t>(floor(dir.z * res));
     const double presence = cl(1.0 - s.quasar_density * 0.06, 0.05, 0.99);
+    #pragma unroll 1
     for (int32_t dz = -1; dz <= 1; ++dz)
+        #pragma unroll 1
         for (int32_t dy = -1; dy <= 1; ++dy)
+            #pragma unroll 1
             for (int32_t dx = -1; dx <= 1; ++dx) {
                 const uint64_t h = hash_3d(cx + dx, cy + dy, cz + dz, seed);
                 if (unit(h) <= presence) continue;
@@ -712,23 +746,23 @@ RT_SKY_HD_NOINLINE void quasars(const V3& dir, const SkyProfile& s, double* acc)
                 if (mu <= 0.985) continue;
                 const double sep2 = 2.0 * mx(0.0, 1.0 - mu);
                 const double jt = unit(h + 41ULL) * kPi, jp = unit(h + 47ULL) * kTwoPi;
-                const double st = sin(jt);
-                const V3 jet{st * cos(jp), st * sin(jp), cos(jt)};
+                const double st = m_sin(jt);
+                const V3 jet{st * m_cos(jp), st * m_sin(jp), m_cos(jt)};
                 const double cv = fabs(dot(dir, jet));
                 const double gamma = mx(s.quasar_jet_lorentz_factor, 1.05);
                 const double beta = sqrt(1.0 - 1.0 / (gamma * gamma));
                 const double dop = 1.0 / (gamma * (1.0 - beta * cv));
-                const double boost = pow(cl(dop, 0.1, 10.0), 3.0);
+                const double boost = m_pow(cl(dop, 0.1, 10.0), 3.0);
                 const double core_r = mx(s.quasar_core_size, 0.0001);
-                const double core = exp(-sep2 / (2.0 * core_r * core_r)) * s.quasar_brightness * 1.5;
+                const double core = m_exp(-sep2 / (2.0 * core_r * core_r)) * s.quasar_brightness * 1.5;
                 const V3 d{dir.x - qd.x, dir.y - qd.y, dir.z - qd.z};
                 const double along = dot(d, jet);
                 const double perp2 = mx(sep2 - along * along, 0.0);
                 const double jlen = mx(s.quasar_jet_length, 0.005);
                 const double open = mx(s.quasar_jet_opening_angle_deg, 1.0) * (kPi / 180.0);
-                const double jw = core_r + fabs(along) * tan(open);
-                const double prof = exp(-perp2 / (2.0 * jw * jw)) * exp(-fabs(along) / jlen);
-                const double knot = 0.8 + 0.2 * cos(fabs(along) * 160.0);
+                const double jw = core_r + fabs(along) * m_tan(open);
+                const double prof = m_exp(-perp2 / (2.0 * jw * jw)) * m_exp(-fabs(along) / jlen);
+                const double knot = 0.8 + 0.2 * m_cos(fabs(along) * 160.0);
                 const double jf = prof * knot * s.quasar_jet_intensity * s.quasar_brightness * boost * 0.4;
                 const double support = mx(jlen * 2.0, core_r * 8.0);
                 const double win = cl(1.0 - sep2 / (support * support), 0.0, 1.0);
@@ -747,8 +781,11 @@ RT_SKY_HD_NOINLINE void pulsars(const V3& dir, const SkyProfile& s, double time,
     const int32_t cx = static_cast<int32_t>(floor(dir.x * res)), cy = static_cast<int32_t>(floor(dir.y * res)),
                   cz = static_cast<int32_t>(floor(dir.z * res));
     const double presence = cl(1.0 - s.pulsar_density * 0.06, 0.05, 0.99);
+    #pragma unroll 1
     for (int32_t dz = -1; dz <= 1; ++dz)
+        #pragma unroll 1
         for (int32_t dy = -1; dy <= 1; ++dy)
+            #pragma unroll 1
             for (int32_t dx = -1; dx <= 1; ++dx) {
                 const uint64_t h = hash_3d(cx + dx, cy + dy, cz + dz, seed);
                 if (unit(h) <= presence) continue;
@@ -758,28 +795,28 @@ RT_SKY_HD_NOINLINE void pulsars(const V3& dir, const SkyProfile& s, double time,
                 if (mu <= 0.996) continue;
                 const double sep2 = 2.0 * mx(0.0, 1.0 - mu);
                 const double at = unit(h + 49ULL) * kPi, ap = unit(h + 53ULL) * kTwoPi;
-                const double sst = sin(at);
-                const V3 axis{sst * cos(ap), sst * sin(ap), cos(at)};
+                const double sst = m_sin(at);
+                const V3 axis{sst * m_cos(ap), sst * m_sin(ap), m_cos(at)};
                 const double tilt = s.pulsar_magnetic_tilt_deg * (kPi / 180.0);
-                const double jitter = exp((unit(h + 83ULL) - 0.5) * s.pulsar_frequency_spread * 2.0);
+                const double jitter = m_exp((unit(h + 83ULL) - 0.5) * s.pulsar_frequency_spread * 2.0);
                 const double rate = s.pulsar_pulse_rate * jitter;
-                const double phase = fmod(time * rate + unit(h + 61ULL), 1.0) * kTwoPi;
+                const double phase = m_fmod(time * rate + unit(h + 61ULL), 1.0) * kTwoPi;
                 V3 u1, u2;
                 tangents(axis, u1, u2);
-                const double sti = sin(tilt), cti = cos(tilt), cph = cos(phase), sph = sin(phase);
+                const double sti = m_sin(tilt), cti = m_cos(tilt), cph = m_cos(phase), sph = m_sin(phase);
                 const V3 beam{cti * axis.x + sti * (cph * u1.x + sph * u2.x), cti * axis.y + sti * (cph * u1.y + sph * u2.y),
                               cti * axis.z + sti * (cph * u1.z + sph * u2.z)};
                 const double mub = fabs(dot(dir, beam));
                 const double bw = mx(s.pulsar_beam_width_deg, 0.5) * (kPi / 180.0);
                 const double bsep2 = 2.0 * mx(0.0, 1.0 - mub);
-                const double duty = exp(-bsep2 / (2.0 * bw * bw));
+                const double duty = m_exp(-bsep2 / (2.0 * bw * bw));
                 const double core_r = 0.0004;
-                const double core = exp(-sep2 / (2.0 * core_r * core_r)) * s.pulsar_brightness * 1.8;
+                const double core = m_exp(-sep2 / (2.0 * core_r * core_r)) * s.pulsar_brightness * 1.8;
                 const double pw = mx(s.pulsar_wind_nebula_scale, 0.0005);
                 const V3 d{dir.x - pd.x, dir.y - pd.y, dir.z - pd.z};
                 const double along = dot(d, axis);
                 const double perp2 = mx(sep2 - along * along, 0.0);
-                const double torus = exp(-perp2 / (2.0 * pw * pw)) * exp(-fabs(along) / (pw * 0.4));
+                const double torus = m_exp(-perp2 / (2.0 * pw * pw)) * m_exp(-fabs(along) / (pw * 0.4));
                 const double pwn = torus * s.pulsar_wind_nebula_intensity * s.pulsar_brightness * 0.5;
                 const double t = core * duty + pwn;
                 acc[0] += t * 0.70;
@@ -796,8 +833,11 @@ RT_SKY_HD_NOINLINE void remnants(const V3& dir, const SkyProfile& s, double* acc
     const int32_t cx = static_cast<int32_t>(floor(dir.x * res)), cy = static_cast<int32_t>(floor(dir.y * res)),
                   cz = static_cast<int32_t>(floor(dir.z * res));
     const double presence = cl(1.0 - s.snr_density * 0.06, 0.05, 0.99);
+    #pragma unroll 1
     for (int32_t dz = -1; dz <= 1; ++dz)
+        #pragma unroll 1
         for (int32_t dy = -1; dy <= 1; ++dy)
+            #pragma unroll 1
             for (int32_t dx = -1; dx <= 1; ++dx) {
                 const uint64_t h = hash_3d(cx + dx, cy + dy, cz + dz, seed);
                 if (unit(h) <= presence) continue;
@@ -820,9 +860,9 @@ RT_SKY_HD_NOINLINE void remnants(const V3& dir, const SkyProfile& s, double* acc
                 const double pr = base * (1.0 + s.snr_asymmetry * 0.35 * static_cast<double>(turb));
                 const double thick = mx(s.snr_shell_thickness * base, 0.0005);
                 const double diff = fabs(dist - pr);
-                const double shell = exp(-(diff * diff) / (2.0 * thick * thick)) * s.snr_brightness * 1.5;
+                const double shell = m_exp(-(diff * diff) / (2.0 * thick * thick)) * s.snr_brightness * 1.5;
                 const double boost = (morph > 0.5) ? 1.6 : 0.4;
-                const double inner = (dist < pr) ? (exp(-dist / pr) * s.snr_interior_glow * s.snr_brightness * boost) : 0.0;
+                const double inner = (dist < pr) ? (m_exp(-dist / pr) * s.snr_interior_glow * s.snr_brightness * boost) : 0.0;
                 const double maxr = base * 1.6;
                 const double win = cl(1.0 - sep2 / (maxr * maxr), 0.0, 1.0);
                 const double herm = win * win;
@@ -848,11 +888,11 @@ RT_SKY_HD_NOINLINE void remnants(const V3& dir, const SkyProfile& s, double* acc
 RT_SKY_HD_NOINLINE double grid(const V3& dir, const SkyProfile& s, double fov, double* col) {
     col[0] = col[1] = col[2] = 0.0;
     if (!s.grid_enabled || (s.grid_opacity <= 0.0 && s.grid_cell_opacity <= 0.0)) return 0.0;
-    const double dec = asin(cl(dir.z, -1.0, 1.0));
-    const double ra = atan2(dir.y, dir.x);
+    const double dec = m_asin(cl(dir.z, -1.0, 1.0));
+    const double ra = m_atan2(dir.y, dir.x);
     const double sp = mx(s.grid_spacing_deg, 0.1) * kDegToRad;
     const double pix = mx(fov / 1080.0, 1.0e-7);
-    const double cdec = mx(cos(dec), 1.0e-6);
+    const double cdec = mx(m_cos(dec), 1.0e-6);
     double alpha = 0.0;
     if (s.grid_cell_fill_mode != 0u && s.grid_cell_opacity > 0.0) {
         const double ds = dec + kHalfPi;
@@ -884,20 +924,20 @@ RT_SKY_HD_NOINLINE double grid(const V3& dir, const SkyProfile& s, double fov, d
     // line coverage at a distance from a line of half width hw
     auto line = [fe](double dist, double hw) { return 1.0 - cl((dist - (hw - fe)) / (2.0 * fe), 0.0, 1.0); };
     const double taper = cl((sp * cdec - hw_maj * 0.5) / mx(hw_maj * 2.5, 1.0e-6), 0.0, 1.0);
-    const double d_dec = fabs(remainder(dec, sp));
-    const double d_ra = fabs(remainder(ra, sp)) * cdec;
+    const double d_dec = fabs(m_remainder(dec, sp));
+    const double d_ra = fabs(m_remainder(ra, sp)) * cdec;
     const double cov_major = mx(line(d_dec, hw_maj), line(d_ra, hw_maj) * taper);
     double cov_sub = 0.0;
     if (s.grid_subdivisions > 0u) {
         const double ssp = sp / static_cast<double>(s.grid_subdivisions + 1u);
-        const double a = line(fabs(remainder(dec, ssp)), hw_min);
+        const double a = line(fabs(m_remainder(dec, ssp)), hw_min);
         const double st = cl((ssp * cdec - hw_min * 0.5) / mx(hw_min * 2.5, 1.0e-6), 0.0, 1.0);
-        const double b = line(fabs(remainder(ra, ssp)) * cdec, hw_min) * st;
+        const double b = line(fabs(m_remainder(ra, ssp)) * cdec, hw_min) * st;
         cov_sub = mx(a, b) * 0.75;
     }
     const double cov_eq = s.grid_show_equator ? line(fabs(dec), hw_eq) * cl(s.grid_equator_opacity, 0.0, 1.0) : 0.0;
     const double cov_pm = s.grid_show_meridians
-                              ? line(fabs(remainder(ra, kPi)) * cdec, hw_mer) * taper * cl(s.grid_meridian_opacity, 0.0, 1.0)
+                              ? line(fabs(m_remainder(ra, kPi)) * cdec, hw_mer) * taper * cl(s.grid_meridian_opacity, 0.0, 1.0)
                               : 0.0;
     const double cov_cap = s.grid_show_polar_caps
                                ? line(fabs(fabs(dec) - (kHalfPi - sp)), hw_pol) * cl(s.grid_polar_opacity, 0.0, 1.0)
@@ -907,19 +947,19 @@ RT_SKY_HD_NOINLINE double grid(const V3& dir, const SkyProfile& s, double fov, d
         const double tsp = mx(s.grid_tick_interval_deg, 0.1) * kDegToRad;
         const double ext = mx(s.grid_tick_length, pix * 2.0);
         if (fabs(dec) < ext) {
-            const double t = line(fabs(remainder(ra, tsp)) * cdec, hw_tick) *
+            const double t = line(fabs(m_remainder(ra, tsp)) * cdec, hw_tick) *
                              (1.0 - cl((fabs(dec) - (ext - fe)) / (2.0 * fe), 0.0, 1.0));
             cov_ticks = mx(cov_ticks, t);
         }
-        const double rq = fabs(remainder(ra, kHalfPi) * cdec);
+        const double rq = fabs(m_remainder(ra, kHalfPi) * cdec);
         if (rq < ext) {
-            const double t = line(fabs(remainder(dec, tsp)), hw_tick) * (1.0 - cl((rq - (ext - fe)) / (2.0 * fe), 0.0, 1.0));
+            const double t = line(fabs(m_remainder(dec, tsp)), hw_tick) * (1.0 - cl((rq - (ext - fe)) / (2.0 * fe), 0.0, 1.0));
             cov_ticks = mx(cov_ticks, t * taper);
         }
     }
     const double gr = mx(hw_maj * 6.0, pix * 4.0);
-    const double gdec = exp(-d_dec * d_dec / (2.0 * gr * gr));
-    const double gra = exp(-d_ra * d_ra / (2.0 * gr * gr)) * taper;
+    const double gdec = m_exp(-d_dec * d_dec / (2.0 * gr * gr));
+    const double gra = m_exp(-d_ra * d_ra / (2.0 * gr * gr)) * taper;
     const double glow = mx(gdec, gra) * cl(s.grid_glow, 0.0, 10.0);
     auto layer = [&](double cov, const float* c, double boost) {
         if (cov <= 0.0) return;
@@ -940,30 +980,65 @@ RT_SKY_HD_NOINLINE double grid(const V3& dir, const SkyProfile& s, double fov, d
 
 // The sky colour in direction (x, y, z) for a camera of field of view `fov`
 // (radians) at time `time` (SkyboxRenderer::sample_sky, :1674-1722, with the
-// profile's time replaced by the scene's).
-RT_SKY_HD_NOINLINE void sample(const SkyProfile& s, double x, double y, double z, double fov, double time, float* out) {
+// profile's time replaced by the scene's), for the threads with `active` set;
+// `between()` runs after each enabled layer on every thread, active or not (a
+// block barrier in the device shading pass, so that the warps of a block run
+// one layer's code at a time and share the instruction cache; nothing on the
+// host).  The layers follow the profile, so every thread calls between() the
+// same number of times.
+template <class Between>
+RT_SKY_HD void sample_phased(const SkyProfile& s, double x, double y, double z, double fov, double time, bool active,
+                             float* out, Between&& between) {
     out[0] = out[1] = out[2] = 0.0f;
     if (!s.enabled) return;
     const double l2 = x * x + y * y + z * z;
-    if (l2 < 1.0e-18) return;
-    const double inv = 1.0 / sqrt(l2);
-    const V3 u{x * inv, y * inv, z * inv};
-    double yaw = s.orientation_yaw_deg;
-    if (s.dynamic_rotation) yaw = remainder(yaw + s.rotation_rate_deg_s * time, 360.0);
-    const V3 d = rotate(u, yaw, s.orientation_pitch_deg, s.orientation_roll_deg);
+    active = active && !(l2 < 1.0e-18);
+    V3 d{0.0, 0.0, 0.0}, u{0.0, 0.0, 0.0};
     double acc[3] = {static_cast<double>(s.background_color[0]), static_cast<double>(s.background_color[1]),
                      static_cast<double>(s.background_color[2])};
+    if (active) {
+        const double inv = 1.0 / sqrt(l2);
+        u = V3{x * inv, y * inv, z * inv};
+        double yaw = s.orientation_yaw_deg;
+        if (s.dynamic_rotation) yaw = m_remainder(yaw + s.rotation_rate_deg_s * time, 360.0);
+        d = rotate(u, yaw, s.orientation_pitch_deg, s.orientation_roll_deg);
+    }
     const double fov_deg = fov * (180.0 / kPi);
     const double zoom = cl(s.adaptive_fov_reference / mx(fov_deg, 0.05), 1.0, 128.0);
     // the layers that move read the scene's time in place of the profile's
-    if (s.nebula_enabled) nebulae(d, s, zoom, acc);
-    if (s.dust_enabled) dust(d, s, acc);
-    if (s.galaxies_enabled) galaxies(d, s, acc);
-    if (s.clusters_enabled) clusters(d, s, fov, acc);
-    if (s.quasar_enabled) quasars(d, s, acc);
-    if (s.pulsar_enabled) pulsars(d, s, time, acc);
-    if (s.snr_enabled) remnants(d, s, acc);
-    if (s.stars_enabled) stars(d, s, fov, time, acc);
+    if (s.nebula_enabled) {
+        if (active) nebulae(d, s, zoom, acc);
+        between();
+    }
+    if (s.dust_enabled) {
+        if (active) dust(d, s, acc);
+        between();
+    }
+    if (s.galaxies_enabled) {
+        if (active) galaxies(d, s, acc);
+        between();
+    }
+    if (s.clusters_enabled) {
+        if (active) clusters(d, s, fov, acc);
+        between();
+    }
+    if (s.quasar_enabled) {
+        if (active) quasars(d, s, acc);
+        between();
+    }
+    if (s.pulsar_enabled) {
+        if (active) pulsars(d, s, time, acc);
+        between();
+    }
+    if (s.snr_enabled) {
+        if (active) remnants(d, s, acc);
+        between();
+    }
+    if (s.stars_enabled) {
+        if (active) stars(d, s, fov, time, acc);
+        between();
+    }
+    if (!active) return;
     const double k = mx(s.master_intensity, 0.0);
     float rgb[3] = {static_cast<float>(mx(0.0, acc[0] * k)), static_cast<float>(mx(0.0, acc[1] * k)),
                     static_cast<float>(mx(0.0, acc[2] * k))};
@@ -978,6 +1053,11 @@ RT_SKY_HD_NOINLINE void sample(const SkyProfile& s, double x, double y, double z
     out[0] = rgb[0];
     out[1] = rgb[1];
     out[2] = rgb[2];
+}
+
+// The sky colour of one direction (sample_phased for a lone thread).
+RT_SKY_HD_NOINLINE void sample(const SkyProfile& s, double x, double y, double z, double fov, double time, float* out) {
+    sample_phased(s, x, y, z, fov, time, true, out, [] {});
 }
 
 }  // namespace sky
