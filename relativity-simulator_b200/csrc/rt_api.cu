@@ -395,7 +395,7 @@ int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
                      c.cont.cross ? ContOut{c.cont.cross + o, c.cont.info + o, c.cont.stride,
                                             c.cont.body ? c.cont.body + o : nullptr,
                                             c.cont.exit ? c.cont.exit + o : nullptr,
-                                            c.cont.tail ? c.cont.tail + o : nullptr}
+                                            c.cont.tail ? c.cont.tail + o * TL_COUNT : nullptr}
                                   : ContOut{},
                      c.dpix + o, count, s);
         const cudaError_t e = cudaGetLastError();

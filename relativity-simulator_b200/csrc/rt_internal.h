@@ -86,13 +86,14 @@ struct ContOut {
     uint32_t* body;   // multi-source: [stride], source of crossing k in bits 4k..4k+3 (else null)
     double* exit;     // Boyer-Lindquist and multi-source tracers, sky on: [3][stride], the
                       // sky-lookup direction at the ray's end (else null)
-    double* tail;     // Kerr-Schild tracers, sky on: [TL_COUNT][stride], the ray's end (else null)
+    double* tail;     // Kerr-Schild tracers, sky on: [stride][TL_COUNT], the ray's end (else null)
 };
 // The end of a Kerr-Schild ray's trace as its tracer leaves it for the shading
 // pass, which derives the sky-lookup direction from it in parallel over the rays
 // rather than on the tracer's divergent end path: the last step's end points and
 // derivatives, its length, the threshold radius the end is interpolated to (0:
-// the end is the point at TL_Y1) and the hole's mass and spin.
+// the end is the point at TL_Y1) and the hole's mass and spin; one 224-byte
+// record per ray, written by the ray's lane alone.
 enum TailField : int { TL_Y0 = 0, TL_F0 = 6, TL_Y1 = 12, TL_F1 = 18, TL_H = 24, TL_TARGET, TL_M, TL_A, TL_COUNT };
 
 // Device counters of one launch.

@@ -339,19 +339,17 @@ __device__ __forceinline__ void end_continuation(const TraceArgs& args, const Bu
                                                  double interp_target = 0.0, double hh = 0.0) {
     const uint64_t o = Bp->out_offset + S.local[j];
     const double* yl = xch + (interp_target > 0.0 ? 12 : 0);
-    if (double* T = args.cont.tail) {
-        const uint64_t st = args.cont.stride;
+    if (args.cont.tail) {
+        double2* T = reinterpret_cast<double2*>(args.cont.tail + o * TL_COUNT);
         if (interp_target > 0.0) {
 #pragma unroll
-            for (int i = 0; i < 24; ++i) T[i * st + o] = xch[i];
+            for (int i = 0; i < 12; ++i) T[i] = make_double2(xch[2 * i], xch[2 * i + 1]);
         } else {
 #pragma unroll
-            for (int i = 0; i < 6; ++i) T[(TL_Y1 + i) * st + o] = xch[i];
+            for (int i = 0; i < 3; ++i) T[TL_Y1 / 2 + i] = make_double2(xch[2 * i], xch[2 * i + 1]);
         }
-        T[TL_H * st + o] = hh;
-        T[TL_TARGET * st + o] = interp_target;
-        T[TL_M * st + o] = Bp->m;
-        T[TL_A * st + o] = Bp->a;
+        T[TL_H / 2] = make_double2(hh, interp_target);
+        T[TL_M / 2] = make_double2(Bp->m, Bp->a);
     }
     cont_finish(args.cont, o, n_cross, status, sqrt(bl_r2<double>(yl[0], yl[1], yl[2], Bp->a * Bp->a)), Bp->m);
 }

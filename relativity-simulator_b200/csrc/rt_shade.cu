@@ -63,23 +63,15 @@ __device__ __forceinline__ double aces(double x) {
 // (TailField): the end interpolated to the threshold radius on the last step's
 // Hermite interpolant when a threshold is set, then -dx/dlambda of that state,
 // normalised (software_compute_engine.hpp:1771-1775).
-__device__ __noinline__ void ks_tail_direction(const double* __restrict__ T, uint64_t st, uint64_t i, double* e) {
+__device__ __noinline__ void ks_tail_direction(const double* __restrict__ rec, double* e) {
     double y[6];
-    const double target = T[TL_TARGET * st + i], M = T[TL_M * st + i], a = T[TL_A * st + i];
+    const double target = rec[TL_TARGET], M = rec[TL_M], a = rec[TL_A];
     if (target > 0.0) {
-        double y0[6], f0[6], y1[6], f1[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            y0[k] = T[(TL_Y0 + k) * st + i];
-            f0[k] = T[(TL_F0 + k) * st + i];
-            y1[k] = T[(TL_Y1 + k) * st + i];
-            f1[k] = T[(TL_F1 + k) * st + i];
-        }
-        const double h = T[TL_H * st + i];
-        hermite(y0, f0, y1, f1, h, crossing_fraction(y0, f0, y1, f1, h, a, target), 6, y);
+        hermite(rec + TL_Y0, rec + TL_F0, rec + TL_Y1, rec + TL_F1, rec[TL_H],
+                crossing_fraction(rec + TL_Y0, rec + TL_F0, rec + TL_Y1, rec + TL_F1, rec[TL_H], a, target), 6, y);
     } else {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) y[k] = T[(TL_Y1 + k) * st + i];
+        for (int k = 0; k < 6; ++k) y[k] = rec[TL_Y1 + k];
     }
     double k[3], hf;
     ks_field64(y, M, a, k, hf);
@@ -140,7 +132,7 @@ __global__ void __launch_bounds__(512) shade_kernel(const ShadeDesc* __restrict_
             if (sky_pass && add == RT_PIXEL_CELESTIAL_HIT) {
                 sky_here = true;
                 if (cont.tail) {
-                    ks_tail_direction(cont.tail, cont.stride, i, e);
+                    ks_tail_direction(cont.tail + i * TL_COUNT, e);
                 } else {
                     e[0] = cont.exit[i];
                     e[1] = cont.exit[cont.stride + i];
