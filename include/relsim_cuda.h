@@ -179,7 +179,7 @@ typedef struct rt_shading {
     double disk_temperature_floor_k;      /* overrides disk.floor_temperature_k */
     double disk_color_saturation;         /* overrides disk.color_saturation */
     double disk_doppler_beaming_exponent; /* overrides disk.extra_beaming_exponent */
-    double time;                          /* animation time of the disk pattern */
+    double time;                          /* animation time of the disk pattern and the sky */
     double camera_exposure;               /* EV */
     uint32_t tonemapping_mode;            /* 0 clamp, 1 ACES fit, 2 log luminance, 3 extended Reinhard */
     uint32_t hydro_model;                 /* hydro_disk.model: 0 procedural profile, 1 Novikov-Thorne flux */
@@ -355,7 +355,9 @@ rt_status rt_set_launch_config(rt_handle* h, const rt_launch_config* cfg);
  * and rt_dispatch_multi* calls on this handle; NULL turns shading off
  * (r = g = b = 0, a = 1, the default).  RT_ERR_INVALID_ARG for hydro_model 2
  * (the Fishbone-Moncrief torus) or sky_enabled > 1.  rt_shading_defaults
- * gives the reference's defaults, the sky off. */
+ * gives the reference's defaults for the disk and the tonemap, GpuSkyProfile's
+ * defaults in sky, and sky_enabled = 0 (black behind the disk; set it to 1 for
+ * the reference's sky). */
 void rt_shading_defaults(rt_shading* s);
 rt_status rt_set_shading(rt_handle* h, const rt_shading* s);
 /* GpuSkyProfile's defaults, and one field by name (see rt_sky_profile):
