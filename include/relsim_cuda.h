@@ -398,9 +398,9 @@ typedef struct rt_server_config {
     uint32_t max_requests;         /* waiting + admitted requests; more: RT_ERR_AGAIN */
     uint32_t chunk_rays;           /* cost units a request contributes to one epoch (whole rows) */
     uint32_t epoch_rays;           /* cost units per epoch launch; also its ray capacity.  A ray costs
-                                      1 unit (mixed Kerr-Schild), 2 (FP64), 4 (Boyer-Lindquist) or
-                                      5 per hole (multi-source); an epoch's first chunk takes at least
-                                      one row */
+                                      1 unit (mixed Kerr-Schild), 2 (FP64), 4 (Boyer-Lindquist) or,
+                                      multi-source, 2 per hole at rtol >= 1e-9 and 4 below; an epoch's
+                                      first chunk takes at least one row */
     uint32_t max_epoch_bundles;    /* row chunks per epoch launch */
     uint32_t record_mask;          /* bit f: rt_ray_out field f (declaration order) is recorded;
                                       bit 14: the 32-byte pixels */
@@ -409,6 +409,10 @@ typedef struct rt_server_config {
                                       the GPU); capped at epoch_rays */
     rt_launch_config launch_fp64;  /* launch shapes; zeros select the defaults */
     rt_launch_config launch_mixed;
+    uint32_t multi_source_sms;     /* SMs' worth of persistent CTAs a multi-source epoch launches
+                                      (0: every SM); fewer leave room for a single-hole epoch on the
+                                      other slot to run beside it */
+    uint32_t reserved;
 } rt_server_config;
 
 typedef struct rt_request_done {

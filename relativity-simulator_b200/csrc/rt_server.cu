@@ -406,7 +406,10 @@ bool launch_epoch(rt_server* s, Slot& slot) {
         ma.queue = slot.counters;
         ma.stats = slot.counters + 8;
         ma.out = args.out;
-        launch_ms_trace(ma, ms_trace_grid(s->sm_count), st);
+        const int ms_sms = (s->cfg.multi_source_sms > 0 && s->cfg.multi_source_sms < static_cast<uint32_t>(s->sm_count))
+                               ? static_cast<int>(s->cfg.multi_source_sms)
+                               : s->sm_count;
+        launch_ms_trace(ma, ms_trace_grid(ms_sms), st);
         e = cudaGetLastError();
     } else if (bl) {
         BlArgs ba{};

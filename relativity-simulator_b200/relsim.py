@@ -128,7 +128,8 @@ def make_source(position, mass: float = 1.0, spin_parameter: float = 0.0, axis=(
 class ServerConfig(ctypes.Structure):
     _fields_ = [("memory_budget_bytes", ctypes.c_uint64), ("max_requests", _u32), ("chunk_rays", _u32),
                 ("epoch_rays", _u32), ("max_epoch_bundles", _u32), ("record_mask", _u32), ("min_epoch_rays", _u32),
-                ("launch_fp64", LaunchConfig), ("launch_mixed", LaunchConfig)]
+                ("launch_fp64", LaunchConfig), ("launch_mixed", LaunchConfig), ("multi_source_sms", _u32),
+                ("reserved", _u32)]
 
 
 class RequestDone(ctypes.Structure):

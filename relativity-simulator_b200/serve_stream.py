@@ -118,7 +118,8 @@ def request_error(kept: dict, device: int = 0) -> dict:
 
 
 def run(requests: int = 2000, budget_gb: float = 120.0, precision: str = "mixed", check_requests: int = 16,
-        speed: float = 1.0, epoch_units: int = 0, min_epoch_rays: int = -1, device: int = 0) -> dict:
+        speed: float = 1.0, epoch_units: int = 0, min_epoch_rays: int = -1, device: int = 0,
+        multi_source_sms: int = -1) -> dict:
     """Replay the seeded stream through a server on `device` (library defaults
     for the epoch sizes unless given, autotuned launch shapes) and return the
     measurements; `check_requests` single-source requests are compared with
@@ -134,6 +135,8 @@ def run(requests: int = 2000, budget_gb: float = 120.0, precision: str = "mixed"
         cfg.epoch_rays = epoch_units
     if min_epoch_rays >= 0:
         cfg.min_epoch_rays = min_epoch_rays
+    if multi_source_sms >= 0:
+        cfg.multi_source_sms = multi_source_sms
     tuned = load_tuned()
     for prec_name, field in (("fp64", "launch_fp64"), ("mixed", "launch_mixed")):
         t = tuned.get(prec_name)
@@ -150,6 +153,7 @@ def run(requests: int = 2000, budget_gb: float = 120.0, precision: str = "mixed"
                 "budget_bytes": int(st.budget_bytes), "peak_bytes_in_use": int(st.peak_bytes_in_use),
                 "peak_active": int(st.peak_active), "epochs": int(st.epochs), "chunks": int(st.bundles),
                 "epoch_units": int(cfg.epoch_rays), "min_epoch_rays": int(cfg.min_epoch_rays),
+                "multi_source_sms": int(cfg.multi_source_sms),
                 "peak_epoch_rays": int(st.peak_epoch_rays)})
     return res
 
@@ -163,9 +167,11 @@ def main() -> None:
     ap.add_argument("--speed", type=float, default=1.0, help="arrival-rate multiplier")
     ap.add_argument("--epoch-units", type=int, default=0, help="rt_server_config.epoch_rays (0: default)")
     ap.add_argument("--min-epoch-rays", type=int, default=-1, help="rt_server_config.min_epoch_rays (-1: default)")
+    ap.add_argument("--multi-source-sms", type=int, default=-1,
+                    help="rt_server_config.multi_source_sms (-1: default, 0: every SM)")
     a = ap.parse_args()
     print(json.dumps(run(a.requests, a.budget_gb, a.precision, a.check_requests, a.speed, a.epoch_units,
-                         a.min_epoch_rays)))
+                         a.min_epoch_rays, multi_source_sms=a.multi_source_sms)))
 
 
 if __name__ == "__main__":

@@ -19,10 +19,11 @@ disk hits are exactly black with alpha 1 when the sky is off.
 With the sky on, a ray that escapes with throughput left adds the procedural
 sky at its exit direction; the oracle side samples the reference's own
 SkyboxRenderer::sample_sky (compiled from the reference headers into
-oracle/_ref) at the oracle's exit direction.  Bar SKY_BAR in sRGB for 99.5 %
-of those rays and SKY_MAX for every one: a point-like star's flux changes as
-theta dtheta / sigma^2 with the 1e-9 rad difference of the two traces' exit
-directions, and CUDA's transcendental functions differ from the host's.
+oracle/_ref) at the oracle's exit direction.  Bar SKY_BAR (1e-6) in sRGB
+for 99.5 % of the compared rays and SKY_MAX for every one: a point-like
+star's flux changes as theta dtheta / sigma^2 with the 1e-9 rad difference
+of the two traces' exit directions, and CUDA's transcendental functions
+differ from the host's (measured on B200: every ray within 9e-7).
 """
 import ctypes
 import math
@@ -235,8 +236,8 @@ def test_unsupported_settings_rejected(tracer):
 
 
 
-SKY_BAR = 1e-5
-SKY_MAX = 1e-3
+SKY_BAR = 1e-6
+SKY_MAX = 1e-4
 
 
 @pytest.fixture(scope="module")
