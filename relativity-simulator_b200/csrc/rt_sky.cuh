@@ -95,30 +95,54 @@ RT_SKY_HD uint32_t sectors_of_ring(uint32_t ring, uint32_t rings) {
     return static_cast<uint32_t>(mx(1.0, round(static_cast<double>(rings) * kPi * 0.5 * st)));
 }
 
-// Sample of a size or luminosity distribution from one hash (:342-385):
-// 0 uniform, 1 power law, 2 truncated exponential, 3 log-normal, 4 two-part.
-RT_SKY_HD double draw(uint32_t kind, double lo, double hi, double shape, uint64_t h) {
-    const double u = unit(h);
-    if (lo >= hi) return lo;
-    switch (kind) {
-        case 1: {
-            const double alpha = mx(shape, 0.05);
-            if (fabs(alpha - 1.0) < 1.0e-4) return lo * m_pow(hi / lo, u);
+// A size or luminosity distribution (:342-385): 0 uniform, 1 power law, 2
+// truncated exponential, 3 log-normal, 4 two-part; the terms that depend only
+// on its parameters are formed once (make_dist), the rest per sample (draw).
+struct Dist {
+    uint32_t kind;
+    double lo, hi, shape;
+    double k0, k1, k2;
+    bool log_uniform;  // power law of exponent 1
+};
+RT_SKY_HD Dist make_dist(uint32_t kind, double lo, double hi, double shape) {
+    Dist d{kind, lo, hi, shape, 0.0, 0.0, 0.0, false};
+    if (lo >= hi) return d;
+    if (kind == 1u) {
+        const double alpha = mx(shape, 0.05);
+        if (fabs(alpha - 1.0) < 1.0e-4) {
+            d.log_uniform = true;
+            d.k0 = hi / lo;
+        } else {
             const double e = 1.0 - alpha;
-            const double t = (1.0 - u) * m_pow(lo, e) + u * m_pow(hi, e);
-            return cl(m_pow(mx(t, 1.0e-30), 1.0 / e), lo, hi);
+            d.k0 = m_pow(lo, e);
+            d.k1 = m_pow(hi, e);
+            d.k2 = 1.0 / e;
         }
-        case 2: {
-            const double lambda = mx(shape, 0.1);
-            const double norm = 1.0 - m_exp(-lambda * (hi - lo));
-            return lo - m_log(mx(1.0 - u * norm, 1.0e-15)) / lambda;
-        }
+    } else if (kind == 2u) {
+        d.k0 = mx(shape, 0.1);                   // rate
+        d.k1 = 1.0 - m_exp(-d.k0 * (hi - lo));   // normalisation
+    } else if (kind == 3u) {
+        const double a = m_log(mx(lo, 1.0e-12)), b = m_log(mx(hi, 1.0e-11));
+        d.k0 = 0.5 * (a + b);
+        d.k1 = cl(shape * 0.35, 0.05, 2.5) * (b - a);
+    }
+    return d;
+}
+// One sample from one hash.
+RT_SKY_HD double draw(const Dist& d, uint64_t h) {
+    const double u = unit(h);
+    const double lo = d.lo, hi = d.hi;
+    if (lo >= hi) return lo;
+    switch (d.kind) {
+        case 1:
+            if (d.log_uniform) return lo * m_pow(d.k0, u);
+            return cl(m_pow(mx((1.0 - u) * d.k0 + u * d.k1, 1.0e-30), d.k2), lo, hi);
+        case 2:
+            return lo - m_log(mx(1.0 - u * d.k1, 1.0e-15)) / d.k0;
         case 3: {
             const double u2 = mx(unit(h ^ 0x94d049bb133111ebULL), 1.0e-15);
             const double z = sqrt(-2.0 * m_log(mx(u, 1.0e-15))) * m_cos(2.0 * kPi * u2);
-            const double a = m_log(mx(lo, 1.0e-12)), b = m_log(mx(hi, 1.0e-11));
-            const double spread = cl(shape * 0.35, 0.05, 2.5) * (b - a);
-            return cl(m_exp(0.5 * (a + b) + spread * z), lo, hi);
+            return cl(m_exp(d.k0 + d.k1 * z), lo, hi);
         }
         case 4: {
             if (u < 0.85) return lo + (u / 0.85) * (lo + 0.12 * (hi - lo) - lo);
@@ -128,6 +152,9 @@ RT_SKY_HD double draw(uint32_t kind, double lo, double hi, double shape, uint64_
         default:
             return lo + u * (hi - lo);
     }
+}
+RT_SKY_HD double draw(uint32_t kind, double lo, double hi, double shape, uint64_t h) {
+    return draw(make_dist(kind, lo, hi, shape), h);
 }
 
 // ---- value noise (:387-448) ----
@@ -340,6 +367,9 @@ RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, do
     const int32_t cx = static_cast<int32_t>(floor(dir.x * res)), cy = static_cast<int32_t>(floor(dir.y * res)),
                   cz = static_cast<int32_t>(floor(dir.z * res));
     const double presence = cl(1.0 - (s.star_density * q) * 0.16, 0.01, 0.99);
+    const Dist size_dist = make_dist(s.star_size_distribution, s.star_size_min, s.star_size_max, s.star_size_param);
+    const Dist lum_dist = make_dist(s.star_luminosity_distribution, 0.2, 25.0, s.star_luminosity_param);
+    const double size_scale = mx(s.star_size_scale, 0.05);
     #pragma unroll 1
     for (int32_t dz = -1; dz <= 1; ++dz)
         #pragma unroll 1
@@ -351,6 +381,27 @@ RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, do
                 if (unit(h) <= presence) continue;
                 V3 sd;
                 if (!cell_point(ix, iy, iz, h, sd)) continue;
+                // the star's angular distance, size and support (the tests of its
+                // distance and of the placement model are pure: a star that does not
+                // move is measured first, so that most stars skip the placement model)
+                double th2 = 0.0, rad = 0.0, sig = 0.0, sig2 = 0.0, support2 = 0.0;
+                auto within = [&]() -> bool {
+                    const double mu = dot(dir, sd);
+                    if (mu <= 0.994) return false;
+                    th2 = 2.0 * mx(0.0, 1.0 - mu);
+                    rad = draw(size_dist, h + 31ULL) * size_scale;
+                    const double sub = (model == 6u) ? 0.04 : 0.35;
+                    sig = sqrt(rad * rad * (model == 4u ? 1.0 : 1.96) + pix * pix * sub);
+                    sig2 = sig * sig;
+                    double support = sig * 6.0;
+                    if (model == 5u) support = mx(support, sig * cl(s.star_spike_length, 1.0, 60.0));
+                    else if (model == 7u) support = mx(support, sig * cl(s.star_bloom_radius, 1.0, 30.0));
+                    else if (model == 3u) support = mx(support, sig * 12.0);
+                    else if (model == 1u || model == 2u) support = mx(support, sig * 10.0);
+                    support2 = support * support;
+                    return !(th2 > support2);
+                };
+                if (!s.dynamic_motion && !within()) continue;
                 // placement models: 1 galactic disk, 2 fractal clusters, 3 two
                 // populations, 4 spiral-arm density, 5 constellation associations
                 if (s.star_placement_model == 1u) {
@@ -384,26 +435,11 @@ RT_SKY_HD_NOINLINE void stars(const V3& dir, const SkyProfile& s, double fov, do
                     const double phase = unit(h + 47ULL) * kTwoPi;
                     const double ang = m_sin(time * 0.18 + phase) * rate;
                     sd = rotate(sd, ang * (180.0 / kPi), 0.0, 0.0);
+                    if (!within()) continue;
                 }
-                const double mu = dot(dir, sd);
-                if (mu <= 0.994) continue;
-                const double th2 = 2.0 * mx(0.0, 1.0 - mu);
-                const double rad = draw(s.star_size_distribution, s.star_size_min, s.star_size_max, s.star_size_param,
-                                        h + 31ULL) * mx(s.star_size_scale, 0.05);
-                const double sub = (model == 6u) ? 0.04 : 0.35;
-                const double sig = sqrt(rad * rad * (model == 4u ? 1.0 : 1.96) + pix * pix * sub);
-                const double sig2 = sig * sig;
-                double support = sig * 6.0;
-                if (model == 5u) support = mx(support, sig * cl(s.star_spike_length, 1.0, 60.0));
-                else if (model == 7u) support = mx(support, sig * cl(s.star_bloom_radius, 1.0, 30.0));
-                else if (model == 3u) support = mx(support, sig * 12.0);
-                else if (model == 1u || model == 2u) support = mx(support, sig * 10.0);
-                const double support2 = support * support;
-                if (th2 > support2) continue;
                 const double wu = cl(th2 / support2, 0.0, 1.0);
                 const double window = (1.0 - wu) * (1.0 - wu);
-                double lum = draw(s.star_luminosity_distribution, 0.2, 25.0, s.star_luminosity_param, h + 53ULL) *
-                             s.star_brightness;
+                double lum = draw(lum_dist, h + 53ULL) * s.star_brightness;
                 if (s.dynamic_motion && s.star_scintillation > 0.0) {
                     const double tw = unit(h + 67ULL) * kTwoPi;
                     lum *= (1.0 + s.star_scintillation * m_sin(time * 3.8 + tw));
@@ -745,6 +781,9 @@ RT_SKY_HD_NOINLINE void quasars(const V3& dir, const SkyProfile& s, double* acc)
                 const double mu = dot(dir, qd);
                 if (mu <= 0.985) continue;
                 const double sep2 = 2.0 * mx(0.0, 1.0 - mu);
+                // outside the window the quasar adds exactly zero: skip its jet
+                const double support = mx(mx(s.quasar_jet_length, 0.005) * 2.0, mx(s.quasar_core_size, 0.0001) * 8.0);
+                if (1.0 - sep2 / (support * support) <= 0.0) continue;
                 const double jt = unit(h + 41ULL) * kPi, jp = unit(h + 47ULL) * kTwoPi;
                 const double st = m_sin(jt);
                 const V3 jet{st * m_cos(jp), st * m_sin(jp), m_cos(jt)};
@@ -764,7 +803,6 @@ RT_SKY_HD_NOINLINE void quasars(const V3& dir, const SkyProfile& s, double* acc)
                 const double prof = m_exp(-perp2 / (2.0 * jw * jw)) * m_exp(-fabs(along) / jlen);
                 const double knot = 0.8 + 0.2 * m_cos(fabs(along) * 160.0);
                 const double jf = prof * knot * s.quasar_jet_intensity * s.quasar_brightness * boost * 0.4;
-                const double support = mx(jlen * 2.0, core_r * 8.0);
                 const double win = cl(1.0 - sep2 / (support * support), 0.0, 1.0);
                 const double t = (core + jf) * win * win;
                 acc[0] += t * 0.90;
