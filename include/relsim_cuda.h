@@ -189,6 +189,15 @@ typedef struct rt_shading {
                                              panoramas (sky_background_source != 0) are not part of
                                              this library */
     rt_sky_profile sky;                   /* sky (GpuSkyProfile) */
+    /* hydro model 2, the Fishbone-Moncrief torus (hydro_disk, GpuHydroDiskProfile,
+       gpu_types.hpp:91-107): inner edge and pressure maximum in units of M, the
+       adiabatic index, the optical depth scale and the samples per M of chord */
+    float torus_inner_radius;
+    float torus_center_radius;
+    float adiabatic_index;
+    float optical_depth_scale;
+    float sampling_density;
+    float reserved_torus;
 } rt_shading;
 
 /* Per-ray record, structure of arrays.  Any pointer may be NULL (not written).

@@ -103,8 +103,8 @@ rt_camera camera_from_push_constants(const PushConstants& p, const TraceSettings
 
 // rt_shading from the reference's push constants: primary_disk (a
 // GpuDiskProfile, copied as it lies), the disk temperature, saturation and
-// beaming overrides, time, exposure, tonemapping mode, and the hydro disk
-// model and accretion rate, and the procedural sky (params.sky, a
+// beaming overrides, time, exposure, tonemapping mode, the hydro disk model
+// with its accretion rate and torus settings, and the procedural sky (params.sky, a
 // GpuSkyProfile copied as it lies).  The reference's image panoramas
 // (sky_background_source != 0) are not part of the library: such a scene
 // keeps the procedural sky.
@@ -123,6 +123,11 @@ rt_shading shading_from_push_constants(const PushConstants& p) {
     s.tonemapping_mode = p.tonemapping_mode;
     s.hydro_model = p.hydro_disk.model;
     s.accretion_rate_scale = p.hydro_disk.accretion_rate_scale;
+    s.torus_inner_radius = p.hydro_disk.torus_inner_radius;
+    s.torus_center_radius = p.hydro_disk.torus_center_radius;
+    s.adiabatic_index = p.hydro_disk.adiabatic_index;
+    s.optical_depth_scale = p.hydro_disk.optical_depth_scale;
+    s.sampling_density = p.hydro_disk.sampling_density;
     static_assert(sizeof(p.sky) == sizeof(rt_sky_profile), "GpuSkyProfile layout");
     std::memcpy(&s.sky, &p.sky, sizeof s.sky);
     s.sky_enabled = 1;

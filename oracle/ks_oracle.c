@@ -543,8 +543,20 @@ static inline float pi30f(float le, float lp, float order_p1)
  * up to ORC_MAX_CROSSINGS crossings; the record `out` still describes the
  * first hit, and cont holds the crossings, the ray's final class and its
  * exit direction. */
+/* Boyer-Lindquist (r, theta, phi) of a Kerr-Schild point as Cartesian
+ * (spherical_to_cartesian, software_compute_engine.hpp:1063-1066). */
+static void bl_cartesian(const double* x, double a, double* out)
+{
+    double bl[3];
+    orc_bl_from_ks(x, a, 0.0, bl);
+    const double st = sin(bl[1]);
+    out[0] = bl[0] * st * cos(bl[2]);
+    out[1] = bl[0] * st * sin(bl[2]);
+    out[2] = bl[0] * cos(bl[1]);
+}
+
 static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, uint32_t py, orc_ray* out,
-                      orc_cont* cont)
+                      orc_cont* cont, const orc_fm* fm, double* vol)
 {
     const double m = c->m, a = c->a;
     double y[6];
@@ -697,6 +709,12 @@ static void trace_one(const orc_camera* cam, const cam_consts* c, uint32_t px, u
                 }
             }
             dH = max_d(dH, project_null(m, a, yn, cam->projection_tol));
+            if (fm) { /* hydro model 2: the step's chord through the torus (:1725-1731) */
+                double from[3], to[3];
+                bl_cartesian(y, a, from);
+                bl_cartesian(yn, a, to);
+                orc_fm_accumulate(fm, from, to, lz0, vol);
+            }
             /* phi unwrapping, kerr_schild_null_integrator.hpp:61-63 */
             {
                 const double raw = atan2(yn[1], yn[0]) - atan2(a, rn);
@@ -786,6 +804,8 @@ typedef struct {
     uint64_t first, count;
     orc_ray* out;
     orc_cont* cont;
+    const orc_fm* fm;
+    double* vol;
     atomic_ullong next;
 } work_t;
 
@@ -801,29 +821,37 @@ static void* worker(void* arg)
             const uint64_t pix = w->idx ? w->idx[i] : w->first + i;
             const uint32_t px = (uint32_t)(pix % w->cam->screen_width);
             const uint32_t py = (uint32_t)(pix / w->cam->screen_width);
-            trace_one(w->cam, w->c, px, py, &w->out[i], w->cont ? &w->cont[i] : NULL);
+            trace_one(w->cam, w->c, px, py, &w->out[i], w->cont ? &w->cont[i] : NULL, w->fm,
+                      w->vol ? w->vol + 6 * i : NULL);
         }
     }
     return NULL;
 }
 
 static void trace_range(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
-                        orc_ray* out, orc_cont* cont, int threads);
+                        orc_ray* out, orc_cont* cont, const orc_fm* fm, double* vol, int threads);
 
 void orc_trace(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count, orc_ray* out,
                int threads)
 {
-    trace_range(cam, pixel_index, first, count, out, NULL, threads);
+    trace_range(cam, pixel_index, first, count, out, NULL, NULL, NULL, threads);
 }
 
 void orc_trace_cont(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
                     orc_ray* out, orc_cont* cont, int threads)
 {
-    trace_range(cam, pixel_index, first, count, out, cont, threads);
+    trace_range(cam, pixel_index, first, count, out, cont, NULL, NULL, threads);
+}
+
+void orc_trace_volume(const orc_camera* cam, const orc_fm* fm, const uint64_t* pixel_index, uint64_t first,
+                      uint64_t count, orc_ray* out, orc_cont* cont, double* vol, int threads)
+{
+    memset(vol, 0, sizeof(double) * 6 * count);
+    trace_range(cam, pixel_index, first, count, out, cont, fm, vol, threads);
 }
 
 static void trace_range(const orc_camera* cam, const uint64_t* pixel_index, uint64_t first, uint64_t count,
-                        orc_ray* out, orc_cont* cont, int threads)
+                        orc_ray* out, orc_cont* cont, const orc_fm* fm, double* vol, int threads)
 {
     cam_consts c;
     camera_consts(cam, &c);
@@ -837,6 +865,8 @@ static void trace_range(const orc_camera* cam, const uint64_t* pixel_index, uint
     w.count = count;
     w.out = out;
     w.cont = cont;
+    w.fm = fm;
+    w.vol = vol;
     atomic_init(&w.next, 0);
     if (threads == 1) {
         worker(&w);

@@ -120,6 +120,27 @@ typedef struct orc_cont {
     uint32_t pad;
 } orc_cont;
 
+/* Hydro model 2, the Fishbone-Moncrief torus: its constants with the resolved
+ * disk profile (shade_oracle.c orc_fm_context), one chord's emission and
+ * absorption (orc_fm_segment: radiance r, g, b, opacity, redshift) and the
+ * accumulation into a ray's gathered light (orc_fm_accumulate: r, g, b,
+ * throughput, redshift, seen; all 0 before the first emitting segment). */
+typedef struct orc_fm {
+    double m, a, rh, l, w_in, h_max, inner, outer, exponent, kappa, density;
+    uint32_t valid, closed;
+    float profile[32];
+} orc_fm;
+void orc_fm_context(double mass, double spin, double r_in_units, double r_center_units, double gamma,
+                    double optical_depth_scale, double sampling_density, const float resolved_profile[32], orc_fm* out);
+void orc_fm_segment(const orc_fm* t, const double from[3], const double to[3], double l_over_e, double out[5]);
+void orc_fm_accumulate(const orc_fm* t, const double from[3], const double to[3], double l_over_e, double vol[6]);
+/* Trace with the torus: every accepted step's chord between the Boyer-Lindquist
+ * points of its ends, as Cartesian, is accumulated into vol[6 * i] (the camera
+ * as given; the caller turns the thin disk and early capture off, as the
+ * library does for hydro model 2). */
+void orc_trace_volume(const orc_camera* cam, const orc_fm* fm, const uint64_t* pixel_index, uint64_t first,
+                      uint64_t count, orc_ray* out, orc_cont* cont, double* vol, int threads);
+
 /* --- single-function checks (pinned against the reference) --- */
 void orc_ks_field(const double x[3], double mass, double spin, double* r, double* h, double k[3]);
 void orc_ks_rhs(const double y[6], double mass, double spin, double dy[6]);

@@ -64,6 +64,13 @@ CONT_DTYPE = np.dtype([
     ("near_source", "u4"), ("pad", "u4"),
 ])
 
+# orc_fm: the Fishbone-Moncrief torus of hydro model 2 with the resolved disk profile (ks_oracle.h)
+FM_DTYPE = np.dtype([
+    ("m", "f8"), ("a", "f8"), ("rh", "f8"), ("l", "f8"), ("w_in", "f8"), ("h_max", "f8"), ("inner", "f8"),
+    ("outer", "f8"), ("exponent", "f8"), ("kappa", "f8"), ("density", "f8"), ("valid", "u4"), ("closed", "u4"),
+    ("profile", "f4", 32),
+])
+
 # orc_source: a black-hole body beside the camera's hole (ms_oracle.c)
 SOURCE_DTYPE = np.dtype([
     ("position", "f8", 3), ("mass", "f8"), ("spin_parameter", "f8"), ("axis", "f8", 3),
@@ -164,6 +171,10 @@ def lib() -> ctypes.CDLL:
                                      v, v, v, v]
         L.orc_shade_pixel.argtypes = [v, ctypes.c_uint32, f, ctypes.c_uint32, d, d, d, d, d, d, d, ctypes.c_uint32,
                                       d, d, d, v]
+        L.orc_fm_context.argtypes = [d, d, d, d, d, d, d, v, v]
+        L.orc_fm_segment.argtypes = [v, v, v, d, v]
+        L.orc_fm_accumulate.argtypes = [v, v, v, d, v]
+        L.orc_trace_volume.argtypes = [v, v, v, ctypes.c_uint64, ctypes.c_uint64, v, v, v, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -209,6 +220,8 @@ def ref() -> ctypes.CDLL:
         L.ref_kn_horizon.restype = d
         L.ref_kn_zamo_ray.argtypes = [d, d, d, d, d, d, d, d, d, v]
         L.ref_kn_rk45_trace.argtypes = [v, d, d, d, d, d, d, d, d, d, d, ctypes.c_int, v]
+        L.ref_fm_context.argtypes = [v, d, d, v]
+        L.ref_fm_segment.argtypes = [v, v, d, d, v, v, d, v]
         _ref = L
     return _ref
 
@@ -353,3 +366,36 @@ def bl_trace_cont(cam: dict, charge: float, pixels: np.ndarray | None = None,
     cont = np.zeros(n, dtype=CONT_DTYPE)
     lib().orc_bl_trace_cont(_p(c), charge, _p(idx) if idx is not None else None, 0, n, _p(out), _p(cont), threads)
     return out, cont
+
+
+def fm_context(mass: float, spin: float, torus: tuple, resolved_profile: np.ndarray) -> np.ndarray:
+    """The oracle's torus (FM_DTYPE) for (r_in, r_center, gamma, optical_depth_scale,
+    sampling_density) = torus and a resolved disk profile (32 floats)."""
+    out = np.zeros(1, dtype=FM_DTYPE)
+    prof = np.ascontiguousarray(resolved_profile, dtype=np.float32)
+    lib().orc_fm_context(mass, spin, *[float(t) for t in torus], _p(prof), _p(out))
+    return out
+
+
+def fm_segment(fm: np.ndarray, frm, to, l_over_e: float) -> np.ndarray:
+    """One chord through the torus: radiance r, g, b, opacity, redshift."""
+    a = np.ascontiguousarray(frm, dtype=np.float64)
+    b = np.ascontiguousarray(to, dtype=np.float64)
+    out = np.zeros(5)
+    lib().orc_fm_segment(_p(fm), _p(a), _p(b), l_over_e, _p(out))
+    return out
+
+
+def trace_volume(cam: dict, fm: np.ndarray, pixels: np.ndarray | None = None,
+                 threads: int = 0) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Trace with the torus (the camera as given: the caller turns the thin disk
+    and early capture off): (records, continuation ends, gathered light [n, 6]:
+    r, g, b, throughput, redshift, seen)."""
+    c = to_camera(cam)
+    idx = None if pixels is None else np.ascontiguousarray(pixels, dtype=np.uint64)
+    n = int(cam["screen_width"]) * int(cam["screen_height"]) if idx is None else idx.size
+    out = np.zeros(n, dtype=RAY_DTYPE)
+    cont = np.zeros(n, dtype=CONT_DTYPE)
+    vol = np.zeros((n, 6))
+    lib().orc_trace_volume(_p(c), _p(fm), None if idx is None else _p(idx), 0, n, _p(out), _p(cont), _p(vol), threads)
+    return out, cont, vol

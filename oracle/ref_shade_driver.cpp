@@ -143,6 +143,45 @@ void ref_sky_profile_defaults(void* out) {
 	std::memcpy(out, &p, sizeof p);
 }
 
+// Hydro model 2: the reference's HydroDiskContext for the Fishbone-Moncrief
+// torus (hydro_disk_shading.hpp:76-110): out = valid, closed, max enthalpy,
+// inner and outer bounds, specific angular momentum, W_in.
+static R::GpuHydroDiskProfile hydro_from(const double torus[5]) {
+	R::GpuHydroDiskProfile p{};
+	p.model = 2;
+	p.torus_inner_radius = static_cast<float>(torus[0]);
+	p.torus_center_radius = static_cast<float>(torus[1]);
+	p.adiabatic_index = static_cast<float>(torus[2]);
+	p.optical_depth_scale = static_cast<float>(torus[3]);
+	p.sampling_density = static_cast<float>(torus[4]);
+	return p;
+}
+
+void ref_fm_context(const double torus[5], double mass, double spin, double out[7]) {
+	const R::HydroDiskContext c(hydro_from(torus), mass, spin, 6.0 * mass, 24.0 * mass);
+	out[0] = c.torus_valid() ? 1.0 : 0.0;
+	out[1] = c.torus_closed() ? 1.0 : 0.0;
+	out[2] = c.max_enthalpy();
+	out[3] = c.torus_inner_bound();
+	out[4] = c.torus_outer_bound();
+	out[5] = c.torus_specific_angular_momentum();
+	out[6] = c.torus_potential_inner();
+}
+
+// HydroDiskContext::integrate_segment (:173-269) of one chord with a disk
+// profile as it stands: out = radiance r, g, b, opacity, redshift.
+void ref_fm_segment(const double torus[5], const float profile[32], double mass, double spin, const double from[3],
+                    const double to[3], double l_over_e, double out[5]) {
+	const R::HydroDiskContext c(hydro_from(torus), mass, spin, 6.0 * mass, 24.0 * mass);
+	const auto s = c.integrate_segment(profile_from(profile), {from[0], from[1], from[2]}, {to[0], to[1], to[2]},
+	                                   l_over_e);
+	out[0] = s.radiance[0];
+	out[1] = s.radiance[1];
+	out[2] = s.radiance[2];
+	out[3] = s.opacity;
+	out[4] = s.redshift;
+}
+
 void ref_tonemap(const double rgb[3], uint32_t mode, double exposure_ev, float out[3]) {
 	const auto c = R::SoftwareComputeEngine::apply_tonemapping({rgb[0], rgb[1], rgb[2]}, mode, exposure_ev);
 	out[0] = c[0];

@@ -431,3 +431,209 @@ void orc_shade_cont(const float resolved_profile[32], uint32_t hydro_model, floa
     }
     orc_tonemap(accum, tonemap_mode, exposure_ev, out);
 }
+
+/* ---- hydro model 2: the Fishbone-Moncrief torus ------------------------
+ * Restated from hydro/fishbone_moncrief.hpp (the Fishbone & Moncrief 1976
+ * constant-l torus, G = c = 1) and render/accretion_disk/hydro_disk_shading.hpp
+ * (HydroDiskContext::build_torus :76-110, integrate_segment :173-269). */
+static double fm_horizon(double m, double a)
+{
+    const double d = m * m - a * a;
+    return (d < 0.0) ? m : m + sqrt(d);
+}
+
+static double fm_keplerian_l(double m, double a, double rh, double r) /* fishbone_moncrief.hpp:98-116 */
+{
+    const double rs = max_d(r, 1.001 * rh);
+    const double sm = sqrt(m), sr = sqrt(rs);
+    const double num = sm * (rs * rs - 2.0 * a * sm * sr + a * a);
+    const double den = rs * sr - 2.0 * m * sr + a * sm;
+    return (fabs(den) < 1e-30) ? 0.0 : num / den;
+}
+
+static double fm_potential(const orc_fm* t, double r, double theta) /* :118-150 */
+{
+    if (r <= t->rh * 1.0001) return 1e30;
+    const double st = sin(theta), ct = cos(theta);
+    const double s2 = max_d(st * st, 1e-30), c2 = ct * ct;
+    const double r2 = r * r, a2 = t->a * t->a;
+    const double rho2 = r2 + a2 * c2;
+    const double delta = r2 - 2.0 * t->m * r + a2;
+    const double sigma = (r2 + a2) * (r2 + a2) - a2 * delta * s2;
+    const double den = sigma * s2 - 4.0 * t->m * r * t->a * t->l * s2 - t->l * t->l * (delta - a2 * s2);
+    if (den <= 0.0 || delta <= 0.0) return 1e30;
+    return 0.5 * log(max_d((rho2 * delta * s2) / den, 1e-30));
+}
+
+static double fm_enthalpy(const orc_fm* t, double r, double theta) /* :152-159 */
+{
+    const double w = fm_potential(t, r, theta);
+    if (w >= t->w_in) return 1.0;
+    return max_d(1.0, exp(t->w_in - w));
+}
+
+/* u^t, u^phi of the fluid (:210-224) with the Boyer-Lindquist Kerr inverse
+ * metric (metrics/kerr.hpp:151-177). */
+static void fm_four_velocity(const orc_fm* t, double r, double theta, double* ut, double* uphi)
+{
+    const double w = fm_potential(t, r, theta);
+    if (w >= 1e20) {
+        *ut = 1.0;
+        *uphi = 0.0;
+        return;
+    }
+    const double lt = -exp(w), lphi = -t->l * lt;
+    const double rr = max_d(r, 1e-12);
+    const double st = sin(theta), ct = cos(theta);
+    const double s2 = max_d(st * st, 1e-30), c2 = ct * ct;
+    const double a2 = t->a * t->a, r2 = rr * rr;
+    const double rho2 = r2 + a2 * c2;
+    const double delta = r2 - 2.0 * t->m * rr + a2;
+    const double sigma = (r2 + a2) * (r2 + a2) - a2 * delta * s2;
+    const double gtt = -sigma / (rho2 * delta);
+    const double gtp = -(2.0 * t->m * rr * t->a) / (rho2 * delta);
+    const double gpp = (delta - a2 * s2) / (rho2 * delta * s2);
+    *ut = gtt * lt + gtp * lphi;
+    *uphi = gtp * lt + gpp * lphi;
+}
+
+void orc_fm_context(double mass, double spin, double r_in_units, double r_center_units, double gamma,
+                    double optical_depth_scale, double sampling_density, const float resolved_profile[32], orc_fm* out)
+{
+    memset(out, 0, sizeof *out);
+    memcpy(out->profile, resolved_profile, sizeof out->profile);
+    /* the settings are floats in GpuHydroDiskProfile */
+    r_in_units = (double)(float)r_in_units;
+    r_center_units = (double)(float)r_center_units;
+    gamma = (double)(float)gamma;
+    optical_depth_scale = (double)(float)optical_depth_scale;
+    sampling_density = (double)(float)sampling_density;
+    const double m = max_d(mass, 1e-9);
+    const double a = clamp_d(spin, -0.999 * m, 0.999 * m);
+    out->m = m;
+    out->a = a;
+    out->rh = fm_horizon(m, a);
+    const double r_c = (r_center_units * m > 0.0) ? r_center_units * m : 12.0 * m;
+    const double r_in = (r_in_units * m > 0.0) ? r_in_units * m : 6.0 * m;
+    const double half_pi = 0.5 * SH_PI;
+    out->l = fm_keplerian_l(m, a, out->rh, r_c);
+    out->w_in = fm_potential(out, r_in, half_pi);
+    const double w_center = fm_potential(out, r_c, half_pi);
+    out->h_max = exp(max_d(0.0, out->w_in - w_center));
+    out->valid = isfinite(out->h_max) && out->h_max > 1.0 + 1e-9;
+    out->inner = 0.8 * r_in;
+    out->exponent = 1.0 / max_d(gamma - 1.0, 1e-3);
+    out->kappa = optical_depth_scale * max_d((double)resolved_profile[DP_OPACITY_SCALE], 0.0);
+    out->density = max_d(sampling_density, 0.1);
+    if (!out->valid) return;
+    const double step = 0.25 * r_c, limit = 200.0 * r_c;
+    double inside = r_c, outside = r_c;
+    int found = 0;
+    while (outside < limit) {
+        outside += step;
+        if (!(fm_potential(out, outside, half_pi) < out->w_in)) {
+            found = 1;
+            break;
+        }
+        inside = outside;
+    }
+    if (found) {
+        for (int it = 0; it < 48; ++it) {
+            const double mid = 0.5 * (inside + outside);
+            if (fm_potential(out, mid, half_pi) < out->w_in) inside = mid;
+            else outside = mid;
+        }
+        out->outer = 1.05 * outside;
+    } else {
+        out->outer = limit;
+    }
+    out->closed = (uint32_t)found;
+}
+
+void orc_fm_segment(const orc_fm* t, const double from[3], const double to[3], double l_over_e, double out[5])
+{
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+    out[4] = 1.0;
+    if (!t->valid) return;
+    const double dx = to[0] - from[0], dy = to[1] - from[1], dz = to[2] - from[2];
+    const double len2 = dx * dx + dy * dy + dz * dz;
+    if (len2 < 1e-24) return;
+    const double len = sqrt(len2);
+    const double b = (from[0] * dx + from[1] * dy + from[2] * dz) / len2;
+    const double c = (from[0] * from[0] + from[1] * from[1] + from[2] * from[2] - t->outer * t->outer) / len2;
+    const double disc = b * b - c;
+    if (disc <= 0.0) return;
+    const double root = sqrt(disc);
+    const double t0 = clamp_d(-b - root, 0.0, 1.0), t1 = clamp_d(-b + root, 0.0, 1.0);
+    if (t1 <= t0) return;
+    const double clipped = len * (t1 - t0);
+    int count = (int)ceil(clipped * t->density / t->m);
+    count = count < 1 ? 1 : (count > 128 ? 128 : count);
+    const double step = clipped / (double)count;
+    const float* P = t->profile;
+    const double span = max_d(t->h_max - 1.0, 1e-12);
+    double trans = 1.0, wsum = 0.0, zsum = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const double u = t0 + (t1 - t0) * (((double)i + 0.5) / (double)count);
+        const double px = from[0] + u * dx, py = from[1] + u * dy, pz = from[2] + u * dz;
+        const double radius = sqrt(px * px + py * py + pz * pz);
+        if (radius < t->inner || radius > t->outer) continue;
+        const double theta = acos(clamp_d(pz / radius, -1.0, 1.0));
+        const double h = fm_enthalpy(t, radius, theta);
+        if (!(h > 1.0 + 1e-9)) continue;
+        const double ratio = clamp_d((h - 1.0) / span, 0.0, 1.0);
+        const double tau = t->kappa * pow(ratio, t->exponent) * step / t->m;
+        if (tau < 1e-12) continue;
+        double ut, uphi;
+        fm_four_velocity(t, radius, theta, &ut, &uphi);
+        if (ut <= 1e-12) continue;
+        /* AccretionDiskModel::redshift_factor (accretion_disk_model.hpp:218-221) */
+        const double den = ut * (1.0 - (uphi / ut) * l_over_e);
+        const double g = (fabs(den) > 1e-9) ? clamp_d(1.0 / den, 0.05, 4.0) : 1.0;
+        double lin[3];
+        orc_blackbody_rgb(((double)P[DP_FLOOR_T] + ((double)P[DP_PEAK_T] - (double)P[DP_FLOOR_T]) * ratio) * g,
+                          (double)P[DP_REF_LUMINANCE], lin);
+        const double gain = (double)P[DP_BRIGHTNESS] * pow(g, (double)P[DP_BEAMING]);
+        double red = lin[0] * gain, green = lin[1] * gain, blue = lin[2] * gain;
+        const double luma = 0.2126 * red + 0.7152 * green + 0.0722 * blue;
+        const double sat = (double)P[DP_SATURATION];
+        red = max_d(0.0, luma + (red - luma) * sat);
+        green = max_d(0.0, luma + (green - luma) * sat);
+        blue = max_d(0.0, luma + (blue - luma) * sat);
+        const double ts = (double)P[DP_TINT_STRENGTH];
+        red *= 1.0 + ((double)P[DP_TINT_R] - 1.0) * ts;
+        green *= 1.0 + ((double)P[DP_TINT_G] - 1.0) * ts;
+        blue *= 1.0 + ((double)P[DP_TINT_B] - 1.0) * ts;
+        const double st = exp(-tau);
+        const double w = trans * (1.0 - st);
+        out[0] += w * red;
+        out[1] += w * green;
+        out[2] += w * blue;
+        wsum += w;
+        zsum += w * g;
+        trans *= st;
+        if (trans < 0.002) break;
+    }
+    out[3] = 1.0 - trans;
+    out[4] = (wsum > 1e-30) ? (zsum / wsum) : 1.0;
+}
+
+/* accumulate_fishbone_moncrief_segment (software_compute_engine.hpp:1117-1144)
+ * into a ray's gathered light vol[6] (r, g, b, throughput, redshift, seen),
+ * all 0 before its first emitting segment; nothing once the throughput is
+ * 0.01 or less (the reference's loop ends there). */
+void orc_fm_accumulate(const orc_fm* t, const double from[3], const double to[3], double l_over_e, double vol[6])
+{
+    const int seen = vol[5] != 0.0;
+    if (seen && !(vol[3] > 0.01)) return;
+    double s[5];
+    orc_fm_segment(t, from, to, l_over_e, s);
+    if (s[3] <= 1e-6) return;
+    const double thr = seen ? vol[3] : 1.0;
+    vol[0] += thr * s[0];
+    vol[1] += thr * s[1];
+    vol[2] += thr * s[2];
+    vol[3] = thr * (1.0 - s[3]);
+    vol[4] = s[4];
+    vol[5] = 1.0;
+}

@@ -56,7 +56,7 @@ struct rt_handle {
     bool shade_on = false;               // rt_set_shading
     // translucent-disk continuation of a shaded dispatch: each ray's disk crossings
     // and how it ended, and what the launches pass the tracer
-    DevBuf cont_cross, cont_info, cont_body, cont_exit, cont_tail;
+    DevBuf cont_cross, cont_info, cont_body, cont_exit, cont_tail, cont_vol;
     DevBuf ms_shade;  // multi-source shading: one descriptor per source
     ContOut cur_cont{};
     rt_shading shading{};
@@ -332,7 +332,16 @@ rt_status shade_prepare(rt_handle* h, const rt_camera* cam, cudaStream_t s) {
 // The sky needs each ray's direction at its end: the Boyer-Lindquist and
 // multi-source tracers write it (exit); the Kerr-Schild tracers leave the end of
 // the trace to the shading pass (tail, `kerr_schild`).
-rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false, bool kerr_schild = false) {
+rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false, bool kerr_schild = false,
+                             cudaStream_t s = nullptr) {
+    // hydro model 2: the Kerr-Schild FP64 tracer gathers the torus's light into
+    // per-ray records, zeroed here
+    const bool volume = kerr_schild && h->shading.hydro_model == 2u;
+    if (volume) {
+        rt_status vs = ensure(h, h->cont_vol, sizeof(double) * VL_COUNT * n);
+        if (vs != RT_OK) return vs;
+        RT_CUDA(h, cudaMemsetAsync(h->cont_vol.ptr, 0, sizeof(double) * VL_COUNT * n, s));
+    }
     double sky_enabled = 0.0;
     rt_sky_profile_get(&h->shading.sky, "enabled", &sky_enabled);
     const bool sky = h->shading.sky_enabled == 1u && sky_enabled != 0.0;
@@ -346,8 +355,23 @@ rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false, bool k
     h->cur_cont = ContOut{static_cast<double*>(h->cont_cross.ptr), static_cast<uint32_t*>(h->cont_info.ptr), n,
                           bodies ? static_cast<uint32_t*>(h->cont_body.ptr) : nullptr,
                           exit ? static_cast<double*>(h->cont_exit.ptr) : nullptr,
-                          tail ? static_cast<double*>(h->cont_tail.ptr) : nullptr};
+                          tail ? static_cast<double*>(h->cont_tail.ptr) : nullptr,
+                          volume ? static_cast<double*>(h->cont_vol.ptr) : nullptr,
+                          volume ? static_cast<const ShadeDesc*>(h->shade_desc.ptr) : nullptr};
     return RT_OK;
+}
+
+// Hydro model 2 traces the camera as the reference's image path does with the
+// torus: no thin disk, the FP64 tracer at the camera's tolerances, and no
+// early capture (a ray certain to be captured may still cross the torus on its
+// way in).  Boyer-Lindquist cameras are refused.
+bool volume_shading(const rt_handle* h, bool pixels) { return h->shade_on && pixels && h->shading.hydro_model == 2u; }
+rt_camera volume_camera(const rt_camera& cam) {
+    rt_camera c = cam;
+    c.disk_outer_radius = 0.0;
+    c.precision_mode = RT_PRECISION_FP64;
+    c.early_capture = 0;
+    return c;
 }
 
 void end_continuation_state(rt_handle* h) { h->cur_cont = ContOut{}; }
@@ -395,7 +419,8 @@ int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
                      c.cont.cross ? ContOut{c.cont.cross + o, c.cont.info + o, c.cont.stride,
                                             c.cont.body ? c.cont.body + o : nullptr,
                                             c.cont.exit ? c.cont.exit + o : nullptr,
-                                            c.cont.tail ? c.cont.tail + o * TL_COUNT : nullptr}
+                                            c.cont.tail ? c.cont.tail + o * TL_COUNT : nullptr,
+                                            c.cont.vol ? c.cont.vol + o * VL_COUNT : nullptr, c.cont.shade}
                                   : ContOut{},
                      c.dpix + o, count, s);
         const cudaError_t e = cudaGetLastError();
@@ -452,7 +477,7 @@ rt_status dispatch_window(rt_handle* h, const rt_camera* cam, uint32_t col0, uin
     ContinuationScope cont_scope{h};
     if (shade && (st = add_shade_fields(h, dev, n)) != RT_OK) return st;
     if (shade && (st = shade_prepare(h, cam, h->stream)) != RT_OK) return st;
-    if (shade && (st = begin_continuation(h, n, false, !is_bl(cam))) != RT_OK) return st;
+    if (shade && (st = begin_continuation(h, n, false, !is_bl(cam), h->stream)) != RT_OK) return st;
     // bands of at most 2^24 rays; the cancel flag is polled between bands.  Each
     // band's shading and copies follow its trace; on the two-pass tracer a band
     // is traced in sub-bands whose copies overlap the next sub-band's trace.
@@ -692,6 +717,8 @@ rt_status ms_dispatch_window(rt_handle* h, const rt_camera* cam, const rt_source
     const bool shade = h->shade_on && out.pixels;
     rt_status st;
     ContinuationScope cont_scope{h};
+    if (volume_shading(h, out.pixels != nullptr))
+        return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades single-hole Kerr-Schild cameras only");
     if (shade && (st = ms_shade_prepare(h, cam, sources, n_sources, s)) != RT_OK) return st;
     if (shade && (st = begin_continuation(h, n, true)) != RT_OK) return st;
     if ((st = ms_launch(h, cam, sources, n_sources, row0, nrows, out, s)) != RT_OK) return st;
@@ -818,6 +845,7 @@ void rt_destroy(rt_handle* h) {
     release(h->cont_body);
     release(h->cont_exit);
     release(h->cont_tail);
+    release(h->cont_vol);
     release(h->park_d);
     release(h->park_u);
     release(h->pass_queues);
@@ -908,6 +936,12 @@ void rt_shading_defaults(rt_shading* s) {
     s->accretion_rate_scale = 1.0f;
     s->sky_enabled = 0;
     rt_sky_profile_defaults(&s->sky);
+    // GpuHydroDiskProfile's torus defaults (gpu_types.hpp:91-98)
+    s->torus_inner_radius = 6.0f;
+    s->torus_center_radius = 12.0f;
+    s->adiabatic_index = 1.3333334f;
+    s->optical_depth_scale = 0.35f;
+    s->sampling_density = 2.0f;
 }
 
 void rt_sky_profile_defaults(rt_sky_profile* p) {
@@ -990,7 +1024,7 @@ rt_status rt_set_shading(rt_handle* h, const rt_shading* s) {
     rt_camera_defaults(&probe);
     ShadeDesc d;
     if (!build_shade_desc(probe, *s, d))
-        return fail(h, RT_ERR_INVALID_ARG, "shading: hydro_model 0 or 1, tonemapping_mode 0..3, sky_enabled 0 or 1");
+        return fail(h, RT_ERR_INVALID_ARG, "shading: hydro_model 0..2, tonemapping_mode 0..3, sky_enabled 0 or 1");
     h->shading = *s;
     h->shade_on = true;
     return RT_OK;
@@ -1005,6 +1039,11 @@ rt_status rt_dispatch(rt_handle* h, const rt_camera* cam, rt_pixel_out* pixels, 
     row_window(*cam, row0, nrows);
     if (nrows == 0) return fail(h, RT_ERR_INVALID_ARG, "empty row window");
     RT_CUDA(h, cudaSetDevice(h->device));
+    if (volume_shading(h, pixels != nullptr)) {
+        if (is_bl(cam)) return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades Kerr-Schild cameras only");
+        const rt_camera vc = volume_camera(*cam);
+        return dispatch_window(h, &vc, 0, vc.screen_width, row0, nrows, pixels, rays, capacity, cancel);
+    }
     return dispatch_window(h, cam, 0, cam->screen_width, row0, nrows, pixels, rays, capacity, cancel);
 }
 
@@ -1020,6 +1059,11 @@ rt_status rt_dispatch_tile(rt_handle* h, const rt_camera* cam, rt_pixel_out* pix
     const uint32_t w = std::min(cam->tile_extent_x, cam->screen_width - cam->tile_origin_x);
     const uint32_t hgt = std::min(cam->tile_extent_y, cam->screen_height - cam->tile_origin_y);
     RT_CUDA(h, cudaSetDevice(h->device));
+    if (volume_shading(h, pixels != nullptr)) {
+        if (is_bl(cam)) return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades Kerr-Schild cameras only");
+        const rt_camera vc = volume_camera(*cam);
+        return dispatch_window(h, &vc, vc.tile_origin_x, w, vc.tile_origin_y, hgt, pixels, rays, capacity, nullptr);
+    }
     return dispatch_window(h, cam, cam->tile_origin_x, w, cam->tile_origin_y, hgt, pixels, rays, capacity, nullptr);
 }
 
@@ -1036,6 +1080,12 @@ rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* p
     if (capacity < n) return fail(h, RT_ERR_INVALID_ARG, "capacity smaller than the window");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
     RT_CUDA(h, cudaSetDevice(h->device));
+    rt_camera vc;
+    if (volume_shading(h, pixels != nullptr)) {
+        if (is_bl(cam)) return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades Kerr-Schild cameras only");
+        vc = volume_camera(*cam);
+        cam = &vc;
+    }
     rt_ray_out dev = rays ? *rays : rt_ray_out{};
     const bool shade = h->shade_on && pixels;
     rt_status st;
@@ -1058,7 +1108,7 @@ rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* p
     // shaded: the shading constants go up before the trace, which follows each
     // ray through the translucent disk
     if (shade && (st = shade_prepare(h, cam, s)) != RT_OK) return st;
-    if (shade && (st = begin_continuation(h, n, false, true)) != RT_OK) return st;
+    if (shade && (st = begin_continuation(h, n, false, true, s)) != RT_OK) return st;
     if ((st = launch(h, 1, n, OutPtrs{pixels, dev}, cam->precision_mode == RT_PRECISION_MIXED, s)) != RT_OK) return st;
     return shade ? shade_launch(h, cam, dev, pixels, n, s, true) : RT_OK;
 }

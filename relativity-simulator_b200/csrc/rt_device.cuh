@@ -235,6 +235,21 @@ static __device__ double crossing_fraction(const double* y0, const double* f0, c
     return t;
 }
 
+// Boyer-Lindquist (r, theta, phi) of a Kerr-Schild point, as Cartesian
+// (r sin th cos ph, r sin th sin ph, r cos th): the points the reference's image
+// path hands to its volume tests (boyer_lindquist_from_kerr_schild and
+// spherical_to_cartesian, software_compute_engine.hpp:1063-1066).
+__device__ __forceinline__ void bl_cartesian(const double* x, double a, double* out) {
+    const double r = sqrt(bl_r2<double>(x[0], x[1], x[2], a * a));
+    const double rho = sqrt(fmax(r * r - x[2] * x[2], 0.0));
+    const double th = atan2(rho, x[2]);
+    const double ph = atan2(x[1], x[0]) - atan2(a, r);
+    const double st = sin(th);
+    out[0] = r * st * cos(ph);
+    out[1] = r * st * sin(ph);
+    out[2] = r * cos(th);
+}
+
 // PI30 factor (step_controller.hpp:51-58) from base-2 logs of the errors.
 __device__ __forceinline__ float pi30_factor(float le, float lp, float order_p1) {
     return exp2f(-(0.7f / order_p1) * le + (0.3f / order_p1) * (lp - le));

@@ -79,6 +79,7 @@ enum : uint32_t {
     CI_FATE_SHIFT = 8u,     // bits 8..11: RT_RAY_* class at the ray's end
     CI_INSIDE_3RS = 1u << 12  // last point inside 3 r_s (6 M; multi-source: within 6 m of a source)
 };
+struct ShadeDesc;
 struct ContOut {
     double* cross;    // [3 * kMaxCrossings][stride]: r_k at [3k], phi_k at [3k + 1], g_k at [3k + 2]
     uint32_t* info;   // [stride]
@@ -87,7 +88,15 @@ struct ContOut {
     double* exit;     // Boyer-Lindquist and multi-source tracers, sky on: [3][stride], the
                       // sky-lookup direction at the ray's end (else null)
     double* tail;     // Kerr-Schild tracers, sky on: [stride][TL_COUNT], the ray's end (else null)
+    double* vol;      // hydro model 2 (Kerr-Schild FP64 tracer): [stride][VL_COUNT], the light the
+                      // ray gathered in the Fishbone-Moncrief torus (else null)
+    const ShadeDesc* shade;  // with vol: the torus and the disk profile (device)
 };
+// The torus's light along a ray, gathered by the tracer step by step (every
+// field 0 before the ray's first emitting segment): radiance r, g, b, the
+// throughput left, the redshift of the last segment, and 1 once a segment
+// emitted.
+enum VolField : int { VL_R = 0, VL_G, VL_B, VL_THR, VL_Z, VL_HIT, VL_COUNT };
 // The end of a Kerr-Schild ray's trace as its tracer leaves it for the shading
 // pass, which derives the sky-lookup direction from it in parallel over the rays
 // rather than on the tracer's divergent end path: the last step's end points and
@@ -237,10 +246,16 @@ struct alignas(16) ShadeDesc {
     double weight[33][3];
     double fov;      // the camera's field of view (the sky's level of detail)
     SkyProfile sky;  // the procedural sky, read when sky_on
+    // hydro model 2, the Fishbone-Moncrief torus: the hole (mass, clamped spin,
+    // horizon), l and W_in, the peak enthalpy, the sampled radii, the density
+    // exponent 1 / (gamma - 1), kappa (optical depth per M at peak enthalpy) and
+    // samples per M of chord
+    double fm_m, fm_a, fm_rh, fm_l, fm_w_in, fm_h_max, fm_inner, fm_outer, fm_exponent, fm_kappa, fm_density;
+    uint32_t fm_valid, pad2;
 };
 
 // Build the shading constants of a camera; false if the settings are not
-// supported (hydro model 2, sky_enabled above 1).
+// supported (hydro model above 2, sky_enabled above 1).
 bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d);
 void build_source_shade_desc(const ShadeDesc& base, const float* profile, double mass, double spin, double inner,
                              double outer, ShadeDesc& d);

@@ -775,7 +775,8 @@ rt_status rt_server_set_shading(rt_server* s, const rt_shading* sh) {
     rt_camera_defaults(&probe);
     ShadeDesc d;
     // no sky: the server's epochs record no exit directions
-    if (sh->sky_enabled != 0u || !build_shade_desc(probe, *sh, d) || (s->cfg.record_mask & kShadeMask) != kShadeMask)
+    if (sh->sky_enabled != 0u || sh->hydro_model > 1u || !build_shade_desc(probe, *sh, d) ||
+        (s->cfg.record_mask & kShadeMask) != kShadeMask)
         return RT_ERR_INVALID_ARG;
     if (!s->dev_shade) {
         cudaSetDevice(s->device);

@@ -108,6 +108,19 @@ __global__ void __launch_bounds__(512) shade_kernel(const ShadeDesc* __restrict_
             const uint32_t n_cross = info & CI_COUNT_MASK;
             const uint32_t bodies = cont.body ? cont.body[i] : 0u;  // source of each crossing
             double last_g = 1.0;
+            if (cont.vol) {
+                // hydro model 2: the light the tracer gathered in the torus
+                // (no thin-disk crossings); its redshift is the last segment's
+                const double* V = cont.vol + i * VL_COUNT;
+                if (V[VL_HIT] != 0.0) {
+                    acc[0] = V[VL_R];
+                    acc[1] = V[VL_G];
+                    acc[2] = V[VL_B];
+                    thr = V[VL_THR];
+                    pixels[i].status_flags |= RT_PIXEL_ACCRETION_DISK_HIT;
+                    pixels[i].redshift = static_cast<float>(V[VL_Z]);
+                }
+            }
             for (uint32_t k = 0; k < n_cross && thr > kMinThroughput; ++k) {
                 double sh[4];
                 const double gk = cont.cross[(3 * k + 2) * cont.stride + i];
@@ -201,7 +214,7 @@ double temperature_shape_peak(double exponent, double zero_torque) {
 }  // namespace
 
 bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d) {
-    if (s.hydro_model > 1u || s.sky_enabled > 1u || s.tonemapping_mode > 3u) return false;
+    if (s.hydro_model > 2u || s.sky_enabled > 1u || s.tonemapping_mode > 3u) return false;
     d = ShadeDesc{};
     // spectral table (accretion_disk_model.hpp:52-69)
     const double step = (780.0 - 380.0) / 32.0;
@@ -277,6 +290,24 @@ bool build_shade_desc(const rt_camera& cam, const rt_shading& s, ShadeDesc& d) {
         for (int i = 0; i < 192; ++i) pk = mxd(pk, nt_flux(d, lo * std::pow(ratio, static_cast<double>(i) / 191.0)));
         d.nt_flux_peak = (pk > 1e-300) ? pk : 1.0;
         d.nt_rate_factor = std::pow(mxd(static_cast<double>(s.accretion_rate_scale), 1e-6), 0.25);
+    }
+    // hydro model 2: the Fishbone-Moncrief torus of the camera's hole
+    // (HydroDiskContext::build_torus, hydro_disk_shading.hpp:76-110)
+    if (s.hydro_model == 2u) {
+        const torus::TorusContext c = torus::make_torus(d.mass, a, static_cast<double>(s.torus_inner_radius),
+                                                        static_cast<double>(s.torus_center_radius));
+        d.fm_valid = c.valid ? 1u : 0u;
+        d.fm_m = c.t.m;
+        d.fm_a = c.t.a;
+        d.fm_rh = c.t.rh;
+        d.fm_l = c.t.l;
+        d.fm_w_in = c.t.w_in;
+        d.fm_h_max = c.h_max;
+        d.fm_inner = c.inner_bound;
+        d.fm_outer = c.outer_bound;
+        d.fm_exponent = 1.0 / mxd(static_cast<double>(s.adiabatic_index) - 1.0, 1e-3);
+        d.fm_kappa = static_cast<double>(s.optical_depth_scale) * mxd(static_cast<double>(P[DP_OPACITY_SCALE]), 0.0);
+        d.fm_density = mxd(static_cast<double>(s.sampling_density), 0.1);
     }
     return true;
 }

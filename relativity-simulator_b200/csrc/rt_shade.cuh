@@ -12,6 +12,7 @@
 #include <cstdint>
 
 #include "rt_internal.h"
+#include "rt_torus.cuh"
 
 namespace relsim {
 
@@ -217,6 +218,99 @@ __device__ __noinline__ void disk_radiance(const ShadeDesc& D, double radius_in,
     out[3] = cd(envelope * 0.95 * static_cast<double>(P[DP_OPACITY_SCALE]) *
                     cd(sqrt(fmin(static_cast<double>(flux_mod), 1.0)), 0.15, 1.0),
                 0.0, 0.98);
+}
+
+// ---- hydro model 2: the Fishbone-Moncrief torus ----
+constexpr double kMinThroughputVol = 0.01;  // the reference's loop condition (throughput > 0.01)
+// One step's chord through the torus, from and to Boyer-Lindquist points as
+// Cartesian (r sin th cos ph, r sin th sin ph, r cos th), for a ray of L_z / E
+// = l_over_e: the emission-absorption integral over samples at the chord's
+// midpoints within the bounding sphere, sampling_density per M, at most 128
+// (HydroDiskContext::integrate_segment, hydro_disk_shading.hpp:173-269), added
+// to the ray's gathered light at the throughput left
+// (accumulate_fishbone_moncrief_segment, software_compute_engine.hpp:1117-1144).
+// A ray gathers nothing once its throughput is 0.01 or less (the reference's
+// loop ends there).
+__device__ __noinline__ void fm_segment(const ShadeDesc& D, const double* from, const double* to, double l_over_e,
+                                        double* V) {
+    if (!D.fm_valid) return;
+    const bool seen = V[VL_HIT] != 0.0;
+    if (seen && !(V[VL_THR] > kMinThroughputVol)) return;
+    const double dx = to[0] - from[0], dy = to[1] - from[1], dz = to[2] - from[2];
+    const double len2 = dx * dx + dy * dy + dz * dz;
+    if (len2 < 1e-24) return;
+    const double len = sqrt(len2);
+    const double b = (from[0] * dx + from[1] * dy + from[2] * dz) / len2;
+    const double c = (from[0] * from[0] + from[1] * from[1] + from[2] * from[2] - D.fm_outer * D.fm_outer) / len2;
+    const double disc = b * b - c;
+    if (disc <= 0.0) return;
+    const double root = sqrt(disc);
+    const double t0 = cd(-b - root, 0.0, 1.0), t1 = cd(-b + root, 0.0, 1.0);
+    if (t1 <= t0) return;
+    const double clipped = len * (t1 - t0);
+    const double m = D.fm_m;
+    int count = static_cast<int>(ceil(clipped * D.fm_density / m));
+    count = count < 1 ? 1 : (count > 128 ? 128 : count);
+    const double step = clipped / static_cast<double>(count);
+    const float* P = D.profile;
+    const double span = mxd(D.fm_h_max - 1.0, 1e-12);
+    const double peak_t = static_cast<double>(P[DP_PEAK_T]), floor_t = static_cast<double>(P[DP_FLOOR_T]);
+    const double beaming = static_cast<double>(P[DP_BEAMING]), brightness = static_cast<double>(P[DP_BRIGHTNESS]);
+    const double inv_ref = 1.0 / mxd(static_cast<double>(P[DP_REF_LUMINANCE]), 1e-30);
+    const double sat = static_cast<double>(P[DP_SATURATION]), ts = static_cast<double>(P[DP_TINT_STRENGTH]);
+    const torus::Torus T{D.fm_m, D.fm_a, D.fm_rh, D.fm_l, D.fm_w_in};
+    double rad[3] = {0.0, 0.0, 0.0}, trans = 1.0, wsum = 0.0, zsum = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const double t = t0 + (t1 - t0) * ((static_cast<double>(i) + 0.5) / static_cast<double>(count));
+        const double px = from[0] + t * dx, py = from[1] + t * dy, pz = from[2] + t * dz;
+        const double radius = sqrt(px * px + py * py + pz * pz);
+        if (radius < D.fm_inner || radius > D.fm_outer) continue;
+        const double theta = acos(cd(pz / radius, -1.0, 1.0));
+        const double h = torus::enthalpy(T, radius, theta);
+        if (!(h > 1.0 + 1e-9)) continue;
+        const double ratio = cd((h - 1.0) / span, 0.0, 1.0);
+        const double tau = D.fm_kappa * pow(ratio, D.fm_exponent) * step / m;
+        if (tau < 1e-12) continue;
+        double ut, uphi;
+        torus::four_velocity(T, radius, theta, ut, uphi);
+        if (ut <= 1e-12) continue;
+        // AccretionDiskModel::redshift_factor (accretion_disk_model.hpp:218-221)
+        const double den = ut * (1.0 - (uphi / ut) * l_over_e);
+        const double g = (fabs(den) > 1e-9) ? cd(1.0 / den, 0.05, 4.0) : 1.0;
+        // blackbody colour of the observed temperature, then the disk profile's grading
+        double xyz[3];
+        planck_xyz(D.lambda_um, D.weight, (floor_t + (peak_t - floor_t) * ratio) * g, xyz);
+        const double X = xyz[0] * inv_ref, Y = xyz[1] * inv_ref, Z = xyz[2] * inv_ref;
+        const double gain = brightness * pow(g, beaming);
+        double red = mxd(3.2404542 * X - 1.5371385 * Y - 0.4985314 * Z, 0.0) * gain;
+        double green = mxd(-0.9692660 * X + 1.8760108 * Y + 0.0415560 * Z, 0.0) * gain;
+        double blue = mxd(0.0556434 * X - 0.2040259 * Y + 1.0572252 * Z, 0.0) * gain;
+        const double luma = 0.2126 * red + 0.7152 * green + 0.0722 * blue;
+        red = mxd(0.0, luma + (red - luma) * sat);
+        green = mxd(0.0, luma + (green - luma) * sat);
+        blue = mxd(0.0, luma + (blue - luma) * sat);
+        red *= 1.0 + (static_cast<double>(P[DP_TINT_R]) - 1.0) * ts;
+        green *= 1.0 + (static_cast<double>(P[DP_TINT_G]) - 1.0) * ts;
+        blue *= 1.0 + (static_cast<double>(P[DP_TINT_B]) - 1.0) * ts;
+        const double st = exp(-tau);
+        const double w = trans * (1.0 - st);
+        rad[0] += w * red;
+        rad[1] += w * green;
+        rad[2] += w * blue;
+        wsum += w;
+        zsum += w * g;
+        trans *= st;
+        if (trans < 0.002) break;
+    }
+    const double opacity = 1.0 - trans;
+    if (opacity <= 1e-6) return;
+    const double thr = seen ? V[VL_THR] : 1.0;
+    V[VL_R] += thr * rad[0];
+    V[VL_G] += thr * rad[1];
+    V[VL_B] += thr * rad[2];
+    V[VL_THR] = thr * (1.0 - opacity);
+    V[VL_Z] = (wsum > 1e-30) ? (zsum / wsum) : 1.0;
+    V[VL_HIT] = 1.0;
 }
 
 // ---- translucent-disk continuation ----

@@ -223,7 +223,7 @@ __device__ __forceinline__ void fp64_stages_rolled(const double* __restrict__ y,
 // which rays share its warp.
 // Every form runs 12 warps per SM (168 registers); the pass kernels spill a
 // little there, which measured faster than 8 warps without spills.
-template <int BLOCK, bool MIXED, bool ROLLED, int PASS = PASS_SINGLE, bool CONT = false>
+template <int BLOCK, bool MIXED, bool ROLLED, int PASS = PASS_SINGLE, int CONT = 0>
 __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs args) {
     __shared__ Cold<BLOCK> S;
     __shared__ KStore<ROLLED ? BLOCK : 1> K;
@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                             wind = static_cast<int>(uch[PU_WIND]);
                             has_hist = (uch[PU_MISC] & PM_HAS_HIST) != 0u;
                             can_early = static_cast<int>((uch[PU_MISC] >> PM_EARLY_SHIFT) & 3u) - 1;
-                            if constexpr (CONT) n_cross = (uch[PU_MISC] >> PM_CROSS_SHIFT) & 31u;
+                            if constexpr (CONT != 0) n_cross = (uch[PU_MISC] >> PM_CROSS_SHIFT) & 31u;
                             lnp = __uint_as_float(uch[PU_LNP]);
                             k1_fp32 = false;
                             mode = MODE_STEP;
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
             double xch[6];
 #pragma unroll
             for (int i = 0; i < 6; ++i) xch[i] = y[i];
-            end_ray<CONT>(args, Bp, S, tid, n_cross, RT_RAY_UNFINISHED, flags, acc, rej, wind, 0.0, 0.0, xch);
+            end_ray<(CONT != 0)>(args, Bp, S, tid, n_cross, RT_RAY_UNFINISHED, flags, acc, rej, wind, 0.0, 0.0, xch);
             mode = MODE_IDLE;
             continue;
         }
@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 double xch[6];
 #pragma unroll
                 for (int i = 0; i < 6; ++i) xch[i] = y[i];
-                end_ray<CONT>(args, Bp, S, tid, n_cross, term & 15u, flags, acc, rej, wind, 0.0, 0.0, xch);
+                end_ray<(CONT != 0)>(args, Bp, S, tid, n_cross, term & 15u, flags, acc, rej, wind, 0.0, 0.0, xch);
                 mode = MODE_IDLE;
                 continue;
             }
@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                         finish_ray(Bp, S, tid, RT_RAY_DISK, flags, acc, rej, wind, 0.0, 0.0, rr,
                                    disk_redshift(M, a, rr, S.lz0[tid]), args.out, xch);
                     mode = MODE_IDLE;
-                    if constexpr (CONT) {
+                    if constexpr (CONT != 0) {
                         // translucent disk: record the crossing and go on through it
                         record_crossing(args, Bp, S, tid, n_cross, y5,
                                         wind + branch_winding(y[0], y[1], y5[0], y5[1]));
@@ -689,7 +689,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                 double xch[6];
 #pragma unroll
                 for (int i = 0; i < 6; ++i) xch[i] = y[i];
-                end_ray<CONT>(args, Bp, S, tid, n_cross, RT_RAY_CAPTURED, flags, acc, rej, wind, 0.0, 0.0, xch);
+                end_ray<(CONT != 0)>(args, Bp, S, tid, n_cross, RT_RAY_CAPTURED, flags, acc, rej, wind, 0.0, 0.0, xch);
                 mode = MODE_IDLE;
                 continue;
             }
@@ -789,7 +789,7 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                     xch[12 + i] = y5[i];
                     xch[18 + i] = kA[i];
                 }
-                end_ray<CONT>(args, Bp, S, tid, n_cross, term, flags, acc, rej, wind, target, hh, xch);
+                end_ray<(CONT != 0)>(args, Bp, S, tid, n_cross, term, flags, acc, rej, wind, target, hh, xch);
                 mode = MODE_IDLE;
                 continue;
             }
@@ -819,6 +819,15 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
                     }
                 }
             }
+        }
+        if constexpr (CONT == 2) {
+            // hydro model 2: the step's chord through the Fishbone-Moncrief torus
+            // (software_compute_engine.hpp:1725-1731)
+            double from[3], to[3];
+            bl_cartesian(y, a, from);
+            bl_cartesian(y5, a, to);
+            fm_segment(*args.cont.shade, from, to, S.lz0[tid],
+                       args.cont.vol + (Bp->out_offset + S.local[tid]) * VL_COUNT);
         }
         wind += branch_winding(y[0], y[1], y5[0], y5[1]);
         S.lambda[tid] += hh;
@@ -858,8 +867,9 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) trace_kernel_t(TraceArgs a
     }
 }
 
-// unshaded launches (CONT = false) and shaded ones that follow rays through the
-// translucent disk (CONT = true)
+// unshaded launches (CONT = 0), shaded ones that follow rays through the
+// translucent disk (CONT = 1) and, for hydro model 2, the FP64 tracer that
+// gathers the Fishbone-Moncrief torus's light step by step (CONT = 2)
 template __global__ void trace_kernel_t<64, false, false>(TraceArgs);
 template __global__ void trace_kernel_t<128, false, false>(TraceArgs);
 template __global__ void trace_kernel_t<256, false, false>(TraceArgs);
@@ -871,13 +881,14 @@ template __global__ void trace_kernel_t<64, true, false, PASS_FAR>(TraceArgs);
 template __global__ void trace_kernel_t<128, true, false, PASS_FAR>(TraceArgs);
 template __global__ void trace_kernel_t<64, false, false, PASS_NEAR>(TraceArgs);
 template __global__ void trace_kernel_t<128, false, false, PASS_NEAR>(TraceArgs);
-template __global__ void trace_kernel_t<64, false, false, PASS_SINGLE, true>(TraceArgs);
-template __global__ void trace_kernel_t<128, false, false, PASS_SINGLE, true>(TraceArgs);
-template __global__ void trace_kernel_t<256, false, false, PASS_SINGLE, true>(TraceArgs);
-template __global__ void trace_kernel_t<64, false, true, PASS_SINGLE, true>(TraceArgs);
-template __global__ void trace_kernel_t<128, false, true, PASS_SINGLE, true>(TraceArgs);
-template __global__ void trace_kernel_t<64, true, true, PASS_SINGLE, true>(TraceArgs);
-template __global__ void trace_kernel_t<128, true, true, PASS_SINGLE, true>(TraceArgs);
+template __global__ void trace_kernel_t<64, false, false, PASS_SINGLE, 1>(TraceArgs);
+template __global__ void trace_kernel_t<128, false, false, PASS_SINGLE, 1>(TraceArgs);
+template __global__ void trace_kernel_t<256, false, false, PASS_SINGLE, 1>(TraceArgs);
+template __global__ void trace_kernel_t<64, false, true, PASS_SINGLE, 1>(TraceArgs);
+template __global__ void trace_kernel_t<128, false, true, PASS_SINGLE, 1>(TraceArgs);
+template __global__ void trace_kernel_t<64, true, true, PASS_SINGLE, 1>(TraceArgs);
+template __global__ void trace_kernel_t<128, true, true, PASS_SINGLE, 1>(TraceArgs);
+template __global__ void trace_kernel_t<128, false, false, PASS_SINGLE, 2>(TraceArgs);
 template __global__ void trace_kernel_t<64, true, false, PASS_FAR, true>(TraceArgs);
 template __global__ void trace_kernel_t<128, true, false, PASS_FAR, true>(TraceArgs);
 template __global__ void trace_kernel_t<64, false, false, PASS_NEAR, true>(TraceArgs);
@@ -887,7 +898,7 @@ namespace {
 // Mixed precision always uses the rolled FP64 step (its FP64 steps are a
 // minority; the rolled form keeps the loop small).  Rolled kernels exist for
 // 64- and 128-thread blocks (their stage store is 36 KB of shared memory at 128).
-template <bool CONT>
+template <int CONT>
 const void* kernel_for_t(uint32_t block, bool mixed, bool rolled) {
     if (mixed) {
         return (block == 64) ? reinterpret_cast<const void*>(&trace_kernel_t<64, true, true, PASS_SINGLE, CONT>)
@@ -904,8 +915,9 @@ const void* kernel_for_t(uint32_t block, bool mixed, bool rolled) {
     }
 }
 
-const void* kernel_for(uint32_t block, bool mixed, bool rolled, bool cont = false) {
-    return cont ? kernel_for_t<true>(block, mixed, rolled) : kernel_for_t<false>(block, mixed, rolled);
+const void* kernel_for(uint32_t block, bool mixed, bool rolled, int cont = 0) {
+    if (cont == 2) return reinterpret_cast<const void*>(&trace_kernel_t<128, false, false, PASS_SINGLE, 2>);
+    return (cont == 1) ? kernel_for_t<1>(block, mixed, rolled) : kernel_for_t<0>(block, mixed, rolled);
 }
 }  // namespace
 
@@ -1139,8 +1151,10 @@ int enqueue_two_pass(const TraceArgs& base, const TwoPassBuffers& buf, int sm_co
 
 void launch_trace(const TraceArgs& args, uint32_t grid, uint32_t block, bool mixed, bool rolled, void* stream) {
     void* params[] = {const_cast<TraceArgs*>(&args)};
-    block = kernel_block(block, mixed, rolled);
-    cudaLaunchKernel(kernel_for(block, mixed, rolled, args.cont.cross != nullptr), dim3(grid), dim3(block), params, 0,
+    // hydro model 2: the FP64 straight-line tracer in 128-thread blocks
+    const int cont = args.cont.vol ? 2 : (args.cont.cross ? 1 : 0);
+    block = (cont == 2) ? 128u : kernel_block(block, mixed, rolled);
+    cudaLaunchKernel(kernel_for(block, mixed, rolled, cont), dim3(grid), dim3(block), params, 0,
                      static_cast<cudaStream_t>(stream));
 }
 

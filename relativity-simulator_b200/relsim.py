@@ -72,7 +72,10 @@ class Shading(ctypes.Structure):
     _fields_ = [("disk", DiskProfile), ("disk_temperature_scale_k", _d), ("disk_temperature_floor_k", _d),
                 ("disk_color_saturation", _d), ("disk_doppler_beaming_exponent", _d), ("time", _d),
                 ("camera_exposure", _d), ("tonemapping_mode", _u32), ("hydro_model", _u32),
-                ("accretion_rate_scale", ctypes.c_float), ("sky_enabled", _u32), ("sky", SkyProfile)]
+                ("accretion_rate_scale", ctypes.c_float), ("sky_enabled", _u32), ("sky", SkyProfile),
+                ("torus_inner_radius", ctypes.c_float), ("torus_center_radius", ctypes.c_float),
+                ("adiabatic_index", ctypes.c_float), ("optical_depth_scale", ctypes.c_float),
+                ("sampling_density", ctypes.c_float), ("reserved_torus", ctypes.c_float)]
 
 
 class PixelOut(ctypes.Structure):

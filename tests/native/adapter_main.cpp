@@ -28,6 +28,8 @@ struct DiskProfile {  // GpuDiskProfile's 32 floats (gpu_types.hpp:42-75)
 struct HydroDisk {
     uint32_t model = 0;
     float accretion_rate_scale = 1.0f;
+    float torus_inner_radius = 6.0f, torus_center_radius = 12.0f, adiabatic_index = 1.3333334f;
+    float optical_depth_scale = 0.35f, sampling_density = 2.0f;
 };
 struct Push {  // the fields of GpuCameraPushConstants the tracer reads (gpu_types.hpp:966-1109)
     std::array<double, 4> observer_position{}, tetrad_e1{}, tetrad_e2{}, tetrad_e3{};

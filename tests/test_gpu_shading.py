@@ -230,7 +230,7 @@ def test_unsupported_settings_rejected(tracer):
     with pytest.raises(relsim.RelsimError):
         tracer.set_shading(relsim.shading(sky_enabled=2))
     with pytest.raises(relsim.RelsimError):
-        tracer.set_shading(relsim.shading(hydro_model=2))
+        tracer.set_shading(relsim.shading(hydro_model=3))
     with pytest.raises(relsim.RelsimError):
         tracer.set_shading(relsim.shading(tonemapping_mode=4))
 
@@ -403,3 +403,85 @@ def test_server_refuses_the_sky():
     with relsim.Server(0, relsim.server_config(1 << 26)) as srv:
         with pytest.raises(relsim.RelsimError):
             srv.set_shading(relsim.shading(sky_enabled=1))
+
+
+def _resolved_profile(sh):
+    prof_in = np.frombuffer(bytes(sh.disk), np.float32).copy()
+    over = np.array([sh.disk_temperature_scale_k, sh.disk_temperature_floor_k, sh.disk_color_saturation,
+                     sh.disk_doppler_beaming_exponent])
+    out = np.zeros(32, np.float32)
+    O.lib().orc_resolve_profile(O._p(prof_in), O._p(over), O._p(out))
+    return out
+
+
+@pytest.mark.parametrize("sky", [0, 1])
+def test_torus_pixels_match_oracle(tracer, sky_sampler, sky):
+    """Hydro model 2, the Fishbone-Moncrief torus: the FP64 Kerr-Schild tracer
+    gathers each step's chord through the torus (no thin disk, no early
+    capture), against the oracle's trace that does the same
+    (orc_trace_volume, its torus pinned to the reference's HydroDiskContext by
+    tests/test_oracle_torus.py), composed with the sky behind it when on.  A
+    mixed-precision camera traces the same (hydro model 2 uses the FP64
+    tracer at the camera's tolerances).  Bar: sRGB within 1e-6 for 99 % of
+    the rays away from the shadow's edge and 1e-4 for all (a chord whose
+    length rounds to another sample count differs a little more)."""
+    kw = dict(spin=0.6, r_obs=60.0, incl_deg=75.0, fov_deg=50.0, width=40, height=40)
+    cam = relsim.make_camera(**kw)
+    sh = relsim.shading(hydro_model=2, tonemapping_mode=1, sky_enabled=sky, torus_inner_radius=6.0,
+                        torus_center_radius=10.0, time=0.5)
+    out = _shaded(tracer, sh, lambda: tracer.dispatch(cam, fields=["status", "r"], pixels=True))
+    mixed = relsim.make_camera(precision=relsim.PRECISION_MIXED, **kw)
+    again = _shaded(tracer, sh, lambda: tracer.dispatch(mixed, fields=["status", "r"], pixels=True))
+    np.testing.assert_array_equal(again["pixels"], out["pixels"])
+    ocam = relsim.camera_dict(cam)
+    ocam["disk_outer_radius"] = 0.0
+    ocam["early_capture"] = 0
+    m, a = _camera_constants(cam)[:2]
+    fm = O.fm_context(m, a, (sh.torus_inner_radius, sh.torus_center_radius, sh.adiabatic_index,
+                             sh.optical_depth_scale, sh.sampling_density), _resolved_profile(sh))
+    ref, cont, vol = O.trace_volume(ocam, fm)
+    np.testing.assert_array_equal(out["status"], ref["status"])
+    prof = (ctypes.c_uint8 * 1808).from_buffer_copy(bytes(sh.sky))
+    want = np.full((cont.size, 3), np.nan, np.float32)
+    px = np.zeros(3, np.float32)
+    rgb = np.zeros(3, np.float32)
+    for i in range(cont.size):
+        seen = vol[i, 5] != 0.0
+        acc = vol[i, :3].copy() if seen else np.zeros(3)
+        thr = vol[i, 3] if seen else 1.0
+        if sky and thr > 0.01 and cont["fate"][i] == O.ESCAPED:
+            e = cont["exit_dir"][i]
+            sky_sampler(ctypes.addressof(prof), float(e[0]), float(e[1]), float(e[2]), cam.field_of_view_rad, sh.time,
+                        rgb.ctypes.data)
+            acc = acc + thr * rgb.astype(np.float64)
+        O.lib().orc_tonemap(O._p(acc), sh.tonemapping_mode, sh.camera_exposure, O._p(px))
+        want[i] = px
+    want[np.abs(ref["db_shadow"]) < 1e-3] = np.nan
+    got = _rgb(out["pixels"])
+    ok = ~np.isnan(want).any(1)
+    err = np.abs(got - want).max(1)[ok]
+    seen = vol[:, 5] != 0.0
+    print(f"torus (sky {sky}): {seen.sum()} rays through the torus, sRGB within 1e-6 {np.mean(err < 1e-6):.4f}, "
+          f"max {err.max():.2e}")
+    assert seen.sum() > 200 and np.mean(err < 1e-6) >= 0.99 and err.max() < 1e-4
+    flags = out["pixels"]["status_flags"]
+    assert ((flags & relsim.PIXEL_ACCRETION_DISK_HIT) != 0).tolist() == seen.tolist()
+    z = out["pixels"]["redshift"][seen]
+    assert np.allclose(z, vol[seen, 4].astype(np.float32), rtol=1e-5)
+
+
+def test_torus_refused_off_the_kerr_schild_single_hole_path(tracer):
+    sh = relsim.shading(hydro_model=2)
+    bl = relsim.make_camera(width=8, height=8, metric_form=relsim.METRIC_BOYER_LINDQUIST, charge=0.2)
+    tracer.set_shading(sh)
+    try:
+        with pytest.raises(relsim.RelsimError):
+            tracer.dispatch(bl, fields=["status"], pixels=True)
+        with pytest.raises(relsim.RelsimError):
+            tracer.dispatch_multi(relsim.make_camera(width=8, height=8),
+                                  [relsim.make_source((20.0, 0.0, 0.0))], fields=["status"], pixels=True)
+    finally:
+        tracer.set_shading(None)
+    with relsim.Server(0, relsim.server_config(1 << 26)) as srv:
+        with pytest.raises(relsim.RelsimError):
+            srv.set_shading(sh)
