@@ -182,7 +182,8 @@ typedef struct rt_shading {
     double time;                          /* animation time of the disk pattern and the sky */
     double camera_exposure;               /* EV */
     uint32_t tonemapping_mode;            /* 0 clamp, 1 ACES fit, 2 log luminance, 3 extended Reinhard */
-    uint32_t hydro_model;                 /* hydro_disk.model: 0 procedural profile, 1 Novikov-Thorne flux */
+    uint32_t hydro_model;                 /* hydro_disk.model: 0 procedural profile, 1 Novikov-Thorne flux,
+                                             2 Fishbone-Moncrief torus */
     float accretion_rate_scale;           /* hydro_disk.accretion_rate_scale (Novikov-Thorne) */
     uint32_t sky_enabled;                 /* 1: the procedural sky behind escaped rays (sky.enabled
                                              switches it off as well); the reference's image
@@ -362,8 +363,14 @@ rt_status rt_set_launch_config(rt_handle* h, const rt_launch_config* cfg);
 
 /* Shade the pixels of later rt_dispatch, rt_dispatch_tile, rt_dispatch_device
  * and rt_dispatch_multi* calls on this handle; NULL turns shading off
- * (r = g = b = 0, a = 1, the default).  RT_ERR_INVALID_ARG for hydro_model 2
- * (the Fishbone-Moncrief torus) or sky_enabled > 1.  rt_shading_defaults
+ * (r = g = b = 0, a = 1, the default).  RT_ERR_INVALID_ARG for hydro_model
+ * above 2, sky_enabled above 1 or tonemapping_mode above 3.  Hydro model 2,
+ * the Fishbone-Moncrief torus, shades single-hole Kerr-Schild cameras only:
+ * they are traced by the FP64 tracer at the camera's tolerances with no thin
+ * disk and no early capture, gathering each step's chord through the torus
+ * (software_compute_engine.hpp:1725-1731), so their records describe that
+ * trace; Boyer-Lindquist and multi-source dispatches then return
+ * RT_ERR_INVALID_ARG, as rt_server_set_shading does.  rt_shading_defaults
  * gives the reference's defaults for the disk and the tonemap, GpuSkyProfile's
  * defaults in sky, and sky_enabled = 0 (black behind the disk; set it to 1 for
  * the reference's sky). */

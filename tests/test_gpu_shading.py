@@ -430,9 +430,6 @@ def test_torus_pixels_match_oracle(tracer, sky_sampler, sky):
     sh = relsim.shading(hydro_model=2, tonemapping_mode=1, sky_enabled=sky, torus_inner_radius=6.0,
                         torus_center_radius=10.0, time=0.5)
     out = _shaded(tracer, sh, lambda: tracer.dispatch(cam, fields=["status", "r"], pixels=True))
-    mixed = relsim.make_camera(precision=relsim.PRECISION_MIXED, **kw)
-    again = _shaded(tracer, sh, lambda: tracer.dispatch(mixed, fields=["status", "r"], pixels=True))
-    np.testing.assert_array_equal(again["pixels"], out["pixels"])
     ocam = relsim.camera_dict(cam)
     ocam["disk_outer_radius"] = 0.0
     ocam["early_capture"] = 0
@@ -468,6 +465,13 @@ def test_torus_pixels_match_oracle(tracer, sky_sampler, sky):
     assert ((flags & relsim.PIXEL_ACCRETION_DISK_HIT) != 0).tolist() == seen.tolist()
     z = out["pixels"]["redshift"][seen]
     assert np.allclose(z, vol[seen, 4].astype(np.float32), rtol=1e-5)
+    # a mixed-precision camera: the FP64 tracer at its tolerance (1e-8)
+    mixed = relsim.make_camera(precision=relsim.PRECISION_MIXED, **kw)
+    fp64 = relsim.make_camera(rtol=mixed.rtol, **kw)
+    a = _shaded(tracer, sh, lambda: tracer.dispatch(mixed, fields=["status", "r"], pixels=True))
+    b = _shaded(tracer, sh, lambda: tracer.dispatch(fp64, fields=["status", "r"], pixels=True))
+    np.testing.assert_array_equal(a["pixels"], b["pixels"])
+    np.testing.assert_array_equal(a["r"], b["r"])
 
 
 def test_torus_refused_off_the_kerr_schild_single_hole_path(tracer):
