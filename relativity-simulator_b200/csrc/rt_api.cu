@@ -452,8 +452,11 @@ int band_copy_hook(void* vctx, uint64_t begin, uint64_t count, void* stream) {
 }
 
 // Bands of a host dispatch on the two-pass tracer: each band's copies overlap
-// the next band's trace (1 M rays and up).
-constexpr uint32_t kCopyBands = 8;
+// the next band's trace (1 M rays and up).  Four: with every ray followed
+// through the disk and the sky shaded, each band's pass tails cost more than
+// the longer exposed copy of the last band (measured at 2048^2: 2 / 4 / 8 / 16
+// bands 75.7 / 75.2 / 80.9 / 81.3 ms an image).
+constexpr uint32_t kCopyBands = 4;
 constexpr uint64_t kBandedMinRays = uint64_t{1} << 20;
 
 // One host-buffer dispatch over a window (dispatch_and_readback semantics).
