@@ -513,8 +513,17 @@ static void exit_direction(double m, double a, double q2, const double* y, doubl
     }
 }
 
+/* spherical_to_cartesian (software_compute_engine.hpp:1063-1066) */
+static void sph_cartesian(const double* y, double* out)
+{
+    const double st = sin(y[1]);
+    out[0] = y[0] * st * cos(y[2]);
+    out[1] = y[0] * st * sin(y[2]);
+    out[2] = y[0] * cos(y[1]);
+}
+
 static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, uint32_t py, orc_ray* out,
-                      orc_cont* cont)
+                      orc_cont* cont, const orc_fm* fm, double* vol)
 {
     const double m = c->m, a = c->a, q2 = c->q2;
     double y[NB];
@@ -663,6 +672,14 @@ static void trace_one(const orc_camera* cam, const bl_consts* c, uint32_t px, ui
         }
         dH = max_d(dH, project_null(c, yn, cam->projection_tol));
         reflect_pole(yn, k[6]);
+        if (fm) { /* hydro model 2: the step's chord through the torus, L / E taken as
+                   * u^phi r^2 sin^2(theta) at the step's end (:1529-1537) */
+            double from[3], to[3];
+            sph_cartesian(y, from);
+            sph_cartesian(yn, to);
+            const double st = sin(yn[1]);
+            orc_fm_accumulate(fm, from, to, yn[6] * (yn[0] * yn[0] * st * st), vol);
+        }
         lambda += h;
         memcpy(y, yn, sizeof yn);
         memcpy(k[0], k[6], sizeof(double) * NB);
@@ -727,6 +744,8 @@ typedef struct {
     uint64_t first, count;
     orc_ray* out;
     orc_cont* cont;
+    const orc_fm* fm;
+    double* vol;
     atomic_ullong next;
 } work_t;
 
@@ -741,29 +760,38 @@ static void* worker(void* arg)
         for (uint64_t i = b; i < e; ++i) {
             const uint64_t pix = w->idx ? w->idx[i] : w->first + i;
             trace_one(w->cam, w->c, (uint32_t)(pix % w->cam->screen_width), (uint32_t)(pix / w->cam->screen_width),
-                      &w->out[i], w->cont ? &w->cont[i] : NULL);
+                      &w->out[i], w->cont ? &w->cont[i] : NULL, w->fm, w->vol ? w->vol + 6 * i : NULL);
         }
     }
     return NULL;
 }
 
 static void bl_trace_range(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first,
-                           uint64_t count, orc_ray* out, orc_cont* cont, int threads);
+                           uint64_t count, orc_ray* out, orc_cont* cont, const orc_fm* fm, double* vol,
+                           int threads);
 
 void orc_bl_trace(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first, uint64_t count,
                   orc_ray* out, int threads)
 {
-    bl_trace_range(cam, charge, pixel_index, first, count, out, NULL, threads);
+    bl_trace_range(cam, charge, pixel_index, first, count, out, NULL, NULL, NULL, threads);
 }
 
 void orc_bl_trace_cont(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first,
                        uint64_t count, orc_ray* out, orc_cont* cont, int threads)
 {
-    bl_trace_range(cam, charge, pixel_index, first, count, out, cont, threads);
+    bl_trace_range(cam, charge, pixel_index, first, count, out, cont, NULL, NULL, threads);
+}
+
+void orc_bl_trace_volume(const orc_camera* cam, double charge, const orc_fm* fm, const uint64_t* pixel_index,
+                         uint64_t first, uint64_t count, orc_ray* out, orc_cont* cont, double* vol, int threads)
+{
+    memset(vol, 0, sizeof(double) * 6 * count);
+    bl_trace_range(cam, charge, pixel_index, first, count, out, cont, fm, vol, threads);
 }
 
 static void bl_trace_range(const orc_camera* cam, double charge, const uint64_t* pixel_index, uint64_t first,
-                           uint64_t count, orc_ray* out, orc_cont* cont, int threads)
+                           uint64_t count, orc_ray* out, orc_cont* cont, const orc_fm* fm, double* vol,
+                           int threads)
 {
     bl_consts c;
     bl_camera_consts(cam, charge, &c);
@@ -777,6 +805,8 @@ static void bl_trace_range(const orc_camera* cam, double charge, const uint64_t*
     w.count = count;
     w.out = out;
     w.cont = cont;
+    w.fm = fm;
+    w.vol = vol;
     atomic_init(&w.next, 0);
     if (threads == 1) {
         worker(&w);

@@ -140,6 +140,11 @@ void orc_fm_accumulate(const orc_fm* t, const double from[3], const double to[3]
  * library does for hydro model 2). */
 void orc_trace_volume(const orc_camera* cam, const orc_fm* fm, const uint64_t* pixel_index, uint64_t first,
                       uint64_t count, orc_ray* out, orc_cont* cont, double* vol, int threads);
+/* The same for the Boyer-Lindquist Kerr-Newman trace (chords between the
+ * steps' Boyer-Lindquist points; L / E as u^phi r^2 sin^2 theta at each step's
+ * end, as the reference's metric-type path takes it). */
+void orc_bl_trace_volume(const orc_camera* cam, double charge, const orc_fm* fm, const uint64_t* pixel_index,
+                         uint64_t first, uint64_t count, orc_ray* out, orc_cont* cont, double* vol, int threads);
 
 /* --- single-function checks (pinned against the reference) --- */
 void orc_ks_field(const double x[3], double mass, double spin, double* r, double* h, double k[3]);

@@ -175,6 +175,7 @@ def lib() -> ctypes.CDLL:
         L.orc_fm_segment.argtypes = [v, v, v, d, v]
         L.orc_fm_accumulate.argtypes = [v, v, v, d, v]
         L.orc_trace_volume.argtypes = [v, v, v, ctypes.c_uint64, ctypes.c_uint64, v, v, v, ctypes.c_int]
+        L.orc_bl_trace_volume.argtypes = [v, d, v, v, ctypes.c_uint64, ctypes.c_uint64, v, v, v, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -398,4 +399,18 @@ def trace_volume(cam: dict, fm: np.ndarray, pixels: np.ndarray | None = None,
     cont = np.zeros(n, dtype=CONT_DTYPE)
     vol = np.zeros((n, 6))
     lib().orc_trace_volume(_p(c), _p(fm), None if idx is None else _p(idx), 0, n, _p(out), _p(cont), _p(vol), threads)
+    return out, cont, vol
+
+
+def bl_trace_volume(cam: dict, charge: float, fm: np.ndarray, pixels: np.ndarray | None = None,
+                    threads: int = 0) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Boyer-Lindquist trace with the torus (as trace_volume)."""
+    c = to_camera(cam)
+    idx = None if pixels is None else np.ascontiguousarray(pixels, dtype=np.uint64)
+    n = int(cam["screen_width"]) * int(cam["screen_height"]) if idx is None else idx.size
+    out = np.zeros(n, dtype=RAY_DTYPE)
+    cont = np.zeros(n, dtype=CONT_DTYPE)
+    vol = np.zeros((n, 6))
+    lib().orc_bl_trace_volume(_p(c), charge, _p(fm), None if idx is None else _p(idx), 0, n, _p(out), _p(cont),
+                              _p(vol), threads)
     return out, cont, vol

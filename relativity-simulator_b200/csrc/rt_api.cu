@@ -334,9 +334,9 @@ rt_status shade_prepare(rt_handle* h, const rt_camera* cam, cudaStream_t s) {
 // the trace to the shading pass (tail, `kerr_schild`).
 rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false, bool kerr_schild = false,
                              cudaStream_t s = nullptr) {
-    // hydro model 2: the Kerr-Schild FP64 tracer gathers the torus's light into
+    // hydro model 2: the single-hole tracers gather the torus's light into
     // per-ray records, zeroed here
-    const bool volume = kerr_schild && h->shading.hydro_model == 2u;
+    const bool volume = !bodies && h->shading.hydro_model == 2u;
     if (volume) {
         rt_status vs = ensure(h, h->cont_vol, sizeof(double) * VL_COUNT * n);
         if (vs != RT_OK) return vs;
@@ -364,7 +364,7 @@ rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false, bool k
 // Hydro model 2 traces the camera as the reference's image path does with the
 // torus: no thin disk, the FP64 tracer at the camera's tolerances, and no
 // early capture (a ray certain to be captured may still cross the torus on its
-// way in).  Boyer-Lindquist cameras are refused.
+// way in).  Multi-source scenes are refused.
 bool volume_shading(const rt_handle* h, bool pixels) { return h->shade_on && pixels && h->shading.hydro_model == 2u; }
 rt_camera volume_camera(const rt_camera& cam) {
     rt_camera c = cam;
@@ -721,7 +721,7 @@ rt_status ms_dispatch_window(rt_handle* h, const rt_camera* cam, const rt_source
     rt_status st;
     ContinuationScope cont_scope{h};
     if (volume_shading(h, out.pixels != nullptr))
-        return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades single-hole Kerr-Schild cameras only");
+        return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades single-hole cameras only");
     if (shade && (st = ms_shade_prepare(h, cam, sources, n_sources, s)) != RT_OK) return st;
     if (shade && (st = begin_continuation(h, n, true)) != RT_OK) return st;
     if ((st = ms_launch(h, cam, sources, n_sources, row0, nrows, out, s)) != RT_OK) return st;
@@ -1043,7 +1043,6 @@ rt_status rt_dispatch(rt_handle* h, const rt_camera* cam, rt_pixel_out* pixels, 
     if (nrows == 0) return fail(h, RT_ERR_INVALID_ARG, "empty row window");
     RT_CUDA(h, cudaSetDevice(h->device));
     if (volume_shading(h, pixels != nullptr)) {
-        if (is_bl(cam)) return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades Kerr-Schild cameras only");
         const rt_camera vc = volume_camera(*cam);
         return dispatch_window(h, &vc, 0, vc.screen_width, row0, nrows, pixels, rays, capacity, cancel);
     }
@@ -1063,7 +1062,6 @@ rt_status rt_dispatch_tile(rt_handle* h, const rt_camera* cam, rt_pixel_out* pix
     const uint32_t hgt = std::min(cam->tile_extent_y, cam->screen_height - cam->tile_origin_y);
     RT_CUDA(h, cudaSetDevice(h->device));
     if (volume_shading(h, pixels != nullptr)) {
-        if (is_bl(cam)) return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades Kerr-Schild cameras only");
         const rt_camera vc = volume_camera(*cam);
         return dispatch_window(h, &vc, vc.tile_origin_x, w, vc.tile_origin_y, hgt, pixels, rays, capacity, nullptr);
     }
@@ -1085,7 +1083,6 @@ rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* p
     RT_CUDA(h, cudaSetDevice(h->device));
     rt_camera vc;
     if (volume_shading(h, pixels != nullptr)) {
-        if (is_bl(cam)) return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades Kerr-Schild cameras only");
         vc = volume_camera(*cam);
         cam = &vc;
     }
@@ -1098,7 +1095,7 @@ rt_status rt_dispatch_device(rt_handle* h, const rt_camera* cam, rt_pixel_out* p
         // shaded: the shading constants go up before the trace, which follows each
         // ray through the translucent disk
         if (shade && (st = shade_prepare(h, cam, s)) != RT_OK) return st;
-        if (shade && (st = begin_continuation(h, n)) != RT_OK) return st;
+        if (shade && (st = begin_continuation(h, n, false, false, s)) != RT_OK) return st;
         if ((st = bl_launch(h, cam, 0, cam->screen_width, row0, nrows, 0, OutPtrs{pixels, dev}, s)) != RT_OK) return st;
         return shade ? shade_launch(h, cam, dev, pixels, n, s, true) : RT_OK;
     }

@@ -425,7 +425,9 @@ __device__ __noinline__ void bl_finish(const BlDesc* __restrict__ Bp, BlCold<BLO
     }
 }
 
-template <int BLOCK>
+// VOL: hydro model 2, each accepted step's chord through the Fishbone-Moncrief
+// torus gathered into the ray's record (args.cont.vol)
+template <int BLOCK, bool VOL = false>
 __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs args) {
     __shared__ BlCold<BLOCK> S;
     const unsigned FULL = 0xffffffffu;
@@ -663,6 +665,15 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
         }
         S.dH[tid] = fmax(S.dH[tid], bl_project(B, y5));
         bl_reflect(y5, k7);
+        if constexpr (VOL) {
+            // the step's chord through the torus, L / E taken as u^phi r^2 sin^2 theta
+            // at the step's end (software_compute_engine.hpp:1529-1537)
+            const double s0 = sin(y[1]), s1 = sin(y5[1]);
+            const double from[3] = {y[0] * s0 * cos(y[2]), y[0] * s0 * sin(y[2]), y[0] * cos(y[1])};
+            const double to[3] = {y5[0] * s1 * cos(y5[2]), y5[0] * s1 * sin(y5[2]), y5[0] * cos(y5[1])};
+            fm_segment(*args.cont.shade, from, to, y5[6] * (y5[0] * y5[0] * s1 * s1),
+                       args.cont.vol + (B.out_offset + S.local[tid]) * VL_COUNT);
+        }
         S.lambda[tid] += hh;
 #pragma unroll
         for (int i = 0; i < NB; ++i) {
@@ -693,13 +704,14 @@ __global__ void __launch_bounds__(BLOCK, 384 / BLOCK) bl_trace_kernel(BlArgs arg
     }
 }
 
-template __global__ void bl_trace_kernel<128>(BlArgs);
+template __global__ void bl_trace_kernel<128, false>(BlArgs);
+template __global__ void bl_trace_kernel<128, true>(BlArgs);
 
 }  // namespace
 
 uint32_t bl_trace_grid(int sm_count) {
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bl_trace_kernel<128>, 128, 0) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bl_trace_kernel<128, false>, 128, 0) != cudaSuccess) {
         cudaGetLastError();
         occ = 1;
     }
@@ -707,7 +719,10 @@ uint32_t bl_trace_grid(int sm_count) {
 }
 
 void launch_bl_trace(const BlArgs& args, uint32_t grid, void* stream) {
-    bl_trace_kernel<128><<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(args);
+    if (args.cont.vol)
+        bl_trace_kernel<128, true><<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(args);
+    else
+        bl_trace_kernel<128, false><<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(args);
 }
 
 }  // namespace relsim
