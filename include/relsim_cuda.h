@@ -365,11 +365,11 @@ rt_status rt_set_launch_config(rt_handle* h, const rt_launch_config* cfg);
  * and rt_dispatch_multi* calls on this handle; NULL turns shading off
  * (r = g = b = 0, a = 1, the default).  RT_ERR_INVALID_ARG for hydro_model
  * above 2, sky_enabled above 1 or tonemapping_mode above 3.  Hydro model 2,
- * the Fishbone-Moncrief torus, shades single-hole Kerr-Schild cameras only:
- * they are traced by the FP64 tracer at the camera's tolerances with no thin
- * disk and no early capture, gathering each step's chord through the torus
- * (software_compute_engine.hpp:1725-1731), so their records describe that
- * trace; Boyer-Lindquist and multi-source dispatches then return
+ * the Fishbone-Moncrief torus, shades single-hole cameras: they are traced by
+ * an FP64 tracer at the camera's tolerances with no thin disk and no early
+ * capture, gathering each step's chord through the torus
+ * (software_compute_engine.hpp:1529-1537, 1725-1731), so their records
+ * describe that trace; multi-source dispatches then return
  * RT_ERR_INVALID_ARG, as rt_server_set_shading does.  rt_shading_defaults
  * gives the reference's defaults for the disk and the tonemap, GpuSkyProfile's
  * defaults in sky, and sky_enabled = 0 (black behind the disk; set it to 1 for
