@@ -1019,11 +1019,14 @@ RT_SKY_HD_NOINLINE double grid(const V3& dir, const SkyProfile& s, double fov, d
 // The sky colour in direction (x, y, z) for a camera of field of view `fov`
 // (radians) at time `time` (SkyboxRenderer::sample_sky, :1674-1722, with the
 // profile's time replaced by the scene's), for the threads with `active` set;
-// `between()` runs after each enabled layer on every thread, active or not (a
+// `between(layer)` runs after each enabled layer on every thread, active or not (a
 // block barrier in the device shading pass, so that the warps of a block run
 // one layer's code at a time and share the instruction cache; nothing on the
 // host).  The layers follow the profile, so every thread calls between() the
 // same number of times.
+// The layers in their order, as between() is told which one ended.
+enum Layer : int { L_NEBULAE = 0, L_DUST, L_GALAXIES, L_CLUSTERS, L_QUASARS, L_PULSARS, L_REMNANTS, L_STARS };
+
 template <class Between>
 RT_SKY_HD void sample_phased(const SkyProfile& s, double x, double y, double z, double fov, double time, bool active,
                              float* out, Between&& between) {
@@ -1046,35 +1049,35 @@ RT_SKY_HD void sample_phased(const SkyProfile& s, double x, double y, double z, 
     // the layers that move read the scene's time in place of the profile's
     if (s.nebula_enabled) {
         if (active) nebulae(d, s, zoom, acc);
-        between();
+        between(L_NEBULAE);
     }
     if (s.dust_enabled) {
         if (active) dust(d, s, acc);
-        between();
+        between(L_DUST);
     }
     if (s.galaxies_enabled) {
         if (active) galaxies(d, s, acc);
-        between();
+        between(L_GALAXIES);
     }
     if (s.clusters_enabled) {
         if (active) clusters(d, s, fov, acc);
-        between();
+        between(L_CLUSTERS);
     }
     if (s.quasar_enabled) {
         if (active) quasars(d, s, acc);
-        between();
+        between(L_QUASARS);
     }
     if (s.pulsar_enabled) {
         if (active) pulsars(d, s, time, acc);
-        between();
+        between(L_PULSARS);
     }
     if (s.snr_enabled) {
         if (active) remnants(d, s, acc);
-        between();
+        between(L_REMNANTS);
     }
     if (s.stars_enabled) {
         if (active) stars(d, s, fov, time, acc);
-        between();
+        between(L_STARS);
     }
     if (!active) return;
     const double k = mx(s.master_intensity, 0.0);
@@ -1095,7 +1098,7 @@ RT_SKY_HD void sample_phased(const SkyProfile& s, double x, double y, double z, 
 
 // The sky colour of one direction (sample_phased for a lone thread).
 RT_SKY_HD_NOINLINE void sample(const SkyProfile& s, double x, double y, double z, double fov, double time, float* out) {
-    sample_phased(s, x, y, z, fov, time, true, out, [] {});
+    sample_phased(s, x, y, z, fov, time, true, out, [](int) {});
 }
 
 }  // namespace sky
