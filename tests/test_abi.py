@@ -98,7 +98,7 @@ def test_server_config_defaults_and_no_device():
 
 def test_host_only_entry_points():
     L = relsim.lib()
-    assert L.rt_abi_version() == 4
+    assert L.rt_abi_version() == 5
     c = relsim.Camera()
     L.rt_camera_defaults(ctypes.byref(c))
     assert c.screen_width == 2048 and c.metric_spin == 0.94 and c.rtol == 1e-10 and c.mixed_critical_band == 0.0
