@@ -65,7 +65,7 @@ BL_FLOP_PER_ATTEMPT = 3542.0
 MIXED_TWO_PASS_LAUNCHES = 2 * 4 + 1
 BL_CAMERA = dict(spin=0.9, charge=0.3, r_obs=50.0, incl_deg=75.0, fov_deg=30.0)
 BL_H2D_BYTES_PER_IMAGE = 352  # the Boyer-Lindquist camera descriptor (sizeof BlDesc)
-SHADE_H2D_BYTES = 3152  # the shading pass's per-camera constants with the sky profile (sizeof ShadeDesc)
+SHADE_H2D_BYTES = 3248  # the shading pass's per-camera constants with the sky profile and torus (sizeof ShadeDesc)
 # what the e2e pixels hold: the reference's CPU dispatch shades every pixel the same way
 # (its push-constant defaults have the procedural sky on)
 PIXELS_NOTE = ("shaded: translucent disk (colour and opacity at every crossing), the default procedural sky "

@@ -121,3 +121,23 @@ def test_no_device_is_reported_not_hidden():
     assert relsim.lib().rt_is_platform_supported() == 0
     with pytest.raises(relsim.RelsimError):
         relsim.Tracer(0)
+
+
+def test_bench_descriptor_byte_counts(tmp_path):
+    """bench.py's host-to-device bytes per image are the descriptors' sizes."""
+    import shutil
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not found")
+    prog = tmp_path / "sz.cu"
+    prog.write_text('#include <cstdio>\n#include "rt_internal.h"\nint main(){ std::printf("%zu %zu %zu\\n", '
+                    'sizeof(relsim::BundleDesc), sizeof(relsim::BlDesc), sizeof(relsim::ShadeDesc)); }\n')
+    exe = tmp_path / "sz"
+    subprocess.run([nvcc, "-std=c++17", "-Wno-deprecated-gpu-targets", "-I", os.path.join(ROOT, "include"), "-I",
+                    os.path.join(ROOT, "relativity-simulator_b200", "csrc"), str(prog), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    assert got == [bench.H2D_BYTES_PER_IMAGE, bench.BL_H2D_BYTES_PER_IMAGE, bench.SHADE_H2D_BYTES]
