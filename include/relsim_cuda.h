@@ -369,8 +369,10 @@ rt_status rt_set_launch_config(rt_handle* h, const rt_launch_config* cfg);
  * an FP64 tracer at the camera's tolerances with no thin disk and no early
  * capture, gathering each step's chord through the torus
  * (software_compute_engine.hpp:1529-1537, 1725-1731), so their records
- * describe that trace; multi-source dispatches then return
- * RT_ERR_INVALID_ARG, as rt_server_set_shading does.  rt_shading_defaults
+ * describe that trace.  Multi-source dispatches draw no torus: the camera
+ * hole's disk is off and the bodies' disks are shaded as usual, as the
+ * reference's multi-source path does (:2752).  rt_server_set_shading refuses
+ * hydro_model 2.  rt_shading_defaults
  * gives the reference's defaults for the disk and the tonemap, GpuSkyProfile's
  * defaults in sky, and sky_enabled = 0 (black behind the disk; set it to 1 for
  * the reference's sky). */

@@ -364,7 +364,8 @@ rt_status begin_continuation(rt_handle* h, size_t n, bool bodies = false, bool k
 // Hydro model 2 traces the camera as the reference's image path does with the
 // torus: no thin disk, the FP64 tracer at the camera's tolerances, and no
 // early capture (a ray certain to be captured may still cross the torus on its
-// way in).  Multi-source scenes are refused.
+// way in).  Multi-source scenes keep the bodies' disks and lose the camera
+// hole's, as the reference's multi-source path does (ms_dispatch_window).
 bool volume_shading(const rt_handle* h, bool pixels) { return h->shade_on && pixels && h->shading.hydro_model == 2u; }
 rt_camera volume_camera(const rt_camera& cam) {
     rt_camera c = cam;
@@ -720,8 +721,15 @@ rt_status ms_dispatch_window(rt_handle* h, const rt_camera* cam, const rt_source
     const bool shade = h->shade_on && out.pixels;
     rt_status st;
     ContinuationScope cont_scope{h};
-    if (volume_shading(h, out.pixels != nullptr))
-        return fail(h, RT_ERR_INVALID_ARG, "hydro model 2 (the torus) shades single-hole cameras only");
+    // hydro model 2: the reference's multi-source path draws no torus and turns
+    // the camera hole's disk off (software_compute_engine.hpp:2752); the bodies'
+    // disks stay
+    rt_camera vc;
+    if (volume_shading(h, out.pixels != nullptr)) {
+        vc = *cam;
+        vc.disk_outer_radius = 0.0;
+        cam = &vc;
+    }
     if (shade && (st = ms_shade_prepare(h, cam, sources, n_sources, s)) != RT_OK) return st;
     if (shade && (st = begin_continuation(h, n, true)) != RT_OK) return st;
     if ((st = ms_launch(h, cam, sources, n_sources, row0, nrows, out, s)) != RT_OK) return st;

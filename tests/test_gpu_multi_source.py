@@ -254,3 +254,35 @@ def test_multi_source_shaded_pixels_match_oracle(tracer, k):
           f"{np.mean(d < 1e-5):.4f}, max {d.max():.2e}")
     assert np.mean(d < 1e-5) >= 0.99
     assert (cont["n_cross"] > 1).any() and got.max() > 0.0
+
+
+def test_multi_source_with_the_torus_model_drops_the_primary_disk(tracer):
+    """Hydro model 2 in a multi-source scene: the reference's multi-source path
+    draws no torus and turns the camera hole's disk off
+    (software_compute_engine.hpp:2752), the bodies' disks shaded as usual.
+    Against the oracle's continuation trace of the scene with the camera's
+    disk off, composed the same way: sRGB within 1e-5 for 99 % of the rays."""
+    req = [r for r in scenes.request_stream() if r.multi_source][1]
+    srcs = scenes.rt_sources(req.sources)
+    cam = req.bundle.camera(relsim.PRECISION_FP64)
+    cam.screen_width = cam.screen_height = 40
+    sh = relsim.shading(hydro_model=2, tonemapping_mode=1, time=2.0)
+    tracer.set_shading(sh)
+    try:
+        shaded = tracer.dispatch_multi(cam, srcs, fields=["status", "body"], pixels=True)
+    finally:
+        tracer.set_shading(None)
+    off = type(cam).from_buffer_copy(cam)
+    off.disk_outer_radius = 0.0
+    ref, cont = O.ms_trace_cont(relsim.camera_dict(off), _oracle_sources(srcs))
+    eq = shaded["status"] == ref["status"]
+    assert eq.mean() >= 0.99
+    crossed = cont["n_cross"] > 0
+    assert crossed.any() and (cont["cross_src"][crossed][:, 0] != 0).all()
+    assert (shaded["body"][eq & (ref["status"] == O.DISK)] != 0).all()
+    want = _ms_oracle_pixels(off, relsim.shading(tonemapping_mode=1, time=2.0), srcs, cont)
+    got = np.stack([shaded["pixels"]["r"], shaded["pixels"]["g"], shaded["pixels"]["b"]], 1)
+    d = np.max(np.abs(got - want), axis=1)
+    print(f"torus model, multi-source: {int(crossed.sum())} rays cross a body's disk; sRGB within 1e-5 "
+          f"{np.mean(d < 1e-5):.4f}, max {d.max():.2e}")
+    assert np.mean(d < 1e-5) >= 0.99

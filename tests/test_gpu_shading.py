@@ -506,15 +506,7 @@ def test_torus_boyer_lindquist_pixels_match_oracle(tracer):
     assert seen.sum() > 200 and np.mean(err < 1e-6) >= 0.99 and err.max() < 1e-4
 
 
-def test_torus_refused_off_the_single_hole_path(tracer):
-    sh = relsim.shading(hydro_model=2)
-    tracer.set_shading(sh)
-    try:
-        with pytest.raises(relsim.RelsimError):
-            tracer.dispatch_multi(relsim.make_camera(width=8, height=8),
-                                  [relsim.make_source((20.0, 0.0, 0.0))], fields=["status"], pixels=True)
-    finally:
-        tracer.set_shading(None)
+def test_torus_model_refused_by_the_server():
     with relsim.Server(0, relsim.server_config(1 << 26)) as srv:
         with pytest.raises(relsim.RelsimError):
-            srv.set_shading(sh)
+            srv.set_shading(relsim.shading(hydro_model=2))
