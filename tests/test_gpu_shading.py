@@ -368,8 +368,8 @@ def test_sky_behind_mixed_rays_matches_oracle(tracer, sky_sampler):
 
 
 def test_sky_behind_boyer_lindquist_rays_matches_oracle(tracer, sky_sampler):
-    """A Kerr-Newman Boyer-Lindquist image with a sky of other models: the
-    Airy-disk star profile, denser galaxies and the coordinate grid."""
+    """A Kerr-Newman Boyer-Lindquist image with a sky of other models: stars
+    with diffraction spikes, denser galaxies and the coordinate grid."""
     cam = relsim.make_camera(spin=0.9, r_obs=50.0, incl_deg=75.0, fov_deg=40.0, width=48, height=48,
                              metric_form=relsim.METRIC_BOYER_LINDQUIST, charge=0.3)
     sky = relsim.sky_profile(star_profile_model=5, galaxy_density=1.5, grid_enabled=1, grid_show_equator=1)
