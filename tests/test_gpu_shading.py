@@ -510,3 +510,26 @@ def test_torus_model_refused_by_the_server():
     with relsim.Server(0, relsim.server_config(1 << 26)) as srv:
         with pytest.raises(relsim.RelsimError):
             srv.set_shading(relsim.shading(hydro_model=2))
+
+
+def test_headline_image_with_the_sky_matches_oracle_sample(tracer, sky_sampler):
+    """The headline image (Kerr a = 0.94, 2048^2, mixed precision) shaded as the
+    bench's end-to-end number is (translucent disk, the default sky, ACES),
+    through rt_dispatch into host pixels: 3,000 random pixels against the FP64
+    oracle's continuation traces composed with the reference's sky, away from
+    the critical curve and the disk edges.  Bars of the mixed tracer: sRGB
+    within MIXED_CONT_BAR for 99.5 % of the sample, 1e-2 for all."""
+    cam = relsim.make_camera(width=2048, height=2048, precision=relsim.PRECISION_MIXED)
+    sh = relsim.shading(tonemapping_mode=1, sky_enabled=1)
+    out = _shaded(tracer, sh, lambda: tracer.dispatch(cam, fields=["status"], pixels=True))
+    ocam = relsim.make_camera(width=2048, height=2048)
+    rng = np.random.default_rng(7)
+    pix = np.sort(rng.choice(2048 * 2048, 3000, replace=False)).astype(np.uint64)
+    ref, cont = O.trace_cont(relsim.camera_dict(ocam), pixels=pix)
+    want = oracle_sky_pixels(sky_sampler, ocam, sh, cont)
+    want[O.boundary_band(ref, _camera_constants(ocam)[2], ocam.disk_outer_radius, 1e-3) |
+         (np.abs(ref["db_shadow"]) < 1e-2)] = np.nan
+    got = _rgb(out["pixels"][pix.astype(np.int64)])
+    _sky_check(got, want, "headline 2048^2 sample", MIXED_CONT_BAR, 1e-2)
+    sky_seen = (cont["fate"] == O.ESCAPED)
+    assert sky_seen.mean() > 0.5
