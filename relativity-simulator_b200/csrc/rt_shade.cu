@@ -12,9 +12,14 @@
 // render/accretion_disk/accretion_disk_model.hpp:245-316, with the
 // Novikov-Thorne base temperature of hydro model 1,
 // render/accretion_disk/hydro_disk_shading.hpp:160-171).  The radiance is
-// tonemapped (apply_tonemapping, :3461-3516).  With the sky on, a ray that
-// escapes, or ends outside 3 r_s with throughput left, adds the procedural sky
-// (rt_sky.cuh) at the direction the tracer recorded at its end.
+// tonemapped (apply_tonemapping, :3461-3516).  Hydro model 2 replaces the
+// crossings by the light the tracer gathered in the Fishbone-Moncrief torus.
+// With the sky on, a ray that escapes, or ends outside 3 r_s with throughput
+// left, adds the procedural sky (rt_sky.cuh) at its exit direction: recorded
+// by the Boyer-Lindquist and multi-source tracers, and formed here from the
+// tail record of a Kerr-Schild ray's end.  The sky's layers run between block
+// barriers (one 16-warp block per SM), so that an SM's warps share one phase's
+// code in the instruction cache.
 //
 // Per-camera constants (the resolved profile, the Novikov-Thorne flux
 // normalisation, the spectral table of the blackbody colour) are computed on

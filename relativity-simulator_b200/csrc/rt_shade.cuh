@@ -1,9 +1,10 @@
-// rt_shade.cuh -- thin-disk shading on the device: the radiance and opacity of
-// a disk crossing (AccretionDiskModel::shade,
+// rt_shade.cuh -- disk shading on the device: the radiance and opacity of a
+// thin-disk crossing (AccretionDiskModel::shade,
 // render/accretion_disk/accretion_disk_model.hpp:245-316; the Novikov-Thorne
-// base temperature of hydro model 1, hydro_disk_shading.hpp:160-171).  Used by
-// the shading pass (rt_shade.cu) and, for the translucent-disk continuation,
-// by the tracers at each crossing.
+// base temperature of hydro model 1, hydro_disk_shading.hpp:160-171), used by
+// the shading pass (rt_shade.cu); the continuation records the tracers write
+// for it; and the Fishbone-Moncrief torus's chord integral of hydro model 2,
+// which the tracers call step by step.
 #pragma once
 
 #include <cuda_runtime.h>
