@@ -116,10 +116,13 @@ int main(int argc, char** argv) {
         p.tonemapping_mode = 1;
         p.hydro_disk.model = 1;
         p.hydro_disk.accretion_rate_scale = 2.0f;
+        p.hydro_disk.torus_center_radius = 11.0f;
+        p.hydro_disk.sampling_density = 3.0f;
         const rt_shading s = relsim::shading_from_push_constants(p);
-        std::printf("%g %g %g %g %g %u %u %g %u %g\n", s.disk.ring_frequency, s.disk_temperature_scale_k,
+        std::printf("%g %g %g %g %g %u %u %g %u %g %g %g %g %g %g\n", s.disk.ring_frequency, s.disk_temperature_scale_k,
                     s.disk_doppler_beaming_exponent, s.time, s.camera_exposure, s.tonemapping_mode, s.hydro_model,
-                    s.accretion_rate_scale, s.sky_enabled, s.disk.edge_softness);
+                    s.accretion_rate_scale, s.sky_enabled, s.disk.edge_softness, s.torus_inner_radius,
+                    s.torus_center_radius, s.adiabatic_index, s.optical_depth_scale, s.sampling_density);
         return 0;
     }
     if (!std::strcmp(mode, "cpu")) {

@@ -55,10 +55,10 @@ def test_metric_type_routing(tmp_path):
 
 def test_shading_mapping(tmp_path):
     """The push constants' disk profile, overrides, time, exposure, tonemapping,
-    hydro model and procedural sky (the GpuSkyProfile image) become rt_shading,
-    with the sky drawn."""
+    hydro model with its torus settings and procedural sky (the GpuSkyProfile
+    image) become rt_shading, with the sky drawn."""
     out = subprocess.run([_build(tmp_path), "shade"], capture_output=True, text=True, check=True).stdout.split()
-    assert out == ["7", "15000", "3", "2.5", "-1", "1", "1", "2", "1", "1"]
+    assert out == ["7", "15000", "3", "2.5", "-1", "1", "1", "2", "1", "1", "6", "11", "1.33333", "0.35", "3"]
 
 
 @pytest.mark.skipif(not os.path.isdir(REFERENCE_INCLUDE), reason="reference headers not present")
